@@ -1,0 +1,1294 @@
+// NDDO (MNDO / AM1 / PM6) FP64 CPU oracle.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA engine in
+// sparrow_b200/: only tests/, __graft_entry__.smoke() and the cpu_baseline leg
+// of bench.py load it (as oracle/liboracle_nddo.so through ctypes).  The
+// product never links or calls it.
+//
+// It is a scalar restatement of the reference's NDDO hot path for elements
+// with an s or sp valence basis.  Each routine cites the reference file it
+// follows (paths relative to src/Sparrow/Sparrow/Implementations/Nddo/):
+//   parameters      Utils/ParameterUtils/RawParameterProcessor.cpp:42-190,
+//                   KlopmanParameter.cpp:26-92, ChargeSeparationParameter.cpp:24-47,
+//                   PrincipalQuantumNumbers.cpp:20-160
+//   local 2c2e      Utils/IntegralsEvaluationUtils/Local2c2eIntegralCalculator.cpp:39-292,
+//                   ChargesInMultipoles.cpp:27-125, MultipoleMultipoleTerm.h:58-98,
+//                   Local2c2eMatrix.cpp:39-149
+//   rotation        OrbitalRotation.cpp:78-154, Global2c2eTerms.cpp:20-79,
+//                   Global2c2eMatrix.cpp:46-162
+//   core attraction VuvB.cpp:17-31, Utils/OneElectronMatrix.cpp:43-134
+//   overlap         GTOOverlapMatrixBlock.cpp:49-165, OverlapMatrix.cpp:32-64
+//   Fock / energy   Utils/TwoElectronMatrix.cpp:63-166, FockMatrix.cpp:40-150,
+//                   NDDOElectronicEnergyCalculator.cpp:48-67, NDDODensityGuess.cpp:31-66
+//   repulsion       Pm6/PM6PairwiseRepulsion.h:76-192 (+ .cpp:17-31),
+//                   Am1/AM1PairwiseRepulsion.h:64-151, Mndo/MNDOPairwiseRepulsion.h
+//   gradient        Utils/OneElectronMatrix.cpp:136-229, Utils/TwoElectronMatrix.cpp:168-241
+// The SCF driver, Pulay DIIS, eigensolver and aufbau occupation live in the
+// reference's un-vendored dependency (scine_utilities 10.0.0); they are
+// restated here from the standard algorithms (Householder tridiagonalisation
+// plus implicit-shift QL, Pulay commutator DIIS, lowest-n_occ occupation).
+//
+// Physical constants: Bohr radius 0.52917721067 Angstrom and
+// E_h = 27.21138602 eV (CODATA 2014), the values this oracle is pinned with
+// against the reference's known-answer tests.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../sparrow_b200/csrc/nddo_raw.h"
+#include "../sparrow_b200/csrc/nddo_tables.inc"
+
+namespace oracle {
+
+constexpr double kBohrRadiusAngstrom = 0.52917721067;
+constexpr double kAngstromPerBohr = kBohrRadiusAngstrom;
+constexpr double kBohrPerAngstrom = 1.0 / kBohrRadiusAngstrom;
+constexpr double kEvPerHartree = 4.359744650e-18 / 1.6021766208e-19;
+constexpr double kHartreePerEv = 1.0 / kEvPerHartree;
+
+// ---------------------------------------------------------------------------
+// Forward-mode dual number carrying d/dX, d/dY, d/dZ of the pair vector.
+// ---------------------------------------------------------------------------
+struct D3 {
+  double v = 0, g[3] = {0, 0, 0};
+  D3() = default;
+  D3(double x) : v(x) {}
+  D3(double x, double a, double b, double c) : v(x) { g[0] = a; g[1] = b; g[2] = c; }
+};
+inline D3 operator+(const D3& a, const D3& b) { return D3(a.v + b.v, a.g[0] + b.g[0], a.g[1] + b.g[1], a.g[2] + b.g[2]); }
+inline D3 operator-(const D3& a, const D3& b) { return D3(a.v - b.v, a.g[0] - b.g[0], a.g[1] - b.g[1], a.g[2] - b.g[2]); }
+inline D3 operator-(const D3& a) { return D3(-a.v, -a.g[0], -a.g[1], -a.g[2]); }
+inline D3 operator*(const D3& a, const D3& b) {
+  return D3(a.v * b.v, a.g[0] * b.v + a.v * b.g[0], a.g[1] * b.v + a.v * b.g[1], a.g[2] * b.v + a.v * b.g[2]);
+}
+inline D3 operator/(const D3& a, const D3& b) {
+  double inv = 1.0 / b.v, q = a.v * inv;
+  return D3(q, (a.g[0] - q * b.g[0]) * inv, (a.g[1] - q * b.g[1]) * inv, (a.g[2] - q * b.g[2]) * inv);
+}
+inline D3& operator+=(D3& a, const D3& b) { a = a + b; return a; }
+inline D3 sqrt(const D3& a) {
+  double s = std::sqrt(a.v), h = 0.5 / s;
+  return D3(s, a.g[0] * h, a.g[1] * h, a.g[2] * h);
+}
+inline D3 exp(const D3& a) {
+  double e = std::exp(a.v);
+  return D3(e, a.g[0] * e, a.g[1] * e, a.g[2] * e);
+}
+inline double sqrt(double x) { return std::sqrt(x); }
+inline double exp(double x) { return std::exp(x); }
+inline double val(double x) { return x; }
+inline double val(const D3& x) { return x.v; }
+
+// ---------------------------------------------------------------------------
+// Element rules (PrincipalQuantumNumbers.cpp:20-160)
+// ---------------------------------------------------------------------------
+enum Method { kMNDO = 0, kAM1 = 1, kPM6 = 2 };
+
+int n_aos_for(int Z, Method m) {
+  if (Z == 1) return 1;
+  if (m != kPM6) return 4;  // MNDO and AM1 use an sp basis for every heavy element
+  // PM6 uses spd; only report elements whose PM6 basis is s or sp.
+  if (Z <= 12) return 4;
+  if (Z <= 17) return 9;
+  if (Z <= 20) return 4;
+  if (Z <= 29) return 9;
+  if (Z <= 32) return 4;
+  if (Z <= 33) return 9;
+  if (Z <= 34) return 4;
+  if (Z <= 35) return 9;
+  if (Z <= 38) return 4;
+  if (Z <= 47) return 9;
+  if (Z <= 50) return 4;
+  if (Z <= 51) return 9;
+  if (Z <= 52) return 4;
+  if (Z <= 53) return 9;
+  if (Z <= 56) return 4;
+  if (Z <= 79) return 9;
+  if (Z <= 83) return 4;
+  return 0;
+}
+
+double core_charge_for(int Z) {
+  if (Z == 10 || Z == 18 || Z == 36 || Z == 54) return 6;
+  int core = 0;
+  if (Z > 86) core = 86;
+  else if (Z > 79) core = 78;
+  else if (Z > 70) core = 68;
+  else if (Z > 54) core = 54;
+  else if (Z > 47) core = 46;
+  else if (Z > 36) core = 36;
+  else if (Z > 29) core = 28;
+  else if (Z > 18) core = 18;
+  else if (Z > 10) core = 10;
+  else if (Z > 2) core = 2;
+  return Z - core;
+}
+
+int principal_s(int Z) {
+  if (Z <= 2) return 1;
+  if (Z <= 9) return 2;
+  if (Z <= 17) return 3;
+  if (Z <= 35) return 4;
+  if (Z <= 53) return 5;
+  if (Z <= 83) return 6;
+  return 7;
+}
+int principal_p(int Z) {
+  if (Z <= 10) return 2;
+  if (Z <= 18) return 3;
+  if (Z <= 36) return 4;
+  if (Z <= 54) return 5;
+  if (Z <= 83) return 6;
+  return 7;
+}
+
+// ---------------------------------------------------------------------------
+// Runtime (atomic-unit) parameters per element
+// ---------------------------------------------------------------------------
+struct Element {
+  int Z = 0, nao = 0;
+  double core = 0, cbrtZ = 0;
+  double Uss = 0, Upp = 0, betaS = 0, betaP = 0, alpha = 0;
+  double D_sp1 = 0, D_pp2 = 0;                // charge separations (bohr)
+  double rho_ss0 = 0, rho_sp1 = 0, rho_pp0 = 0, rho_pp2 = 0;  // Klopman radii (bohr)
+  double pcore = 0;
+  double gss = 0, gsp = 0, gpp = 0, gp2 = 0, hsp = 0, hpp = 0;  // one-centre integrals (Eh)
+  int n_gauss = 0;
+  double ga[4], gb[4], gc[4];  // converted Gaussian repulsion terms
+  double s_exp[6], s_coef[6], p_exp[6], p_coef[6];
+};
+
+static long long fact(long long n) { return n <= 1 ? 1 : n * fact(n - 1); }
+
+// ChargeSeparationParameter.cpp:40-47
+static double A_factor(int n1, int n2, double z1, double z2, int L) {
+  double f1 = std::pow(2 * z1, n1 + 0.5);
+  double f2 = std::pow(2 * z2, n2 + 0.5);
+  double f3 = std::pow(z1 + z2, -1.0 * (n1 + n2 + L + 1));
+  double f4 = 1.0 / std::sqrt((double)fact(2 * n1) * (double)fact(2 * n2));
+  double f5 = (double)fact(n1 + n2 + L);
+  return f1 * f2 * f3 * f4 * f5;
+}
+
+// KlopmanParameter.cpp:49-92 (Newton iterations from 0.001 until the step is below 1e-8)
+static double klopman_var1(double D, double shift) {
+  double guess = 0.001, previous = 0;
+  while (std::fabs(guess - previous) > 1e-8) {
+    double r = guess, r2 = r * r, sq = std::sqrt(r2 + D * D);
+    double f = 1.0 / r - 1.0 / sq - shift;
+    double der = -1.0 / r2 + r / (sq * sq * sq);
+    previous = guess;
+    guess = r - f / der;
+  }
+  return guess;
+}
+static double klopman_var2(double D, double shift) {
+  double guess = 0.001, previous = 0;
+  while (std::fabs(guess - previous) > 1e-8) {
+    double r = guess, r2 = r * r, d2 = D * D;
+    double sq1 = std::sqrt(r2 + d2), sq2 = std::sqrt(r2 + 2 * d2);
+    double f = 1.0 / r - 2.0 / sq1 + 1.0 / sq2 - shift;
+    double der = -1.0 / r2 + 2 * r / (sq1 * sq1 * sq1) - r / (sq2 * sq2 * sq2);
+    previous = guess;
+    guess = r - f / der;
+  }
+  return guess;
+}
+
+const NddoRawAtomic* find_raw(Method m, int Z) {
+  const NddoRawAtomic* tab = m == kPM6 ? kPM6Atomic : (m == kAM1 ? kAM1Atomic : kMNDOAtomic);
+  size_t n = m == kPM6 ? sizeof(kPM6Atomic) / sizeof(kPM6Atomic[0])
+                       : (m == kAM1 ? sizeof(kAM1Atomic) / sizeof(kAM1Atomic[0]) : sizeof(kMNDOAtomic) / sizeof(kMNDOAtomic[0]));
+  for (size_t i = 0; i < n; ++i)
+    if (tab[i].Z == Z) return &tab[i];
+  return nullptr;
+}
+
+// RawParameterProcessor.cpp:67-99 with setKlopman (:126-159), setChargeSeparations (:161-174)
+bool make_element(Method m, int Z, Element& e) {
+  const NddoRawAtomic* r = find_raw(m, Z);
+  if (!r) return false;
+  e.Z = Z;
+  e.nao = n_aos_for(Z, m);
+  if (e.nao != 1 && e.nao != 4) return false;
+  e.core = core_charge_for(Z);
+  e.cbrtZ = std::pow((double)Z, 1.0 / 3.0);
+  const double* v = r->v;
+  e.betaS = v[kRawBetaS] * kHartreePerEv;
+  e.betaP = v[kRawBetaP] * kHartreePerEv;
+  e.Uss = v[kRawUss] * kHartreePerEv;
+  e.Upp = v[kRawUpp] * kHartreePerEv;
+  e.alpha = v[kRawAlpha] * kAngstromPerBohr;
+  if (e.nao == 4) {
+    int ns = principal_s(Z), np = principal_p(Z);
+    int n = ns <= np ? ns : np;  // the reference uses min(ns, np) for both separations
+    e.D_sp1 = A_factor(n, n, v[kRawZetaS], v[kRawZetaP], 1) / std::sqrt(3.0);
+    e.D_pp2 = std::sqrt(A_factor(n, n, v[kRawZetaP], v[kRawZetaP], 2)) / std::sqrt(5.0);
+  }
+  double gss = v[kRawGss] * kHartreePerEv;
+  e.rho_ss0 = 1.0 / (2.0 * gss);
+  if (e.nao == 4) {
+    double hpp = 0.5 * (v[kRawGpp] - v[kRawGp2]) * kHartreePerEv;
+    hpp = std::max(0.1 * kHartreePerEv, hpp);  // REPRODUCE_PM6_ERRORS (on by default)
+    e.rho_pp0 = e.rho_ss0;
+    e.rho_sp1 = klopman_var1(e.D_sp1, 4 * v[kRawHsp] * kHartreePerEv);
+    e.rho_pp2 = klopman_var2(e.D_pp2, 8 * hpp);
+  }
+  if (v[kRawPcore] == 0) e.pcore = e.rho_ss0;
+  else e.pcore = v[kRawPcore];
+  e.n_gauss = r->n_gauss;
+  for (int i = 0; i < 4; ++i) {
+    e.ga[i] = r->ga[i] * kBohrPerAngstrom;
+    e.gb[i] = r->gb[i] * kAngstromPerBohr * kAngstromPerBohr;
+    e.gc[i] = r->gc[i] * kBohrPerAngstrom;
+  }
+  // one-centre two-electron integrals (RawParameterProcessor.cpp:42-65,
+  // oneCenterTwoElectronIntegrals.cpp: <pp'|pp'> = (gpp - gp2)/2)
+  e.gss = gss;
+  e.gsp = v[kRawGsp] * kHartreePerEv;
+  e.gpp = v[kRawGpp] * kHartreePerEv;
+  e.gp2 = v[kRawGp2] * kHartreePerEv;
+  e.hsp = v[kRawHsp] * kHartreePerEv;
+  e.hpp = 0.5 * (e.gpp - e.gp2);
+  for (int i = 0; i < 6; ++i) {
+    e.s_exp[i] = r->s_exp[i];
+    e.s_coef[i] = r->s_coef[i];
+    e.p_exp[i] = r->p_exp[i];
+    e.p_coef[i] = r->p_coef[i];
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Local two-centre two-electron integrals (multipole point-charge model)
+// ---------------------------------------------------------------------------
+// Orbital-pair index (twoElIntegral_t, GeneralTypes.h:38-55) for s=0,x=1,y=2,z=3:
+// pair(mu<=nu) = nu*(nu+1)/2 + mu  ->  s_s, s_x, x_x, s_y, x_y, y_y, s_z, x_z, y_z, z_z
+inline int pidx(int a, int b) { return a <= b ? b * (b + 1) / 2 + a : a * (a + 1) / 2 + b; }
+
+enum MP { M00, Qxx, Qyy, Qzz, M1m1, M10, M11, M2m2, M2m1, M21 };
+struct Charge { double x, y, z, q; };
+// ChargesInMultipoles.cpp:27-125 (the configurations used by s/p orbital pairs)
+static const std::vector<Charge>& charges(MP m) {
+  static const std::vector<Charge> c[10] = {
+      {{0, 0, 0, 1}},
+      {{-2, 0, 0, .25}, {2, 0, 0, .25}, {0, 0, 0, -.5}},
+      {{0, -2, 0, .25}, {0, 2, 0, .25}, {0, 0, 0, -.5}},
+      {{0, 0, -2, .25}, {0, 0, 2, .25}, {0, 0, 0, -.5}},
+      {{0, -1, 0, -.5}, {0, 1, 0, .5}},
+      {{0, 0, -1, -.5}, {0, 0, 1, .5}},
+      {{-1, 0, 0, -.5}, {1, 0, 0, .5}},
+      {{1, 1, 0, .25}, {-1, -1, 0, .25}, {1, -1, 0, -.25}, {-1, 1, 0, -.25}},
+      {{0, 1, 1, .25}, {0, -1, -1, .25}, {0, 1, -1, -.25}, {0, -1, 1, -.25}},
+      {{1, 0, 1, .25}, {-1, 0, -1, .25}, {1, 0, -1, -.25}, {-1, 0, 1, -.25}},
+  };
+  return c[m];
+}
+static int mq(MP m) {
+  switch (m) {
+    case M1m1: case M2m1: return -1;
+    case M11: case M21: return 1;
+    case M2m2: return -2;
+    default: return 0;
+  }
+}
+// Multipole pair classes: 0 ss0, 1 sp1, 2 pp0, 3 pp2
+struct MTerm { double f; MP m; int cls; };
+// Local2c2eIntegralCalculator.cpp:125-292 (s/p pairs, no d functions present)
+static std::vector<MTerm> multipoles(int pair) {
+  switch (pair) {
+    case 0: return {{1, M00, 0}};
+    case 1: return {{1, M11, 1}};
+    case 3: return {{1, M1m1, 1}};
+    case 6: return {{1, M10, 1}};
+    case 7: return {{1, M21, 3}};
+    case 8: return {{1, M2m1, 3}};
+    case 4: return {{1, M2m2, 3}};
+    case 9: return {{1, M00, 2}, {1, Qzz, 3}};
+    case 2: return {{1, M00, 2}, {1, Qxx, 3}};
+    case 5: return {{1, M00, 2}, {1, Qyy, 3}};
+  }
+  return {};
+}
+
+static double rho_of(const Element& e, int cls) {
+  switch (cls) {
+    case 0: return e.rho_ss0;
+    case 1: return e.rho_sp1;
+    case 2: return e.rho_pp0;
+    default: return e.rho_pp2;
+  }
+}
+static double D_of(const Element& e, int cls) { return cls == 1 ? e.D_sp1 : (cls == 3 ? e.D_pp2 : 0.0); }
+
+// One local integral (pair1 on A | pair2 on B) with its derivative d/dR.
+static void local_integral(int p1, int p2, double R, const Element& A, const Element& B,
+                           bool coreB, double pcoreB, double& value, double& dR) {
+  value = 0;
+  dR = 0;
+  for (const MTerm& t1 : multipoles(p1)) {
+    for (const MTerm& t2 : multipoles(p2)) {
+      if (mq(t1.m) != mq(t2.m)) continue;
+      double rhoA = rho_of(A, t1.cls);
+      double rhoB = coreB ? (t2.cls == 0 ? pcoreB : 0.0) : rho_of(B, t2.cls);
+      double rr = (rhoA + rhoB) * (rhoA + rhoB);
+      double D1 = D_of(A, t1.cls);
+      double d2 = coreB ? 0.0 : D_of(B, t2.cls);
+      double f = t1.f * t2.f;
+      for (const Charge& c1 : charges(t1.m)) {
+        for (const Charge& c2 : charges(t2.m)) {
+          double dx = d2 * c2.x - D1 * c1.x;
+          double dy = d2 * c2.y - D1 * c1.y;
+          double dz = R + d2 * c2.z - D1 * c1.z;
+          double inv = 1.0 / std::sqrt(dx * dx + dy * dy + dz * dz + rr);
+          double q = f * c1.q * c2.q;
+          value += q * inv;
+          dR += -dz * q * inv * inv * inv;
+        }
+      }
+    }
+  }
+}
+
+// Local2c2eMatrix.cpp:39-149: the entries the reference evaluates for s/p
+// atoms; everything else in the 10x10 block is zero, and <xy|xy> is the
+// combination 0.5*(<xx|xx> - <xx|yy>).
+static void local_matrix(int dA, int dB, double R, const Element& A, const Element& B, bool coreB, double pcoreB,
+                         double L[10][10], double dL[10][10]) {
+  for (int i = 0; i < 10; ++i)
+    for (int j = 0; j < 10; ++j) L[i][j] = dL[i][j] = 0;
+  static const int kDirect[][2] = {{0, 0}, {0, 2}, {0, 5}, {0, 6}, {0, 9}, {2, 0}, {5, 0}, {6, 0}, {9, 0},
+                                   {1, 1}, {1, 7}, {2, 2}, {2, 5}, {2, 6}, {2, 9}, {3, 3}, {3, 8}, {5, 2},
+                                   {5, 5}, {5, 6}, {5, 9}, {6, 2}, {6, 5}, {6, 6}, {6, 9}, {7, 1}, {7, 7},
+                                   {8, 3}, {8, 8}, {9, 2}, {9, 5}, {9, 6}, {9, 9}};
+  for (const auto& ij : kDirect) {
+    int i = ij[0], j = ij[1];
+    if (i >= dA || j >= dB) continue;
+    local_integral(i, j, R, A, B, coreB, pcoreB, L[i][j], dL[i][j]);
+  }
+  if (dA == 10 && dB == 10) {
+    L[4][4] = 0.5 * (L[2][2] - L[2][5]);
+    dL[4][4] = 0.5 * (dL[2][2] - dL[2][5]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Rotation to the molecular frame (OrbitalRotation.cpp:78-154)
+// T[g][l]: coefficient of local orbital l in global orbital g (s=0,x,y,z)
+// ---------------------------------------------------------------------------
+template <class T>
+static void rotation(const T& X, const T& Y, const T& Z, double Xv, double Yv, T rot[4][4], T& R) {
+  R = sqrt(X * X + Y * Y + Z * Z);
+  T proj = T(0.0);
+  if (std::sqrt(Xv * Xv + Yv * Yv) != 0) proj = sqrt(X * X + Y * Y);
+  T cosa, sina;
+  if (val(proj) != 0) {
+    cosa = X / proj;
+    sina = Y / proj;
+  } else {
+    cosa = T(1.0);
+    sina = T(0.0);
+  }
+  T cosb = Z / R, sinb = proj / R;
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) rot[i][j] = T(0.0);
+  rot[0][0] = T(1.0);
+  rot[1][1] = cosa * cosb;  // x_x
+  rot[2][1] = sina * cosb;  // y_x
+  rot[3][1] = -sinb;        // z_x
+  rot[1][2] = -sina;        // x_y
+  rot[2][2] = cosa;         // y_y
+  rot[1][3] = cosa * sinb;  // x_z
+  rot[2][3] = sina * sinb;  // y_z
+  rot[3][3] = cosb;         // z_z
+}
+
+
+inline double make_local(double L, double, const double&) { return L; }
+inline D3 make_local(double L, double dL, const D3& R) { return D3(L, dL * R.g[0], dL * R.g[1], dL * R.g[2]); }
+
+// Global block G[pair(mu,nu) on A][pair(lam,sig) on B] for the pair vector
+// Rab = pos_B - pos_A: the four-index rotation of the local block
+// (Global2c2eMatrix.cpp:46-151, Global2c2eTerms.cpp:20-79).  The sum runs over
+// every ordering of the local orbitals, so the pair-rotation matrix is
+// W[pair(mu,nu)][pair(mu',nu')] = sum over orderings of rot[mu][mu'] rot[nu][nu'].
+// With coreB the second centre is a bare core (s function, Klopman radius
+// pcoreB, no multipoles): the VuvB block (VuvB.cpp:17-31).
+template <class T>
+static void global_block(int nA, int nB, const T& X, const T& Y, const T& Z, const Element& A, const Element& B,
+                         bool coreB, double pcoreB, T G[10][10]) {
+  double Xv = val(X), Yv = val(Y), Zv = val(Z);
+  T rot[4][4], R;
+  rotation(X, Y, Z, Xv, Yv, rot, R);
+  int dA = nA == 1 ? 1 : 10, dB = nB == 1 ? 1 : 10;
+  double Rv = std::sqrt(Xv * Xv + Yv * Yv + Zv * Zv);
+  double L[10][10], dL[10][10];
+  local_matrix(dA, dB, Rv, A, B, coreB, pcoreB, L, dL);
+  T Lt[10][10];
+  for (int i = 0; i < dA; ++i)
+    for (int j = 0; j < dB; ++j) Lt[i][j] = make_local(L[i][j], dL[i][j], R);
+  auto W = [&](int n, T out[10][10]) {
+    for (int a = 0; a < 10; ++a)
+      for (int b = 0; b < 10; ++b) out[a][b] = T(0.0);
+    for (int mu = 0; mu < n; ++mu)
+      for (int nu = mu; nu < n; ++nu)
+        for (int m2 = 0; m2 < n; ++m2)
+          for (int n2 = 0; n2 < n; ++n2) {
+            if (val(rot[mu][m2]) == 0 && val(rot[nu][n2]) == 0) continue;
+            out[pidx(mu, nu)][pidx(m2, n2)] += rot[mu][m2] * rot[nu][n2];
+          }
+  };
+  T WA[10][10], WB[10][10];
+  W(nA, WA);
+  W(nB, WB);
+  T tmp[10][10];
+  for (int a = 0; a < dA; ++a)
+    for (int l = 0; l < dB; ++l) {
+      T s = T(0.0);
+      for (int k = 0; k < dB; ++k) s += Lt[a][k] * WB[l][k];
+      tmp[a][l] = s;
+    }
+  for (int g = 0; g < dA; ++g)
+    for (int l = 0; l < dB; ++l) {
+      T s = T(0.0);
+      for (int a = 0; a < dA; ++a) s += WA[g][a] * tmp[a][l];
+      G[g][l] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// STO-6G overlap (GTOOverlapMatrixBlock.cpp:70-165): orbitals of A at the
+// origin, orbitals of B at R = pos_B - pos_A; AO order s, x, y, z.
+// ---------------------------------------------------------------------------
+template <class T>
+static void overlap_block(const Element& A, const Element& B, const T R[3], T S[4][4]) {
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) S[i][j] = T(0.0);
+  const double pi = 4.0 * std::atan(1.0);
+  T R2 = R[0] * R[0] + R[1] * R[1] + R[2] * R[2];
+  for (int la = 0; la < (A.nao == 4 ? 2 : 1); ++la)
+    for (int lb = 0; lb < (B.nao == 4 ? 2 : 1); ++lb)
+      for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) {
+          double a = la ? A.p_exp[i] : A.s_exp[i], ca = la ? A.p_coef[i] : A.s_coef[i];
+          double b = lb ? B.p_exp[j] : B.s_exp[j], cb = lb ? B.p_coef[j] : B.s_coef[j];
+          double p = a + b;
+          T K = exp(R2 * T(-a * b / p)) * T(ca * cb);
+          double s00 = std::sqrt(pi / p);
+          T PA[3], PB[3];
+          for (int d = 0; d < 3; ++d) {
+            PA[d] = R[d] * T(b / p);
+            PB[d] = PA[d] - R[d];
+          }
+          // 1D overlaps for powers (k on A, l on B) in {0,1}
+          T s1d[3][2][2];
+          for (int d = 0; d < 3; ++d) {
+            s1d[d][0][0] = T(s00);
+            s1d[d][1][0] = PA[d] * T(s00);
+            s1d[d][0][1] = PB[d] * T(s00);
+            s1d[d][1][1] = PA[d] * PB[d] * T(s00) + T(s00 / (2 * p));
+          }
+          int na = la ? 3 : 1, nb = lb ? 3 : 1;
+          for (int u = 0; u < na; ++u)
+            for (int v = 0; v < nb; ++v) {
+              int pa[3] = {0, 0, 0}, pb[3] = {0, 0, 0};
+              if (la) pa[u] = 1;
+              if (lb) pb[v] = 1;
+              T prod = K * s1d[0][pa[0]][pb[0]] * s1d[1][pa[1]][pb[1]] * s1d[2][pa[2]][pb[2]];
+              S[la ? 1 + u : 0][lb ? 1 + v : 0] += prod;
+            }
+        }
+}
+
+// ---------------------------------------------------------------------------
+// Core-core repulsion (PM6PairwiseRepulsion.h:76-192, AM1PairwiseRepulsion.h:64-151)
+// ---------------------------------------------------------------------------
+struct PairParams { double alphaAB = 0, xAB = 0; bool found = false; };
+
+static PairParams pm6_pair(const Element& A, const Element& B) {
+  PairParams pp;
+  for (int i = 0; i < kPM6NumDiatomic; ++i) {
+    const NddoRawDiatomic& d = kPM6Diatomic[i];
+    if ((d.z1 == A.Z && d.z2 == B.Z) || (d.z1 == B.Z && d.z2 == A.Z)) {
+      bool xh = (A.Z == 1 && (B.Z == 8 || B.Z == 7 || B.Z == 6)) || (B.Z == 1 && (A.Z == 8 || A.Z == 7 || A.Z == 6));
+      pp.alphaAB = xh ? d.exponent * kAngstromPerBohr * kAngstromPerBohr : d.exponent * kAngstromPerBohr;
+      pp.xAB = d.factor;
+      pp.found = true;
+      return pp;
+    }
+  }
+  return pp;
+}
+
+// energy and dE/dR of one pair at distance R
+static void repulsion(Method m, const Element& A, const Element& B, double R, double& E, double& dE) {
+  double ps = A.pcore + B.pcore;
+  double g = 1.0 / std::sqrt(R * R + ps * ps);
+  double dg = -g * g * g * R;
+  double f = 1, df = 0;
+  double ZZ = A.core * B.core;
+  E = 0;
+  dE = 0;
+  if (m == kPM6) {
+    PairParams pp = pm6_pair(A, B);
+    const double cAdd = 0.0000207389327971913490822259;
+    const double expC = 0.00001244878365801758178693335;
+    const double ccExp = 3.1644797213016;
+    const double sioDist = 5.480205761238679760340424;
+    bool xh = (A.Z == 1 && (B.Z == 8 || B.Z == 7 || B.Z == 6)) || (B.Z == 1 && (A.Z == 8 || A.Z == 7 || A.Z == 6));
+    if (xh) {
+      double e = std::exp(-pp.alphaAB * R * R);
+      f = 1 + 2 * pp.xAB * e;
+      df = 2 * pp.xAB * e * (-2 * pp.alphaAB * R);
+    } else {
+      double R6 = std::pow(R, 6);
+      double e = std::exp(-pp.alphaAB * (R + expC * R6));
+      f = 1 + 2 * pp.xAB * e;
+      df = 2 * pp.xAB * e * (-pp.alphaAB * (1 + 6 * expC * R6 / R));
+      if (A.Z == 6 && B.Z == 6) {
+        double c = 9.28 * std::exp(-ccExp * R);
+        f += c;
+        df += -ccExp * c;
+      }
+      if ((A.Z == 14 && B.Z == 8) || (A.Z == 8 && B.Z == 14)) {
+        double r1 = R - sioDist;
+        double c = -0.0007 * std::exp(-r1 * r1);
+        f += c;
+        df += -2 * r1 * c;
+      }
+    }
+    E = ZZ * g * f;
+    dE = ZZ * (dg * f + g * df);
+    // additional r^-12 term with atomic numbers
+    double v = (A.cbrtZ + B.cbrtZ) / R;
+    double v12 = std::pow(v, 12);
+    E += cAdd * v12 / kEvPerHartree;
+    dE += cAdd * (-12.0 * v12 / R) / kEvPerHartree;
+    // Gaussian term: only the first Gaussian of each atom contributes
+    double gs = 0, dgs = 0;
+    for (const Element* X : {&A, &B}) {
+      if (X->n_gauss > 0) {
+        double rc = R - X->gc[0];
+        double e = X->ga[0] * std::exp(-X->gb[0] * rc * rc);
+        gs += e;
+        dgs += e * (-2 * X->gb[0] * rc);
+      }
+    }
+    double pref = ZZ / kEvPerHartree;
+    E += gs / R * pref;
+    dE += (dgs / R - gs / (R * R)) * pref;
+    return;
+  }
+  // MNDO / AM1 parenthesis
+  bool hA = A.Z == 1 && (B.Z == 7 || B.Z == 8);
+  bool hB = B.Z == 1 && (A.Z == 7 || A.Z == 8);
+  double eA = std::exp(-A.alpha * R), eB = std::exp(-B.alpha * R);
+  if (hA) {
+    f = 1 + eA + R * kAngstromPerBohr * eB;
+    df = -A.alpha * eA + kAngstromPerBohr * eB * (1 - B.alpha * R);
+  } else if (hB) {
+    f = 1 + R * kAngstromPerBohr * eA + eB;
+    df = kAngstromPerBohr * eA * (1 - A.alpha * R) - B.alpha * eB;
+  } else {
+    f = 1 + eA + eB;
+    df = -A.alpha * eA - B.alpha * eB;
+  }
+  E = ZZ * g * f;
+  dE = ZZ * (dg * f + g * df);
+  if (m == kAM1) {
+    double gs = 0, dgs = 0;
+    for (const Element* X : {&A, &B})
+      for (int k = 0; k < X->n_gauss; ++k) {
+        double rc = R - X->gc[k];
+        double e = X->ga[k] * std::exp(-X->gb[k] * rc * rc);
+        gs += e;
+        dgs += e * (-2 * X->gb[k] * rc);
+      }
+    double pref = ZZ / kEvPerHartree;
+    E += gs / R * pref;
+    dE += (dgs / R - gs / (R * R)) * pref;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// One-centre two-electron integrals (ij|kl) for s/p (OneCenterTwoElectronCalculator.cpp:84-120)
+// ---------------------------------------------------------------------------
+static double one_center(const Element& e, int i, int j, int k, int l) {
+  // normalise orbital pairs
+  auto same = [](int a, int b) { return a == b; };
+  if (e.nao == 1) return (i == 0 && j == 0 && k == 0 && l == 0) ? e.gss : 0.0;
+  // classify
+  int nS = (i == 0) + (j == 0) + (k == 0) + (l == 0);
+  if (nS == 4) return e.gss;
+  if (same(i, j) && same(k, l)) {
+    if (i == 0 || k == 0) return e.gsp;         // (ss|pp) or (pp|ss)
+    if (i == k) return e.gpp;                   // (pp|pp)
+    return e.gp2;                               // (pp|p'p')
+  }
+  // exchange-type (ab|ab) / (ab|ba) with a != b
+  if (!same(i, j) && ((i == k && j == l) || (i == l && j == k))) {
+    if (i == 0 || j == 0) return e.hsp;         // (sp|sp)
+    return e.hpp;                               // (pp'|pp')
+  }
+  return 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// Small dense linear algebra (row-major, N x N)
+// ---------------------------------------------------------------------------
+// Householder reduction of symmetric A to tridiagonal form; A is overwritten
+// with the accumulated orthogonal transform Q (A_in = Q T Q^T); d = diagonal,
+// e[i] = sub-diagonal T(i, i-1) for i >= 1.
+static void tridiagonalise(int n, std::vector<double>& a, std::vector<double>& d, std::vector<double>& e) {
+  d.assign(n, 0);
+  e.assign(n, 0);
+  auto A = [&](int i, int j) -> double& { return a[(size_t)i * n + j]; };
+  for (int i = n - 1; i > 0; --i) {
+    int l = i - 1;
+    double h = 0, scale = 0;
+    if (l > 0) {
+      for (int k = 0; k <= l; ++k) scale += std::fabs(A(i, k));
+      if (scale == 0.0) {
+        e[i] = A(i, l);
+      } else {
+        for (int k = 0; k <= l; ++k) {
+          A(i, k) /= scale;
+          h += A(i, k) * A(i, k);
+        }
+        double f = A(i, l);
+        double g = f >= 0 ? -std::sqrt(h) : std::sqrt(h);
+        e[i] = scale * g;
+        h -= f * g;
+        A(i, l) = f - g;
+        f = 0;
+        for (int j = 0; j <= l; ++j) {
+          A(j, i) = A(i, j) / h;
+          double gg = 0;
+          for (int k = 0; k <= j; ++k) gg += A(j, k) * A(i, k);
+          for (int k = j + 1; k <= l; ++k) gg += A(k, j) * A(i, k);
+          e[j] = gg / h;
+          f += e[j] * A(i, j);
+        }
+        double hh = f / (h + h);
+        for (int j = 0; j <= l; ++j) {
+          double ff = A(i, j);
+          double gg = e[j] - hh * ff;
+          e[j] = gg;
+          for (int k = 0; k <= j; ++k) A(j, k) -= (ff * e[k] + gg * A(i, k));
+        }
+      }
+    } else {
+      e[i] = A(i, l);
+    }
+    d[i] = h;
+  }
+  d[0] = 0;
+  e[0] = 0;
+  for (int i = 0; i < n; ++i) {
+    int l = i - 1;
+    if (d[i] != 0.0) {
+      for (int j = 0; j <= l; ++j) {
+        double g = 0;
+        for (int k = 0; k <= l; ++k) g += A(i, k) * A(k, j);
+        for (int k = 0; k <= l; ++k) A(k, j) -= g * A(k, i);
+      }
+    }
+    d[i] = A(i, i);
+    A(i, i) = 1;
+    for (int j = 0; j <= l; ++j) A(j, i) = A(i, j) = 0;
+  }
+}
+
+// Implicit-shift QL on the tridiagonal (d, e) with eigenvector accumulation
+// into z (columns).  Returns false if an eigenvalue fails to converge.
+static bool tridiagonal_ql(int n, std::vector<double>& d, std::vector<double>& e, std::vector<double>& z) {
+  for (int i = 1; i < n; ++i) e[i - 1] = e[i];
+  if (n > 0) e[n - 1] = 0;
+  auto Z = [&](int i, int j) -> double& { return z[(size_t)i * n + j]; };
+  for (int l = 0; l < n; ++l) {
+    int iter = 0, m;
+    do {
+      for (m = l; m < n - 1; ++m) {
+        double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
+        if (std::fabs(e[m]) <= 1e-16 * dd) break;
+      }
+      if (m != l) {
+        if (iter++ == 200) return false;
+        double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+        double r = std::hypot(g, 1.0);
+        g = d[m] - d[l] + e[l] / (g + (g >= 0 ? std::fabs(r) : -std::fabs(r)));
+        double s = 1, c = 1, p = 0;
+        int i;
+        for (i = m - 1; i >= l; --i) {
+          double f = s * e[i], b = c * e[i];
+          r = std::hypot(f, g);
+          e[i + 1] = r;
+          if (r == 0.0) {
+            d[i + 1] -= p;
+            e[m] = 0;
+            break;
+          }
+          s = f / r;
+          c = g / r;
+          g = d[i + 1] - p;
+          r = (d[i] - g) * s + 2.0 * c * b;
+          p = s * r;
+          d[i + 1] = g + p;
+          g = c * r - b;
+          for (int k = 0; k < n; ++k) {
+            f = Z(k, i + 1);
+            Z(k, i + 1) = s * Z(k, i) + c * f;
+            Z(k, i) = c * Z(k, i) - s * f;
+          }
+        }
+        if (r == 0.0 && i >= l) continue;
+        d[l] -= p;
+        e[l] = g;
+        e[m] = 0;
+      }
+    } while (m != l);
+  }
+  return true;
+}
+
+// Symmetric eigen-decomposition: eigenvalues ascending in w, eigenvectors in
+// the columns of v (row-major N x N).
+static bool eigh(int n, const std::vector<double>& a, std::vector<double>& w, std::vector<double>& v) {
+  v = a;
+  std::vector<double> e;
+  tridiagonalise(n, v, w, e);
+  if (!tridiagonal_ql(n, w, e, v)) return false;
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return w[x] < w[y]; });
+  std::vector<double> w2(n), v2((size_t)n * n);
+  for (int j = 0; j < n; ++j) {
+    w2[j] = w[order[j]];
+    for (int i = 0; i < n; ++i) v2[(size_t)i * n + j] = v[(size_t)i * n + order[j]];
+  }
+  w.swap(w2);
+  v.swap(v2);
+  return true;
+}
+
+// Solve the small dense system M x = b by Gaussian elimination with partial pivoting.
+static bool solve_dense(int n, std::vector<double> M, std::vector<double>& b) {
+  for (int c = 0; c < n; ++c) {
+    int piv = c;
+    for (int r = c + 1; r < n; ++r)
+      if (std::fabs(M[r * n + c]) > std::fabs(M[piv * n + c])) piv = r;
+    if (std::fabs(M[piv * n + c]) < 1e-300) return false;
+    if (piv != c) {
+      for (int k = 0; k < n; ++k) std::swap(M[c * n + k], M[piv * n + k]);
+      std::swap(b[c], b[piv]);
+    }
+    for (int r = c + 1; r < n; ++r) {
+      double f = M[r * n + c] / M[c * n + c];
+      for (int k = c; k < n; ++k) M[r * n + k] -= f * M[c * n + k];
+      b[r] -= f * b[c];
+    }
+  }
+  for (int c = n - 1; c >= 0; --c) {
+    double s = b[c];
+    for (int k = c + 1; k < n; ++k) s -= M[c * n + k] * b[k];
+    b[c] = s / M[c * n + c];
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Molecule-level calculation
+// ---------------------------------------------------------------------------
+struct Molecule {
+  Method method;
+  int nat = 0, nao = 0, nel = 0, nocc = 0;
+  std::vector<Element> el;
+  std::vector<double> pos;  // bohr, 3*nat
+  std::vector<int> ao0;     // first AO of each atom
+  // pair data for i<j: global 2c2e block and core-attraction vectors
+  struct Pair {
+    int a, b;
+    double G[10][10];
+    double VA[10];  // -Z_B (mu nu | s_B s_B)_core for mu<=nu on A
+    double VB[10];  // -Z_A (lam sig | s_A s_A)_core for lam<=sig on B
+  };
+  std::vector<Pair> pairs;
+  std::vector<double> H, S;
+  double Erep = 0;
+};
+
+static int setup(Molecule& M, Method m, int nat, const int* Z, const double* xyz, int charge, std::string& err) {
+  M.method = m;
+  M.nat = nat;
+  M.el.resize(nat);
+  M.pos.assign(xyz, xyz + 3 * nat);
+  M.ao0.resize(nat);
+  int nao = 0;
+  double ncore = 0;
+  for (int i = 0; i < nat; ++i) {
+    if (!make_element(m, Z[i], M.el[i])) {
+      err = "no s/p parameters for element Z=" + std::to_string(Z[i]);
+      return 2;
+    }
+    M.ao0[i] = nao;
+    nao += M.el[i].nao;
+    ncore += M.el[i].core;
+  }
+  M.nao = nao;
+  M.nel = (int)std::lround(ncore) - charge;
+  if (M.nel < 0 || M.nel % 2 != 0) {
+    err = "restricted closed-shell calculation needs an even electron count";
+    return 3;
+  }
+  M.nocc = M.nel / 2;
+  return 0;
+}
+
+static void build_pairs(Molecule& M) {
+  int n = M.nat;
+  M.pairs.clear();
+  for (int a = 0; a < n; ++a)
+    for (int b = a + 1; b < n; ++b) {
+      Molecule::Pair P;
+      P.a = a;
+      P.b = b;
+      const Element &A = M.el[a], &B = M.el[b];
+      double X = M.pos[3 * b] - M.pos[3 * a], Y = M.pos[3 * b + 1] - M.pos[3 * a + 1],
+             Zc = M.pos[3 * b + 2] - M.pos[3 * a + 2];
+      global_block<double>(A.nao, B.nao, X, Y, Zc, A, B, false, 0.0, P.G);
+      double V[10][10];
+      global_block<double>(A.nao, 1, X, Y, Zc, A, B, true, B.pcore, V);
+      for (int k = 0; k < 10; ++k) P.VA[k] = k < (A.nao == 1 ? 1 : 10) ? -B.core * V[k][0] : 0;
+      global_block<double>(B.nao, 1, -X, -Y, -Zc, B, A, true, A.pcore, V);
+      for (int k = 0; k < 10; ++k) P.VB[k] = k < (B.nao == 1 ? 1 : 10) ? -A.core * V[k][0] : 0;
+      M.pairs.push_back(P);
+    }
+}
+
+// H (full symmetric), S (full symmetric, identity within atoms), E_rep
+static void build_one_electron(Molecule& M) {
+  int N = M.nao;
+  M.H.assign((size_t)N * N, 0);
+  M.S.assign((size_t)N * N, 0);
+  for (int i = 0; i < N; ++i) M.S[(size_t)i * N + i] = 1;
+  auto H = [&](int i, int j) -> double& { return M.H[(size_t)i * N + j]; };
+  for (int a = 0; a < M.nat; ++a) {
+    const Element& e = M.el[a];
+    for (int k = 0; k < e.nao; ++k) H(M.ao0[a] + k, M.ao0[a] + k) = k == 0 ? e.Uss : e.Upp;
+  }
+  M.Erep = 0;
+  for (const auto& P : M.pairs) {
+    const Element &A = M.el[P.a], &B = M.el[P.b];
+    int oa = M.ao0[P.a], ob = M.ao0[P.b];
+    for (int mu = 0; mu < A.nao; ++mu)
+      for (int nu = 0; nu <= mu; ++nu) {
+        H(oa + mu, oa + nu) += P.VA[pidx(mu, nu)];
+        if (mu != nu) H(oa + nu, oa + mu) += P.VA[pidx(mu, nu)];
+      }
+    for (int mu = 0; mu < B.nao; ++mu)
+      for (int nu = 0; nu <= mu; ++nu) {
+        H(ob + mu, ob + nu) += P.VB[pidx(mu, nu)];
+        if (mu != nu) H(ob + nu, ob + mu) += P.VB[pidx(mu, nu)];
+      }
+    double R[3] = {M.pos[3 * P.b] - M.pos[3 * P.a], M.pos[3 * P.b + 1] - M.pos[3 * P.a + 1],
+                   M.pos[3 * P.b + 2] - M.pos[3 * P.a + 2]};
+    double Sb[4][4];
+    overlap_block<double>(A, B, R, Sb);
+    for (int mu = 0; mu < A.nao; ++mu)
+      for (int nu = 0; nu < B.nao; ++nu) {
+        double ba = mu == 0 ? A.betaS : A.betaP, bb = nu == 0 ? B.betaS : B.betaP;
+        double h = 0.5 * (ba + bb) * Sb[mu][nu];
+        H(oa + mu, ob + nu) = H(ob + nu, oa + mu) = h;
+        M.S[(size_t)(oa + mu) * N + ob + nu] = M.S[(size_t)(ob + nu) * N + oa + mu] = Sb[mu][nu];
+      }
+    double Rabs = std::sqrt(R[0] * R[0] + R[1] * R[1] + R[2] * R[2]);
+    double E, dE;
+    repulsion(M.method, A, B, Rabs, E, dE);
+    M.Erep += E;
+  }
+}
+
+// Full two-electron matrix G(P) (TwoElectronMatrix.cpp:82-166, written for the
+// full symmetric matrix: G_mn = sum_ls P_ls [(mn|ls) - 1/2 (ml|ns)]).
+static void build_G(const Molecule& M, const std::vector<double>& P, std::vector<double>& G) {
+  int N = M.nao;
+  G.assign((size_t)N * N, 0);
+  auto Pm = [&](int i, int j) { return P[(size_t)i * N + j]; };
+  auto Gm = [&](int i, int j) -> double& { return G[(size_t)i * N + j]; };
+  for (int a = 0; a < M.nat; ++a) {
+    const Element& e = M.el[a];
+    int o = M.ao0[a];
+    for (int i = 0; i < e.nao; ++i)
+      for (int j = 0; j < e.nao; ++j) {
+        double s = 0;
+        for (int k = 0; k < e.nao; ++k)
+          for (int l = 0; l < e.nao; ++l)
+            s += Pm(o + k, o + l) * (one_center(e, i, j, k, l) - 0.5 * one_center(e, i, k, j, l));
+        Gm(o + i, o + j) += s;
+      }
+  }
+  for (const auto& Pr : M.pairs) {
+    const Element &A = M.el[Pr.a], &B = M.el[Pr.b];
+    int oa = M.ao0[Pr.a], ob = M.ao0[Pr.b];
+    auto I = [&](int mu, int nu, int la, int si) { return Pr.G[pidx(mu, nu)][pidx(la, si)]; };
+    for (int mu = 0; mu < A.nao; ++mu)
+      for (int nu = 0; nu < A.nao; ++nu) {
+        double s = 0;
+        for (int la = 0; la < B.nao; ++la)
+          for (int si = 0; si < B.nao; ++si) s += Pm(ob + la, ob + si) * I(mu, nu, la, si);
+        Gm(oa + mu, oa + nu) += s;
+      }
+    for (int la = 0; la < B.nao; ++la)
+      for (int si = 0; si < B.nao; ++si) {
+        double s = 0;
+        for (int mu = 0; mu < A.nao; ++mu)
+          for (int nu = 0; nu < A.nao; ++nu) s += Pm(oa + mu, oa + nu) * I(mu, nu, la, si);
+        Gm(ob + la, ob + si) += s;
+      }
+    for (int mu = 0; mu < A.nao; ++mu)
+      for (int la = 0; la < B.nao; ++la) {
+        double s = 0;
+        for (int nu = 0; nu < A.nao; ++nu)
+          for (int si = 0; si < B.nao; ++si) s += Pm(oa + nu, ob + si) * I(mu, nu, la, si);
+        Gm(oa + mu, ob + la) -= 0.5 * s;
+        Gm(ob + la, oa + mu) -= 0.5 * s;
+      }
+  }
+}
+
+static double electronic_energy(const std::vector<double>& P, const std::vector<double>& H, const std::vector<double>& G) {
+  double e = 0;
+  for (size_t k = 0; k < P.size(); ++k) e += 0.5 * P[k] * (2 * H[k] + G[k]);
+  return e;
+}
+
+struct ScfSettings {
+  double scc = 1e-7, rmsd = 1e-5;
+  int max_iter = 100;
+  int diis_size = 8;
+};
+
+struct ScfResult {
+  double Eel = 0, Erep = 0, Etot = 0;
+  int iterations = 0;
+  bool converged = false;
+  std::vector<double> P, G, eps, C;
+};
+
+// Restricted SCF with Pulay (commutator) DIIS.
+static bool run_scf(Molecule& M, const ScfSettings& st, ScfResult& r, const std::vector<double>* Pguess) {
+  int N = M.nao;
+  std::vector<double> P((size_t)N * N, 0);
+  if (Pguess) {
+    P = *Pguess;
+  } else {
+    // NDDODensityGuess.cpp:31-66
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j) P[(size_t)i * N + j] = M.S[(size_t)i * N + j] * M.nel / (2.0 * N);
+    for (int a = 0; a < M.nat; ++a)
+      for (int k = 0; k < M.el[a].nao; ++k)
+        P[(size_t)(M.ao0[a] + k) * N + M.ao0[a] + k] = M.el[a].core / M.el[a].nao;
+  }
+  std::vector<double> G, F((size_t)N * N), w, C;
+  std::vector<std::vector<double>> hF, hE;
+  double Eold = 0;
+  bool have_old = false;
+  r.converged = false;
+  int it;
+  for (it = 1; it <= st.max_iter; ++it) {
+    build_G(M, P, G);
+    for (size_t k = 0; k < F.size(); ++k) F[k] = M.H[k] + G[k];
+    double E = electronic_energy(P, M.H, G);
+    // DIIS error FP - PF (orthonormal NDDO basis)
+    std::vector<double> FP((size_t)N * N, 0), err((size_t)N * N);
+    for (int i = 0; i < N; ++i)
+      for (int k = 0; k < N; ++k) {
+        double f = F[(size_t)i * N + k];
+        if (f == 0) continue;
+        for (int j = 0; j < N; ++j) FP[(size_t)i * N + j] += f * P[(size_t)k * N + j];
+      }
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j) err[(size_t)i * N + j] = FP[(size_t)i * N + j] - FP[(size_t)j * N + i];
+    hF.push_back(F);
+    hE.push_back(err);
+    if ((int)hF.size() > st.diis_size) {
+      hF.erase(hF.begin());
+      hE.erase(hE.begin());
+    }
+    std::vector<double> Fx = F;
+    int m = (int)hF.size();
+    if (m >= 2) {
+      std::vector<double> B((size_t)(m + 1) * (m + 1), 0), rhs(m + 1, 0);
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j <= i; ++j) {
+          double s = 0;
+          for (size_t k = 0; k < err.size(); ++k) s += hE[i][k] * hE[j][k];
+          B[i * (m + 1) + j] = B[j * (m + 1) + i] = s;
+        }
+      for (int i = 0; i < m; ++i) B[i * (m + 1) + m] = B[m * (m + 1) + i] = -1;
+      rhs[m] = -1;
+      if (solve_dense(m + 1, B, rhs)) {
+        std::fill(Fx.begin(), Fx.end(), 0.0);
+        for (int i = 0; i < m; ++i)
+          for (size_t k = 0; k < Fx.size(); ++k) Fx[k] += rhs[i] * hF[i][k];
+      }
+    }
+    if (!eigh(N, Fx, w, C)) return false;
+    std::vector<double> Pn((size_t)N * N, 0);
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j) {
+        double s = 0;
+        for (int o = 0; o < M.nocc; ++o) s += C[(size_t)i * N + o] * C[(size_t)j * N + o];
+        Pn[(size_t)i * N + j] = 2 * s;
+      }
+    double rms = 0;
+    for (size_t k = 0; k < P.size(); ++k) rms += (Pn[k] - P[k]) * (Pn[k] - P[k]);
+    rms = std::sqrt(rms / (double)P.size());
+    P.swap(Pn);
+    bool dE_ok = have_old && std::fabs(E - Eold) < st.scc;
+    Eold = E;
+    have_old = true;
+    if (dE_ok && rms < st.rmsd) {
+      r.converged = true;
+      break;
+    }
+  }
+  r.iterations = std::min(it, st.max_iter);
+  build_G(M, P, G);  // FockMatrix::finalize: G consistent with the final density
+  r.Eel = electronic_energy(P, M.H, G);
+  r.Erep = M.Erep;
+  r.Etot = r.Eel + r.Erep;
+  // orbital energies of the final Fock matrix
+  std::vector<double> Fin((size_t)N * N);
+  for (size_t k = 0; k < Fin.size(); ++k) Fin[k] = M.H[k] + G[k];
+  eigh(N, Fin, r.eps, r.C);
+  r.P = P;
+  r.G = G;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// Nuclear gradient (OneElectronMatrix.cpp:136-229, TwoElectronMatrix.cpp:168-241)
+// ---------------------------------------------------------------------------
+static void gradient(const Molecule& M, const std::vector<double>& P, std::vector<double>& grad) {
+  int N = M.nao;
+  grad.assign(3 * M.nat, 0);
+  auto Pm = [&](int i, int j) { return P[(size_t)i * N + j]; };
+  for (int a = 0; a < M.nat; ++a)
+    for (int b = a + 1; b < M.nat; ++b) {
+      const Element &A = M.el[a], &B = M.el[b];
+      int oa = M.ao0[a], ob = M.ao0[b];
+      double Xv = M.pos[3 * b] - M.pos[3 * a], Yv = M.pos[3 * b + 1] - M.pos[3 * a + 1],
+             Zv = M.pos[3 * b + 2] - M.pos[3 * a + 2];
+      D3 X(Xv, 1, 0, 0), Y(Yv, 0, 1, 0), Zd(Zv, 0, 0, 1);
+      double g[3] = {0, 0, 0};
+      // two-electron part
+      D3 G[10][10];
+      global_block<D3>(A.nao, B.nao, X, Y, Zd, A, B, false, 0.0, G);
+      for (int mu = 0; mu < A.nao; ++mu)
+        for (int nu = 0; nu < A.nao; ++nu)
+          for (int la = 0; la < B.nao; ++la)
+            for (int si = 0; si < B.nao; ++si) {
+              double f = Pm(oa + mu, oa + nu) * Pm(ob + la, ob + si) - 0.5 * Pm(oa + mu, ob + la) * Pm(oa + nu, ob + si);
+              const D3& I = G[pidx(mu, nu)][pidx(la, si)];
+              for (int d = 0; d < 3; ++d) g[d] += f * I.g[d];
+            }
+      // core attraction of A's electrons to B's core
+      D3 V[10][10];
+      global_block<D3>(A.nao, 1, X, Y, Zd, A, B, true, B.pcore, V);
+      for (int mu = 0; mu < A.nao; ++mu)
+        for (int nu = 0; nu < A.nao; ++nu) {
+          double f = Pm(oa + mu, oa + nu) * (-B.core);
+          for (int d = 0; d < 3; ++d) g[d] += f * V[pidx(mu, nu)][0].g[d];
+        }
+      // core attraction of B's electrons to A's core (pair vector reversed)
+      D3 Xr(-Xv, 1, 0, 0), Yr(-Yv, 0, 1, 0), Zr(-Zv, 0, 0, 1);
+      global_block<D3>(B.nao, 1, Xr, Yr, Zr, B, A, true, A.pcore, V);
+      for (int mu = 0; mu < B.nao; ++mu)
+        for (int nu = 0; nu < B.nao; ++nu) {
+          double f = Pm(ob + mu, ob + nu) * (-A.core);
+          for (int d = 0; d < 3; ++d) g[d] -= f * V[pidx(mu, nu)][0].g[d];
+        }
+      // resonance: (beta_mu + beta_nu) P_mn dS_mn
+      D3 R[3] = {X, Y, Zd};
+      D3 S[4][4];
+      overlap_block<D3>(A, B, R, S);
+      for (int mu = 0; mu < A.nao; ++mu)
+        for (int nu = 0; nu < B.nao; ++nu) {
+          double ba = mu == 0 ? A.betaS : A.betaP, bb = nu == 0 ? B.betaS : B.betaP;
+          double f = (ba + bb) * Pm(oa + mu, ob + nu);
+          for (int d = 0; d < 3; ++d) g[d] += f * S[mu][nu].g[d];
+        }
+      // core-core repulsion
+      double Rabs = std::sqrt(Xv * Xv + Yv * Yv + Zv * Zv);
+      double E, dE;
+      repulsion(M.method, A, B, Rabs, E, dE);
+      g[0] += dE * Xv / Rabs;
+      g[1] += dE * Yv / Rabs;
+      g[2] += dE * Zv / Rabs;
+      for (int d = 0; d < 3; ++d) {
+        grad[3 * b + d] += g[d];
+        grad[3 * a + d] -= g[d];
+      }
+    }
+}
+
+static bool parse_method(const char* s, Method& m) {
+  std::string t(s ? s : "");
+  for (auto& c : t) c = (char)toupper(c);
+  if (t == "PM6") m = kPM6;
+  else if (t == "AM1") m = kAM1;
+  else if (t == "MNDO") m = kMNDO;
+  else return false;
+  return true;
+}
+
+static thread_local std::string g_err;
+
+}  // namespace oracle
+
+using namespace oracle;
+
+extern "C" {
+
+const char* oracle_last_error() { return g_err.c_str(); }
+
+double oracle_ev_per_hartree() { return kEvPerHartree; }
+double oracle_bohr_per_angstrom() { return kBohrPerAngstrom; }
+
+// Runtime parameters of one element: [nao, core, Uss, Upp, betaS, betaP, alpha,
+// D_sp1, D_pp2, rho_ss0, rho_sp1, rho_pp0, rho_pp2, pcore, gss, gsp, gpp, gp2, hsp, hpp]
+int oracle_element_params(const char* method, int Z, double* out20) {
+  Method m;
+  if (!parse_method(method, m)) return 1;
+  Element e;
+  if (!make_element(m, Z, e)) return 2;
+  double v[20] = {(double)e.nao, e.core, e.Uss, e.Upp, e.betaS, e.betaP, e.alpha, e.D_sp1, e.D_pp2, e.rho_ss0,
+                  e.rho_sp1, e.rho_pp0, e.rho_pp2, e.pcore, e.gss, e.gsp, e.gpp, e.gp2, e.hsp, e.hpp};
+  std::memcpy(out20, v, sizeof(v));
+  return 0;
+}
+
+// Local 10x10 (s/p) two-centre integrals with explicit multipole parameters,
+// for the reference's integral-level tests.  rho/D arrays: [ss0, sp1, pp0, pp2] / [sp1, pp2].
+int oracle_local_block(double R, const double* rhoA, const double* DA, const double* rhoB, const double* DB,
+                       double* out100) {
+  Element A, B;
+  A.nao = B.nao = 4;
+  A.rho_ss0 = rhoA[0]; A.rho_sp1 = rhoA[1]; A.rho_pp0 = rhoA[2]; A.rho_pp2 = rhoA[3];
+  B.rho_ss0 = rhoB[0]; B.rho_sp1 = rhoB[1]; B.rho_pp0 = rhoB[2]; B.rho_pp2 = rhoB[3];
+  A.D_sp1 = DA[0]; A.D_pp2 = DA[1];
+  B.D_sp1 = DB[0]; B.D_pp2 = DB[1];
+  double L[10][10], dL[10][10];
+  local_matrix(10, 10, R, A, B, false, 0.0, L, dL);
+  for (int i = 0; i < 10; ++i)
+    for (int j = 0; j < 10; ++j) out100[i * 10 + j] = L[i][j];
+  return 0;
+}
+
+// Charge separations of an s/p shell pair from Slater exponents (D_sp1, D_pp2).
+int oracle_charge_separations(int ns, int np, double zs, double zp, double* out2) {
+  int n = ns <= np ? ns : np;
+  out2[0] = A_factor(n, n, zs, zp, 1) / std::sqrt(3.0);
+  out2[1] = std::sqrt(A_factor(n, n, zp, zp, 2)) / std::sqrt(5.0);
+  return 0;
+}
+
+// One-electron matrix H and overlap S (N x N, row-major) for a structure.
+int oracle_one_electron(const char* method, int nat, const int* Z, const double* xyz_bohr, int charge, double* H,
+                        double* S, int* nao_out) {
+  Method m;
+  if (!parse_method(method, m)) { g_err = "unknown method"; return 1; }
+  Molecule M;
+  int rc = setup(M, m, nat, Z, xyz_bohr, charge, g_err);
+  if (rc && rc != 3) return rc;  // H and S do not depend on the electron count
+  build_pairs(M);
+  build_one_electron(M);
+  *nao_out = M.nao;
+  if (H) std::memcpy(H, M.H.data(), sizeof(double) * M.H.size());
+  if (S) std::memcpy(S, M.S.data(), sizeof(double) * M.S.size());
+  return 0;
+}
+
+// Global 2c2e blocks of every pair (i<j in input order): out[pair][100], plus
+// core-attraction vectors VA/VB [pair][10].  Returns the pair count in *npairs.
+int oracle_pair_blocks(const char* method, int nat, const int* Z, const double* xyz_bohr, double* G100,
+                       double* VA10, double* VB10, int* npairs) {
+  Method m;
+  if (!parse_method(method, m)) { g_err = "unknown method"; return 1; }
+  Molecule M;
+  int rc = setup(M, m, nat, Z, xyz_bohr, 0, g_err);
+  if (rc && rc != 3) return rc;
+  build_pairs(M);
+  *npairs = (int)M.pairs.size();
+  for (size_t p = 0; p < M.pairs.size(); ++p) {
+    for (int i = 0; i < 10; ++i)
+      for (int j = 0; j < 10; ++j) G100[p * 100 + i * 10 + j] = M.pairs[p].G[i][j];
+    for (int i = 0; i < 10; ++i) {
+      VA10[p * 10 + i] = M.pairs[p].VA[i];
+      VB10[p * 10 + i] = M.pairs[p].VB[i];
+    }
+  }
+  return 0;
+}
+
+// Full single point.  info[8] = {E_el, E_rep, iterations, converged, nao, nocc, nel, 0}.
+// P_out (N*N) and eps_out (N) are optional.
+int oracle_scf(const char* method, int nat, const int* Z, const double* xyz_bohr, int charge, double scc,
+               double rmsd, int max_iter, int want_gradient, double* energy, double* grad, double* info,
+               double* P_out, double* eps_out) {
+  Method m;
+  if (!parse_method(method, m)) { g_err = "unknown method"; return 1; }
+  Molecule M;
+  int rc = setup(M, m, nat, Z, xyz_bohr, charge, g_err);
+  if (rc) return rc;
+  build_pairs(M);
+  build_one_electron(M);
+  ScfSettings st;
+  st.scc = scc;
+  st.rmsd = rmsd;
+  st.max_iter = max_iter;
+  ScfResult r;
+  if (!run_scf(M, st, r, nullptr)) { g_err = "eigensolver failed"; return 5; }
+  *energy = r.Etot;
+  if (info) {
+    double v[8] = {r.Eel, r.Erep, (double)r.iterations, r.converged ? 1.0 : 0.0, (double)M.nao, (double)M.nocc,
+                   (double)M.nel, 0};
+    std::memcpy(info, v, sizeof(v));
+  }
+  if (P_out) std::memcpy(P_out, r.P.data(), sizeof(double) * r.P.size());
+  if (eps_out) std::memcpy(eps_out, r.eps.data(), sizeof(double) * r.eps.size());
+  if (want_gradient && grad) {
+    std::vector<double> g;
+    gradient(M, r.P, g);
+    std::memcpy(grad, g.data(), sizeof(double) * g.size());
+  }
+  return 0;
+}
+
+// Energy of a given density (no SCF): E_el(P) + E_rep, and the gradient at P.
+int oracle_energy_at_density(const char* method, int nat, const int* Z, const double* xyz_bohr, const double* P,
+                             double* energy, double* grad) {
+  Method m;
+  if (!parse_method(method, m)) { g_err = "unknown method"; return 1; }
+  Molecule M;
+  int rc = setup(M, m, nat, Z, xyz_bohr, 0, g_err);
+  if (rc && rc != 3) return rc;
+  build_pairs(M);
+  build_one_electron(M);
+  std::vector<double> Pv(P, P + (size_t)M.nao * M.nao), G;
+  build_G(M, Pv, G);
+  *energy = electronic_energy(Pv, M.H, G) + M.Erep;
+  if (grad) {
+    std::vector<double> g;
+    gradient(M, Pv, g);
+    std::memcpy(grad, g.data(), sizeof(double) * g.size());
+  }
+  return 0;
+}
+
+}  // extern "C"
