@@ -1,0 +1,128 @@
+/*
+ * sparrow_b200 C-ABI: batched NDDO (MNDO / AM1 / PM6) single points on one
+ * NVIDIA B200 (sm_100a), energy and nuclear gradient.
+ *
+ * Every entry point returns an int32 status (SG_OK = 0) and copies caller
+ * buffers in or out; no pointer into engine memory escapes.  Units: positions
+ * in bohr, energies in Hartree, gradients in Hartree/bohr.  A handle is not
+ * thread-safe; independent handles may be used from different threads.
+ *
+ * The entry points replace the reference's Core::Calculator surface as
+ * implemented by GenericMethodWrapper / NDDOMethodWrapper (qcscine/sparrow,
+ * paths relative to src/Sparrow/Sparrow/):
+ *   sg_create                 SparrowModule.cpp:29-49 (ModuleManager::get("calculator", "PM6"))
+ *   sg_set_structure          Implementations/GenericMethodWrapper.cpp:101-107 (setStructure)
+ *   sg_modify_positions       Implementations/GenericMethodWrapper.h:51-134 (modifyPositions)
+ *   sg_get_positions          Implementations/GenericMethodWrapper.h:51-134 (getPositions)
+ *   sg_set_setting_*          Implementations/Nddo/NDDOMethodWrapper.cpp:68-103 (settings())
+ *   sg_set_required_properties Implementations/GenericMethodWrapper.h:51-134 (setRequiredProperties)
+ *   sg_calculate              Implementations/GenericMethodWrapper.cpp:58-99 (calculate)
+ *   sg_get_energy / sg_get_gradients / sg_get_scf_info
+ *                             Implementations/GenericMethodWrapper.cpp:175-262 (results())
+ *   sg_get_density / sg_set_density
+ *                             Implementations/GenericMethodWrapper.cpp:268-282 (getState/loadState)
+ *   sg_get_orbital_energies   results() OrbitalEnergies
+ *   sg_clone                  Implementations/Nddo/Pm6/Wrapper/PM6MethodWrapper.cpp:38-45 (clone)
+ * The batch entry points (sg_batch_*) have no counterpart in the reference:
+ * they run many independent molecules through one device launch sequence.
+ */
+#ifndef SPARROW_B200_H
+#define SPARROW_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define SG_OK 0
+#define SG_ERR_INVALID_ARGUMENT 1
+#define SG_ERR_UNKNOWN_METHOD 2
+#define SG_ERR_UNSUPPORTED_ELEMENT 3
+#define SG_ERR_EMPTY_STRUCTURE 4
+#define SG_ERR_ODD_ELECTRONS 5
+#define SG_ERR_NOT_CONVERGED 6 /* informational: results are still available */
+#define SG_ERR_CUDA 7
+#define SG_ERR_OUT_OF_MEMORY 8
+#define SG_ERR_NO_RESULTS 9
+#define SG_ERR_UNKNOWN_SETTING 10
+#define SG_ERR_DEVICE 11
+
+/* required-property mask */
+#define SG_PROP_ENERGY 1u
+#define SG_PROP_GRADIENTS 2u
+
+typedef struct sg_calculator sg_calculator;
+typedef struct sg_batch sg_batch;
+
+/* version string of the library */
+const char* sg_version(void);
+
+/* ---- single-structure calculator (Core::Calculator surface) ---- */
+int32_t sg_create(const char* method, sg_calculator** out);
+void sg_destroy(sg_calculator* h);
+int32_t sg_clone(const sg_calculator* h, sg_calculator** out);
+const char* sg_last_error(const sg_calculator* h);
+
+int32_t sg_set_structure(sg_calculator* h, int32_t n_atoms, const int32_t* atomic_numbers, const double* xyz_bohr);
+int32_t sg_modify_positions(sg_calculator* h, const double* xyz_bohr);
+int32_t sg_get_positions(const sg_calculator* h, double* xyz_bohr);
+int32_t sg_get_n_atoms(const sg_calculator* h, int32_t* n_atoms);
+
+/* Settings keys follow the reference: "molecular_charge", "spin_multiplicity",
+ * "spin_mode", "self_consistence_criterion", "density_rmsd_criterion",
+ * "max_scf_iterations", "scf_mixer", "method_parameters". */
+int32_t sg_set_setting_int(sg_calculator* h, const char* key, int64_t value);
+int32_t sg_set_setting_double(sg_calculator* h, const char* key, double value);
+int32_t sg_set_setting_string(sg_calculator* h, const char* key, const char* value);
+int32_t sg_get_setting_double(const sg_calculator* h, const char* key, double* value);
+int32_t sg_get_setting_int(const sg_calculator* h, const char* key, int64_t* value);
+
+int32_t sg_set_required_properties(sg_calculator* h, uint32_t mask);
+/* Returns SG_OK, SG_ERR_NOT_CONVERGED (energy still set, like the reference's
+ * SuccessfulCalculation = false) or an error. */
+int32_t sg_calculate(sg_calculator* h);
+int32_t sg_get_energy(const sg_calculator* h, double* energy);
+int32_t sg_get_gradients(const sg_calculator* h, double* gradients);
+int32_t sg_get_scf_info(const sg_calculator* h, int32_t* iterations, int32_t* converged, int32_t* n_aos,
+                        int32_t* n_occupied);
+int32_t sg_get_orbital_energies(const sg_calculator* h, double* eps);
+/* density matrix (n_aos x n_aos, row-major) of the last calculation, and a
+ * start density for the next one (warm start) */
+int32_t sg_get_density(const sg_calculator* h, double* P);
+int32_t sg_set_density(sg_calculator* h, const double* P);
+
+/* ---- batches: many independent molecules per device launch sequence ---- */
+/* Molecule i has n_atoms[i] atoms; atomic_numbers / xyz_bohr are the
+ * concatenation over molecules; charges may be NULL (all neutral). */
+int32_t sg_batch_create(const char* method, int32_t n_molecules, const int32_t* n_atoms,
+                        const int32_t* atomic_numbers, const double* xyz_bohr, const int32_t* charges,
+                        sg_batch** out);
+void sg_batch_destroy(sg_batch* b);
+const char* sg_batch_last_error(const sg_batch* b);
+int32_t sg_batch_set_scf(sg_batch* b, double self_consistence_criterion, double density_rmsd_criterion,
+                         int32_t max_scf_iterations);
+int32_t sg_batch_set_positions(sg_batch* b, const double* xyz_bohr);
+/* enqueue integrals -> SCF -> (gradient) on the device; asynchronous */
+int32_t sg_batch_run(sg_batch* b, uint32_t properties);
+/* wait and copy results: arrays of n_molecules (energies, iterations,
+ * converged) and 3 * total atoms (gradients); any pointer may be NULL */
+int32_t sg_batch_results(sg_batch* b, double* energies, double* gradients, int32_t* iterations, int32_t* converged);
+/* number of device kernel launches issued by the last sg_batch_run */
+int32_t sg_batch_launches(const sg_batch* b);
+/* CUDA stream (cudaStream_t) the batch runs on, for event timing */
+void* sg_batch_stream(const sg_batch* b);
+
+/* one call from host buffers to host results (create, run, fetch, destroy) */
+int32_t sg_batch_calculate(const char* method, int32_t n_molecules, const int32_t* n_atoms,
+                           const int32_t* atomic_numbers, const double* xyz_bohr, const int32_t* charges,
+                           double self_consistence_criterion, double density_rmsd_criterion,
+                           int32_t max_scf_iterations, uint32_t properties, double* energies, double* gradients,
+                           int32_t* iterations, int32_t* converged, char* error_message, int32_t error_capacity);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPARROW_B200_H */

@@ -854,6 +854,7 @@ static void build_pairs(Molecule& M) {
   for (int a = 0; a < n; ++a)
     for (int b = a + 1; b < n; ++b) {
       Molecule::Pair P;
+      std::memset(&P, 0, sizeof(P));
       P.a = a;
       P.b = b;
       const Element &A = M.el[a], &B = M.el[b];

@@ -1,0 +1,359 @@
+"""sparrow_b200: batched NDDO (MNDO/AM1/PM6) SCF on the NVIDIA B200.
+
+Python mirror of the reference's calculator interface (qcscine/sparrow,
+src/Sparrow/Sparrow/Implementations/GenericMethodWrapper.h:51-134 and the
+Python usage in src/Sparrow/Python/Tests/CalculatorTest.py): a Calculator with
+a structure, string-keyed settings, required properties and calculate()
+returning results (energy, gradients, success flag).  Positions are in bohr,
+energies in Hartree, gradients in Hartree/bohr.
+
+Every call goes through the C-ABI of libsparrow_b200.so (include/sparrow_b200.h),
+which runs hand-written sm_100a kernels.  There is no CPU path: if the library
+or a CUDA device is missing, calls raise.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["Calculator", "Batch", "Results", "get_calculator", "batch_calculate", "library_path", "SparrowError"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libsparrow_b200.so")
+_lib = None
+
+SG_PROP_ENERGY = 1
+SG_PROP_GRADIENTS = 2
+SG_ERR_NOT_CONVERGED = 6
+
+_D = ctypes.POINTER(ctypes.c_double)
+_I32 = ctypes.POINTER(ctypes.c_int32)
+_VP = ctypes.c_void_p
+
+
+class SparrowError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__("sparrow_b200 error %d: %s" % (code, message))
+        self.code = code
+
+
+def library_path():
+    return _LIB_PATH
+
+
+def lib():
+    """Load libsparrow_b200.so (built by __graft_entry__.build() / `make -C sparrow_b200/csrc`)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError("libsparrow_b200.so is not built: run `make -C sparrow_b200/csrc`")
+    L = ctypes.CDLL(_LIB_PATH)
+    sig = {
+        "sg_version": (ctypes.c_char_p, []),
+        "sg_create": (ctypes.c_int32, [ctypes.c_char_p, ctypes.POINTER(_VP)]),
+        "sg_destroy": (None, [_VP]),
+        "sg_clone": (ctypes.c_int32, [_VP, ctypes.POINTER(_VP)]),
+        "sg_last_error": (ctypes.c_char_p, [_VP]),
+        "sg_set_structure": (ctypes.c_int32, [_VP, ctypes.c_int32, _I32, _D]),
+        "sg_modify_positions": (ctypes.c_int32, [_VP, _D]),
+        "sg_get_positions": (ctypes.c_int32, [_VP, _D]),
+        "sg_get_n_atoms": (ctypes.c_int32, [_VP, _I32]),
+        "sg_set_setting_int": (ctypes.c_int32, [_VP, ctypes.c_char_p, ctypes.c_int64]),
+        "sg_set_setting_double": (ctypes.c_int32, [_VP, ctypes.c_char_p, ctypes.c_double]),
+        "sg_set_setting_string": (ctypes.c_int32, [_VP, ctypes.c_char_p, ctypes.c_char_p]),
+        "sg_get_setting_double": (ctypes.c_int32, [_VP, ctypes.c_char_p, _D]),
+        "sg_get_setting_int": (ctypes.c_int32, [_VP, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64)]),
+        "sg_set_required_properties": (ctypes.c_int32, [_VP, ctypes.c_uint32]),
+        "sg_calculate": (ctypes.c_int32, [_VP]),
+        "sg_get_energy": (ctypes.c_int32, [_VP, _D]),
+        "sg_get_gradients": (ctypes.c_int32, [_VP, _D]),
+        "sg_get_scf_info": (ctypes.c_int32, [_VP, _I32, _I32, _I32, _I32]),
+        "sg_get_orbital_energies": (ctypes.c_int32, [_VP, _D]),
+        "sg_get_density": (ctypes.c_int32, [_VP, _D]),
+        "sg_set_density": (ctypes.c_int32, [_VP, _D]),
+        "sg_batch_create": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _I32, _D, _I32,
+                                             ctypes.POINTER(_VP)]),
+        "sg_batch_destroy": (None, [_VP]),
+        "sg_batch_last_error": (ctypes.c_char_p, [_VP]),
+        "sg_batch_set_scf": (ctypes.c_int32, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int32]),
+        "sg_batch_set_positions": (ctypes.c_int32, [_VP, _D]),
+        "sg_batch_run": (ctypes.c_int32, [_VP, ctypes.c_uint32]),
+        "sg_batch_results": (ctypes.c_int32, [_VP, _D, _D, _I32, _I32]),
+        "sg_batch_launches": (ctypes.c_int32, [_VP]),
+        "sg_batch_stream": (_VP, [_VP]),
+        "sg_batch_calculate": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _I32, _D, _I32,
+                                                ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_uint32,
+                                                _D, _D, _I32, _I32, ctypes.c_char_p, ctypes.c_int32]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _dptr(a):
+    return a.ctypes.data_as(_D)
+
+
+def _iptr(a):
+    return a.ctypes.data_as(_I32)
+
+
+class Results:
+    """Results of one calculation (subset of the reference's Utils::Results)."""
+
+    def __init__(self, energy, gradients, successful_calculation, iterations, n_aos, n_occupied):
+        self.energy = energy
+        self.gradients = gradients
+        self.successful_calculation = successful_calculation
+        self.iterations = iterations
+        self.n_aos = n_aos
+        self.n_occupied = n_occupied
+
+
+class _Settings:
+    """String-keyed settings with the reference's names and defaults."""
+
+    _INT = ("molecular_charge", "spin_multiplicity", "max_scf_iterations")
+    _REAL = ("self_consistence_criterion", "density_rmsd_criterion")
+    _STR = ("spin_mode", "scf_mixer", "method_parameters")
+
+    def __init__(self, calc):
+        self._calc = calc
+        self._str = {"spin_mode": "any", "scf_mixer": "diis", "method_parameters": ""}
+
+    def __setitem__(self, key, value):
+        L, h = lib(), self._calc._h
+        if key in self._INT:
+            rc = L.sg_set_setting_int(h, key.encode(), int(value))
+        elif key in self._REAL:
+            rc = L.sg_set_setting_double(h, key.encode(), float(value))
+        elif key in self._STR:
+            rc = L.sg_set_setting_string(h, key.encode(), str(value).encode())
+            if rc == 0:
+                self._str[key] = str(value)
+        else:
+            raise KeyError("unknown setting %r" % key)
+        self._calc._check(rc)
+
+    def __getitem__(self, key):
+        L, h = lib(), self._calc._h
+        if key in self._INT:
+            v = ctypes.c_int64()
+            self._calc._check(L.sg_get_setting_int(h, key.encode(), ctypes.byref(v)))
+            return v.value
+        if key in self._REAL:
+            v = ctypes.c_double()
+            self._calc._check(L.sg_get_setting_double(h, key.encode(), ctypes.byref(v)))
+            return v.value
+        if key in self._STR:
+            return self._str[key]
+        raise KeyError("unknown setting %r" % key)
+
+
+class Calculator:
+    """Single-structure calculator ("PM6", "AM1" or "MNDO")."""
+
+    def __init__(self, method="PM6", _handle=None):
+        L = lib()
+        if _handle is None:
+            h = _VP()
+            rc = L.sg_create(method.encode(), ctypes.byref(h))
+            if rc != 0:
+                raise SparrowError(rc, L.sg_last_error(None).decode())
+            _handle = h
+        self._h = _handle
+        self.method = method.upper()
+        self.settings = _Settings(self)
+        self._n_atoms = 0
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.sg_destroy(self._h)
+            self._h = None
+
+    def _check(self, rc, allow=()):
+        if rc != 0 and rc not in allow:
+            raise SparrowError(rc, lib().sg_last_error(self._h).decode())
+        return rc
+
+    def set_structure(self, atomic_numbers, positions_bohr):
+        Z = np.ascontiguousarray(atomic_numbers, dtype=np.int32)
+        x = np.ascontiguousarray(positions_bohr, dtype=np.float64).reshape(-1)
+        if x.size != 3 * Z.size:
+            raise ValueError("positions must be (n_atoms, 3)")
+        self._check(lib().sg_set_structure(self._h, Z.size, _iptr(Z), _dptr(x)))
+        self._n_atoms = Z.size
+
+    @property
+    def structure(self):
+        return self._n_atoms
+
+    @structure.setter
+    def structure(self, value):
+        self.set_structure(*value)
+
+    @property
+    def positions(self):
+        out = np.zeros(3 * self._n_atoms)
+        self._check(lib().sg_get_positions(self._h, _dptr(out)))
+        return out.reshape(-1, 3)
+
+    @positions.setter
+    def positions(self, xyz_bohr):
+        x = np.ascontiguousarray(xyz_bohr, dtype=np.float64).reshape(-1)
+        if x.size != 3 * self._n_atoms:
+            raise ValueError("positions must be (n_atoms, 3)")
+        self._check(lib().sg_modify_positions(self._h, _dptr(x)))
+
+    def set_required_properties(self, props):
+        mask = 0
+        for p in props:
+            p = p.lower()
+            if p == "energy":
+                mask |= SG_PROP_ENERGY
+            elif p in ("gradients", "gradient"):
+                mask |= SG_PROP_GRADIENTS | SG_PROP_ENERGY
+            else:
+                raise ValueError("unsupported property %r" % p)
+        self._check(lib().sg_set_required_properties(self._h, mask))
+        self._mask = mask
+
+    def calculate(self):
+        L = lib()
+        rc = self._check(L.sg_calculate(self._h), allow=(SG_ERR_NOT_CONVERGED,))
+        e = ctypes.c_double()
+        self._check(L.sg_get_energy(self._h, ctypes.byref(e)))
+        it, conv, nao, nocc = (ctypes.c_int32() for _ in range(4))
+        self._check(L.sg_get_scf_info(self._h, ctypes.byref(it), ctypes.byref(conv), ctypes.byref(nao),
+                                      ctypes.byref(nocc)))
+        grad = None
+        if getattr(self, "_mask", SG_PROP_ENERGY) & SG_PROP_GRADIENTS:
+            g = np.zeros(3 * self._n_atoms)
+            self._check(L.sg_get_gradients(self._h, _dptr(g)))
+            grad = g.reshape(-1, 3)
+        self._nao = nao.value
+        return Results(e.value, grad, rc == 0 and bool(conv.value), it.value, nao.value, nocc.value)
+
+    def density(self):
+        n = self._nao
+        P = np.zeros(n * n)
+        self._check(lib().sg_get_density(self._h, _dptr(P)))
+        return P.reshape(n, n)
+
+    def orbital_energies(self):
+        e = np.zeros(self._nao)
+        self._check(lib().sg_get_orbital_energies(self._h, _dptr(e)))
+        return e
+
+    def set_density(self, P):
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        self._check(lib().sg_set_density(self._h, _dptr(P)))
+
+    def clone(self):
+        h = _VP()
+        self._check(lib().sg_clone(self._h, ctypes.byref(h)))
+        c = Calculator(self.method, _handle=h)
+        c._n_atoms = self._n_atoms
+        c._str = dict(self.settings._str)
+        if hasattr(self, "_mask"):
+            c._mask = self._mask
+        return c
+
+
+def get_calculator(method="PM6"):
+    """Equivalent of ModuleManager.get('calculator', method) in the reference."""
+    return Calculator(method)
+
+
+def _flatten(molecules):
+    n_atoms = np.array([len(z) for z, _ in molecules], dtype=np.int32)
+    Z = np.ascontiguousarray(np.concatenate([np.asarray(z) for z, _ in molecules]), dtype=np.int32)
+    X = np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=np.float64).reshape(-1) for _, x in molecules]))
+    return n_atoms, Z, X
+
+
+class Batch:
+    """Many independent molecules resident on the device.
+
+    molecules: list of (atomic_numbers, positions_bohr).  run() enqueues the
+    integral, SCF and (optionally) gradient kernels; results() waits and
+    copies the energies / gradients back.
+    """
+
+    def __init__(self, method, molecules, charges=None, scc=1e-7, rmsd=1e-5, max_iter=100):
+        L = lib()
+        self.n_atoms, Z, X = _flatten(molecules)
+        ch = None if charges is None else np.ascontiguousarray(charges, dtype=np.int32)
+        h = _VP()
+        rc = L.sg_batch_create(method.encode(), len(molecules), _iptr(self.n_atoms), _iptr(Z), _dptr(X),
+                               _iptr(ch) if ch is not None else None, ctypes.byref(h))
+        if rc != 0:
+            raise SparrowError(rc, L.sg_batch_last_error(None).decode())
+        self._h = h
+        self.n_molecules = len(molecules)
+        self._check(L.sg_batch_set_scf(h, scc, rmsd, max_iter))
+        self._props = SG_PROP_ENERGY
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.sg_batch_destroy(self._h)
+            self._h = None
+
+    def _check(self, rc, allow=()):
+        if rc != 0 and rc not in allow:
+            raise SparrowError(rc, lib().sg_batch_last_error(self._h).decode())
+        return rc
+
+    def set_positions(self, xyz_bohr_all):
+        x = np.ascontiguousarray(xyz_bohr_all, dtype=np.float64).reshape(-1)
+        self._check(lib().sg_batch_set_positions(self._h, _dptr(x)))
+
+    def run(self, gradients=False):
+        self._props = SG_PROP_ENERGY | (SG_PROP_GRADIENTS if gradients else 0)
+        self._check(lib().sg_batch_run(self._h, self._props))
+
+    def results(self):
+        n = self.n_molecules
+        e = np.zeros(n)
+        it = np.zeros(n, dtype=np.int32)
+        conv = np.zeros(n, dtype=np.int32)
+        g = np.zeros(3 * int(self.n_atoms.sum())) if self._props & SG_PROP_GRADIENTS else None
+        rc = lib().sg_batch_results(self._h, _dptr(e), _dptr(g) if g is not None else None, _iptr(it), _iptr(conv))
+        self._check(rc, allow=(SG_ERR_NOT_CONVERGED,))
+        grads = None
+        if g is not None:
+            grads = np.split(g.reshape(-1, 3), np.cumsum(self.n_atoms)[:-1])
+        return e, grads, it, conv.astype(bool)
+
+    @property
+    def launches(self):
+        return lib().sg_batch_launches(self._h)
+
+    @property
+    def stream(self):
+        return lib().sg_batch_stream(self._h)
+
+
+def batch_calculate(method, molecules, charges=None, scc=1e-7, rmsd=1e-5, max_iter=100, gradients=False):
+    """One call from host arrays to host results (sg_batch_calculate)."""
+    L = lib()
+    n_atoms, Z, X = _flatten(molecules)
+    n = len(molecules)
+    ch = None if charges is None else np.ascontiguousarray(charges, dtype=np.int32)
+    e = np.zeros(n)
+    it = np.zeros(n, dtype=np.int32)
+    conv = np.zeros(n, dtype=np.int32)
+    g = np.zeros(3 * int(n_atoms.sum())) if gradients else None
+    msg = ctypes.create_string_buffer(512)
+    props = SG_PROP_ENERGY | (SG_PROP_GRADIENTS if gradients else 0)
+    rc = L.sg_batch_calculate(method.encode(), n, _iptr(n_atoms), _iptr(Z), _dptr(X),
+                              _iptr(ch) if ch is not None else None, scc, rmsd, max_iter, props, _dptr(e),
+                              _dptr(g) if g is not None else None, _iptr(it), _iptr(conv), msg, 512)
+    if rc != 0 and rc != SG_ERR_NOT_CONVERGED:
+        raise SparrowError(rc, msg.value.decode())
+    grads = np.split(g.reshape(-1, 3), np.cumsum(n_atoms)[:-1]) if g is not None else None
+    return e, grads, it, conv.astype(bool)

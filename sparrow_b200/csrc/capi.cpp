@@ -1,0 +1,485 @@
+// C-ABI and the C++ Calculator facade (see include/sparrow_b200.h).
+//
+// Calculator mirrors the reference's GenericMethodWrapper behaviour
+// (src/Sparrow/Sparrow/Implementations/GenericMethodWrapper.cpp:58-282):
+// settings are applied at calculate(), results are invalidated by a new
+// structure or new positions, non-convergence is reported but the energy is
+// still returned, and the state is the density matrix.
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/sparrow_b200.h"
+#include "engine.h"
+#include "params.h"
+
+namespace sgb {
+
+struct Settings {
+  int charge = 0;
+  int multiplicity = 1;
+  std::string spin_mode = "any";
+  double scc = 1e-7;
+  double rmsd = 1e-5;
+  int max_iter = 100;
+  std::string mixer = "diis";
+  std::string parameters;
+};
+
+class Calculator {
+ public:
+  explicit Calculator(Method m) : method_(m), batch_(new Batch(m)) {}
+  Method method() const { return method_; }
+  Settings& settings() { return settings_; }
+  const Settings& settings() const { return settings_; }
+  std::string error;
+
+  int set_structure(int n, const int* Z, const double* xyz) {
+    if (n <= 0 || !Z || !xyz) {
+      error = "empty molecular structure";
+      return kErrEmptyStructure;
+    }
+    Z_.assign(Z, Z + n);
+    xyz_.assign(xyz, xyz + 3 * n);
+    invalidate(true);
+    return kOk;
+  }
+  int modify_positions(const double* xyz) {
+    if (Z_.empty()) {
+      error = "no structure set";
+      return kErrEmptyStructure;
+    }
+    xyz_.assign(xyz, xyz + xyz_.size());
+    invalidate(false);
+    return kOk;
+  }
+  int n_atoms() const { return (int)Z_.size(); }
+  const std::vector<double>& positions() const { return xyz_; }
+  void set_required(uint32_t mask) { required_ = mask; }
+
+  int calculate() {
+    if (Z_.empty()) {
+      error = "empty molecular structure";
+      return kErrEmptyStructure;
+    }
+    if (!settings_.parameters.empty()) {
+      error = "method_parameters: only the embedded parameter sets are available";
+      return kErrInvalidArgument;
+    }
+    if (settings_.multiplicity != 1 || settings_.spin_mode == "unrestricted") {
+      error = "only restricted closed-shell singlets are supported";
+      return kErrInvalidArgument;
+    }
+    ScfParams sp;
+    sp.scc = settings_.scc;
+    sp.rmsd = settings_.rmsd;
+    sp.max_iter = settings_.max_iter;
+    sp.diis_size = settings_.mixer == "diis" ? kDiisMax : 1;
+    std::vector<MoleculeInput> in(1);
+    in[0].Z = Z_;
+    in[0].xyz = xyz_;
+    in[0].charge = settings_.charge;
+    int rc = batch_->setup(in, error);
+    if (rc) return rc;
+    if (!state_.empty()) {
+      rc = batch_->set_start_density(state_.data(), error);
+      if (rc) return rc;
+    }
+    const bool grad = (required_ & SG_PROP_GRADIENTS) != 0;
+    rc = batch_->run(sp, grad, error);
+    if (rc) return rc;
+    std::vector<MoleculeOutput> out;
+    rc = batch_->fetch(out, grad, error);
+    if (rc) return rc;
+    result_ = out[0];
+    have_result_ = true;
+    have_gradient_ = grad;
+    batch_->fetch_density(0, density_, error);
+    batch_->fetch_orbital_energies(0, eps_, error);
+    if (result_.status != kDevOk) {
+      error = "device SCF failure code " + std::to_string(result_.status);
+      return kErrDevice;
+    }
+    if (!result_.converged) {
+      error = "SCF did not converge in " + std::to_string(result_.iterations) + " iterations";
+      return kErrNotConverged;
+    }
+    return kOk;
+  }
+
+  bool have_result() const { return have_result_; }
+  bool have_gradient() const { return have_gradient_; }
+  const MoleculeOutput& result() const { return result_; }
+  const std::vector<double>& density() const { return density_; }
+  const std::vector<double>& orbital_energies() const { return eps_; }
+  int set_density(const double* P) {
+    if (Z_.empty()) {
+      error = "no structure set";
+      return kErrEmptyStructure;
+    }
+    int n = 0;
+    for (int z : Z_) {
+      int k = engine_n_aos(method_, z);
+      if (!k) {
+        error = "unsupported element";
+        return kErrUnsupportedElement;
+      }
+      n += k;
+    }
+    state_.assign(P, P + (size_t)n * n);
+    return kOk;
+  }
+  int n_aos() const {
+    int n = 0;
+    for (int z : Z_) n += engine_n_aos(method_, z);
+    return n;
+  }
+  std::unique_ptr<Calculator> clone() const {
+    std::unique_ptr<Calculator> c(new Calculator(method_));
+    c->settings_ = settings_;
+    c->Z_ = Z_;
+    c->xyz_ = xyz_;
+    c->required_ = required_;
+    return c;
+  }
+
+ private:
+  void invalidate(bool new_structure) {
+    have_result_ = have_gradient_ = false;
+    if (new_structure) state_.clear();
+  }
+  Method method_;
+  Settings settings_;
+  std::unique_ptr<Batch> batch_;
+  std::vector<int> Z_;
+  std::vector<double> xyz_;
+  uint32_t required_ = SG_PROP_ENERGY;
+  MoleculeOutput result_;
+  bool have_result_ = false, have_gradient_ = false;
+  std::vector<double> density_, eps_, state_;
+};
+
+}  // namespace sgb
+
+using namespace sgb;
+
+struct sg_calculator {
+  std::unique_ptr<Calculator> impl;
+};
+
+struct sg_batch {
+  std::unique_ptr<Batch> impl;
+  ScfParams sp;
+  uint32_t props = SG_PROP_ENERGY;
+  std::string error;
+};
+
+namespace {
+thread_local std::string g_create_error;
+
+int32_t fail(sg_calculator* h, int32_t code, const std::string& msg) {
+  if (h) h->impl->error = msg;
+  return code;
+}
+
+bool read_molecules(int32_t n_mol, const int32_t* n_atoms, const int32_t* Z, const double* xyz,
+                    const int32_t* charges, std::vector<MoleculeInput>& mols, std::string& err) {
+  if (n_mol <= 0 || !n_atoms || !Z || !xyz) {
+    err = "empty batch";
+    return false;
+  }
+  mols.resize(n_mol);
+  size_t a = 0;
+  for (int i = 0; i < n_mol; ++i) {
+    if (n_atoms[i] <= 0) {
+      err = "molecule " + std::to_string(i) + " has no atoms";
+      return false;
+    }
+    mols[i].Z.assign(Z + a, Z + a + n_atoms[i]);
+    mols[i].xyz.assign(xyz + 3 * a, xyz + 3 * (a + n_atoms[i]));
+    mols[i].charge = charges ? charges[i] : 0;
+    a += n_atoms[i];
+  }
+  return true;
+}
+}  // namespace
+
+extern "C" {
+
+const char* sg_version(void) { return "sparrow_b200 0.1 (NDDO MNDO/AM1/PM6, s/p elements, sm_100a)"; }
+
+int32_t sg_create(const char* method, sg_calculator** out) {
+  if (!out) return SG_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  Method m;
+  if (!method || !parse_method(method, m)) {
+    g_create_error = std::string("unknown method '") + (method ? method : "") + "' (PM6, AM1, MNDO)";
+    return SG_ERR_UNKNOWN_METHOD;
+  }
+  *out = new sg_calculator{std::unique_ptr<Calculator>(new Calculator(m))};
+  return SG_OK;
+}
+
+void sg_destroy(sg_calculator* h) { delete h; }
+
+int32_t sg_clone(const sg_calculator* h, sg_calculator** out) {
+  if (!h || !out) return SG_ERR_INVALID_ARGUMENT;
+  *out = new sg_calculator{h->impl->clone()};
+  return SG_OK;
+}
+
+const char* sg_last_error(const sg_calculator* h) { return h ? h->impl->error.c_str() : g_create_error.c_str(); }
+
+int32_t sg_set_structure(sg_calculator* h, int32_t n, const int32_t* Z, const double* xyz) {
+  if (!h) return SG_ERR_INVALID_ARGUMENT;
+  return h->impl->set_structure(n, Z, xyz);
+}
+
+int32_t sg_modify_positions(sg_calculator* h, const double* xyz) {
+  if (!h || !xyz) return SG_ERR_INVALID_ARGUMENT;
+  return h->impl->modify_positions(xyz);
+}
+
+int32_t sg_get_positions(const sg_calculator* h, double* xyz) {
+  if (!h || !xyz) return SG_ERR_INVALID_ARGUMENT;
+  const auto& p = h->impl->positions();
+  std::memcpy(xyz, p.data(), sizeof(double) * p.size());
+  return SG_OK;
+}
+
+int32_t sg_get_n_atoms(const sg_calculator* h, int32_t* n) {
+  if (!h || !n) return SG_ERR_INVALID_ARGUMENT;
+  *n = h->impl->n_atoms();
+  return SG_OK;
+}
+
+int32_t sg_set_setting_int(sg_calculator* h, const char* key, int64_t v) {
+  if (!h || !key) return SG_ERR_INVALID_ARGUMENT;
+  Settings& s = h->impl->settings();
+  std::string k(key);
+  if (k == "molecular_charge") s.charge = (int)v;
+  else if (k == "spin_multiplicity") {
+    if (v < 1) return fail(h, SG_ERR_INVALID_ARGUMENT, "spin_multiplicity must be >= 1");
+    s.multiplicity = (int)v;
+  } else if (k == "max_scf_iterations") {
+    if (v < 1) return fail(h, SG_ERR_INVALID_ARGUMENT, "max_scf_iterations must be >= 1");
+    s.max_iter = (int)v;
+  } else
+    return fail(h, SG_ERR_UNKNOWN_SETTING, "unknown integer setting '" + k + "'");
+  return SG_OK;
+}
+
+int32_t sg_set_setting_double(sg_calculator* h, const char* key, double v) {
+  if (!h || !key) return SG_ERR_INVALID_ARGUMENT;
+  Settings& s = h->impl->settings();
+  std::string k(key);
+  if (!(v > 0) || !std::isfinite(v)) return fail(h, SG_ERR_INVALID_ARGUMENT, k + " must be a positive number");
+  if (k == "self_consistence_criterion") s.scc = v;
+  else if (k == "density_rmsd_criterion") s.rmsd = v;
+  else
+    return fail(h, SG_ERR_UNKNOWN_SETTING, "unknown real setting '" + k + "'");
+  return SG_OK;
+}
+
+int32_t sg_set_setting_string(sg_calculator* h, const char* key, const char* v) {
+  if (!h || !key || !v) return SG_ERR_INVALID_ARGUMENT;
+  Settings& s = h->impl->settings();
+  std::string k(key), val(v);
+  if (k == "spin_mode") {
+    if (val != "any" && val != "restricted" && val != "unrestricted" && val != "restricted_open_shell")
+      return fail(h, SG_ERR_INVALID_ARGUMENT, "unknown spin_mode '" + val + "'");
+    s.spin_mode = val;
+  } else if (k == "scf_mixer") {
+    if (val != "diis" && val != "no_mixer" && val != "none")
+      return fail(h, SG_ERR_INVALID_ARGUMENT, "unsupported scf_mixer '" + val + "' (diis, no_mixer)");
+    s.mixer = val == "diis" ? "diis" : "none";
+  } else if (k == "method_parameters") {
+    s.parameters = val;
+  } else
+    return fail(h, SG_ERR_UNKNOWN_SETTING, "unknown string setting '" + k + "'");
+  return SG_OK;
+}
+
+int32_t sg_get_setting_double(const sg_calculator* h, const char* key, double* v) {
+  if (!h || !key || !v) return SG_ERR_INVALID_ARGUMENT;
+  const Settings& s = h->impl->settings();
+  std::string k(key);
+  if (k == "self_consistence_criterion") *v = s.scc;
+  else if (k == "density_rmsd_criterion") *v = s.rmsd;
+  else
+    return SG_ERR_UNKNOWN_SETTING;
+  return SG_OK;
+}
+
+int32_t sg_get_setting_int(const sg_calculator* h, const char* key, int64_t* v) {
+  if (!h || !key || !v) return SG_ERR_INVALID_ARGUMENT;
+  const Settings& s = h->impl->settings();
+  std::string k(key);
+  if (k == "molecular_charge") *v = s.charge;
+  else if (k == "spin_multiplicity") *v = s.multiplicity;
+  else if (k == "max_scf_iterations") *v = s.max_iter;
+  else
+    return SG_ERR_UNKNOWN_SETTING;
+  return SG_OK;
+}
+
+int32_t sg_set_required_properties(sg_calculator* h, uint32_t mask) {
+  if (!h) return SG_ERR_INVALID_ARGUMENT;
+  if (mask & ~(SG_PROP_ENERGY | SG_PROP_GRADIENTS)) return fail(h, SG_ERR_INVALID_ARGUMENT, "unknown property bit");
+  h->impl->set_required(mask);
+  return SG_OK;
+}
+
+int32_t sg_calculate(sg_calculator* h) {
+  if (!h) return SG_ERR_INVALID_ARGUMENT;
+  return h->impl->calculate();
+}
+
+int32_t sg_get_energy(const sg_calculator* h, double* e) {
+  if (!h || !e) return SG_ERR_INVALID_ARGUMENT;
+  if (!h->impl->have_result()) return SG_ERR_NO_RESULTS;
+  *e = h->impl->result().energy;
+  return SG_OK;
+}
+
+int32_t sg_get_gradients(const sg_calculator* h, double* g) {
+  if (!h || !g) return SG_ERR_INVALID_ARGUMENT;
+  if (!h->impl->have_result() || !h->impl->have_gradient()) return SG_ERR_NO_RESULTS;
+  const auto& v = h->impl->result().gradient;
+  std::memcpy(g, v.data(), sizeof(double) * v.size());
+  return SG_OK;
+}
+
+int32_t sg_get_scf_info(const sg_calculator* h, int32_t* it, int32_t* conv, int32_t* nao, int32_t* nocc) {
+  if (!h) return SG_ERR_INVALID_ARGUMENT;
+  if (!h->impl->have_result()) return SG_ERR_NO_RESULTS;
+  const auto& r = h->impl->result();
+  if (it) *it = r.iterations;
+  if (conv) *conv = r.converged;
+  if (nao) *nao = r.nao;
+  if (nocc) *nocc = r.nocc;
+  return SG_OK;
+}
+
+int32_t sg_get_orbital_energies(const sg_calculator* h, double* eps) {
+  if (!h || !eps) return SG_ERR_INVALID_ARGUMENT;
+  if (!h->impl->have_result()) return SG_ERR_NO_RESULTS;
+  const auto& v = h->impl->orbital_energies();
+  std::memcpy(eps, v.data(), sizeof(double) * v.size());
+  return SG_OK;
+}
+
+int32_t sg_get_density(const sg_calculator* h, double* P) {
+  if (!h || !P) return SG_ERR_INVALID_ARGUMENT;
+  if (!h->impl->have_result()) return SG_ERR_NO_RESULTS;
+  const auto& v = h->impl->density();
+  std::memcpy(P, v.data(), sizeof(double) * v.size());
+  return SG_OK;
+}
+
+int32_t sg_set_density(sg_calculator* h, const double* P) {
+  if (!h || !P) return SG_ERR_INVALID_ARGUMENT;
+  return h->impl->set_density(P);
+}
+
+int32_t sg_batch_create(const char* method, int32_t n_mol, const int32_t* n_atoms, const int32_t* Z,
+                        const double* xyz, const int32_t* charges, sg_batch** out) {
+  if (!out) return SG_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  Method m;
+  if (!method || !parse_method(method, m)) {
+    g_create_error = "unknown method";
+    return SG_ERR_UNKNOWN_METHOD;
+  }
+  std::vector<MoleculeInput> mols;
+  std::string err;
+  if (!read_molecules(n_mol, n_atoms, Z, xyz, charges, mols, err)) {
+    g_create_error = err;
+    return SG_ERR_EMPTY_STRUCTURE;
+  }
+  std::unique_ptr<sg_batch> b(new sg_batch);
+  b->impl.reset(new Batch(m));
+  int rc = b->impl->setup(mols, err);
+  if (rc) {
+    g_create_error = err;
+    return rc;
+  }
+  *out = b.release();
+  return SG_OK;
+}
+
+void sg_batch_destroy(sg_batch* b) { delete b; }
+
+const char* sg_batch_last_error(const sg_batch* b) { return b ? b->error.c_str() : g_create_error.c_str(); }
+
+int32_t sg_batch_set_scf(sg_batch* b, double scc, double rmsd, int32_t max_iter) {
+  if (!b || !(scc > 0) || !(rmsd > 0) || max_iter < 1) return SG_ERR_INVALID_ARGUMENT;
+  b->sp.scc = scc;
+  b->sp.rmsd = rmsd;
+  b->sp.max_iter = max_iter;
+  return SG_OK;
+}
+
+int32_t sg_batch_set_positions(sg_batch* b, const double* xyz) {
+  if (!b || !xyz) return SG_ERR_INVALID_ARGUMENT;
+  return b->impl->set_positions(xyz, b->error);
+}
+
+int32_t sg_batch_run(sg_batch* b, uint32_t props) {
+  if (!b) return SG_ERR_INVALID_ARGUMENT;
+  b->props = props;
+  return b->impl->run(b->sp, (props & SG_PROP_GRADIENTS) != 0, b->error);
+}
+
+int32_t sg_batch_results(sg_batch* b, double* energies, double* gradients, int32_t* iterations, int32_t* converged) {
+  if (!b) return SG_ERR_INVALID_ARGUMENT;
+  const bool grad = gradients && (b->props & SG_PROP_GRADIENTS);
+  std::vector<MoleculeOutput> out;
+  int rc = b->impl->fetch(out, grad, b->error);
+  if (rc) return rc;
+  size_t a = 0;
+  int status = SG_OK;
+  for (size_t i = 0; i < out.size(); ++i) {
+    if (energies) energies[i] = out[i].energy;
+    if (iterations) iterations[i] = out[i].iterations;
+    if (converged) converged[i] = out[i].converged;
+    if (grad) {
+      std::memcpy(gradients + 3 * a, out[i].gradient.data(), sizeof(double) * out[i].gradient.size());
+      a += out[i].gradient.size() / 3;
+    }
+    if (out[i].status != kDevOk) status = SG_ERR_DEVICE;
+    else if (!out[i].converged && status == SG_OK) status = SG_ERR_NOT_CONVERGED;
+  }
+  return status;
+}
+
+int32_t sg_batch_launches(const sg_batch* b) { return b ? b->impl->launches_last_run() : 0; }
+
+void* sg_batch_stream(const sg_batch* b) { return b ? (void*)b->impl->stream() : nullptr; }
+
+int32_t sg_batch_calculate(const char* method, int32_t n_mol, const int32_t* n_atoms, const int32_t* Z,
+                           const double* xyz, const int32_t* charges, double scc, double rmsd, int32_t max_iter,
+                           uint32_t props, double* energies, double* gradients, int32_t* iterations,
+                           int32_t* converged, char* errmsg, int32_t errcap) {
+  sg_batch* b = nullptr;
+  int32_t rc = sg_batch_create(method, n_mol, n_atoms, Z, xyz, charges, &b);
+  std::string err;
+  if (rc == SG_OK) {
+    rc = sg_batch_set_scf(b, scc, rmsd, max_iter);
+    if (rc == SG_OK) rc = sg_batch_run(b, props);
+    if (rc == SG_OK) rc = sg_batch_results(b, energies, gradients, iterations, converged);
+    err = b->error;
+    sg_batch_destroy(b);
+  } else {
+    err = g_create_error;
+  }
+  if (errmsg && errcap > 0) {
+    std::strncpy(errmsg, err.c_str(), (size_t)errcap - 1);
+    errmsg[errcap - 1] = 0;
+  }
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,445 @@
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <mutex>
+
+#include "nddo_math.cuh"
+#include "params.h"
+
+namespace sgb {
+
+void build_local_term_table(LocalTermTable& tab);
+
+std::string cuda_message(cudaError_t e) { return std::string("CUDA error: ") + cudaGetErrorString(e); }
+
+namespace {
+
+// The local term table lives in __constant__ memory of each device; upload it
+// once per device.
+std::mutex g_terms_mu;
+std::map<int, bool> g_terms_uploaded;
+
+int ensure_terms(cudaStream_t s, std::string& err) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  std::lock_guard<std::mutex> lk(g_terms_mu);
+  if (g_terms_uploaded[dev]) return kOk;
+  static LocalTermTable tab;
+  build_local_term_table(tab);
+  upload_local_terms(tab, s);
+  e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  g_terms_uploaded[dev] = true;
+  return kOk;
+}
+
+size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
+
+}  // namespace
+
+Batch::Batch(Method m) : method_(m) {}
+
+Batch::~Batch() {
+  if (arena_) cudaFree(arena_);
+  if (pinned_) cudaFreeHost(pinned_);
+  if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Batch::ensure_arena(size_t bytes, std::string& err) {
+  if (!stream_) {
+    cudaError_t e = cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+      err = cuda_message(e);
+      return kErrCuda;
+    }
+  }
+  if (bytes <= arena_bytes_) return kOk;
+  if (arena_) {
+    cudaStreamSynchronize(stream_);
+    cudaFree(arena_);
+    arena_ = nullptr;
+    arena_bytes_ = 0;
+  }
+  cudaError_t e = cudaMalloc(&arena_, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    err = "device allocation of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? kErrOutOfMemory : kErrCuda;
+  }
+  arena_bytes_ = bytes;
+  return kOk;
+}
+
+int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
+  mols_.clear();
+  atoms_.clear();
+  pairs_.clear();
+  elems_.clear();
+  ao_atom_.clear();
+  order_.clear();
+  density_given_ = false;
+  if (in.empty()) {
+    err = "empty batch";
+    return kErrEmptyStructure;
+  }
+  // element slots
+  std::map<int, int> slot_of;
+  for (const auto& m : in) {
+    if (m.Z.empty()) {
+      err = "molecule without atoms";
+      return kErrEmptyStructure;
+    }
+    if (m.xyz.size() != 3 * m.Z.size()) {
+      err = "positions must have 3 entries per atom";
+      return kErrInvalidArgument;
+    }
+    for (int z : m.Z) {
+      if (slot_of.count(z)) continue;
+      ElemDev e;
+      std::string why;
+      if (!make_elem(method_, z, e, why)) {
+        err = why;
+        return kErrUnsupportedElement;
+      }
+      if ((int)elems_.size() >= kMaxElementSlots) {
+        err = "more than 16 distinct elements in one batch";
+        return kErrInvalidArgument;
+      }
+      slot_of[z] = (int)elems_.size();
+      elems_.push_back(e);
+    }
+  }
+  diat_.assign(kMaxElementSlots * kMaxElementSlots, DiatomicDev());
+  for (size_t i = 0; i < elems_.size(); ++i)
+    for (size_t j = 0; j < elems_.size(); ++j) {
+      DiatomicDev d = make_diatomic(method_, elems_[i].Z, elems_[j].Z);
+      if (method_ == kPM6 && !d.present) {
+        err = "no PM6 diatomic parameters for the element pair Z=" + std::to_string(elems_[i].Z) + ", Z=" +
+              std::to_string(elems_[j].Z);
+        return kErrUnsupportedElement;
+      }
+      diat_[i * kMaxElementSlots + j] = d;
+    }
+  long long int_off = 0, mat_off = 0, diis_off = 0;
+  int ao_base = 0, max_nao = 0;
+  for (size_t mi = 0; mi < in.size(); ++mi) {
+    const auto& mol = in[mi];
+    MolDev md{};
+    md.nat = (int)mol.Z.size();
+    if (md.nat > kMaxAtomsPerMolecule) {
+      err = "molecule larger than the per-molecule atom limit";
+      return kErrInvalidArgument;
+    }
+    md.atom0 = (int)atoms_.size();
+    md.pair0 = (int)pairs_.size();
+    md.ao_base = ao_base;
+    int nao = 0;
+    double ncore = 0;
+    for (int a = 0; a < md.nat; ++a) {
+      const ElemDev& e = elems_[slot_of[mol.Z[a]]];
+      AtomDev ad{};
+      ad.x = mol.xyz[3 * a];
+      ad.y = mol.xyz[3 * a + 1];
+      ad.z = mol.xyz[3 * a + 2];
+      if (!std::isfinite(ad.x) || !std::isfinite(ad.y) || !std::isfinite(ad.z)) {
+        err = "non-finite position in molecule " + std::to_string(mi);
+        return kErrInvalidArgument;
+      }
+      ad.slot = slot_of[mol.Z[a]];
+      ad.ao0 = nao;
+      ad.mol = (int)mi;
+      atoms_.push_back(ad);
+      for (int k = 0; k < e.nao; ++k) ao_atom_.push_back(md.atom0 + a);
+      nao += e.nao;
+      ncore += e.core;
+    }
+    md.nao = nao;
+    md.nel = (int)std::lround(ncore) - mol.charge;
+    if (md.nel < 0 || (md.nel & 1)) {
+      err = "molecule " + std::to_string(mi) + " has " + std::to_string(md.nel) +
+            " electrons: the restricted closed-shell SCF needs an even, non-negative count";
+      return kErrOddElectrons;
+    }
+    md.nocc = md.nel / 2;
+    if (nao > 1024) {
+      err = "molecule " + std::to_string(mi) + " has more than 1024 AOs (batched SCF limit)";
+      return kErrInvalidArgument;
+    }
+    md.int_off = int_off;
+    for (int a = 0; a < md.nat; ++a)
+      for (int b = a + 1; b < md.nat; ++b) {
+        const int na = elems_[atoms_[md.atom0 + a].slot].nao, nb = elems_[atoms_[md.atom0 + b].slot].nao;
+        PairDev pd{md.atom0 + a, md.atom0 + b, (int)mi, (int)int_off};
+        const double dx = mol.xyz[3 * b] - mol.xyz[3 * a], dy = mol.xyz[3 * b + 1] - mol.xyz[3 * a + 1],
+                     dz = mol.xyz[3 * b + 2] - mol.xyz[3 * a + 2];
+        if (dx * dx + dy * dy + dz * dz < 1e-12) {
+          err = "atoms " + std::to_string(a) + " and " + std::to_string(b) + " of molecule " + std::to_string(mi) +
+                " coincide";
+          return kErrInvalidArgument;
+        }
+        pairs_.push_back(pd);
+        int_off += (na == 1 ? 1 : 10) * (nb == 1 ? 1 : 10);
+        if (int_off > 2000000000LL) {
+          err = "batch too large: more than 2e9 two-centre integrals";
+          return kErrInvalidArgument;
+        }
+      }
+    md.npairs = (int)pairs_.size() - md.pair0;
+    md.mat_off = mat_off;
+    md.diis_off = diis_off;
+    mat_off += (long long)nao * nao;
+    diis_off += 2LL * kDiisMax * nao * nao;
+    ao_base += nao;
+    max_nao = std::max(max_nao, nao);
+    mols_.push_back(md);
+  }
+  order_.resize(mols_.size());
+  for (size_t i = 0; i < order_.size(); ++i) order_[i] = (int)i;
+  std::stable_sort(order_.begin(), order_.end(), [&](int a, int b) { return mols_[a].nao > mols_[b].nao; });
+
+  // arena layout
+  DeviceBatch d;
+  d.method = method_;
+  d.nmol = (int)mols_.size();
+  d.natoms = (int)atoms_.size();
+  d.npairs = (int)pairs_.size();
+  d.nao_total = ao_base;
+  d.mat_total = mat_off;
+  d.diis_total = diis_off;
+  d.int_total = int_off;
+  d.max_nao = max_nao;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off = align_up(off + bytes);
+    return o;
+  };
+  const size_t o_mols = take(sizeof(MolDev) * mols_.size());
+  const size_t o_atoms = take(sizeof(AtomDev) * atoms_.size());
+  const size_t o_pairs = take(sizeof(PairDev) * std::max<size_t>(pairs_.size(), 1));
+  const size_t o_elems = take(sizeof(ElemDev) * elems_.size());
+  const size_t o_diat = take(sizeof(DiatomicDev) * diat_.size());
+  const size_t o_ao = take(sizeof(int) * ao_atom_.size());
+  const size_t o_order = take(sizeof(int) * order_.size());
+  const size_t upload_end = off;
+  const size_t o_counter = take(sizeof(int));
+  const size_t o_ints = take(sizeof(double) * std::max<long long>(int_off, 1));
+  const size_t np = std::max<size_t>(pairs_.size(), 1);
+  const size_t o_vcore = take(sizeof(double) * 20 * np);
+  const size_t o_ovl = take(sizeof(double) * 16 * np);
+  const size_t o_erep = take(sizeof(double) * np);
+  const size_t o_gpair = take(sizeof(double) * 3 * np);
+  const size_t mat_bytes = sizeof(double) * (size_t)mat_off;
+  const size_t o_H = take(mat_bytes), o_P = take(mat_bytes), o_F = take(mat_bytes), o_C = take(mat_bytes);
+  const size_t o_W1 = take(mat_bytes), o_W2 = take(mat_bytes);
+  const size_t o_eps = take(sizeof(double) * (size_t)ao_base);
+  const size_t o_diis = take(sizeof(double) * (size_t)diis_off);
+  const size_t o_grad = take(sizeof(double) * 3 * atoms_.size());
+  const size_t o_res = take(sizeof(MolResult) * mols_.size());
+  int rc = ensure_arena(off, err);
+  if (rc) return rc;
+  rc = ensure_terms(stream_, err);
+  if (rc) return rc;
+  char* base = static_cast<char*>(arena_);
+  d.mols = reinterpret_cast<MolDev*>(base + o_mols);
+  d.atoms = reinterpret_cast<AtomDev*>(base + o_atoms);
+  d.pairs = reinterpret_cast<PairDev*>(base + o_pairs);
+  d.elems = reinterpret_cast<ElemDev*>(base + o_elems);
+  d.diat = reinterpret_cast<DiatomicDev*>(base + o_diat);
+  d.ao_atom = reinterpret_cast<int*>(base + o_ao);
+  d.order = reinterpret_cast<int*>(base + o_order);
+  d.counter = reinterpret_cast<int*>(base + o_counter);
+  d.ints = reinterpret_cast<double*>(base + o_ints);
+  d.vcore = reinterpret_cast<double*>(base + o_vcore);
+  d.ovl = reinterpret_cast<double*>(base + o_ovl);
+  d.erep = reinterpret_cast<double*>(base + o_erep);
+  d.gpair = reinterpret_cast<double*>(base + o_gpair);
+  d.H = reinterpret_cast<double*>(base + o_H);
+  d.P = reinterpret_cast<double*>(base + o_P);
+  d.F = reinterpret_cast<double*>(base + o_F);
+  d.C = reinterpret_cast<double*>(base + o_C);
+  d.W1 = reinterpret_cast<double*>(base + o_W1);
+  d.W2 = reinterpret_cast<double*>(base + o_W2);
+  d.eps = reinterpret_cast<double*>(base + o_eps);
+  d.diis = reinterpret_cast<double*>(base + o_diis);
+  d.grad = reinterpret_cast<double*>(base + o_grad);
+  d.res = reinterpret_cast<MolResult*>(base + o_res);
+  dev_ = d;
+
+  // stage the descriptors in pinned memory and upload them with one copy
+  if (pinned_bytes_ < upload_end) {
+    if (pinned_) cudaFreeHost(pinned_);
+    pinned_ = nullptr;
+    pinned_bytes_ = 0;
+    cudaError_t e = cudaMallocHost(&pinned_, upload_end);
+    if (e != cudaSuccess) {
+      err = cuda_message(e);
+      return kErrCuda;
+    }
+    pinned_bytes_ = upload_end;
+  }
+  cudaStreamSynchronize(stream_);
+  char* h = static_cast<char*>(pinned_);
+  std::memcpy(h + o_mols, mols_.data(), sizeof(MolDev) * mols_.size());
+  std::memcpy(h + o_atoms, atoms_.data(), sizeof(AtomDev) * atoms_.size());
+  if (!pairs_.empty()) std::memcpy(h + o_pairs, pairs_.data(), sizeof(PairDev) * pairs_.size());
+  std::memcpy(h + o_elems, elems_.data(), sizeof(ElemDev) * elems_.size());
+  std::memcpy(h + o_diat, diat_.data(), sizeof(DiatomicDev) * diat_.size());
+  std::memcpy(h + o_ao, ao_atom_.data(), sizeof(int) * ao_atom_.size());
+  std::memcpy(h + o_order, order_.data(), sizeof(int) * order_.size());
+  cudaError_t e = cudaMemcpyAsync(arena_, pinned_, upload_end, cudaMemcpyHostToDevice, stream_);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  e = cudaMemsetAsync(d.res, 0, sizeof(MolResult) * mols_.size(), stream_);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  if (scf_grid_ == 0) scf_grid_ = scf_max_grid(max_nao);
+  return kOk;
+}
+
+int Batch::set_positions(const double* xyz, std::string& err) {
+  if (mols_.empty()) {
+    err = "no structure";
+    return kErrEmptyStructure;
+  }
+  for (size_t a = 0; a < atoms_.size(); ++a) {
+    atoms_[a].x = xyz[3 * a];
+    atoms_[a].y = xyz[3 * a + 1];
+    atoms_[a].z = xyz[3 * a + 2];
+    if (!std::isfinite(atoms_[a].x) || !std::isfinite(atoms_[a].y) || !std::isfinite(atoms_[a].z)) {
+      err = "non-finite position";
+      return kErrInvalidArgument;
+    }
+  }
+  cudaStreamSynchronize(stream_);
+  cudaError_t e = cudaMemcpyAsync(dev_.atoms, atoms_.data(), sizeof(AtomDev) * atoms_.size(), cudaMemcpyHostToDevice,
+                                  stream_);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  return cudaStreamSynchronize(stream_) == cudaSuccess ? kOk : kErrCuda;
+}
+
+int Batch::set_start_density(const double* P, std::string& err) {
+  if (mols_.empty()) {
+    err = "no structure";
+    return kErrEmptyStructure;
+  }
+  cudaError_t e = cudaMemcpyAsync(dev_.P, P, sizeof(double) * (size_t)dev_.mat_total, cudaMemcpyHostToDevice, stream_);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  density_given_ = true;
+  return cudaStreamSynchronize(stream_) == cudaSuccess ? kOk : kErrCuda;
+}
+
+int Batch::run(const ScfParams& sp, bool gradient, std::string& err) {
+  if (mols_.empty()) {
+    err = "no structure";
+    return kErrEmptyStructure;
+  }
+  dev_.use_guess = density_given_ ? 0 : 1;
+  launches_ = 0;
+  launch_pair_values(dev_, stream_);
+  launches_ += dev_.npairs > 0 ? 1 : 0;
+  launch_one_electron(dev_, stream_);
+  launches_ += 1;
+  launch_scf(dev_, sp, scf_grid_, stream_);
+  launches_ += 1;
+  if (gradient) {
+    launch_gradient(dev_, stream_);
+    launches_ += dev_.npairs > 0 ? 2 : 1;
+  }
+  density_given_ = false;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  return kOk;
+}
+
+int Batch::fetch(std::vector<MoleculeOutput>& out, bool gradient, std::string& err) {
+  std::vector<MolResult> r(mols_.size());
+  cudaError_t e = cudaMemcpyAsync(r.data(), dev_.res, sizeof(MolResult) * r.size(), cudaMemcpyDeviceToHost, stream_);
+  std::vector<double> g;
+  if (e == cudaSuccess && gradient) {
+    g.resize(3 * atoms_.size());
+    e = cudaMemcpyAsync(g.data(), dev_.grad, sizeof(double) * g.size(), cudaMemcpyDeviceToHost, stream_);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  out.resize(mols_.size());
+  for (size_t i = 0; i < mols_.size(); ++i) {
+    MoleculeOutput& o = out[i];
+    o.energy = r[i].energy;
+    o.e_el = r[i].e_el;
+    o.e_rep = r[i].e_rep;
+    o.iterations = r[i].iterations;
+    o.converged = r[i].converged;
+    o.status = r[i].status;
+    o.nao = mols_[i].nao;
+    o.nocc = mols_[i].nocc;
+    o.nel = mols_[i].nel;
+    if (gradient)
+      o.gradient.assign(g.begin() + 3 * mols_[i].atom0, g.begin() + 3 * (mols_[i].atom0 + mols_[i].nat));
+    else
+      o.gradient.clear();
+  }
+  return kOk;
+}
+
+int Batch::fetch_density(int mol, std::vector<double>& P, std::string& err) {
+  if (mol < 0 || mol >= (int)mols_.size()) {
+    err = "molecule index out of range";
+    return kErrInvalidArgument;
+  }
+  const MolDev& m = mols_[mol];
+  P.resize((size_t)m.nao * m.nao);
+  cudaError_t e = cudaMemcpyAsync(P.data(), dev_.P + m.mat_off, sizeof(double) * P.size(), cudaMemcpyDeviceToHost,
+                                  stream_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  return kOk;
+}
+
+int Batch::fetch_orbital_energies(int mol, std::vector<double>& eps, std::string& err) {
+  if (mol < 0 || mol >= (int)mols_.size()) {
+    err = "molecule index out of range";
+    return kErrInvalidArgument;
+  }
+  const MolDev& m = mols_[mol];
+  eps.resize(m.nao);
+  cudaError_t e = cudaMemcpyAsync(eps.data(), dev_.eps + m.ao_base, sizeof(double) * m.nao, cudaMemcpyDeviceToHost,
+                                  stream_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  return kOk;
+}
+
+}  // namespace sgb

@@ -1,0 +1,94 @@
+// Host orchestration of batched NDDO single points on one GPU.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "engine_types.h"
+#include "kernels.h"
+
+namespace sgb {
+
+struct MoleculeInput {
+  std::vector<int> Z;
+  std::vector<double> xyz;  // bohr, 3 per atom
+  int charge = 0;
+};
+
+struct MoleculeOutput {
+  double energy = 0, e_el = 0, e_rep = 0;
+  int iterations = 0, converged = 0, status = 0;
+  int nao = 0, nocc = 0, nel = 0;
+  std::vector<double> gradient;  // 3 per atom (Hartree/bohr)
+};
+
+// Status codes shared with the C-ABI (include/sparrow_b200.h).
+enum Status : int {
+  kOk = 0,
+  kErrInvalidArgument = 1,
+  kErrUnknownMethod = 2,
+  kErrUnsupportedElement = 3,
+  kErrEmptyStructure = 4,
+  kErrOddElectrons = 5,
+  kErrNotConverged = 6,
+  kErrCuda = 7,
+  kErrOutOfMemory = 8,
+  kErrNoResults = 9,
+  kErrUnknownSetting = 10,
+  kErrDevice = 11,
+};
+
+// A batch resident on the device: descriptors, integrals, matrices, results.
+class Batch {
+ public:
+  explicit Batch(Method m);
+  ~Batch();
+  Batch(const Batch&) = delete;
+  Batch& operator=(const Batch&) = delete;
+
+  // Host-side setup and upload of a set of molecules.  Returns a Status.
+  int setup(const std::vector<MoleculeInput>& mols, std::string& err);
+  // Replace positions (same atoms, same order) and upload them.
+  int set_positions(const double* xyz_bohr_all, std::string& err);
+  // Optional start densities (one N x N matrix per molecule, concatenated).
+  int set_start_density(const double* P_all, std::string& err);
+  // Run integrals -> SCF -> (gradient) on the device.  Asynchronous on stream().
+  int run(const ScfParams& sp, bool gradient, std::string& err);
+  // Copy results back (synchronises the stream).
+  int fetch(std::vector<MoleculeOutput>& out, bool gradient, std::string& err);
+  int fetch_density(int mol, std::vector<double>& P, std::string& err);
+  int fetch_orbital_energies(int mol, std::vector<double>& eps, std::string& err);
+
+  cudaStream_t stream() const { return stream_; }
+  int n_molecules() const { return (int)mols_.size(); }
+  int n_atoms() const { return (int)atoms_.size(); }
+  long long device_bytes() const { return arena_bytes_; }
+  const DeviceBatch& device() const { return dev_; }
+  // Kernel launches of the last run() (for accounting)
+  int launches_last_run() const { return launches_; }
+
+ private:
+  int ensure_arena(size_t bytes, std::string& err);
+  Method method_;
+  cudaStream_t stream_ = nullptr;
+  void* arena_ = nullptr;
+  size_t arena_bytes_ = 0;
+  void* pinned_ = nullptr;
+  size_t pinned_bytes_ = 0;
+  DeviceBatch dev_;
+  std::vector<MolDev> mols_;
+  std::vector<AtomDev> atoms_;
+  std::vector<PairDev> pairs_;
+  std::vector<ElemDev> elems_;
+  std::vector<DiatomicDev> diat_;
+  std::vector<int> ao_atom_, order_;
+  int scf_grid_ = 0;
+  int launches_ = 0;
+  bool density_given_ = false;
+};
+
+// Human-readable message for a CUDA error, also used by the C-ABI.
+std::string cuda_message(cudaError_t e);
+
+}  // namespace sgb

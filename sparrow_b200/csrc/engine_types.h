@@ -1,0 +1,106 @@
+// Device-visible data layout of the batched NDDO engine.
+//
+// A batch is a set of independent molecules.  Everything lives in one device
+// arena; the structs below are the descriptors the kernels read.  Layout in
+// HBM (all FP64 unless noted):
+//   atoms      AtomDev[n_atoms]            element slot, AO start, position (bohr)
+//   pairs      PairDev[n_pairs]            i<j atom pairs of every molecule, sorted by
+//                                          molecule and by (i, j); int_off indexes the
+//                                          integral pool
+//   integrals  double[int_total]           per pair: dA x dB global 2c2e block
+//                                          (dA, dB in {1, 10}; packed orbital-pair
+//                                          index p(mu<=nu) = nu(nu+1)/2 + mu)
+//   vcore      double[n_pairs][20]         core-attraction vectors VA[10] | VB[10]
+//   overlap    double[n_pairs][16]         STO-6G overlap block S[mu on i][nu on j]
+//   erep       double[n_pairs]             core-core repulsion of the pair
+//   H, P, F, C double[mat_total]           per molecule N x N, row-major, at mat_off
+//   DIIS       double[diis_total]          per molecule 2 * kDiisMax * N * N
+#pragma once
+#include <cstdint>
+
+namespace sgb {
+
+constexpr int kMaxAtomsPerMolecule = 4096;
+constexpr int kDiisMax = 6;          // Pulay subspace size
+constexpr int kMaxElementSlots = 16; // distinct elements in one batch
+
+enum Method : int { kMNDO = 0, kAM1 = 1, kPM6 = 2 };
+
+struct ElemDev {
+  int Z = 0;
+  int nao = 0;
+  double core = 0;     // core charge
+  double cbrtZ = 0;    // Z^(1/3) with Z the atomic number
+  double Uss = 0, Upp = 0, betaS = 0, betaP = 0;
+  double alpha = 0;    // MNDO/AM1 core-repulsion exponent (1/bohr)
+  double rho[4] = {0, 0, 0, 0};  // Klopman radii by multipole class: ss0, sp1, pp0, pp2
+  double D[4] = {0, 0, 0, 0};    // charge separations by class: 0, D_sp1, 0, D_pp2
+  double pcore = 0;
+  double gss = 0, gsp = 0, gpp = 0, gp2 = 0, hsp = 0, hpp = 0;
+  int n_gauss = 0;
+  double ga[4] = {0, 0, 0, 0}, gb[4] = {0, 0, 0, 0}, gc[4] = {0, 0, 0, 0};
+  double s_exp[6], s_coef[6], p_exp[6], p_coef[6];
+};
+
+struct DiatomicDev {
+  double alpha = 0;  // 1/bohr (1/bohr^2 for X-H with X in C, N, O)
+  double x = 0;
+  int present = 0;
+};
+
+struct AtomDev {
+  double x, y, z;
+  int slot;   // element slot
+  int ao0;    // first AO within the molecule
+  int mol;    // molecule index
+  int pad;
+};
+
+struct PairDev {
+  int a, b;      // global atom indices, a < b, same molecule
+  int mol;
+  int int_off;   // offset into the integral pool
+};
+
+struct MolDev {
+  int nat, nao, nocc, nel;
+  int atom0;      // first atom (global index)
+  int pair0;      // first pair (global index)
+  int npairs;
+  int ao_base;    // first AO (global index) in the ao_atom map
+  long long mat_off;   // N*N matrices (H, P, F, C, scratch) at this offset
+  long long diis_off;  // DIIS history
+  long long int_off;   // first integral of the molecule
+};
+
+// Per-molecule result record written by the SCF kernel.
+struct MolResult {
+  double energy;       // E_el + E_rep (Hartree)
+  double e_el;
+  double e_rep;
+  double last_dE;
+  double last_rmsd;
+  int iterations;
+  int converged;       // 1 if both criteria were met
+  int status;          // 0 ok, nonzero = device-side failure code
+  int pad;
+};
+
+struct ScfParams {
+  double scc = 1e-7;   // |Delta E| criterion (Hartree)
+  double rmsd = 1e-5;  // rms(Delta P) criterion
+  int max_iter = 100;
+  int diis_size = kDiisMax;
+  int jacobi_max_sweeps = 30;
+  int pad = 0;
+};
+
+// Device failure codes (MolResult::status)
+enum DeviceStatus : int {
+  kDevOk = 0,
+  kDevJacobiNotConverged = 1,
+  kDevDiisSingular = 2,
+  kDevNonFinite = 3,
+};
+
+}  // namespace sgb

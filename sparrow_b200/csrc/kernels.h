@@ -1,0 +1,50 @@
+// Kernel launch interface of the batched NDDO engine.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "engine_types.h"
+
+namespace sgb {
+
+struct LocalTermTable;
+
+// Device pointers of one batch (all inside one arena).
+struct DeviceBatch {
+  int method = kPM6;
+  int nmol = 0, natoms = 0, npairs = 0;
+  long long nao_total = 0, mat_total = 0, diis_total = 0, int_total = 0;
+  int max_nao = 0;
+  MolDev* mols = nullptr;
+  AtomDev* atoms = nullptr;
+  PairDev* pairs = nullptr;
+  ElemDev* elems = nullptr;
+  DiatomicDev* diat = nullptr;      // [kMaxElementSlots * kMaxElementSlots]
+  int* ao_atom = nullptr;           // [nao_total] global atom of each AO
+  int* order = nullptr;             // molecule processing order (largest first)
+  int* counter = nullptr;           // work counter of the persistent SCF kernel
+  double* ints = nullptr;           // [int_total]
+  double* vcore = nullptr;          // [npairs * 20]
+  double* ovl = nullptr;            // [npairs * 16]
+  double* erep = nullptr;           // [npairs]
+  double* H = nullptr;              // [mat_total]
+  double* P = nullptr;
+  double* F = nullptr;
+  double* C = nullptr;
+  double* W1 = nullptr;
+  double* W2 = nullptr;
+  double* eps = nullptr;            // [nao_total] orbital energies
+  double* diis = nullptr;           // [diis_total]
+  double* gpair = nullptr;          // [npairs * 3]
+  double* grad = nullptr;           // [natoms * 3]
+  MolResult* res = nullptr;         // [nmol]
+  int use_guess = 1;                // 0: P already holds a start density
+};
+
+void upload_local_terms(const LocalTermTable& tab, cudaStream_t stream);
+void launch_pair_values(const DeviceBatch& b, cudaStream_t s);
+void launch_one_electron(const DeviceBatch& b, cudaStream_t s);
+void launch_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s);
+void launch_gradient(const DeviceBatch& b, cudaStream_t s);
+int scf_max_grid(int max_nao);
+
+}  // namespace sgb

@@ -1,0 +1,187 @@
+// Pair kernels: two-centre integrals (values) and the nuclear gradient.
+//
+// One thread per atom pair.  The value kernel writes, per pair, the global
+// two-electron block, both core-attraction vectors, the overlap block and
+// the core-core repulsion (the density-independent part that the reference
+// builds in TwoCenterIntegralContainer::update, OneElectronMatrix::calculate
+// and PM6RepulsionEnergy::calculateRepulsion).  The gradient kernel repeats
+// the pair math in dual numbers and contracts it with the converged density
+// (OneElectronMatrix.cpp:136-229, TwoElectronMatrix.cpp:168-241).
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+#include "nddo_math.cuh"
+
+namespace sgb {
+
+__constant__ LocalTermTable c_local_terms;
+
+void upload_local_terms(const LocalTermTable& tab, cudaStream_t stream) {
+  cudaMemcpyToSymbolAsync(c_local_terms, &tab, sizeof(LocalTermTable), 0, cudaMemcpyHostToDevice, stream);
+}
+
+__global__ void __launch_bounds__(128) k_pair_values(const PairDev* __restrict__ pairs, int npairs,
+                                                      const AtomDev* __restrict__ atoms,
+                                                      const ElemDev* __restrict__ elems,
+                                                      const DiatomicDev* __restrict__ diat, int method,
+                                                      double* __restrict__ ints, double* __restrict__ vcore,
+                                                      double* __restrict__ ovl, double* __restrict__ erep) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npairs) return;
+  const PairDev pr = pairs[p];
+  const AtomDev a = atoms[pr.a], b = atoms[pr.b];
+  const ElemDev& A = elems[a.slot];
+  const ElemDev& B = elems[b.slot];
+  const double X = b.x - a.x, Y = b.y - a.y, Z = b.z - a.z;
+  const int dA = A.nao == 1 ? 1 : 10, dB = B.nao == 1 ? 1 : 10;
+
+  double G[10][10];
+  global_block<double>(c_local_terms, A, B, X, Y, Z, G);
+  double* out = ints + pr.int_off;
+  for (int i = 0; i < dA; ++i)
+    for (int j = 0; j < dB; ++j) out[i * dB + j] = G[i][j];
+
+  double V[10];
+  core_vector<double>(c_local_terms, A, B, X, Y, Z, V);
+  double* vc = vcore + (size_t)p * 20;
+  for (int i = 0; i < 10; ++i) vc[i] = i < dA ? V[i] : 0.0;
+  core_vector<double>(c_local_terms, B, A, -X, -Y, -Z, V);
+  for (int i = 0; i < 10; ++i) vc[10 + i] = i < dB ? V[i] : 0.0;
+
+  double R[3] = {X, Y, Z};
+  double S[4][4];
+  overlap_block<double>(A, B, R, S);
+  double* so = ovl + (size_t)p * 16;
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) so[i * 4 + j] = S[i][j];
+
+  double E, dE;
+  core_repulsion(method, A, B, diat[a.slot * kMaxElementSlots + b.slot], sqrt(X * X + Y * Y + Z * Z), E, dE);
+  erep[p] = E;
+}
+
+// Per pair: dE/dR_AB (R_AB = pos_B - pos_A) at density P.
+__global__ void __launch_bounds__(64) k_pair_gradient(const PairDev* __restrict__ pairs, int npairs,
+                                                       const AtomDev* __restrict__ atoms,
+                                                       const ElemDev* __restrict__ elems,
+                                                       const DiatomicDev* __restrict__ diat,
+                                                       const MolDev* __restrict__ mols, int method,
+                                                       const double* __restrict__ Pall, double* __restrict__ gpair) {
+  int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npairs) return;
+  const PairDev pr = pairs[p];
+  const AtomDev a = atoms[pr.a], b = atoms[pr.b];
+  const ElemDev& A = elems[a.slot];
+  const ElemDev& B = elems[b.slot];
+  const MolDev m = mols[pr.mol];
+  const int N = m.nao;
+  const double* P = Pall + m.mat_off;
+  const int oa = a.ao0, ob = b.ao0;
+  const double Xv = b.x - a.x, Yv = b.y - a.y, Zv = b.z - a.z;
+  const Dual3 X(Xv, 1, 0, 0), Y(Yv, 0, 1, 0), Z(Zv, 0, 0, 1);
+  const int nA = A.nao, nB = B.nao;
+  double g0 = 0, g1 = 0, g2 = 0;
+
+  // two-electron: sum over ordered orbital quadruples of
+  // (mu nu|lam sig)' [P_mn P_ls - 1/2 P_ml P_ns]
+  {
+    Dual3 G[10][10];
+    global_block<Dual3>(c_local_terms, A, B, X, Y, Z, G);
+    for (int mu = 0; mu < nA; ++mu)
+      for (int nu = 0; nu < nA; ++nu)
+        for (int la = 0; la < nB; ++la)
+          for (int si = 0; si < nB; ++si) {
+            double f = P[(oa + mu) * N + oa + nu] * P[(ob + la) * N + ob + si] -
+                       0.5 * P[(oa + mu) * N + ob + la] * P[(oa + nu) * N + ob + si];
+            const Dual3& I = G[pair_index(mu, nu)][pair_index(la, si)];
+            g0 += f * I.dx;
+            g1 += f * I.dy;
+            g2 += f * I.dz;
+          }
+  }
+  // electrons of A attracted by the core of B, and vice versa
+  {
+    Dual3 V[10];
+    core_vector<Dual3>(c_local_terms, A, B, X, Y, Z, V);
+    for (int mu = 0; mu < nA; ++mu)
+      for (int nu = 0; nu < nA; ++nu) {
+        double f = P[(oa + mu) * N + oa + nu];
+        const Dual3& v = V[pair_index(mu, nu)];
+        g0 += f * v.dx;
+        g1 += f * v.dy;
+        g2 += f * v.dz;
+      }
+    const Dual3 Xr(-Xv, -1, 0, 0), Yr(-Yv, 0, -1, 0), Zr(-Zv, 0, 0, -1);
+    core_vector<Dual3>(c_local_terms, B, A, Xr, Yr, Zr, V);
+    for (int mu = 0; mu < nB; ++mu)
+      for (int nu = 0; nu < nB; ++nu) {
+        double f = P[(ob + mu) * N + ob + nu];
+        const Dual3& v = V[pair_index(mu, nu)];
+        g0 += f * v.dx;
+        g1 += f * v.dy;
+        g2 += f * v.dz;
+      }
+  }
+  // resonance integrals 1/2 (beta_mu + beta_nu) S_mn, both triangles
+  {
+    Dual3 R[3] = {X, Y, Z};
+    Dual3 S[4][4];
+    overlap_block<Dual3>(A, B, R, S);
+    for (int mu = 0; mu < nA; ++mu)
+      for (int nu = 0; nu < nB; ++nu) {
+        double f = ((mu == 0 ? A.betaS : A.betaP) + (nu == 0 ? B.betaS : B.betaP)) * P[(oa + mu) * N + ob + nu];
+        g0 += f * S[mu][nu].dx;
+        g1 += f * S[mu][nu].dy;
+        g2 += f * S[mu][nu].dz;
+      }
+  }
+  {
+    double Rabs = sqrt(Xv * Xv + Yv * Yv + Zv * Zv), E, dE;
+    core_repulsion(method, A, B, diat[a.slot * kMaxElementSlots + b.slot], Rabs, E, dE);
+    g0 += dE * Xv / Rabs;
+    g1 += dE * Yv / Rabs;
+    g2 += dE * Zv / Rabs;
+  }
+  gpair[(size_t)p * 3 + 0] = g0;
+  gpair[(size_t)p * 3 + 1] = g1;
+  gpair[(size_t)p * 3 + 2] = g2;
+}
+
+// Atom gradient: sum of the pair gradients (+ for the second atom of a pair,
+// - for the first).  Pairs of a molecule are stored for i<j in row order, so
+// the index of pair (i, j) is i*n - i(i+1)/2 + (j - i - 1).
+__global__ void k_gather_gradient(const MolDev* __restrict__ mols, const AtomDev* __restrict__ atoms, int natoms,
+                                  const double* __restrict__ gpair, double* __restrict__ grad) {
+  int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= natoms) return;
+  const MolDev m = mols[atoms[a].mol];
+  const int n = m.nat, i = a - m.atom0;
+  double g[3] = {0, 0, 0};
+  for (int j = 0; j < n; ++j) {
+    if (j == i) continue;
+    int lo = i < j ? i : j, hi = i < j ? j : i;
+    long long pidx = (long long)m.pair0 + (long long)lo * n - (long long)lo * (lo + 1) / 2 + (hi - lo - 1);
+    double s = (i == hi) ? 1.0 : -1.0;
+    for (int d = 0; d < 3; ++d) g[d] += s * gpair[pidx * 3 + d];
+  }
+  for (int d = 0; d < 3; ++d) grad[(size_t)a * 3 + d] = g[d];
+}
+
+void launch_pair_values(const DeviceBatch& b, cudaStream_t s) {
+  if (b.npairs == 0) return;
+  int th = 128;
+  k_pair_values<<<(b.npairs + th - 1) / th, th, 0, s>>>(b.pairs, b.npairs, b.atoms, b.elems, b.diat, b.method,
+                                                         b.ints, b.vcore, b.ovl, b.erep);
+}
+
+void launch_gradient(const DeviceBatch& b, cudaStream_t s) {
+  if (b.npairs > 0) {
+    int th = 64;
+    k_pair_gradient<<<(b.npairs + th - 1) / th, th, 0, s>>>(b.pairs, b.npairs, b.atoms, b.elems, b.diat, b.mols,
+                                                             b.method, b.P, b.gpair);
+  }
+  int th = 128;
+  k_gather_gradient<<<(b.natoms + th - 1) / th, th, 0, s>>>(b.mols, b.atoms, b.natoms, b.gpair, b.grad);
+}
+
+}  // namespace sgb

@@ -1,0 +1,75 @@
+"""C-ABI library checks that need no GPU: it loads, exports every declared
+entry point, and rejects bad input on the host before touching a device."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import sparrow_b200
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    text = open(os.path.join(ROOT, "include", "sparrow_b200.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:const char\*|int32_t|void\*|void)\s+(sg_\w+)\(", text, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = sparrow_b200.lib()
+    names = _declared_symbols()
+    assert len(names) >= 30
+    for n in names:
+        assert hasattr(L, n), n
+
+
+def test_version_string():
+    assert b"sm_100a" in sparrow_b200.lib().sg_version()
+
+
+def test_unknown_method_is_rejected():
+    with pytest.raises(sparrow_b200.SparrowError) as e:
+        sparrow_b200.get_calculator("HF")
+    assert e.value.code == 2
+
+
+def test_settings_round_trip_and_validation():
+    c = sparrow_b200.get_calculator("AM1")
+    assert c.settings["self_consistence_criterion"] == pytest.approx(1e-7)
+    assert c.settings["density_rmsd_criterion"] == pytest.approx(1e-5)
+    assert c.settings["max_scf_iterations"] == 100
+    c.settings["molecular_charge"] = 1
+    c.settings["density_rmsd_criterion"] = 1e-8
+    assert c.settings["molecular_charge"] == 1
+    assert c.settings["density_rmsd_criterion"] == pytest.approx(1e-8)
+    with pytest.raises(sparrow_b200.SparrowError):
+        c.settings["max_scf_iterations"] = 0
+    with pytest.raises(sparrow_b200.SparrowError):
+        c.settings["scf_mixer"] = "ediis"
+    with pytest.raises(KeyError):
+        c.settings["no_such_key"] = 1
+
+
+def test_empty_structure_and_bad_input_fail_on_host():
+    c = sparrow_b200.get_calculator("PM6")
+    with pytest.raises(sparrow_b200.SparrowError) as e:
+        c.calculate()
+    assert e.value.code == 4
+    with pytest.raises(ValueError):
+        c.set_structure([1, 1], np.zeros((3, 3)))
+    # no results before a calculation
+    L = sparrow_b200.lib()
+    e_out = ctypes.c_double()
+    assert L.sg_get_energy(c._h, ctypes.byref(e_out)) == 9
+
+
+def test_clone_keeps_settings_and_structure():
+    c = sparrow_b200.get_calculator("PM6")
+    c.set_structure([8, 1, 1], np.array([[0, 0, 0], [1.8, 0, 0], [-0.4, 1.7, 0.0]]))
+    c.settings["molecular_charge"] = 0
+    c.settings["self_consistence_criterion"] = 1e-9
+    d = c.clone()
+    assert d.settings["self_consistence_criterion"] == pytest.approx(1e-9)
+    assert np.allclose(d.positions, c.positions)

@@ -1,0 +1,187 @@
+"""Parity of the sm_100a engine (through the C-ABI) with the CPU oracle.
+
+Tolerances: total energy 1e-6 Hartree, gradient 1e-5 Hartree/bohr (the
+contract for this path); integer bookkeeping (AO count, occupied orbitals)
+bit-exact.  The reference's own known-answer vectors are checked through the
+engine as well.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import sparrow_b200
+from sparrow_b200 import geometry
+from tests import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+
+E_TOL = 1e-6
+G_TOL = 1e-5
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "nddo_known_answers.json")))
+
+
+def engine_single(method, Z, x, charge=0, rmsd=1e-8, scc=1e-7, gradients=True, max_iter=200):
+    c = sparrow_b200.get_calculator(method)
+    c.set_structure(Z, x)
+    c.settings["molecular_charge"] = charge
+    c.settings["density_rmsd_criterion"] = rmsd
+    c.settings["self_consistence_criterion"] = scc
+    c.settings["max_scf_iterations"] = max_iter
+    c.set_required_properties(["energy", "gradients"] if gradients else ["energy"])
+    return c, c.calculate()
+
+
+def test_python_binding_h2_through_engine():
+    r = GOLD["python_h2"]
+    _, res = engine_single("PM6", [1, 1], np.array(r["xyz_bohr"]), rmsd=1e-10, scc=1e-10)
+    assert res.successful_calculation
+    assert abs(res.energy - r["energy_hartree"]) < 1e-9
+    assert abs(res.gradients[0, 0] - r["gradient_x_atom0"]) < 1e-9
+    assert abs(res.gradients[1, 0] + r["gradient_x_atom0"]) < 1e-9
+
+
+@pytest.mark.parametrize("method", ["PM6", "AM1"])
+def test_reference_energies_through_engine(method):
+    ev = O.ev_per_hartree()
+    ran = 0
+    for rec in GOLD["methods"][method]:
+        if rec["name"].startswith("DISABLED") or rec["unrestricted"] or rec["charge"]:
+            continue
+        if "electronic_ev" not in rec and "total_ev" not in rec:
+            continue
+        try:
+            Z = [O.SYMBOLS[e] for e in rec["elements"]]
+            if any(O.element_params(method, z)[0] not in (1, 4) for z in Z):
+                continue
+        except RuntimeError:
+            continue
+        x = np.array(rec["xyz_angstrom"]) * O.bohr_per_angstrom()
+        if sum(O.element_params(method, z)[1] for z in Z) % 2:
+            continue
+        _, res = engine_single(method, Z, x, gradients=False)
+        ref = O.scf(method, Z, x, gradient=False)
+        assert abs(res.energy - ref["energy"]) < E_TOL, rec["name"]
+        if "total_ev" in rec:
+            v, tol = rec["total_ev"]
+            assert abs(res.energy * ev - v) < tol, rec["name"]
+        ran += 1
+    assert ran >= 4
+
+
+@pytest.mark.parametrize("method", ["PM6", "AM1", "MNDO"])
+def test_water_cluster_energy_and_gradient(method):
+    Z, xa = geometry.water_cluster(8, seed=4)
+    x = geometry.to_bohr(xa)
+    _, res = engine_single(method, Z, x)
+    ref = O.scf(method, Z, x)
+    assert res.successful_calculation and ref["converged"]
+    assert (res.n_aos, res.n_occupied) == (ref["nao"], ref["nocc"])
+    assert abs(res.energy - ref["energy"]) < E_TOL
+    assert np.max(np.abs(res.gradients - ref["gradient"])) < G_TOL
+
+
+def test_water32_pm6_single_point():
+    # the (H2O)_32 PM6 energy + gradient workload: 96 atoms, 192 AOs, rms dP 1e-8
+    Z, xa = geometry.water_cluster(32, seed=0)
+    x = geometry.to_bohr(xa)
+    _, res = engine_single("PM6", Z, x)
+    ref = O.scf("PM6", Z, x)
+    assert res.n_aos == 192 and res.n_occupied == 128
+    assert abs(res.energy - ref["energy"]) < E_TOL
+    assert np.max(np.abs(res.gradients - ref["gradient"])) < G_TOL
+
+
+@pytest.mark.parametrize("method", ["PM6", "AM1"])
+def test_alkane_batch_matches_oracle(method):
+    mols = geometry.alkane_batch(12, seed=7, n_min=2, n_max=14)
+    mols_b = [(z, geometry.to_bohr(x)) for z, x in mols]
+    b = sparrow_b200.Batch(method, mols_b, rmsd=1e-8)
+    b.run(gradients=True)
+    e, g, it, conv = b.results()
+    assert conv.all()
+    for i, (Z, x) in enumerate(mols_b):
+        ref = O.scf(method, Z, x)
+        assert abs(e[i] - ref["energy"]) < E_TOL, i
+        assert np.max(np.abs(g[i] - ref["gradient"])) < G_TOL, i
+
+
+def test_batch_result_equals_single_result():
+    # every molecule gives the same answer alone and inside a mixed batch
+    mols = geometry.alkane_batch(5, seed=9, n_min=2, n_max=10)
+    Zw, xw = geometry.water_cluster(6, seed=2)
+    mols = [(z, geometry.to_bohr(x)) for z, x in mols] + [(Zw, geometry.to_bohr(xw))]
+    b = sparrow_b200.Batch("PM6", mols, rmsd=1e-9, scc=1e-9)
+    b.run(gradients=True)
+    e, g, _, conv = b.results()
+    assert conv.all()
+    for i, (Z, x) in enumerate(mols):
+        _, res = engine_single("PM6", Z, x, rmsd=1e-9, scc=1e-9)
+        assert abs(res.energy - e[i]) < 1e-8
+        assert np.max(np.abs(res.gradients - g[i])) < 1e-7
+
+
+def test_batch_calculate_from_host_buffers():
+    mols = geometry.alkane_batch(4, seed=5, n_min=3, n_max=8)
+    mols = [(z, geometry.to_bohr(x)) for z, x in mols]
+    e, g, it, conv = sparrow_b200.batch_calculate("AM1", mols, rmsd=1e-8, gradients=True)
+    b = sparrow_b200.Batch("AM1", mols, rmsd=1e-8)
+    b.run(gradients=True)
+    e2, g2, _, _ = b.results()
+    assert np.allclose(e, e2, atol=1e-10, rtol=0)
+    assert conv.all()
+
+
+def test_non_convergence_is_a_flag_not_an_error():
+    Z, xa = geometry.water_cluster(4, seed=1)
+    _, res = engine_single("PM6", Z, geometry.to_bohr(xa), max_iter=2)
+    assert not res.successful_calculation
+    assert res.iterations == 2
+    assert np.isfinite(res.energy)
+
+
+def test_warm_start_from_converged_density():
+    Z, xa = geometry.water_cluster(5, seed=8)
+    x = geometry.to_bohr(xa)
+    c, res = engine_single("PM6", Z, x, rmsd=1e-9, scc=1e-9)
+    P = c.density()
+    c.set_density(P)
+    res2 = c.calculate()
+    assert res2.successful_calculation
+    assert res2.iterations <= 3
+    assert abs(res2.energy - res.energy) < 1e-8
+
+
+def test_host_side_errors():
+    c = sparrow_b200.get_calculator("PM6")
+    c.set_structure([6, 1, 1, 1], np.array([[0, 0, 0], [2, 0, 0], [0, 2, 0], [0, 0, 2.0]]))
+    with pytest.raises(sparrow_b200.SparrowError) as e:
+        c.calculate()
+    assert e.value.code == 5  # odd electron count
+    c.set_structure([17, 17], np.array([[0, 0, 0], [3.8, 0, 0]]))
+    with pytest.raises(sparrow_b200.SparrowError) as e:
+        c.calculate()
+    assert e.value.code == 3  # Cl carries d orbitals in PM6
+    c2 = sparrow_b200.get_calculator("AM1")
+    c2.set_structure([17, 17], np.array([[0, 0, 0], [3.8, 0, 0]]))
+    res = c2.calculate()  # AM1 treats Cl with an s/p basis
+    ref = O.scf("AM1", [17, 17], np.array([[0, 0, 0], [3.8, 0, 0]]), gradient=False, rmsd=1e-5)
+    assert abs(res.energy - ref["energy"]) < E_TOL
+
+
+def test_single_atom_and_positions_update():
+    c, res = engine_single("PM6", [6], np.zeros((1, 3)))
+    ref = O.scf("PM6", [6], np.zeros((1, 3)))
+    assert abs(res.energy - ref["energy"]) < E_TOL
+    assert np.allclose(res.gradients, 0)
+    # modify positions keeps the atoms and recomputes
+    Z, xa = geometry.water_cluster(2, seed=3)
+    x = geometry.to_bohr(xa)
+    c, _ = engine_single("AM1", Z, x)
+    x2 = x.copy()
+    x2[0, 0] += 0.05
+    c.positions = x2
+    r2 = c.calculate()
+    ref2 = O.scf("AM1", Z, x2, rmsd=1e-8)
+    assert abs(r2.energy - ref2["energy"]) < E_TOL
