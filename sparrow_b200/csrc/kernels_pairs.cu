@@ -71,80 +71,13 @@ __global__ void __launch_bounds__(64) k_pair_gradient(const PairDev* __restrict_
   if (p >= npairs) return;
   const PairDev pr = pairs[p];
   const AtomDev a = atoms[pr.a], b = atoms[pr.b];
-  const ElemDev& A = elems[a.slot];
-  const ElemDev& B = elems[b.slot];
   const MolDev m = mols[pr.mol];
-  const int N = m.nao;
-  const double* P = Pall + m.mat_off;
-  const int oa = a.ao0, ob = b.ao0;
-  const double Xv = b.x - a.x, Yv = b.y - a.y, Zv = b.z - a.z;
-  const Dual3 X(Xv, 1, 0, 0), Y(Yv, 0, 1, 0), Z(Zv, 0, 0, 1);
-  const int nA = A.nao, nB = B.nao;
-  double g0 = 0, g1 = 0, g2 = 0;
-
-  // two-electron: sum over ordered orbital quadruples of
-  // (mu nu|lam sig)' [P_mn P_ls - 1/2 P_ml P_ns]
-  {
-    Dual3 G[10][10];
-    global_block<Dual3>(c_local_terms, A, B, X, Y, Z, G);
-    for (int mu = 0; mu < nA; ++mu)
-      for (int nu = 0; nu < nA; ++nu)
-        for (int la = 0; la < nB; ++la)
-          for (int si = 0; si < nB; ++si) {
-            double f = P[(oa + mu) * N + oa + nu] * P[(ob + la) * N + ob + si] -
-                       0.5 * P[(oa + mu) * N + ob + la] * P[(oa + nu) * N + ob + si];
-            const Dual3& I = G[pair_index(mu, nu)][pair_index(la, si)];
-            g0 += f * I.dx;
-            g1 += f * I.dy;
-            g2 += f * I.dz;
-          }
-  }
-  // electrons of A attracted by the core of B, and vice versa
-  {
-    Dual3 V[10];
-    core_vector<Dual3>(c_local_terms, A, B, X, Y, Z, V);
-    for (int mu = 0; mu < nA; ++mu)
-      for (int nu = 0; nu < nA; ++nu) {
-        double f = P[(oa + mu) * N + oa + nu];
-        const Dual3& v = V[pair_index(mu, nu)];
-        g0 += f * v.dx;
-        g1 += f * v.dy;
-        g2 += f * v.dz;
-      }
-    const Dual3 Xr(-Xv, -1, 0, 0), Yr(-Yv, 0, -1, 0), Zr(-Zv, 0, 0, -1);
-    core_vector<Dual3>(c_local_terms, B, A, Xr, Yr, Zr, V);
-    for (int mu = 0; mu < nB; ++mu)
-      for (int nu = 0; nu < nB; ++nu) {
-        double f = P[(ob + mu) * N + ob + nu];
-        const Dual3& v = V[pair_index(mu, nu)];
-        g0 += f * v.dx;
-        g1 += f * v.dy;
-        g2 += f * v.dz;
-      }
-  }
-  // resonance integrals 1/2 (beta_mu + beta_nu) S_mn, both triangles
-  {
-    Dual3 R[3] = {X, Y, Z};
-    Dual3 S[4][4];
-    overlap_block<Dual3>(A, B, R, S);
-    for (int mu = 0; mu < nA; ++mu)
-      for (int nu = 0; nu < nB; ++nu) {
-        double f = ((mu == 0 ? A.betaS : A.betaP) + (nu == 0 ? B.betaS : B.betaP)) * P[(oa + mu) * N + ob + nu];
-        g0 += f * S[mu][nu].dx;
-        g1 += f * S[mu][nu].dy;
-        g2 += f * S[mu][nu].dz;
-      }
-  }
-  {
-    double Rabs = sqrt(Xv * Xv + Yv * Yv + Zv * Zv), E, dE;
-    core_repulsion(method, A, B, diat[a.slot * kMaxElementSlots + b.slot], Rabs, E, dE);
-    g0 += dE * Xv / Rabs;
-    g1 += dE * Yv / Rabs;
-    g2 += dE * Zv / Rabs;
-  }
-  gpair[(size_t)p * 3 + 0] = g0;
-  gpair[(size_t)p * 3 + 1] = g1;
-  gpair[(size_t)p * 3 + 2] = g2;
+  double g[3];
+  pair_gradient(c_local_terms, method, elems[a.slot], elems[b.slot], diat[a.slot * kMaxElementSlots + b.slot],
+                b.x - a.x, b.y - a.y, b.z - a.z, Pall + m.mat_off, m.nao, a.ao0, b.ao0, g);
+  gpair[(size_t)p * 3 + 0] = g[0];
+  gpair[(size_t)p * 3 + 1] = g[1];
+  gpair[(size_t)p * 3 + 2] = g[2];
 }
 
 // Atom gradient: sum of the pair gradients (+ for the second atom of a pair,

@@ -360,4 +360,76 @@ SGB_HD void core_repulsion(int method, const ElemDev& A, const ElemDev& B, const
   }
 }
 
+// dE/dR_AB of one pair (R_AB = pos_B - pos_A) for the symmetric density P
+// (N x N, row-major; the pair's AOs start at oa and ob).  Contributions
+// (OneElectronMatrix.cpp:136-229, TwoElectronMatrix.cpp:168-241, repulsion):
+//   sum over ordered AO quadruples of (mn|ls)' [P_mn P_ls - 1/2 P_ml P_ns]
+//   + sum_mn P_mn V'_mn on both atoms + sum (beta_m + beta_n) P_mn S'_mn + E_rep'
+SGB_HD void pair_gradient(const LocalTermTable& tab, int method, const ElemDev& A, const ElemDev& B,
+                          const DiatomicDev& AB, double Xv, double Yv, double Zv, const double* P, int N, int oa,
+                          int ob, double g[3]) {
+  const Dual3 X(Xv, 1, 0, 0), Y(Yv, 0, 1, 0), Z(Zv, 0, 0, 1);
+  const int nA = A.nao, nB = B.nao;
+  double g0 = 0, g1 = 0, g2 = 0;
+  {
+    Dual3 G[10][10];
+    global_block<Dual3>(tab, A, B, X, Y, Z, G);
+    for (int mu = 0; mu < nA; ++mu)
+      for (int nu = 0; nu < nA; ++nu)
+        for (int la = 0; la < nB; ++la)
+          for (int si = 0; si < nB; ++si) {
+            double f = P[(oa + mu) * N + oa + nu] * P[(ob + la) * N + ob + si] -
+                       0.5 * P[(oa + mu) * N + ob + la] * P[(oa + nu) * N + ob + si];
+            const Dual3& I = G[pair_index(mu, nu)][pair_index(la, si)];
+            g0 += f * I.dx;
+            g1 += f * I.dy;
+            g2 += f * I.dz;
+          }
+  }
+  {
+    Dual3 V[10];
+    core_vector<Dual3>(tab, A, B, X, Y, Z, V);
+    for (int mu = 0; mu < nA; ++mu)
+      for (int nu = 0; nu < nA; ++nu) {
+        double f = P[(oa + mu) * N + oa + nu];
+        const Dual3& v = V[pair_index(mu, nu)];
+        g0 += f * v.dx;
+        g1 += f * v.dy;
+        g2 += f * v.dz;
+      }
+    const Dual3 Xr(-Xv, -1, 0, 0), Yr(-Yv, 0, -1, 0), Zr(-Zv, 0, 0, -1);
+    core_vector<Dual3>(tab, B, A, Xr, Yr, Zr, V);
+    for (int mu = 0; mu < nB; ++mu)
+      for (int nu = 0; nu < nB; ++nu) {
+        double f = P[(ob + mu) * N + ob + nu];
+        const Dual3& v = V[pair_index(mu, nu)];
+        g0 += f * v.dx;
+        g1 += f * v.dy;
+        g2 += f * v.dz;
+      }
+  }
+  {
+    Dual3 R[3] = {X, Y, Z};
+    Dual3 S[4][4];
+    overlap_block<Dual3>(A, B, R, S);
+    for (int mu = 0; mu < nA; ++mu)
+      for (int nu = 0; nu < nB; ++nu) {
+        double f = ((mu == 0 ? A.betaS : A.betaP) + (nu == 0 ? B.betaS : B.betaP)) * P[(oa + mu) * N + ob + nu];
+        g0 += f * S[mu][nu].dx;
+        g1 += f * S[mu][nu].dy;
+        g2 += f * S[mu][nu].dz;
+      }
+  }
+  {
+    double Rabs = sqrt(Xv * Xv + Yv * Yv + Zv * Zv), E, dE;
+    core_repulsion(method, A, B, AB, Rabs, E, dE);
+    g0 += dE * Xv / Rabs;
+    g1 += dE * Yv / Rabs;
+    g2 += dE * Zv / Rabs;
+  }
+  g[0] = g0;
+  g[1] = g1;
+  g[2] = g2;
+}
+
 }  // namespace sgb
