@@ -1,0 +1,359 @@
+"""Benchmark: batched PM6 SCF solves/s on one B200.
+
+Workload: 4096 saturated hydrocarbons C_nH_{2n+2}, n uniform in [2, 30]
+(8-92 atoms, 14-182 AOs), seeded synthetic geometries (numpy PCG64, seed 1),
+PM6, restricted SCF to |dE| < 1e-7 Eh and rms(dP) < 1e-8, FP64, energy and
+nuclear gradient per molecule.  One step = one batched single point
+(integrals -> SCF -> gradient) over all 4096 molecules.
+
+Arms:
+  default            the sm_100a engine through the C-ABI (libsparrow_b200.so)
+  --impl reference   the reference's path restated on the CPU (the oracle,
+                     oracle/liboracle_nddo.so), timed on this machine's cores
+
+Output: one JSON line (rank 0).  `value` is device-timed throughput with the
+inputs resident in HBM; `e2e` is the same metric through sg_batch_calculate
+from host buffers (host setup, H2D copies, kernels, D2H of energies and
+gradients); `roofline` is the dominant kernel (the persistent SCF kernel)
+against the measured FP64 GEMM rate; `cpu_baseline` is the oracle on a
+bounded random sample of the same molecules.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_MOLECULES = 4096
+SEED = 1
+METHOD = "PM6"
+SCC = 1e-7
+RMSD = 1e-8
+MAX_ITER = 100
+CORE_CHARGE = {1: 1, 6: 4, 7: 5, 8: 6}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="sparrow_b200", choices=["sparrow_b200", "reference"])
+    p.add_argument("--molecules", type=int, default=N_MOLECULES)
+    p.add_argument("--method", default=METHOD)
+    p.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the cpu_baseline sample")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def molecules_for(rank, count, seed=SEED):
+    from sparrow_b200 import geometry
+    mols = geometry.alkane_batch(count, seed=seed + 1000 * rank)
+    return [(z, geometry.to_bohr(x)) for z, x in mols]
+
+
+# ----------------------------------------------------------------------------
+# CPU side (the oracle): molecule-parallel over host processes
+# ----------------------------------------------------------------------------
+def _oracle_solve(args):
+    method, Z, x = args
+    from tests import oracle_lib
+    t0 = time.perf_counter()
+    r = oracle_lib.scf(method, Z, x, scc=SCC, rmsd=RMSD, max_iter=MAX_ITER, gradient=True)
+    return time.perf_counter() - t0, r["energy"], r["iterations"]
+
+
+def cpu_rate(method, mols, target_seconds, procs, rng_seed=12345):
+    """Oracle throughput (solves/s) on a random sample sized to ~target_seconds of wall time."""
+    import multiprocessing as mp
+    import numpy as np
+    rng = np.random.default_rng(rng_seed)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        # calibrate on a few molecules
+        calib = [mols[i] for i in rng.choice(len(mols), size=min(procs, 8), replace=False)]
+        res = pool.map(_oracle_solve, [(method, z, x) for z, x in calib])
+        per_mol = sum(r[0] for r in res) / len(res)
+        count = int(max(procs, min(len(mols), target_seconds * procs / max(per_mol, 1e-3))))
+        sample = [mols[i] for i in rng.choice(len(mols), size=count, replace=False)]
+        t0 = time.perf_counter()
+        res = pool.map(_oracle_solve, [(method, z, x) for z, x in sample], chunksize=1)
+        wall = time.perf_counter() - t0
+    return count / wall, count, wall, [r[1] for r in res]
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# ----------------------------------------------------------------------------
+# roofline bookkeeping (algorithmic FLOPs per SCF iteration)
+# ----------------------------------------------------------------------------
+def scf_flops(mols, iterations, diis=6):
+    """F_eig = 4N^3, F_dens = 2 N^2 n_occ, F_G = 12 nnz(2c2e) + 256 heavy atoms,
+    F_DIIS = 2N^3 + m^2 N^2, per iteration, summed over molecules."""
+    total = 0.0
+    for (Z, _), it in zip(mols, iterations):
+        heavy = int((Z > 1).sum())
+        light = len(Z) - heavy
+        N = 4 * heavy + light
+        nocc = sum(CORE_CHARGE[int(z)] for z in Z) // 2
+        nnz = 100 * heavy * (heavy - 1) // 2 + 10 * heavy * light + light * (light - 1) // 2
+        per = 4 * N ** 3 + 2 * N * N * nocc + 12 * nnz + 256 * heavy + 2 * N ** 3 + diis * diis * N * N
+        total += per * int(it)
+    return total
+
+
+def fp64_gemm_peak():
+    """cuBLAS FP64 GEMM rate (TFLOP/s) measured here: the FP64 roofline denominator."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self):
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "bench_clocks.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self, gpu_index=0):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                if int(parts[0]) != gpu_index:
+                    continue
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_traffic():
+    """Per-launch DRAM bytes of the SCF kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "scf_kernel_ncu.json")
+    try:
+        return json.load(open(path))
+    except Exception:
+        return None
+
+
+# ----------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    mols = molecules_for(0, args.molecules)
+    procs = host_cores()
+    rates = []
+    for step in range(args.warmup + args.steps):
+        rate, count, wall, _ = cpu_rate(args.method, mols, max(3.0, args.cpu_seconds / 2), procs,
+                                        rng_seed=777 + step)
+        if step >= args.warmup:
+            rates.append((rate, count, wall))
+    value = sum(r[0] for r in rates) / len(rates)
+    sample = "%d-%d random molecules of the %d-alkane batch per step, oracle (C++ FP64 restatement), " \
+             "molecule-parallel over %d processes" % (min(r[1] for r in rates), max(r[1] for r in rates),
+                                                       args.molecules, procs)
+    line = {
+        "impl": "reference", "metric": "%s SCF solves/s (energy+gradient)" % args.method, "value": value,
+        "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(r[2] for r in rates) / len(rates), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, no dataset)",
+        "config": {"workload": "%d alkanes C_nH_2n+2, n~U[2,30], %s, rms dP 1e-8" % (args.molecules, args.method),
+                   "molecules": args.molecules, "method": args.method, "parallelism": "cpu processes"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": procs, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_engine(args, rank, world):
+    import numpy as np
+    import sparrow_b200
+
+    mols = molecules_for(rank, args.molecules)
+    # CPU baseline first: its process pool must start before this process touches the GPU
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        procs = host_cores()
+        rate, count, wall, _ = cpu_rate(args.method, mols, args.cpu_seconds, procs)
+        cpu = {"value": rate, "unit": "solves/s", "cores": procs, "kind": "port",
+               "sample": "%d random molecules of the batch, oracle (C++ FP64 restatement of the reference path), "
+                         "molecule-parallel over %d processes, %.1f s wall" % (count, procs, wall)}
+
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as td
+        td.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                              timeout=__import__("datetime").timedelta(seconds=300))
+        dist = td
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    peak = None
+    if rank == 0:
+        try:
+            peak = fp64_gemm_peak()
+        except Exception:
+            peak = None
+
+    b = sparrow_b200.Batch(args.method, mols, scc=SCC, rmsd=RMSD, max_iter=MAX_ITER)
+    for _ in range(args.warmup):
+        b.run(gradients=True)
+        e, g, it, conv = b.results()
+    stage_sum = np.zeros(4)
+    clocks = ClockSampler()
+    barrier()
+    clocks.start()
+    b.record_event(0)
+    for _ in range(args.steps):
+        b.run(gradients=True)
+        e, g, it, conv = b.results()
+        stage_sum += b.stage_times()
+    b.record_event(1)
+    dev_ms = b.elapsed_ms(0, 1)
+    clk = clocks.stop()
+    barrier()
+    dev_ms = max_over_ranks(dev_ms)
+    launches = b.launches * args.steps
+    n_total = args.molecules * world
+    value = n_total * args.steps / (dev_ms / 1e3)
+    not_conv = int((~conv).sum())
+
+    # end to end from host buffers through the public batch call
+    t_e2e = []
+    h2d = d2h = 0
+    for step in range(args.steps + 1):
+        barrier()
+        t0 = time.perf_counter()
+        e2, g2, it2, conv2 = sparrow_b200.batch_calculate(args.method, mols, scc=SCC, rmsd=RMSD, max_iter=MAX_ITER,
+                                                          gradients=True)
+        dt = time.perf_counter() - t0
+        if step > 0:
+            t_e2e.append(dt)
+    t_e2e_max = max_over_ranks(sum(t_e2e))
+    e2e_value = n_total * args.steps / t_e2e_max
+    hb, db = b.transfer_bytes()
+    b_bytes = sum(8 * 20 * (4 * int((z > 1).sum()) + int((z == 1).sum())) ** 2 for z, _ in mols)
+    n_atoms_total = int(sum(len(z) for z, _ in mols))
+    # inputs of one step: the setup upload measured by the batch; results: energies + gradients
+    h2d = hb
+    d2h = 8 * args.molecules + 8 * 3 * n_atoms_total + 40 * args.molecules
+
+    # roofline of the SCF kernel (average launch)
+    scf_ms = stage_sum[2] / args.steps
+    flops = scf_flops(mols, it)
+    achieved = flops / (scf_ms / 1e3) / 1e12
+    traffic = load_traffic()
+    roof = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": (achieved / peak) if peak else None,
+            "traffic": traffic.get("dram_bytes_per_launch") if traffic else None,
+            "kernel": "k_scf (persistent SCF: Fock build, DIIS, Jacobi eigensolver, density)",
+            "peak_source": "FP64 cuBLAS GEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP64 entry)",
+            "algorithmic_flops_per_launch": flops,
+            "stage_ms": {"pair_integrals": stage_sum[0] / args.steps, "one_electron": stage_sum[1] / args.steps,
+                         "scf": scf_ms, "gradient": stage_sum[3] / args.steps}}
+    line = {
+        "metric": "%s SCF solves/s (energy+gradient)" % args.method, "value": value, "unit": "solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, no dataset)",
+        "config": {"workload": "%d alkanes C_nH_2n+2, n~U[2,30] per GPU, %s energy+gradient, rms dP 1e-8" % (
+            args.molecules, args.method), "molecules_per_gpu": args.molecules, "method": args.method,
+                   "parallelism": "replicas x%d (molecules sharded, no collective)" % world,
+                   "l2": "inputs larger than L2: the batch's integrals and matrices occupy ~%.1f GB" % (
+                       b_bytes / 1e9),
+                   "mean_scf_iterations": float(np.mean(it)), "not_converged": not_conv},
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and "CUDA_VISIBLE_DEVICES" not in os.environ:
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_engine(args, rank, world)
+
+
+if __name__ == "__main__":
+    main()

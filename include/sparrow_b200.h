@@ -111,8 +111,18 @@ int32_t sg_batch_run(sg_batch* b, uint32_t properties);
 int32_t sg_batch_results(sg_batch* b, double* energies, double* gradients, int32_t* iterations, int32_t* converged);
 /* number of device kernel launches issued by the last sg_batch_run */
 int32_t sg_batch_launches(const sg_batch* b);
-/* CUDA stream (cudaStream_t) the batch runs on, for event timing */
+/* CUDA stream (cudaStream_t) the batch runs on */
 void* sg_batch_stream(const sg_batch* b);
+/* device milliseconds of the stages of the last run: pair integrals,
+ * one-electron assembly, SCF, gradient (waits for the run to finish) */
+int32_t sg_batch_stage_times(sg_batch* b, double* ms4);
+/* timing events on the batch stream: record in slot 0..7, elapsed s0 -> s1 */
+int32_t sg_batch_record_event(sg_batch* b, int32_t slot);
+int32_t sg_batch_event_elapsed(sg_batch* b, int32_t slot0, int32_t slot1, double* ms);
+/* bytes copied host->device and device->host by this batch so far */
+int32_t sg_batch_transfer_bytes(const sg_batch* b, int64_t* h2d, int64_t* d2h);
+/* free device and pinned host memory cached from destroyed batches */
+void sg_release_cached_memory(void);
 
 /* one call from host buffers to host results (create, run, fetch, destroy) */
 int32_t sg_batch_calculate(const char* method, int32_t n_molecules, const int32_t* n_atoms,

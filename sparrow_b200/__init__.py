@@ -82,6 +82,12 @@ def lib():
         "sg_batch_results": (ctypes.c_int32, [_VP, _D, _D, _I32, _I32]),
         "sg_batch_launches": (ctypes.c_int32, [_VP]),
         "sg_batch_stream": (_VP, [_VP]),
+        "sg_batch_stage_times": (ctypes.c_int32, [_VP, _D]),
+        "sg_batch_record_event": (ctypes.c_int32, [_VP, ctypes.c_int32]),
+        "sg_batch_event_elapsed": (ctypes.c_int32, [_VP, ctypes.c_int32, ctypes.c_int32, _D]),
+        "sg_batch_transfer_bytes": (ctypes.c_int32, [_VP, ctypes.POINTER(ctypes.c_int64),
+                                                     ctypes.POINTER(ctypes.c_int64)]),
+        "sg_release_cached_memory": (None, []),
         "sg_batch_calculate": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _I32, _D, _I32,
                                                 ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_uint32,
                                                 _D, _D, _I32, _I32, ctypes.c_char_p, ctypes.c_int32]),
@@ -332,6 +338,25 @@ class Batch:
     @property
     def launches(self):
         return lib().sg_batch_launches(self._h)
+
+    def stage_times(self):
+        """Device ms of the last run: pair integrals, one-electron, SCF, gradient."""
+        ms = np.zeros(4)
+        self._check(lib().sg_batch_stage_times(self._h, _dptr(ms)))
+        return ms
+
+    def record_event(self, slot):
+        self._check(lib().sg_batch_record_event(self._h, slot))
+
+    def elapsed_ms(self, s0, s1):
+        v = ctypes.c_double()
+        self._check(lib().sg_batch_event_elapsed(self._h, s0, s1, ctypes.byref(v)))
+        return v.value
+
+    def transfer_bytes(self):
+        h, d = ctypes.c_int64(), ctypes.c_int64()
+        self._check(lib().sg_batch_transfer_bytes(self._h, ctypes.byref(h), ctypes.byref(d)))
+        return h.value, d.value
 
     @property
     def stream(self):

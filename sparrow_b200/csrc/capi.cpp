@@ -459,6 +459,30 @@ int32_t sg_batch_launches(const sg_batch* b) { return b ? b->impl->launches_last
 
 void* sg_batch_stream(const sg_batch* b) { return b ? (void*)b->impl->stream() : nullptr; }
 
+int32_t sg_batch_stage_times(sg_batch* b, double* ms4) {
+  if (!b || !ms4) return SG_ERR_INVALID_ARGUMENT;
+  return b->impl->stage_times(ms4, b->error);
+}
+
+int32_t sg_batch_record_event(sg_batch* b, int32_t slot) {
+  if (!b) return SG_ERR_INVALID_ARGUMENT;
+  return b->impl->record_event(slot, b->error);
+}
+
+int32_t sg_batch_event_elapsed(sg_batch* b, int32_t s0, int32_t s1, double* ms) {
+  if (!b || !ms) return SG_ERR_INVALID_ARGUMENT;
+  return b->impl->event_elapsed(s0, s1, ms, b->error);
+}
+
+int32_t sg_batch_transfer_bytes(const sg_batch* b, int64_t* h2d, int64_t* d2h) {
+  if (!b) return SG_ERR_INVALID_ARGUMENT;
+  if (h2d) *h2d = b->impl->h2d_bytes();
+  if (d2h) *d2h = b->impl->d2h_bytes();
+  return SG_OK;
+}
+
+void sg_release_cached_memory(void) { release_cached_memory(); }
+
 int32_t sg_batch_calculate(const char* method, int32_t n_mol, const int32_t* n_atoms, const int32_t* Z,
                            const double* xyz, const int32_t* charges, double scc, double rmsd, int32_t max_iter,
                            uint32_t props, double* energies, double* gradients, int32_t* iterations,

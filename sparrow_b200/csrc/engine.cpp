@@ -45,13 +45,62 @@ int ensure_terms(cudaStream_t s, std::string& err) {
 
 size_t align_up(size_t x, size_t a = 256) { return (x + a - 1) / a * a; }
 
+struct CachedBlock {
+  int device;
+  void* ptr;
+  size_t bytes;
+  bool pinned;
+};
+std::mutex g_pool_mu;
+std::vector<CachedBlock> g_pool;
+
+// Take the smallest cached block of the kind that fits, or nullptr.
+void* pool_take(bool pinned, size_t bytes, size_t* got) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  int best = -1;
+  for (size_t i = 0; i < g_pool.size(); ++i) {
+    const auto& b = g_pool[i];
+    if (b.pinned != pinned || (!pinned && b.device != dev) || b.bytes < bytes) continue;
+    if (best < 0 || b.bytes < g_pool[best].bytes) best = (int)i;
+  }
+  if (best < 0) return nullptr;
+  void* p = g_pool[best].ptr;
+  *got = g_pool[best].bytes;
+  g_pool.erase(g_pool.begin() + best);
+  return p;
+}
+
+void pool_give(bool pinned, void* ptr, size_t bytes) {
+  if (!ptr) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  g_pool.push_back({dev, ptr, bytes, pinned});
+}
+
 }  // namespace
+
+void release_cached_memory() {
+  std::lock_guard<std::mutex> lk(g_pool_mu);
+  for (auto& b : g_pool) {
+    if (b.pinned) cudaFreeHost(b.ptr);
+    else cudaFree(b.ptr);
+  }
+  g_pool.clear();
+}
 
 Batch::Batch(Method m) : method_(m) {}
 
 Batch::~Batch() {
-  if (arena_) cudaFree(arena_);
-  if (pinned_) cudaFreeHost(pinned_);
+  if (stream_) cudaStreamSynchronize(stream_);
+  pool_give(false, arena_, arena_bytes_);
+  pool_give(true, pinned_, pinned_bytes_);
+  for (auto& e : stage_ev_)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : user_ev_)
+    if (e) cudaEventDestroy(e);
   if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -66,11 +115,23 @@ int Batch::ensure_arena(size_t bytes, std::string& err) {
   if (bytes <= arena_bytes_) return kOk;
   if (arena_) {
     cudaStreamSynchronize(stream_);
-    cudaFree(arena_);
+    pool_give(false, arena_, arena_bytes_);
     arena_ = nullptr;
     arena_bytes_ = 0;
   }
+  size_t got = 0;
+  if (void* p = pool_take(false, bytes, &got)) {
+    arena_ = p;
+    arena_bytes_ = got;
+    return kOk;
+  }
   cudaError_t e = cudaMalloc(&arena_, bytes);
+  if (e == cudaErrorMemoryAllocation) {
+    // free cached blocks and retry once
+    cudaGetLastError();
+    release_cached_memory();
+    e = cudaMalloc(&arena_, bytes);
+  }
   if (e != cudaSuccess) {
     cudaGetLastError();
     err = "device allocation of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e);
@@ -278,15 +339,21 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
 
   // stage the descriptors in pinned memory and upload them with one copy
   if (pinned_bytes_ < upload_end) {
-    if (pinned_) cudaFreeHost(pinned_);
+    pool_give(true, pinned_, pinned_bytes_);
     pinned_ = nullptr;
     pinned_bytes_ = 0;
-    cudaError_t e = cudaMallocHost(&pinned_, upload_end);
-    if (e != cudaSuccess) {
-      err = cuda_message(e);
-      return kErrCuda;
+    size_t got = 0;
+    if (void* p = pool_take(true, upload_end, &got)) {
+      pinned_ = p;
+      pinned_bytes_ = got;
+    } else {
+      cudaError_t e = cudaMallocHost(&pinned_, upload_end);
+      if (e != cudaSuccess) {
+        err = cuda_message(e);
+        return kErrCuda;
+      }
+      pinned_bytes_ = upload_end;
     }
-    pinned_bytes_ = upload_end;
   }
   cudaStreamSynchronize(stream_);
   char* h = static_cast<char*>(pinned_);
@@ -302,6 +369,8 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
     err = cuda_message(e);
     return kErrCuda;
   }
+  h2d_bytes_ = (long long)upload_end;
+  d2h_bytes_ = 0;
   e = cudaMemsetAsync(d.res, 0, sizeof(MolResult) * mols_.size(), stream_);
   if (e != cudaSuccess) {
     err = cuda_message(e);
@@ -328,6 +397,7 @@ int Batch::set_positions(const double* xyz, std::string& err) {
   cudaStreamSynchronize(stream_);
   cudaError_t e = cudaMemcpyAsync(dev_.atoms, atoms_.data(), sizeof(AtomDev) * atoms_.size(), cudaMemcpyHostToDevice,
                                   stream_);
+  h2d_bytes_ += (long long)(sizeof(AtomDev) * atoms_.size());
   if (e != cudaSuccess) {
     err = cuda_message(e);
     return kErrCuda;
@@ -355,17 +425,25 @@ int Batch::run(const ScfParams& sp, bool gradient, std::string& err) {
     return kErrEmptyStructure;
   }
   dev_.use_guess = density_given_ ? 0 : 1;
+  for (auto& ev : stage_ev_)
+    if (!ev) cudaEventCreate(&ev);
   launches_ = 0;
+  cudaEventRecord(stage_ev_[0], stream_);
   launch_pair_values(dev_, stream_);
   launches_ += dev_.npairs > 0 ? 1 : 0;
+  cudaEventRecord(stage_ev_[1], stream_);
   launch_one_electron(dev_, stream_);
   launches_ += 1;
+  cudaEventRecord(stage_ev_[2], stream_);
   launch_scf(dev_, sp, scf_grid_, stream_);
   launches_ += 1;
+  cudaEventRecord(stage_ev_[3], stream_);
   if (gradient) {
     launch_gradient(dev_, stream_);
     launches_ += dev_.npairs > 0 ? 2 : 1;
   }
+  cudaEventRecord(stage_ev_[4], stream_);
+  stages_recorded_ = true;
   density_given_ = false;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -388,6 +466,7 @@ int Batch::fetch(std::vector<MoleculeOutput>& out, bool gradient, std::string& e
     err = cuda_message(e);
     return kErrCuda;
   }
+  d2h_bytes_ += (long long)(sizeof(MolResult) * r.size() + sizeof(double) * g.size());
   out.resize(mols_.size());
   for (size_t i = 0; i < mols_.size(); ++i) {
     MoleculeOutput& o = out[i];
@@ -439,6 +518,54 @@ int Batch::fetch_orbital_energies(int mol, std::vector<double>& eps, std::string
     err = cuda_message(e);
     return kErrCuda;
   }
+  return kOk;
+}
+
+int Batch::stage_times(double ms[4], std::string& err) {
+  if (!stages_recorded_) {
+    err = "no run recorded";
+    return kErrNoResults;
+  }
+  cudaError_t e = cudaEventSynchronize(stage_ev_[4]);
+  for (int i = 0; i < 4 && e == cudaSuccess; ++i) {
+    float t = 0;
+    e = cudaEventElapsedTime(&t, stage_ev_[i], stage_ev_[i + 1]);
+    ms[i] = t;
+  }
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  return kOk;
+}
+
+int Batch::record_event(int slot, std::string& err) {
+  if (slot < 0 || slot >= 8 || !stream_) {
+    err = "bad event slot or no stream";
+    return kErrInvalidArgument;
+  }
+  if (!user_ev_[slot]) cudaEventCreate(&user_ev_[slot]);
+  cudaError_t e = cudaEventRecord(user_ev_[slot], stream_);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  return kOk;
+}
+
+int Batch::event_elapsed(int s0, int s1, double* ms, std::string& err) {
+  if (s0 < 0 || s0 >= 8 || s1 < 0 || s1 >= 8 || !user_ev_[s0] || !user_ev_[s1]) {
+    err = "event not recorded";
+    return kErrInvalidArgument;
+  }
+  cudaError_t e = cudaEventSynchronize(user_ev_[s1]);
+  float t = 0;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&t, user_ev_[s0], user_ev_[s1]);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  *ms = t;
   return kOk;
 }
 

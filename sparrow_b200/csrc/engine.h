@@ -67,6 +67,15 @@ class Batch {
   const DeviceBatch& device() const { return dev_; }
   // Kernel launches of the last run() (for accounting)
   int launches_last_run() const { return launches_; }
+  // Device time (ms) of the stages of the last run(): pair integrals,
+  // one-electron assembly, SCF, gradient.  Synchronises on the last event.
+  int stage_times(double ms[4], std::string& err);
+  // Bytes copied host->device and device->host since the batch was set up.
+  long long h2d_bytes() const { return h2d_bytes_; }
+  long long d2h_bytes() const { return d2h_bytes_; }
+  // User timing events on the batch stream (slots 0..7).
+  int record_event(int slot, std::string& err);
+  int event_elapsed(int s0, int s1, double* ms, std::string& err);
 
  private:
   int ensure_arena(size_t bytes, std::string& err);
@@ -86,7 +95,15 @@ class Batch {
   int scf_grid_ = 0;
   int launches_ = 0;
   bool density_given_ = false;
+  long long h2d_bytes_ = 0, d2h_bytes_ = 0;
+  cudaEvent_t stage_ev_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t user_ev_[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  bool stages_recorded_ = false;
 };
+
+// Device arenas and pinned staging buffers are cached per device after a
+// batch is destroyed, so repeated batches do not pay cudaMalloc/cudaFree.
+void release_cached_memory();
 
 // Human-readable message for a CUDA error, also used by the C-ABI.
 std::string cuda_message(cudaError_t e);
