@@ -119,6 +119,11 @@ int32_t sg_batch_stage_times(sg_batch* b, double* ms4);
 /* timing events on the batch stream: record in slot 0..7, elapsed s0 -> s1 */
 int32_t sg_batch_record_event(sg_batch* b, int32_t slot);
 int32_t sg_batch_event_elapsed(sg_batch* b, int32_t slot0, int32_t slot1, double* ms);
+/* per-molecule SCF diagnostics of the last run: full diagonalisations,
+ * Jacobi sweeps, and SM cycles spent in the Fock build, DIIS, occupied-virtual
+ * rotation, full diagonalisation and density phases (5 per molecule);
+ * any pointer may be NULL */
+int32_t sg_batch_scf_stats(sg_batch* b, int32_t* full_diagonalisations, int32_t* jacobi_sweeps, int64_t* cycles5);
 /* bytes copied host->device and device->host by this batch so far */
 int32_t sg_batch_transfer_bytes(const sg_batch* b, int64_t* h2d, int64_t* d2h);
 /* free device and pinned host memory cached from destroyed batches */

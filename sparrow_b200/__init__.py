@@ -88,6 +88,7 @@ def lib():
         "sg_batch_transfer_bytes": (ctypes.c_int32, [_VP, ctypes.POINTER(ctypes.c_int64),
                                                      ctypes.POINTER(ctypes.c_int64)]),
         "sg_release_cached_memory": (None, []),
+        "sg_batch_scf_stats": (ctypes.c_int32, [_VP, _I32, _I32, ctypes.POINTER(ctypes.c_int64)]),
         "sg_batch_calculate": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _I32, _D, _I32,
                                                 ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_uint32,
                                                 _D, _D, _I32, _I32, ctypes.c_char_p, ctypes.c_int32]),
@@ -352,6 +353,17 @@ class Batch:
         v = ctypes.c_double()
         self._check(lib().sg_batch_event_elapsed(self._h, s0, s1, ctypes.byref(v)))
         return v.value
+
+    def scf_stats(self):
+        """Per molecule: full diagonalisations, Jacobi sweeps, SM cycles per SCF phase
+        (Fock build, DIIS, occupied-virtual rotation, full diagonalisation, density)."""
+        n = self.n_molecules
+        nf = np.zeros(n, dtype=np.int32)
+        sw = np.zeros(n, dtype=np.int32)
+        cyc = np.zeros(5 * n, dtype=np.int64)
+        self._check(lib().sg_batch_scf_stats(self._h, _iptr(nf), _iptr(sw),
+                                              cyc.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        return nf, sw, cyc.reshape(n, 5)
 
     def transfer_bytes(self):
         h, d = ctypes.c_int64(), ctypes.c_int64()

@@ -474,6 +474,20 @@ int32_t sg_batch_event_elapsed(sg_batch* b, int32_t s0, int32_t s1, double* ms) 
   return b->impl->event_elapsed(s0, s1, ms, b->error);
 }
 
+int32_t sg_batch_scf_stats(sg_batch* b, int32_t* nfull, int32_t* sweeps, int64_t* cycles5) {
+  if (!b) return SG_ERR_INVALID_ARGUMENT;
+  std::vector<MolResult> r;
+  int rc = b->impl->fetch_raw_results(r, b->error);
+  if (rc) return rc;
+  for (size_t i = 0; i < r.size(); ++i) {
+    if (nfull) nfull[i] = r[i].full_diag;
+    if (sweeps) sweeps[i] = r[i].jacobi_sweeps;
+    if (cycles5)
+      for (int k = 0; k < 5; ++k) cycles5[5 * i + k] = r[i].cycles[k];
+  }
+  return SG_OK;
+}
+
 int32_t sg_batch_transfer_bytes(const sg_batch* b, int64_t* h2d, int64_t* d2h) {
   if (!b) return SG_ERR_INVALID_ARGUMENT;
   if (h2d) *h2d = b->impl->h2d_bytes();

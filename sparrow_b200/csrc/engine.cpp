@@ -148,6 +148,7 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
   elems_.clear();
   ao_atom_.clear();
   order_.clear();
+  hh_pairs_.clear();
   density_given_ = false;
   if (in.empty()) {
     err = "empty batch";
@@ -256,6 +257,11 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
         }
       }
     md.npairs = (int)pairs_.size() - md.pair0;
+    md.hh0 = (int)hh_pairs_.size();
+    for (int k = md.pair0; k < md.pair0 + md.npairs; ++k)
+      if (elems_[atoms_[pairs_[k].a].slot].nao == 4 && elems_[atoms_[pairs_[k].b].slot].nao == 4)
+        hh_pairs_.push_back(k);
+    md.nhh = (int)hh_pairs_.size() - md.hh0;
     md.mat_off = mat_off;
     md.diis_off = diis_off;
     mat_off += (long long)nao * nao;
@@ -292,11 +298,13 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
   const size_t o_diat = take(sizeof(DiatomicDev) * diat_.size());
   const size_t o_ao = take(sizeof(int) * ao_atom_.size());
   const size_t o_order = take(sizeof(int) * order_.size());
+  const size_t o_hh = take(sizeof(int) * std::max<size_t>(hh_pairs_.size(), 1));
   const size_t upload_end = off;
   const size_t o_counter = take(sizeof(int));
   const size_t o_ints = take(sizeof(double) * std::max<long long>(int_off, 1));
   const size_t np = std::max<size_t>(pairs_.size(), 1);
   const size_t o_vcore = take(sizeof(double) * 20 * np);
+  const size_t o_jbuf = take(sizeof(double) * 20 * np);
   const size_t o_ovl = take(sizeof(double) * 16 * np);
   const size_t o_erep = take(sizeof(double) * np);
   const size_t o_gpair = take(sizeof(double) * 3 * np);
@@ -322,6 +330,8 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
   d.counter = reinterpret_cast<int*>(base + o_counter);
   d.ints = reinterpret_cast<double*>(base + o_ints);
   d.vcore = reinterpret_cast<double*>(base + o_vcore);
+  d.jbuf = reinterpret_cast<double*>(base + o_jbuf);
+  d.hh_pairs = reinterpret_cast<int*>(base + o_hh);
   d.ovl = reinterpret_cast<double*>(base + o_ovl);
   d.erep = reinterpret_cast<double*>(base + o_erep);
   d.gpair = reinterpret_cast<double*>(base + o_gpair);
@@ -364,6 +374,7 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
   std::memcpy(h + o_diat, diat_.data(), sizeof(DiatomicDev) * diat_.size());
   std::memcpy(h + o_ao, ao_atom_.data(), sizeof(int) * ao_atom_.size());
   std::memcpy(h + o_order, order_.data(), sizeof(int) * order_.size());
+  if (!hh_pairs_.empty()) std::memcpy(h + o_hh, hh_pairs_.data(), sizeof(int) * hh_pairs_.size());
   cudaError_t e = cudaMemcpyAsync(arena_, pinned_, upload_end, cudaMemcpyHostToDevice, stream_);
   if (e != cudaSuccess) {
     err = cuda_message(e);
@@ -483,6 +494,17 @@ int Batch::fetch(std::vector<MoleculeOutput>& out, bool gradient, std::string& e
       o.gradient.assign(g.begin() + 3 * mols_[i].atom0, g.begin() + 3 * (mols_[i].atom0 + mols_[i].nat));
     else
       o.gradient.clear();
+  }
+  return kOk;
+}
+
+int Batch::fetch_raw_results(std::vector<MolResult>& r, std::string& err) {
+  r.resize(mols_.size());
+  cudaError_t e = cudaMemcpyAsync(r.data(), dev_.res, sizeof(MolResult) * r.size(), cudaMemcpyDeviceToHost, stream_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
   }
   return kOk;
 }

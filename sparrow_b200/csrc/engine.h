@@ -58,6 +58,7 @@ class Batch {
   // Copy results back (synchronises the stream).
   int fetch(std::vector<MoleculeOutput>& out, bool gradient, std::string& err);
   int fetch_density(int mol, std::vector<double>& P, std::string& err);
+  int fetch_raw_results(std::vector<MolResult>& r, std::string& err);
   int fetch_orbital_energies(int mol, std::vector<double>& eps, std::string& err);
 
   cudaStream_t stream() const { return stream_; }
@@ -91,7 +92,7 @@ class Batch {
   std::vector<PairDev> pairs_;
   std::vector<ElemDev> elems_;
   std::vector<DiatomicDev> diat_;
-  std::vector<int> ao_atom_, order_;
+  std::vector<int> ao_atom_, order_, hh_pairs_;
   int scf_grid_ = 0;
   int launches_ = 0;
   bool density_given_ = false;

@@ -68,6 +68,8 @@ struct MolDev {
   int pair0;      // first pair (global index)
   int npairs;
   int ao_base;    // first AO (global index) in the ao_atom map
+  int hh0;        // first entry of this molecule in the list of s/p-s/p pairs
+  int nhh;        // number of pairs where both atoms carry an s/p shell
   long long mat_off;   // N*N matrices (H, P, F, C, scratch) at this offset
   long long diis_off;  // DIIS history
   long long int_off;   // first integral of the molecule
@@ -83,7 +85,12 @@ struct MolResult {
   int iterations;
   int converged;       // 1 if both criteria were met
   int status;          // 0 ok, nonzero = device-side failure code
+  int full_diag;       // full diagonalisations performed
+  int jacobi_sweeps;   // total Jacobi sweeps
   int pad;
+  // SM cycles (clock64 on the CTA) spent per phase: Fock build, DIIS,
+  // occupied-virtual rotation, full diagonalisation, density
+  long long cycles[5];
 };
 
 struct ScfParams {

@@ -24,6 +24,8 @@ struct DeviceBatch {
   int* counter = nullptr;           // work counter of the persistent SCF kernel
   double* ints = nullptr;           // [int_total]
   double* vcore = nullptr;          // [npairs * 20]
+  double* jbuf = nullptr;           // [npairs * 20] per-pair Coulomb vectors of the Fock build
+  int* hh_pairs = nullptr;          // [n_hh] global pair indices of s/p-s/p pairs
   double* ovl = nullptr;            // [npairs * 16]
   double* erep = nullptr;           // [npairs]
   double* H = nullptr;              // [mat_total]

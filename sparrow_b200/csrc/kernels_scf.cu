@@ -8,11 +8,22 @@
 //                                                 NDDOElectronicEnergyCalculator.cpp:48-67
 //   Pulay DIIS on the commutator FP - PF          (restated; the reference's
 //                                                 SCF driver is in scine_utilities)
-//   F_mo = C^T F C, cyclic parallel Jacobi, C <- C J (warm start from the
-//   previous orbitals), aufbau occupation of the n_occ lowest orbitals
+//   new orbitals:
+//     first iteration (and whenever the occupied/virtual ordering changes):
+//       full diagonalisation by cyclic Jacobi with the packed matrix held in
+//       shared memory, orbitals sorted by energy (aufbau: n_occ lowest)
+//     later iterations: occupied-virtual rotation of the previous orbitals
+//       (pseudo-diagonalisation): X_ai = F_ai / (e_i - e_a) from
+//       F_mo = C^T F C, C <- C exp([[0, -X^T], [X, 0]]) to second order, with
+//       a Newton-Schulz re-orthonormalisation when the second-order error can
+//       exceed 1e-14.  The fixed point is the same (F_ov = 0 at
+//       self-consistency), and every step is a dense GEMM.
 //   P = 2 C_occ C_occ^T, convergence on |dE| and rms(dP)
 // and, after convergence, G is rebuilt from the final density
 // (FockMatrix::finalize, FockMatrix.cpp:147-150).
+//
+// Orbitals are stored orbital-major: Ct[k][mu] is the coefficient of AO mu in
+// orbital k (so rotating two orbitals touches two contiguous rows).
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -22,9 +33,11 @@
 
 namespace sgb {
 
-constexpr int kScfThreads = 256;
+constexpr int kScfThreads = 512;
+constexpr int kGemmGroup = 256;       // threads per GEMM tile group
 constexpr int kJacobiMaxPairs = 512;  // supports N <= 1024
 constexpr int kGemmBM = 64, kGemmBN = 64, kGemmBK = 16;
+constexpr int kGemmTileA = kGemmBK * (kGemmBM + 1), kGemmTileB = kGemmBK * (kGemmBN + 1);
 
 // ---------------------------------------------------------------------------
 // CTA helpers
@@ -55,72 +68,105 @@ __device__ double cta_max(double v, double* red) {
   __syncthreads();
   if (lane == 0) red[w] = v;
   __syncthreads();
-  double s = 0;
-  for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s = fmax(s, red[i]);
+  double s = red[0];
+  for (int i = 1; i < (int)(blockDim.x >> 5); ++i) s = fmax(s, red[i]);
   return s;
 }
 
-// C = alpha * op(A) * op(B) + beta * C, row-major, op(X) = X or X^T.
-// 64x64 output tiles, 256 threads with a 4x4 register tile each.
+__device__ __forceinline__ void group_sync(int grp) {
+  asm volatile("bar.sync %0, %1;" ::"r"(grp + 1), "r"(kGemmGroup) : "memory");
+}
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const int n = valid ? 8 : 0;  // zero-fill when out of bounds
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// C = alpha * op(A) * op(B) + beta * C, row-major, op(X) = X or X^T.  The CTA
+// (512 threads) is split into two groups of 256 that work on different 64x64
+// output tiles; each thread accumulates a 4x4 register tile.  The 64x16 and
+// 16x64 input tiles are double-buffered in shared memory with cp.async so
+// the next k-slice streams in while the current one is multiplied.  smem
+// holds 2 groups x 2 stages x (kGemmTileA + kGemmTileB) doubles.
 __device__ void cta_gemm(int M, int Nn, int K, double alpha, const double* __restrict__ A, int lda, bool tA,
                          const double* __restrict__ B, int ldb, bool tB, double beta, double* C, int ldc,
-                         double* smA, double* smB) {
-  const int tid = threadIdx.x;
+                         double* smem) {
+  const int grp = threadIdx.x / kGemmGroup, tid = threadIdx.x % kGemmGroup;
+  double* base = smem + grp * 2 * (kGemmTileA + kGemmTileB);
   const int tx = tid & 15, ty = tid >> 4;
-  for (int m0 = 0; m0 < M; m0 += kGemmBM)
-    for (int n0 = 0; n0 < Nn; n0 += kGemmBN) {
-      double acc[4][4];
+  const int tilesM = (M + kGemmBM - 1) / kGemmBM, tilesN = (Nn + kGemmBN - 1) / kGemmBN;
+  const int ntiles = tilesM * tilesN;
+  const int nk = (K + kGemmBK - 1) / kGemmBK;
+  // the source address is only formed when in bounds; out-of-bounds slots copy 0 bytes from A/B
+  auto load_stage = [&](int stage, int m0, int n0, int k0) {
+    double* smA = base + stage * (kGemmTileA + kGemmTileB);
+    double* smB = smA + kGemmTileA;
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0;
-      for (int k0 = 0; k0 < K; k0 += kGemmBK) {
-        // stage op(A)[m0:m0+64, k0:k0+16] as smA[k][m]
-        for (int e = tid; e < kGemmBM * kGemmBK; e += kScfThreads) {
-          int mm, kk;
-          if (!tA) { mm = e / kGemmBK; kk = e % kGemmBK; }
-          else { kk = e / kGemmBM; mm = e % kGemmBM; }
-          int gm = m0 + mm, gk = k0 + kk;
-          double v = 0;
-          if (gm < M && gk < K) v = tA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk];
-          smA[kk * (kGemmBM + 1) + mm] = v;
-        }
-        // stage op(B)[k0:k0+16, n0:n0+64] as smB[k][n]
-        for (int e = tid; e < kGemmBK * kGemmBN; e += kScfThreads) {
-          int nn, kk;
-          if (!tB) { kk = e / kGemmBN; nn = e % kGemmBN; }
-          else { nn = e / kGemmBK; kk = e % kGemmBK; }
-          int gn = n0 + nn, gk = k0 + kk;
-          double v = 0;
-          if (gn < Nn && gk < K) v = tB ? B[(size_t)gn * ldb + gk] : B[(size_t)gk * ldb + gn];
-          smB[kk * (kGemmBN + 1) + nn] = v;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < kGemmBK; ++kk) {
-          double a[4], b[4];
-#pragma unroll
-          for (int i = 0; i < 4; ++i) a[i] = smA[kk * (kGemmBM + 1) + ty * 4 + i];
-#pragma unroll
-          for (int j = 0; j < 4; ++j) b[j] = smB[kk * (kGemmBN + 1) + tx * 4 + j];
-#pragma unroll
-          for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-        }
-        __syncthreads();
-      }
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          int gm = m0 + ty * 4 + i, gn = n0 + tx * 4 + j;
-          if (gm < M && gn < Nn) {
-            double* c = &C[(size_t)gm * ldc + gn];
-            *c = beta == 0.0 ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*c);
-          }
-        }
+    for (int r = 0; r < (kGemmBM * kGemmBK) / kGemmGroup; ++r) {
+      const int e = tid + r * kGemmGroup;
+      int mm, kk;
+      if (!tA) { mm = e / kGemmBK; kk = e % kGemmBK; }
+      else { kk = e / kGemmBM; mm = e % kGemmBM; }
+      const int gm = m0 + mm, gk = k0 + kk;
+      const bool ok = gm < M && gk < K;
+      const double* src = ok ? (tA ? A + (size_t)gk * lda + gm : A + (size_t)gm * lda + gk) : A;
+      cp_async8(&smA[kk * (kGemmBM + 1) + mm], src, ok);
     }
+#pragma unroll
+    for (int r = 0; r < (kGemmBK * kGemmBN) / kGemmGroup; ++r) {
+      const int e = tid + r * kGemmGroup;
+      int nn, kk;
+      if (!tB) { kk = e / kGemmBN; nn = e % kGemmBN; }
+      else { nn = e / kGemmBK; kk = e % kGemmBK; }
+      const int gn = n0 + nn, gk = k0 + kk;
+      const bool ok = gn < Nn && gk < K;
+      const double* src = ok ? (tB ? B + (size_t)gn * ldb + gk : B + (size_t)gk * ldb + gn) : B;
+      cp_async8(&smB[kk * (kGemmBN + 1) + nn], src, ok);
+    }
+    cp_async_commit();
+  };
+  for (int tile = grp; tile < ntiles; tile += 2) {
+    const int m0 = (tile / tilesN) * kGemmBM, n0 = (tile % tilesN) * kGemmBN;
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) acc[i][j] = 0;
+    load_stage(0, m0, n0, 0);
+    for (int kt = 0; kt < nk; ++kt) {
+      cp_async_wait_all();
+      group_sync(grp);  // stage kt%2 visible; stage (kt+1)%2 no longer read
+      if (kt + 1 < nk) load_stage((kt + 1) & 1, m0, n0, (kt + 1) * kGemmBK);
+      const double* smA = base + (kt & 1) * (kGemmTileA + kGemmTileB);
+      const double* smB = smA + kGemmTileA;
+#pragma unroll
+      for (int kk = 0; kk < kGemmBK; ++kk) {
+        double a[4], b[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) a[i] = smA[kk * (kGemmBM + 1) + ty * 4 + i];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) b[j] = smB[kk * (kGemmBN + 1) + tx + 16 * j];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+      }
+    }
+    group_sync(grp);  // all reads of the last stage done before the next tile overwrites it
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int gm = m0 + ty * 4 + i, gn = n0 + tx + 16 * j;
+        if (gm < M && gn < Nn) {
+          double* c = &C[(size_t)gm * ldc + gn];
+          *c = beta == 0.0 ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*c);
+        }
+      }
+  }
   __syncthreads();
 }
 
@@ -207,71 +253,177 @@ __device__ __forceinline__ double one_centre_g(const ElemDev& e, int mu, int nu,
   return Pm(mu, nu) * (1.5 * e.hpp - 0.5 * e.gp2);
 }
 
+// Orbital pair (mu, nu), mu <= nu, of each packed index p = nu(nu+1)/2 + mu.
+__constant__ int c_pair_mu[10] = {0, 0, 1, 0, 1, 2, 0, 1, 2, 3};
+__constant__ int c_pair_nu[10] = {0, 1, 1, 2, 2, 2, 3, 3, 3, 3};
+
+constexpr int kFockWarpScratch = 100 + 16 + 10 + 10;  // W block, P_AB, pv_A, pv_B
+
+// F = H + G(P) and the electronic energy 1/2 sum P (H + F), pair-centric.
+// Phase 1: per atom pair (A < B) the Coulomb vectors J_A = W pv_B and
+// J_B = W^T pv_A (pv = packed diagonal-block density with the factor 2 for
+// mu != nu) go to jbuf, and the exchange block F_AB = H_AB - 1/2 K_AB with
+// K_AB[mu][lam] = sum P_{nu sig} (mu nu|lam sig) is written directly (each
+// pair owns its block).  s/p-s/p pairs are handled by a warp each, pairs with
+// an s-only atom by a thread each.
+// Phase 2: diagonal blocks F_AA = H_AA + G_1c(P_AA) + sum of the partners' J_A.
 __device__ double build_fock(const MolDev& m, const AtomDev* __restrict__ atoms, const ElemDev* __restrict__ elems,
                              const PairDev* __restrict__ pairs, const double* __restrict__ ints,
-                             const int* __restrict__ ao_atom, const double* __restrict__ H,
-                             const double* __restrict__ P, double* F, double* red) {
+                             const int* __restrict__ hh_pairs, double* __restrict__ jbuf,
+                             const double* __restrict__ H, const double* __restrict__ P, double* F, double* red,
+                             double* wscratch) {
   const int N = m.nao;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   double e = 0;
-  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
-    const int i = idx / N, j = idx % N;
-    const int A = ao_atom[m.ao_base + i], B = ao_atom[m.ao_base + j];
-    const AtomDev aA = atoms[A], aB = atoms[B];
-    const ElemDev& eA = elems[aA.slot];
-    const int mu = i - aA.ao0, nu = j - aB.ao0;
-    const double h = H[idx];
-    double g;
-    if (A == B) {
-      g = one_centre_g(eA, mu, nu, P, N, aA.ao0);
-      const int a = A - m.atom0, pk = pair_index(mu, nu), dA = eA.nao == 1 ? 1 : 10;
-      for (int c = 0; c < m.nat; ++c) {
-        if (c == a) continue;
-        const AtomDev aC = atoms[m.atom0 + c];
-        const int nC = elems[aC.slot].nao, dC = nC == 1 ? 1 : 10, oc = aC.ao0;
-        const bool first = a < c;
-        const double* W = ints + pairs[first ? pair_slot(m, a, c) : pair_slot(m, c, a)].int_off;
-        for (int la = 0; la < nC; ++la)
-          for (int si = la; si < nC; ++si) {
-            const int pl = pair_index(la, si);
-            const double w = first ? W[pk * dC + pl] : W[pl * dA + pk];
-            g += (la == si ? 1.0 : 2.0) * P[(oc + la) * N + oc + si] * w;
-          }
-      }
-    } else {
-      const int nA = eA.nao, nB = elems[aB.slot].nao;
-      const int dA = nA == 1 ? 1 : 10, dB = nB == 1 ? 1 : 10;
-      const int a = A - m.atom0, b = B - m.atom0;
-      const bool first = a < b;
-      const double* W = ints + pairs[first ? pair_slot(m, a, b) : pair_slot(m, b, a)].int_off;
-      double k = 0;
-      for (int n2 = 0; n2 < nA; ++n2)
-        for (int s2 = 0; s2 < nB; ++s2) {
-          const int p1 = pair_index(mu, n2), p2 = pair_index(nu, s2);
-          const double w = first ? W[p1 * dB + p2] : W[p2 * dA + p1];
-          k += P[(aA.ao0 + n2) * N + aB.ao0 + s2] * w;
-        }
-      g = -0.5 * k;
+  // phase 1a: pairs with at most one s/p atom, one thread each
+  for (int k = tid; k < m.npairs; k += blockDim.x) {
+    const int pi = m.pair0 + k;
+    const PairDev pr = pairs[pi];
+    const AtomDev aA = atoms[pr.a], aB = atoms[pr.b];
+    const int nA = elems[aA.slot].nao, nB = elems[aB.slot].nao;
+    if (nA == 4 && nB == 4) continue;
+    const int dA = nA == 1 ? 1 : 10, dB = nB == 1 ? 1 : 10;
+    const int oa = aA.ao0, ob = aB.ao0;
+    const double* W = ints + pr.int_off;
+    double* jb = jbuf + (size_t)pi * 20;
+    if (nA == 1 && nB == 1) {
+      const double w = W[0];
+      jb[0] = w * P[(size_t)ob * N + ob];
+      jb[10] = w * P[(size_t)oa * N + oa];
+      const double pab = P[(size_t)oa * N + ob];
+      const double h = H[(size_t)oa * N + ob];
+      const double f = h - 0.5 * pab * w;
+      F[(size_t)oa * N + ob] = f;
+      F[(size_t)ob * N + oa] = f;
+      e += pab * (h + f);
+      continue;
     }
+    // one s/p atom (X) and one s-only atom (Hs): W is 10 x 1 or 1 x 10
+    const bool xfirst = nA == 4;
+    const int ox = xfirst ? oa : ob, oh = xfirst ? ob : oa;
+    double pvx[10];
+#pragma unroll
+    for (int p = 0; p < 10; ++p) {
+      const int mu = c_pair_mu[p], nu = c_pair_nu[p];
+      pvx[p] = (mu == nu ? 1.0 : 2.0) * P[(size_t)(ox + mu) * N + ox + nu];
+    }
+    const double pvh = P[(size_t)oh * N + oh];
+    double jh = 0;
+#pragma unroll
+    for (int p = 0; p < 10; ++p) {
+      const double w = W[p];  // (p on X | s s on Hs) in either storage order
+      jh += w * pvx[p];
+      jb[(xfirst ? 0 : 10) + p] = w * pvh;
+    }
+    jb[xfirst ? 10 : 0] = jh;
+    // exchange K[mu on X] = sum_nu P[X_nu][Hs] (mu nu | s s)
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+      double kx = 0;
+#pragma unroll
+      for (int nu = 0; nu < 4; ++nu) kx += P[(size_t)(ox + nu) * N + oh] * W[pair_index(mu, nu)];
+      const size_t ixh = (size_t)(ox + mu) * N + oh, ihx = (size_t)oh * N + ox + mu;
+      const double h = H[ixh];
+      const double f = h - 0.5 * kx;
+      F[ixh] = f;
+      F[ihx] = f;
+      e += P[ixh] * (h + f);
+    }
+  }
+  // phase 1b: s/p-s/p pairs, one warp each
+  double* ws = wscratch + (size_t)warp * kFockWarpScratch;
+  double* Wsm = ws;
+  double* Pab = ws + 100;
+  double* pvA = ws + 116;
+  double* pvB = ws + 126;
+  for (int h = warp; h < m.nhh; h += nwarps) {
+    const int pi = hh_pairs[m.hh0 + h];
+    const PairDev pr = pairs[pi];
+    const int oa = atoms[pr.a].ao0, ob = atoms[pr.b].ao0;
+    const double* W = ints + pr.int_off;
+    for (int q = lane; q < 100; q += 32) Wsm[q] = W[q];
+    if (lane < 16) Pab[lane] = P[(size_t)(oa + (lane >> 2)) * N + ob + (lane & 3)];
+    if (lane < 10) {
+      const int mu = c_pair_mu[lane], nu = c_pair_nu[lane];
+      pvA[lane] = (mu == nu ? 1.0 : 2.0) * P[(size_t)(oa + mu) * N + oa + nu];
+      pvB[lane] = (mu == nu ? 1.0 : 2.0) * P[(size_t)(ob + mu) * N + ob + nu];
+    }
+    __syncwarp();
+    double* jb = jbuf + (size_t)pi * 20;
+    if (lane < 10) {
+      double s = 0;
+#pragma unroll
+      for (int q = 0; q < 10; ++q) s += Wsm[lane * 10 + q] * pvB[q];
+      jb[lane] = s;
+    } else if (lane < 20) {
+      const int q = lane - 10;
+      double s = 0;
+#pragma unroll
+      for (int p = 0; p < 10; ++p) s += Wsm[p * 10 + q] * pvA[p];
+      jb[10 + q] = s;
+    }
+    if (lane < 16) {
+      const int mu = lane >> 2, la = lane & 3;
+      double kx = 0;
+#pragma unroll
+      for (int nu = 0; nu < 4; ++nu)
+#pragma unroll
+        for (int si = 0; si < 4; ++si) kx += Pab[nu * 4 + si] * Wsm[pair_index(mu, nu) * 10 + pair_index(la, si)];
+      const size_t iab = (size_t)(oa + mu) * N + ob + la, iba = (size_t)(ob + la) * N + oa + mu;
+      const double hv = H[iab];
+      const double f = hv - 0.5 * kx;
+      F[iab] = f;
+      F[iba] = f;
+      e += Pab[lane] * (hv + f);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  // phase 2: diagonal blocks
+  for (int idx = tid; idx < m.nat * 10; idx += blockDim.x) {
+    const int a = idx / 10, p = idx % 10;
+    const AtomDev aA = atoms[m.atom0 + a];
+    const ElemDev& eA = elems[aA.slot];
+    if (p >= (eA.nao == 1 ? 1 : 10)) continue;
+    const int mu = c_pair_mu[p], nu = c_pair_nu[p];
+    double g = one_centre_g(eA, mu, nu, P, N, aA.ao0);
+    double j0 = 0, j1 = 0;
+    int c = 0;
+    for (; c + 1 < m.nat; c += 2) {
+      const int c0 = c, c1 = c + 1;
+      if (c0 != a) j0 += jbuf[(size_t)(a < c0 ? pair_slot(m, a, c0) : pair_slot(m, c0, a)) * 20 + (a < c0 ? p : 10 + p)];
+      if (c1 != a) j1 += jbuf[(size_t)(a < c1 ? pair_slot(m, a, c1) : pair_slot(m, c1, a)) * 20 + (a < c1 ? p : 10 + p)];
+    }
+    if (c < m.nat && c != a) j0 += jbuf[(size_t)(a < c ? pair_slot(m, a, c) : pair_slot(m, c, a)) * 20 + (a < c ? p : 10 + p)];
+    g += j0 + j1;
+    const size_t i1 = (size_t)(aA.ao0 + mu) * N + aA.ao0 + nu;
+    const double h = H[i1];
     const double f = h + g;
-    F[idx] = f;
-    e += 0.5 * P[idx] * (h + f);
+    F[i1] = f;
+    if (mu != nu) F[(size_t)(aA.ao0 + nu) * N + aA.ao0 + mu] = f;
+    e += (mu == nu ? 0.5 : 1.0) * P[i1] * (h + f);
   }
   __syncthreads();
   return cta_sum(e, red);
 }
 
 // ---------------------------------------------------------------------------
-// Cyclic Jacobi on the symmetric A (N x N) with rotations applied to C's columns
+// Cyclic Jacobi on a packed symmetric matrix (lower triangle, row i holds
+// columns 0..i at i(i+1)/2), rotations applied to the rows of Ct.
 // ---------------------------------------------------------------------------
 struct JacobiShared {
   double c[kJacobiMaxPairs], s[kJacobiMaxPairs], t[kJacobiMaxPairs];
   int p[kJacobiMaxPairs], q[kJacobiMaxPairs];
 };
 
+__device__ __forceinline__ int packed(int i, int j) { return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i; }
+
 // Returns the number of sweeps, or -1 if not converged within max_sweeps.
-__device__ int jacobi_eigh(int N, double* A, double* C, JacobiShared& js, double* red, int max_sweeps, double tol) {
+// Convergence: largest |A_pq| met in a sweep below tol.
+__device__ int jacobi_packed(int N, double* A, double* Ct, JacobiShared& js, double* red, int max_sweeps, double tol) {
   const int Ne = N + (N & 1);
   const int npair = Ne / 2;
+  const int nblk = npair * (npair + 1) / 2;
   for (int sweep = 0; sweep < max_sweeps; ++sweep) {
     double offmax = 0;
     for (int r = 0; r < Ne - 1; ++r) {
@@ -282,10 +434,10 @@ __device__ int jacobi_eigh(int N, double* A, double* C, JacobiShared& js, double
         if (p > q) { int t = p; p = q; q = t; }
         double c = 1, s = 0, t = 0;
         if (q < N) {
-          const double apq = A[(size_t)p * N + q];
+          const double apq = A[packed(q, p)];
           offmax = fmax(offmax, fabs(apq));
           if (apq != 0.0) {
-            const double app = A[(size_t)p * N + p], aqq = A[(size_t)q * N + q];
+            const double app = A[packed(p, p)], aqq = A[packed(q, q)];
             const double tau = (aqq - app) / (2.0 * apq);
             t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
             c = 1.0 / sqrt(1.0 + t * t);
@@ -299,54 +451,72 @@ __device__ int jacobi_eigh(int N, double* A, double* C, JacobiShared& js, double
         js.t[k] = t;
       }
       __syncthreads();
-      // A <- J^T A J on 2x2 blocks of pair k1 (rows) and pair k2 (columns), k1 <= k2
-      const int nblk = npair * (npair + 1) / 2;
-      for (int bidx = threadIdx.x; bidx < nblk; bidx += blockDim.x) {
-        // map triangular index to (k1, k2)
-        int k1 = (int)((sqrt(8.0 * bidx + 1.0) - 1.0) * 0.5);
-        while ((k1 + 1) * (k1 + 2) / 2 <= bidx) ++k1;
-        while (k1 * (k1 + 1) / 2 > bidx) --k1;
-        const int k2 = bidx - k1 * (k1 + 1) / 2;  // k2 <= k1
-        const int p1 = js.p[k1], q1 = js.q[k1], p2 = js.p[k2], q2 = js.q[k2];
-        if (q1 < 0 && q2 < 0) {
-          continue;  // both pairs carry the padding index: only the (p, p) entry, untouched
+      // A <- J^T A J on 2x2 blocks (pair k1 rows, pair k2 columns), k2 <= k1;
+      // one warp per row pair k1
+      {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+        for (int k1 = warp; k1 < npair; k1 += nwarps) {
+          const int p1 = js.p[k1], q1 = js.q[k1];
+          const double c1 = js.c[k1], s1 = js.s[k1];
+          for (int k2 = lane; k2 <= k1; k2 += 32) {
+            const int p2 = js.p[k2], q2 = js.q[k2];
+            if (k1 == k2) {
+              if (q1 < 0) continue;
+              const double t = js.t[k1];
+              const int ipq = packed(q1, p1);
+              const double apq = A[ipq];
+              A[packed(p1, p1)] -= t * apq;
+              A[packed(q1, q1)] += t * apq;
+              A[ipq] = 0.0;
+              continue;
+            }
+            const double c2 = js.c[k2], s2 = js.s[k2];
+            const double m00 = A[packed(p1, p2)];
+            const double m01 = q2 >= 0 ? A[packed(p1, q2)] : 0.0;
+            const double m10 = q1 >= 0 ? A[packed(q1, p2)] : 0.0;
+            const double m11 = (q1 >= 0 && q2 >= 0) ? A[packed(q1, q2)] : 0.0;
+            const double x00 = c1 * m00 - s1 * m10, x01 = c1 * m01 - s1 * m11;
+            const double x10 = s1 * m00 + c1 * m10, x11 = s1 * m01 + c1 * m11;
+            A[packed(p1, p2)] = x00 * c2 - x01 * s2;
+            if (q2 >= 0) A[packed(p1, q2)] = x00 * s2 + x01 * c2;
+            if (q1 >= 0) A[packed(q1, p2)] = x10 * c2 - x11 * s2;
+            if (q1 >= 0 && q2 >= 0) A[packed(q1, q2)] = x10 * s2 + x11 * c2;
+          }
         }
-        const double c1 = js.c[k1], s1 = js.s[k1], c2 = js.c[k2], s2 = js.s[k2];
-        if (k1 == k2) {
-          if (q1 < 0) continue;
-          const double t = js.t[k1];
-          const double apq = A[(size_t)p1 * N + q1];
-          A[(size_t)p1 * N + p1] -= t * apq;
-          A[(size_t)q1 * N + q1] += t * apq;
-          A[(size_t)p1 * N + q1] = 0.0;
-          A[(size_t)q1 * N + p1] = 0.0;
-          continue;
-        }
-        // rows {p1, q1}, cols {p2, q2}; a padding index has no row/column
-        const double m00 = A[(size_t)p1 * N + p2];
-        const double m01 = q2 >= 0 ? A[(size_t)p1 * N + q2] : 0.0;
-        const double m10 = q1 >= 0 ? A[(size_t)q1 * N + p2] : 0.0;
-        const double m11 = (q1 >= 0 && q2 >= 0) ? A[(size_t)q1 * N + q2] : 0.0;
-        const double x00 = c1 * m00 - s1 * m10, x01 = c1 * m01 - s1 * m11;
-        const double x10 = s1 * m00 + c1 * m10, x11 = s1 * m01 + c1 * m11;
-        const double n00 = x00 * c2 - x01 * s2, n01 = x00 * s2 + x01 * c2;
-        const double n10 = x10 * c2 - x11 * s2, n11 = x10 * s2 + x11 * c2;
-        A[(size_t)p1 * N + p2] = n00;
-        A[(size_t)p2 * N + p1] = n00;
-        if (q2 >= 0) { A[(size_t)p1 * N + q2] = n01; A[(size_t)q2 * N + p1] = n01; }
-        if (q1 >= 0) { A[(size_t)q1 * N + p2] = n10; A[(size_t)p2 * N + q1] = n10; }
-        if (q1 >= 0 && q2 >= 0) { A[(size_t)q1 * N + q2] = n11; A[(size_t)q2 * N + q1] = n11; }
       }
-      // C <- C J
-      for (int e = threadIdx.x; e < N * npair; e += blockDim.x) {
-        const int row = e / npair, k = e % npair;
-        const int q = js.q[k];
-        if (q < 0) continue;
-        const int p = js.p[k];
-        const double c = js.c[k], s = js.s[k];
-        const double cp = C[(size_t)row * N + p], cq = C[(size_t)row * N + q];
-        C[(size_t)row * N + p] = c * cp - s * cq;
-        C[(size_t)row * N + q] = s * cp + c * cq;
+      // Ct rows p, q <- c * row_p - s * row_q, s * row_p + c * row_q; four
+      // independent items per thread are loaded before any is stored
+      {
+        const int total = npair * N;
+        const int stride = blockDim.x;
+        for (int base = threadIdx.x; base < total; base += 4 * stride) {
+          double cp[4], cq[4];
+          int rp[4], rq[4];
+          double cc[4], ss[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int e = base + u * stride;
+            rq[u] = -1;
+            if (e < total) {
+              const int k = e / N, j = e % N;
+              const int q = js.q[k];
+              if (q >= 0) {
+                rp[u] = js.p[k] * N + j;
+                rq[u] = q * N + j;
+                cc[u] = js.c[k];
+                ss[u] = js.s[k];
+                cp[u] = Ct[rp[u]];
+                cq[u] = Ct[rq[u]];
+              }
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (rq[u] < 0) continue;
+            Ct[rp[u]] = cc[u] * cp[u] - ss[u] * cq[u];
+            Ct[rq[u]] = ss[u] * cp[u] + cc[u] * cq[u];
+          }
+        }
       }
       __syncthreads();
     }
@@ -364,12 +534,226 @@ struct ScfShared {
   double bmat[kDiisMax * kDiisMax];
   double sys[(kDiisMax + 1) * (kDiisMax + 2)];
   double coef[kDiisMax + 1];
-  double gemmA[kGemmBK * (kGemmBM + 1)];
-  double gemmB[kGemmBK * (kGemmBN + 1)];
-  JacobiShared js;
+  double scal[4];
   int mol;
   int diis_ok;
+  int flag;
+  int pad;
+  // phase scratch: GEMM stages, Fock-build warp buffers and Jacobi rotations
+  // are never live at the same time
+  union {
+    double gemm[4 * (kGemmTileA + kGemmTileB)];
+    double fockw[(kScfThreads / 32) * kFockWarpScratch];
+    JacobiShared js;
+  };
 };
+
+// Pulay DIIS: store (F, FP - PF) in the ring, extend the B matrix, solve.
+// Returns the extrapolated Fock matrix (F itself or dst).
+__device__ const double* diis_step(int N, const double* F, const double* P, double* W, double* dst, double* histF,
+                                   double* histE, int msize, int& nhist, int& head, ScfShared& sh) {
+  const size_t NN = (size_t)N * N;
+  const int tid = threadIdx.x;
+  cta_gemm(N, N, N, 1.0, F, N, false, P, N, false, 0.0, W, N, sh.gemm);
+  const int slot = head;
+  double* eS = histE + (size_t)slot * NN;
+  double* fS = histF + (size_t)slot * NN;
+  for (size_t k = tid; k < NN; k += blockDim.x) {
+    const int i = (int)(k / N), j = (int)(k % N);
+    eS[k] = W[k] - W[(size_t)j * N + i];
+    fS[k] = F[k];
+  }
+  __syncthreads();
+  head = (head + 1) % msize;
+  if (nhist < msize) ++nhist;
+  for (int j = 0; j < nhist; ++j) {
+    const double* eJ = histE + (size_t)j * NN;
+    double d = 0;
+    for (size_t k = tid; k < NN; k += blockDim.x) d += eS[k] * eJ[k];
+    d = cta_sum(d, sh.red);
+    if (tid == 0) {
+      sh.bmat[slot * kDiisMax + j] = d;
+      sh.bmat[j * kDiisMax + slot] = d;
+    }
+  }
+  __syncthreads();
+  if (nhist < 2) return F;
+  if (tid == 0) {
+    const int n = nhist, ld = n + 2;
+    double scale = 0;
+    for (int i = 0; i < n; ++i) scale = fmax(scale, fabs(sh.bmat[i * kDiisMax + i]));
+    scale = scale > 0 ? 1.0 / scale : 1.0;
+    for (int i = 0; i <= n; ++i)
+      for (int j = 0; j <= n; ++j) {
+        double v;
+        if (i < n && j < n) v = sh.bmat[i * kDiisMax + j] * scale;
+        else if (i == n && j == n) v = 0;
+        else v = -1;
+        sh.sys[i * ld + j] = v;
+      }
+    for (int i = 0; i <= n; ++i) sh.sys[i * ld + n + 1] = (i == n) ? -1.0 : 0.0;
+    int ok = 1;
+    for (int c = 0; c <= n && ok; ++c) {
+      int piv = c;
+      for (int r = c + 1; r <= n; ++r)
+        if (fabs(sh.sys[r * ld + c]) > fabs(sh.sys[piv * ld + c])) piv = r;
+      if (fabs(sh.sys[piv * ld + c]) < 1e-300) { ok = 0; break; }
+      if (piv != c)
+        for (int k = 0; k <= n + 1; ++k) {
+          double t = sh.sys[c * ld + k];
+          sh.sys[c * ld + k] = sh.sys[piv * ld + k];
+          sh.sys[piv * ld + k] = t;
+        }
+      for (int r = c + 1; r <= n; ++r) {
+        double f = sh.sys[r * ld + c] / sh.sys[c * ld + c];
+        for (int k = c; k <= n + 1; ++k) sh.sys[r * ld + k] -= f * sh.sys[c * ld + k];
+      }
+    }
+    if (ok) {
+      for (int c = n; c >= 0; --c) {
+        double s = sh.sys[c * ld + n + 1];
+        for (int k = c + 1; k <= n; ++k) s -= sh.sys[c * ld + k] * sh.coef[k];
+        sh.coef[c] = s / sh.sys[c * ld + c];
+      }
+      for (int i = 0; i < n; ++i)
+        if (!isfinite(sh.coef[i])) ok = 0;
+    }
+    sh.diis_ok = ok;
+  }
+  __syncthreads();
+  if (!sh.diis_ok) return F;
+  for (size_t k = tid; k < NN; k += blockDim.x) {
+    double s = 0;
+    for (int i = 0; i < nhist; ++i) s += sh.coef[i] * histF[(size_t)i * NN + k];
+    dst[k] = s;
+  }
+  __syncthreads();
+  return dst;
+}
+
+// Full diagonalisation of Fx (held in F) into orbital-major Ct, sorted by energy.
+// Cold: Ct = I and A = F.  Warm: A = C^T F C from the current Ct.  A is the
+// packed lower triangle, in shared memory or (when it does not fit) in F,
+// which is free once the transform is done.  W1, W2 are scratch.
+__device__ int full_diagonalise(int N, double* F, double* Ct, double* W1, double* W2, double* eps, double* A, bool warm,
+                                int max_sweeps, double tol, ScfShared& sh) {
+  const size_t NN = (size_t)N * N;
+  const int tid = threadIdx.x;
+  const double* src;
+  if (warm) {
+    cta_gemm(N, N, N, 1.0, F, N, false, Ct, N, true, 0.0, W1, N, sh.gemm);  // F C
+    cta_gemm(N, N, N, 1.0, Ct, N, false, W1, N, false, 0.0, W2, N, sh.gemm);  // C^T F C
+    src = W2;
+  } else {
+    for (size_t k = tid; k < NN; k += blockDim.x) {
+      const int i = (int)(k / N), j = (int)(k % N);
+      Ct[k] = (i == j) ? 1.0 : 0.0;
+      W2[k] = F[k];
+    }
+    __syncthreads();
+    src = W2;
+  }
+  for (int e = tid; e < N * (N + 1) / 2; e += blockDim.x) {
+    int i = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+    while ((i + 1) * (i + 2) / 2 <= e) ++i;
+    while (i * (i + 1) / 2 > e) --i;
+    const int j = e - i * (i + 1) / 2;
+    A[e] = 0.5 * (src[(size_t)i * N + j] + src[(size_t)j * N + i]);
+  }
+  __syncthreads();
+  const int sweeps = jacobi_packed(N, A, Ct, sh.js, sh.red, max_sweeps, tol);
+  // sort orbitals by energy: rank of each diagonal entry, rows of Ct permuted through W1
+  for (int k = tid; k < N; k += blockDim.x) {
+    const double ek = A[packed(k, k)];
+    int rank = 0;
+    for (int j = 0; j < N; ++j) {
+      const double ej = A[packed(j, j)];
+      rank += (ej < ek || (ej == ek && j < k)) ? 1 : 0;
+    }
+    eps[rank] = ek;
+    for (int j = 0; j < N; ++j) W1[(size_t)rank * N + j] = Ct[(size_t)k * N + j];
+  }
+  __syncthreads();
+  for (size_t e = tid; e < NN; e += blockDim.x) Ct[e] = W1[e];
+  __syncthreads();
+  return sweeps;
+}
+
+// Occupied-virtual rotation of Ct toward the eigenvectors of F (second order).
+// Returns 1 when the occupied/virtual ordering is broken or the step is too
+// large (a full diagonalisation is needed instead); Ct is unchanged then.
+// F holds the (extrapolated) Fock matrix on entry and is used as scratch.
+// Scratch: W1 (N x N), W2 (N x N).  eps receives diag(C^T F C).
+__device__ int ov_rotation(int N, int no, double* F, double* Ct, double* W1, double* W2, double* eps, double& drift,
+                           ScfShared& sh) {
+  const int nv = N - no;
+  const size_t NN = (size_t)N * N;
+  const int tid = threadIdx.x;
+  if (no == 0 || nv == 0) return 0;
+  cta_gemm(N, N, N, 1.0, Ct, N, false, F, N, false, 0.0, W1, N, sh.gemm);  // W1 = C^T F (row k = c_k^T F)
+  {
+    const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    for (int k = warp; k < N; k += nwarps) {
+      double s = 0;
+      for (int nu = lane; nu < N; nu += 32) s += W1[(size_t)k * N + nu] * Ct[(size_t)k * N + nu];
+      s = warp_sum(s);
+      if (lane == 0) eps[k] = s;
+    }
+  }
+  __syncthreads();
+  double homo = -1e300, lumo = 1e300;
+  for (int k = tid; k < N; k += blockDim.x) {
+    if (k < no) homo = fmax(homo, eps[k]);
+    else lumo = fmin(lumo, eps[k]);
+  }
+  homo = cta_max(homo, sh.red);
+  lumo = -cta_max(-lumo, sh.red);
+  if (!(homo < lumo - 1e-4)) return 1;
+  // X (nv x no) = F_vo / (e_i - e_a), F_vo[a][i] = c_a^T F c_i = sum_nu Ct[a][nu] W1[i][nu]
+  double* X = W2;
+  cta_gemm(nv, no, N, 1.0, Ct + (size_t)no * N, N, false, W1, N, true, 0.0, X, no, sh.gemm);
+  double xmax = 0;
+  for (int e = tid; e < nv * no; e += blockDim.x) {
+    const int a = e / no, i = e % no;
+    double d = eps[i] - eps[no + a];
+    if (d > -0.02) d = -0.02;  // level-shift guard for a tiny gap
+    const double x = X[e] / d;
+    X[e] = x;
+    xmax = fmax(xmax, fabs(x));
+  }
+  xmax = cta_max(xmax, sh.red);
+  if (xmax > 0.5) return 1;
+  // Yo = X^T X, Yv = X X^T (in W1); corrections into F: Do (no x N), Dv (nv x N)
+  double* Yo = W1;
+  double* Yv = W1 + (size_t)no * no;
+  double* Do = F;
+  double* Dv = F + (size_t)no * N;
+  cta_gemm(no, no, nv, 1.0, X, no, true, X, no, false, 0.0, Yo, no, sh.gemm);
+  cta_gemm(nv, nv, no, 1.0, X, no, false, X, no, true, 0.0, Yv, nv, sh.gemm);
+  // Ct_o' = Ct_o + X^T Ct_v - 1/2 Yo Ct_o ;  Ct_v' = Ct_v - X Ct_o - 1/2 Yv Ct_v
+  cta_gemm(no, N, nv, 1.0, X, no, true, Ct + (size_t)no * N, N, false, 0.0, Do, N, sh.gemm);
+  cta_gemm(no, N, no, -0.5, Yo, no, false, Ct, N, false, 1.0, Do, N, sh.gemm);
+  cta_gemm(nv, N, no, -1.0, X, no, false, Ct, N, false, 0.0, Dv, N, sh.gemm);
+  cta_gemm(nv, N, nv, -0.5, Yv, nv, false, Ct + (size_t)no * N, N, false, 1.0, Dv, N, sh.gemm);
+  for (size_t e = tid; e < NN; e += blockDim.x) Ct[e] += F[e];
+  __syncthreads();
+  // the second-order rotation is orthogonal up to |K|^4 / 4: re-orthonormalise when needed
+  drift += 0.25 * xmax * xmax * xmax * xmax;
+  if (drift > 1e-12) {
+    // S = Ct Ct^T, Ct <- (3/2 I - 1/2 S) Ct  (Newton-Schulz step for S^-1/2)
+    cta_gemm(N, N, N, 1.0, Ct, N, false, Ct, N, true, 0.0, W1, N, sh.gemm);
+    for (size_t e = tid; e < NN; e += blockDim.x) {
+      const int i = (int)(e / N), j = (int)(e % N);
+      W1[e] = (i == j ? 1.5 : 0.0) - 0.5 * W1[e];
+    }
+    __syncthreads();
+    cta_gemm(N, N, N, 1.0, W1, N, false, Ct, N, false, 0.0, W2, N, sh.gemm);
+    for (size_t e = tid; e < NN; e += blockDim.x) Ct[e] = W2[e];
+    __syncthreads();
+    drift = 0;
+  }
+  return 0;
+}
 
 __global__ void __launch_bounds__(kScfThreads) k_scf(const MolDev* __restrict__ mols, int nmol,
                                                      const int* __restrict__ order, int* counter,
@@ -377,12 +761,14 @@ __global__ void __launch_bounds__(kScfThreads) k_scf(const MolDev* __restrict__ 
                                                      const ElemDev* __restrict__ elems,
                                                      const PairDev* __restrict__ pairs,
                                                      const double* __restrict__ ints,
-                                                     const int* __restrict__ ao_atom, const double* __restrict__ Hall,
+                                                     const int* __restrict__ hh_pairs, double* jbuf,
+                                                     const double* __restrict__ Hall,
                                                      double* Pall, double* Fall, double* Call, double* W1all,
                                                      double* W2all, double* epsall, double* diisall, MolResult* res,
-                                                     ScfParams sp) {
-  extern __shared__ unsigned char smem_raw[];
+                                                     ScfParams sp, int packed_in_smem) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   ScfShared& sh = *reinterpret_cast<ScfShared*>(smem_raw);
+  double* smemA = reinterpret_cast<double*>(smem_raw + ((sizeof(ScfShared) + 15) / 16) * 16);
   const int tid = threadIdx.x;
   for (;;) {
     if (tid == 0) {
@@ -394,151 +780,62 @@ __global__ void __launch_bounds__(kScfThreads) k_scf(const MolDev* __restrict__ 
     __syncthreads();
     if (mi < 0) return;
     const MolDev m = mols[mi];
-    const int N = m.nao;
+    const int N = m.nao, no = m.nocc;
     const size_t NN = (size_t)N * N;
     const double* H = Hall + m.mat_off;
     double* P = Pall + m.mat_off;
     double* F = Fall + m.mat_off;
-    double* C = Call + m.mat_off;
+    double* Ct = Call + m.mat_off;
     double* W1 = W1all + m.mat_off;
     double* W2 = W2all + m.mat_off;
     double* eps = epsall + m.ao_base;
     double* histF = diisall + m.diis_off;
     double* histE = histF + (size_t)kDiisMax * NN;
+    // packed matrix of the Jacobi solver: shared memory when it fits, else F
+    double* Apk = packed_in_smem ? smemA : nullptr;
     const int msize = sp.diis_size < 1 ? 1 : (sp.diis_size > kDiisMax ? kDiisMax : sp.diis_size);
-    int nhist = 0, head = 0;  // ring buffer of DIIS vectors
+    int nhist = 0, head = 0;
     bool have_orbitals = false;
+    double drift = 0;
     double Eold = 0;
     int it = 0, converged = 0, status = kDevOk;
     double last_dE = 0, last_rms = 0;
 
+    long long cyc[5] = {0, 0, 0, 0, 0};
+    int nfull = 0, nsweeps = 0;
     for (it = 1; it <= sp.max_iter; ++it) {
-      // F = H + G(P), energy of the current density
-      const double E = build_fock(m, atoms, elems, pairs, ints, ao_atom, H, P, F, sh.red);
+      long long t0 = clock64();
+      const double E = build_fock(m, atoms, elems, pairs, ints, hh_pairs, jbuf, H, P, F, sh.red, sh.fockw);
       __syncthreads();
-      // DIIS error e = FP - PF (F, P symmetric: PF = (FP)^T)
-      cta_gemm(N, N, N, 1.0, F, N, false, P, N, false, 0.0, W1, N, sh.gemmA, sh.gemmB);
-      const int slot = head;
-      double* eS = histE + (size_t)slot * NN;
-      double* fS = histF + (size_t)slot * NN;
-      for (size_t k = tid; k < NN; k += blockDim.x) {
-        const int i = (int)(k / N), j = (int)(k % N);
-        eS[k] = W1[k] - W1[(size_t)j * N + i];
-        fS[k] = F[k];
-      }
-      __syncthreads();
-      head = (head + 1) % msize;
-      if (nhist < msize) ++nhist;
-      // new row of the B matrix
-      for (int j = 0; j < nhist; ++j) {
-        const double* eJ = histE + (size_t)j * NN;
-        double d = 0;
-        for (size_t k = tid; k < NN; k += blockDim.x) d += eS[k] * eJ[k];
-        d = cta_sum(d, sh.red);
-        if (tid == 0) {
-          sh.bmat[slot * kDiisMax + j] = d;
-          sh.bmat[j * kDiisMax + slot] = d;
-        }
-      }
-      __syncthreads();
-      const double* Fx = F;
-      if (nhist >= 2) {
-        if (tid == 0) {
-          // (n+1) x (n+1) Pulay system, scaled by the largest diagonal entry
-          const int n = nhist, ld = n + 2;
-          double scale = 0;
-          for (int i = 0; i < n; ++i) scale = fmax(scale, fabs(sh.bmat[i * kDiisMax + i]));
-          scale = scale > 0 ? 1.0 / scale : 1.0;
-          for (int i = 0; i <= n; ++i)
-            for (int j = 0; j <= n; ++j) {
-              double v;
-              if (i < n && j < n) v = sh.bmat[i * kDiisMax + j] * scale;
-              else if (i == n && j == n) v = 0;
-              else v = -1;
-              sh.sys[i * ld + j] = v;
-            }
-          for (int i = 0; i <= n; ++i) sh.sys[i * ld + n + 1] = (i == n) ? -1.0 : 0.0;
-          int ok = 1;
-          for (int c = 0; c <= n && ok; ++c) {
-            int piv = c;
-            for (int r = c + 1; r <= n; ++r)
-              if (fabs(sh.sys[r * ld + c]) > fabs(sh.sys[piv * ld + c])) piv = r;
-            if (fabs(sh.sys[piv * ld + c]) < 1e-300) { ok = 0; break; }
-            if (piv != c)
-              for (int k = 0; k <= n + 1; ++k) {
-                double t = sh.sys[c * ld + k];
-                sh.sys[c * ld + k] = sh.sys[piv * ld + k];
-                sh.sys[piv * ld + k] = t;
-              }
-            for (int r = c + 1; r <= n; ++r) {
-              double f = sh.sys[r * ld + c] / sh.sys[c * ld + c];
-              for (int k = c; k <= n + 1; ++k) sh.sys[r * ld + k] -= f * sh.sys[c * ld + k];
-            }
-          }
-          if (ok) {
-            for (int c = n; c >= 0; --c) {
-              double s = sh.sys[c * ld + n + 1];
-              for (int k = c + 1; k <= n; ++k) s -= sh.sys[c * ld + k] * sh.coef[k];
-              sh.coef[c] = s / sh.sys[c * ld + c];
-            }
-            for (int i = 0; i < n; ++i)
-              if (!isfinite(sh.coef[i])) ok = 0;
-          }
-          sh.diis_ok = ok;
-        }
-        __syncthreads();
-        if (sh.diis_ok) {
-          for (size_t k = tid; k < NN; k += blockDim.x) {
-            double s = 0;
-            for (int i = 0; i < nhist; ++i) s += sh.coef[i] * histF[(size_t)i * NN + k];
-            W1[k] = s;
-          }
-          Fx = W1;
-        }
+      long long t1 = clock64();
+      cyc[0] += t1 - t0;
+      const double* Fx = diis_step(N, F, P, W1, W2, histF, histE, msize, nhist, head, sh);
+      // Fx lives in F or W2; move it to F so W1/W2 are free as scratch
+      if (Fx != F) {
+        for (size_t k = tid; k < NN; k += blockDim.x) F[k] = W2[k];
         __syncthreads();
       }
-      // eigen-decomposition of Fx, warm-started from the previous orbitals
-      if (!have_orbitals) {
-        for (size_t k = tid; k < NN; k += blockDim.x) {
-          const int i = (int)(k / N), j = (int)(k % N);
-          C[k] = (i == j) ? 1.0 : 0.0;
-          W2[k] = Fx[k];
-        }
-        __syncthreads();
-      } else {
-        // W2 = C^T Fx C  (Fx may live in W1; use F as the temporary)
-        cta_gemm(N, N, N, 1.0, Fx, N, false, C, N, false, 0.0, Fx == F ? W1 : F, N, sh.gemmA, sh.gemmB);
-        cta_gemm(N, N, N, 1.0, C, N, true, Fx == F ? W1 : F, N, false, 0.0, W2, N, sh.gemmA, sh.gemmB);
-        // symmetrise against rounding
-        for (size_t k = tid; k < NN; k += blockDim.x) {
-          const int i = (int)(k / N), j = (int)(k % N);
-          if (i < j) {
-            double v = 0.5 * (W2[k] + W2[(size_t)j * N + i]);
-            W2[k] = v;
-            W2[(size_t)j * N + i] = v;
-          }
-        }
-        __syncthreads();
+      long long t2 = clock64();
+      cyc[1] += t2 - t1;
+      int need_full = !have_orbitals;
+      if (have_orbitals) need_full = ov_rotation(N, no, F, Ct, W1, W2, eps, drift, sh);
+      long long t3 = clock64();
+      cyc[2] += t3 - t2;
+      if (need_full) {
+        // the first (cold) diagonalisation only has to separate occupied from virtual
+        // orbitals; the rotations of the later iterations converge them
+        const int sw = full_diagonalise(N, F, Ct, W1, W2, eps, Apk ? Apk : F, have_orbitals,
+                                        have_orbitals ? sp.jacobi_max_sweeps : 6, have_orbitals ? 1e-10 : 1e-3, sh);
+        if (sw < 0 && have_orbitals) status = kDevJacobiNotConverged;
+        nsweeps += sw < 0 ? (have_orbitals ? sp.jacobi_max_sweeps : 6) : sw;
+        ++nfull;
+        have_orbitals = true;
+        drift = 0;
       }
-      const int sweeps = jacobi_eigh(N, W2, C, sh.js, sh.red, sp.jacobi_max_sweeps, 1e-12);
-      if (sweeps < 0) status = kDevJacobiNotConverged;
-      have_orbitals = true;
-      // sort orbitals by energy: rank of each diagonal entry
-      for (int k = tid; k < N; k += blockDim.x) {
-        const double ek = W2[(size_t)k * N + k];
-        int rank = 0;
-        for (int j = 0; j < N; ++j) {
-          const double ej = W2[(size_t)j * N + j];
-          rank += (ej < ek || (ej == ek && j < k)) ? 1 : 0;
-        }
-        eps[rank] = ek;
-        for (int row = 0; row < N; ++row) W1[(size_t)row * N + rank] = C[(size_t)row * N + k];
-      }
-      __syncthreads();
-      for (size_t k = tid; k < NN; k += blockDim.x) C[k] = W1[k];
-      __syncthreads();
-      // new density P = 2 C_occ C_occ^T into W1, rms change against P
-      cta_gemm(N, N, m.nocc, 2.0, C, N, false, C, N, true, 0.0, W1, N, sh.gemmA, sh.gemmB);
+      long long t4 = clock64();
+      cyc[3] += t4 - t3;
+      // new density P = 2 C_occ C_occ^T = 2 Ct_o^T Ct_o into W1, rms change against P
+      cta_gemm(N, N, no, 2.0, Ct, N, true, Ct, N, false, 0.0, W1, N, sh.gemm);
       double d2 = 0;
       for (size_t k = tid; k < NN; k += blockDim.x) {
         const double d = W1[k] - P[k];
@@ -551,14 +848,14 @@ __global__ void __launch_bounds__(kScfThreads) k_scf(const MolDev* __restrict__ 
       last_dE = it > 1 ? fabs(E - Eold) : 0.0;
       const bool dE_ok = it > 1 && fabs(E - Eold) < sp.scc;
       Eold = E;
+      cyc[4] += clock64() - t4;
       if (!isfinite(E) || !isfinite(rms)) { status = kDevNonFinite; break; }
       if (dE_ok && rms < sp.rmsd) { converged = 1; break; }
       __syncthreads();
     }
     if (it > sp.max_iter) it = sp.max_iter;
     __syncthreads();
-    // finalize: Fock matrix and energy consistent with the final density
-    const double Efin = build_fock(m, atoms, elems, pairs, ints, ao_atom, H, P, F, sh.red);
+    const double Efin = build_fock(m, atoms, elems, pairs, ints, hh_pairs, jbuf, H, P, F, sh.red, sh.fockw);
     if (tid == 0) {
       MolResult& r = res[mi];
       r.e_el = Efin;
@@ -568,29 +865,51 @@ __global__ void __launch_bounds__(kScfThreads) k_scf(const MolDev* __restrict__ 
       r.status = status;
       r.last_dE = last_dE;
       r.last_rmsd = last_rms;
+      r.full_diag = nfull;
+      r.jacobi_sweeps = nsweeps;
+      for (int k = 0; k < 5; ++k) r.cycles[k] = cyc[k];
     }
     __syncthreads();
   }
 }
 
-int scf_max_grid(int) {
-  int dev = 0, sms = 0, per_sm = 0;
+namespace {
+size_t scf_smem_bytes(int max_nao, int* packed_in_smem) {
+  const size_t base = ((sizeof(ScfShared) + 15) / 16) * 16;
+  const size_t pk = sizeof(double) * (size_t)max_nao * (max_nao + 1) / 2;
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (base + pk <= (size_t)optin) {
+    *packed_in_smem = 1;
+    return base + pk;
+  }
+  *packed_in_smem = 0;
+  return base;
+}
+}  // namespace
+
+int scf_max_grid(int max_nao) {
+  int dev = 0, sms = 0, per_sm = 0, in_smem = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaFuncSetAttribute(k_scf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(ScfShared));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scf, kScfThreads, sizeof(ScfShared));
+  const size_t bytes = scf_smem_bytes(max_nao, &in_smem);
+  cudaFuncSetAttribute(k_scf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_scf, kScfThreads, bytes);
   if (per_sm < 1) per_sm = 1;
   return sms * per_sm;
 }
 
 void launch_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s) {
   if (b.nmol == 0) return;
-  cudaFuncSetAttribute(k_scf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(ScfShared));
+  int in_smem = 0;
+  const size_t bytes = scf_smem_bytes(b.max_nao, &in_smem);
+  cudaFuncSetAttribute(k_scf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   cudaMemsetAsync(b.counter, 0, sizeof(int), s);
   if (grid > b.nmol) grid = b.nmol;
-  k_scf<<<grid, kScfThreads, sizeof(ScfShared), s>>>(b.mols, b.nmol, b.order, b.counter, b.atoms, b.elems, b.pairs,
-                                                     b.ints, b.ao_atom, b.H, b.P, b.F, b.C, b.W1, b.W2, b.eps,
-                                                     b.diis, b.res, sp);
+  k_scf<<<grid, kScfThreads, bytes, s>>>(b.mols, b.nmol, b.order, b.counter, b.atoms, b.elems, b.pairs, b.ints,
+                                         b.hh_pairs, b.jbuf, b.H, b.P, b.F, b.C, b.W1, b.W2, b.eps, b.diis, b.res,
+                                         sp, in_smem);
 }
 
 }  // namespace sgb
