@@ -314,6 +314,12 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
   const size_t o_eps = take(sizeof(double) * (size_t)ao_base);
   const size_t o_diis = take(sizeof(double) * (size_t)diis_off);
   const size_t o_grad = take(sizeof(double) * 3 * atoms_.size());
+  if (scf_grid_ == 0 || max_nao > scf_grid_nao_) {
+    scf_grid_ = scf_max_grid(max_nao);
+    scf_grid_nao_ = max_nao;
+  }
+  const int grid_eff = std::min<int>(scf_grid_, (int)mols_.size());
+  const size_t o_rot = take(scf_rotation_bytes_per_cta() * (size_t)grid_eff);
   const size_t o_res = take(sizeof(MolResult) * mols_.size());
   int rc = ensure_arena(off, err);
   if (rc) return rc;
@@ -344,6 +350,8 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
   d.eps = reinterpret_cast<double*>(base + o_eps);
   d.diis = reinterpret_cast<double*>(base + o_diis);
   d.grad = reinterpret_cast<double*>(base + o_grad);
+  d.rotbuf = reinterpret_cast<double*>(base + o_rot);
+  d.scf_grid = grid_eff;
   d.res = reinterpret_cast<MolResult*>(base + o_res);
   dev_ = d;
 
@@ -387,7 +395,6 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
     err = cuda_message(e);
     return kErrCuda;
   }
-  if (scf_grid_ == 0) scf_grid_ = scf_max_grid(max_nao);
   return kOk;
 }
 
@@ -446,7 +453,7 @@ int Batch::run(const ScfParams& sp, bool gradient, std::string& err) {
   launch_one_electron(dev_, stream_);
   launches_ += 1;
   cudaEventRecord(stage_ev_[2], stream_);
-  launch_scf(dev_, sp, scf_grid_, stream_);
+  launch_scf(dev_, sp, dev_.scf_grid, stream_);
   launches_ += 1;
   cudaEventRecord(stage_ev_[3], stream_);
   if (gradient) {

@@ -94,6 +94,7 @@ class Batch {
   std::vector<DiatomicDev> diat_;
   std::vector<int> ao_atom_, order_, hh_pairs_;
   int scf_grid_ = 0;
+  int scf_grid_nao_ = 0;
   int launches_ = 0;
   bool density_given_ = false;
   long long h2d_bytes_ = 0, d2h_bytes_ = 0;

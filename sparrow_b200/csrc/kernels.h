@@ -36,6 +36,8 @@ struct DeviceBatch {
   double* W2 = nullptr;
   double* eps = nullptr;            // [nao_total] orbital energies
   double* diis = nullptr;           // [diis_total]
+  double* rotbuf = nullptr;         // [scf_grid * rot_budget] recorded Jacobi rotations per SCF CTA
+  int scf_grid = 0;
   double* gpair = nullptr;          // [npairs * 3]
   double* grad = nullptr;           // [natoms * 3]
   MolResult* res = nullptr;         // [nmol]
@@ -48,5 +50,6 @@ void launch_one_electron(const DeviceBatch& b, cudaStream_t s);
 void launch_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s);
 void launch_gradient(const DeviceBatch& b, cudaStream_t s);
 int scf_max_grid(int max_nao);
+size_t scf_rotation_bytes_per_cta();
 
 }  // namespace sgb

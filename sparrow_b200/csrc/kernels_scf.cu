@@ -37,6 +37,7 @@ constexpr int kScfThreads = 512;
 constexpr int kGemmGroup = 256;       // threads per GEMM tile group
 constexpr int kJacobiMaxPairs = 512;  // supports N <= 1024
 constexpr int kGemmBM = 64, kGemmBN = 64, kGemmBK = 16;
+constexpr size_t kRotBudgetBytes = size_t(1) << 20;  // recorded Jacobi rotations per CTA
 constexpr int kGemmTileA = kGemmBK * (kGemmBM + 1), kGemmTileB = kGemmBK * (kGemmBN + 1);
 
 // ---------------------------------------------------------------------------
@@ -409,7 +410,13 @@ __device__ double build_fock(const MolDev& m, const AtomDev* __restrict__ atoms,
 
 // ---------------------------------------------------------------------------
 // Cyclic Jacobi on a packed symmetric matrix (lower triangle, row i holds
-// columns 0..i at i(i+1)/2), rotations applied to the rows of Ct.
+// columns 0..i at i(i+1)/2) with deferred eigenvector accumulation.
+//
+// The sweeps only touch the packed matrix A (shared memory).  Every round's
+// rotation parameters are recorded to a per-CTA list in global memory; the
+// recorded rounds are then replayed onto the orbital matrix Ct (rows =
+// orbitals) one AO-column tile at a time, with the tile held in shared
+// memory.  Ct therefore crosses L2 once per flush instead of once per round.
 // ---------------------------------------------------------------------------
 struct JacobiShared {
   double c[kJacobiMaxPairs], s[kJacobiMaxPairs], t[kJacobiMaxPairs];
@@ -418,20 +425,142 @@ struct JacobiShared {
 
 __device__ __forceinline__ int packed(int i, int j) { return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i; }
 
-// Returns the number of sweeps, or -1 if not converged within max_sweeps.
-// Convergence: largest |A_pq| met in a sweep below tol.
-__device__ int jacobi_packed(int N, double* A, double* Ct, JacobiShared& js, double* red, int max_sweeps, double tol) {
+// Round-robin pairing of round r (Ne even, index Ne-1 is padding when N is
+// odd): pair 0 is (r, Ne-1), pair k >= 1 is (r+k, r-k) mod (Ne-1); p < q.
+__device__ __forceinline__ void rr_pair(int r, int k, int Ne, int& p, int& q) {
+  const int m = Ne - 1;
+  if (k == 0) {
+    p = r;
+    q = m;
+  } else {
+    p = r + k;
+    if (p >= m) p -= m;
+    q = r - k;
+    if (q < 0) q += m;
+    if (p > q) { const int t = p; p = q; q = t; }
+  }
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// Replay nrec recorded rounds (the first is global round g0) onto Ct.
+// Ct is processed in tiles of w AO columns (w a power of two, T laid out
+// [row][w]); the rounds' (c, s) are streamed into the staging buffer St in
+// chunks of rb rounds, double-buffered with cp.async.  cold: Ct is the
+// identity and is not read.  rank: when non-null, row k of the result is
+// written to row rank[k] (eigenvalue order).
+__device__ void replay_rotations(int N, int Ne, int npair, long long g0, int nrec, const double* __restrict__ rot,
+                                 double* Ct, bool cold, const int* rank, double* T, int w, double* St, int rb) {
+  const int tid = threadIdx.x, bd = blockDim.x;
+  const int lw = __ffs(w) - 1;
+  const int jj = tid & (w - 1), k_first = tid >> lw, k_step = bd >> lw;
+  const int round_doubles = 2 * npair;  // a multiple of 2: 16-byte chunks
+  const int nchunk = (nrec + rb - 1) / rb;
+  for (int j0 = 0; j0 < N; j0 += w) {
+    const int wj = min(w, N - j0);
+    auto stage = [&](int c) {
+      const int g = c * rb, n = min(rb, nrec - g);
+      const double* src = rot + (size_t)g * round_doubles;
+      double* dst = St + (size_t)(c & 1) * rb * round_doubles;
+      for (int e = tid; e < n * round_doubles / 2; e += bd) cp_async16(dst + 2 * e, src + 2 * e);
+    };
+    if (nchunk > 0) stage(0);
+    cp_async_commit();
+    for (int e = tid; e < N * w; e += bd) {
+      const int k = e >> lw, j = e & (w - 1);
+      T[e] = (j >= wj) ? 0.0 : cold ? (k == j0 + j ? 1.0 : 0.0) : Ct[(size_t)k * N + j0 + j];
+    }
+    for (int c = 0; c < nchunk; ++c) {
+      if (c + 1 < nchunk) stage(c + 1);
+      cp_async_commit();
+      cp_async_wait_one();
+      __syncthreads();
+      const double* buf = St + (size_t)(c & 1) * rb * round_doubles;
+      const int n = min(rb, nrec - c * rb);
+      for (int g = 0; g < n; ++g) {
+        const long long gg = g0 + (long long)c * rb + g;
+        const int r = (int)(gg % (Ne - 1));
+        const double* rc = buf + (size_t)g * round_doubles;
+        if (jj < wj) {
+          for (int k = k_first; k < npair; k += k_step) {
+            const double sn = rc[npair + k];
+            if (sn == 0.0) continue;
+            int p, q;
+            rr_pair(r, k, Ne, p, q);
+            const double cs = rc[k];
+            const double tp = T[(p << lw) + jj], tq = T[(q << lw) + jj];
+            T[(p << lw) + jj] = cs * tp - sn * tq;
+            T[(q << lw) + jj] = sn * tp + cs * tq;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    for (int e = tid; e < N * w; e += bd) {
+      const int k = e >> lw, j = e & (w - 1);
+      if (j < wj) Ct[(size_t)(rank ? rank[k] : k) * N + j0 + j] = T[e];
+    }
+    __syncthreads();
+  }
+}
+
+// Split a shared region between the replay tile (N x w doubles) and the
+// double-buffered staging of recorded rounds.  Region 'tile' may be separate
+// (tile_bytes > 0) or carved from 'shared' (tile == nullptr).
+struct ReplayPlan {
+  double* T;
+  int w;
+  double* St;
+  int rb;
+};
+__device__ __forceinline__ int pow2_floor(int x) { return x <= 0 ? 0 : 1 << (31 - __clz(x)); }
+__device__ ReplayPlan plan_replay(int N, int npair, double* tile, size_t tile_bytes, double* shared,
+                                  size_t shared_bytes, int max_w) {
+  ReplayPlan pl;
+  const size_t round_bytes = sizeof(double) * 2 * (size_t)npair;
+  if (tile) {
+    pl.T = tile;
+    pl.w = min(max_w, pow2_floor((int)(tile_bytes / (sizeof(double) * N))));
+    pl.St = shared;
+    pl.rb = (int)(shared_bytes / (2 * round_bytes));
+  } else {
+    const size_t st_min = 2 * round_bytes;
+    pl.w = min(max_w, pow2_floor((int)((shared_bytes - st_min) / (sizeof(double) * N))));
+    pl.T = shared;
+    const size_t tb = ((sizeof(double) * N * pl.w + 15) / 16) * 16;
+    pl.St = shared + tb / sizeof(double);
+    pl.rb = (int)((shared_bytes - tb) / (2 * round_bytes));
+  }
+  return pl;
+}
+
+// Diagonalise the packed A; Ct <- Ct J (all rotations), sorted by eigenvalue
+// into eps / rows of Ct.  Returns the sweep count (-1 if not converged).
+// U: the shared phase-scratch region (tiles and staging while A is alive);
+// Afree: A's shared storage, reused as the tile of the last replay (or null).
+__device__ int jacobi_diagonalise(int N, double* A, double* Ct, bool cold, double* rot, int cap_rounds,
+                                  double* U, size_t U_bytes, double* Afree, size_t Afree_bytes, int* rank, double* eps,
+                                  JacobiShared& js, double* red, int max_sweeps, double tol) {
   const int Ne = N + (N & 1);
   const int npair = Ne / 2;
-  const int nblk = npair * (npair + 1) / 2;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  long long g_all = 0, g0 = 0;
+  int nrec = 0;
+  bool identity = cold;
+  int sweeps = -1;
   for (int sweep = 0; sweep < max_sweeps; ++sweep) {
     double offmax = 0;
     for (int r = 0; r < Ne - 1; ++r) {
-      for (int k = threadIdx.x; k < npair; k += blockDim.x) {
+      double* rc = rot + (size_t)nrec * 2 * npair;
+      for (int k = tid; k < npair; k += blockDim.x) {
         int p, q;
-        if (k == 0) { p = Ne - 1; q = r; }
-        else { p = (r + k) % (Ne - 1); q = (r - k + Ne - 1) % (Ne - 1); }
-        if (p > q) { int t = p; p = q; q = t; }
+        rr_pair(r, k, Ne, p, q);
         double c = 1, s = 0, t = 0;
         if (q < N) {
           const double apq = A[packed(q, p)];
@@ -449,81 +578,73 @@ __device__ int jacobi_packed(int N, double* A, double* Ct, JacobiShared& js, dou
         js.c[k] = c;
         js.s[k] = s;
         js.t[k] = t;
+        rc[k] = c;
+        rc[npair + k] = s;
       }
       __syncthreads();
-      // A <- J^T A J on 2x2 blocks (pair k1 rows, pair k2 columns), k2 <= k1;
-      // one warp per row pair k1
-      {
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-        for (int k1 = warp; k1 < npair; k1 += nwarps) {
-          const int p1 = js.p[k1], q1 = js.q[k1];
-          const double c1 = js.c[k1], s1 = js.s[k1];
-          for (int k2 = lane; k2 <= k1; k2 += 32) {
-            const int p2 = js.p[k2], q2 = js.q[k2];
-            if (k1 == k2) {
-              if (q1 < 0) continue;
-              const double t = js.t[k1];
-              const int ipq = packed(q1, p1);
-              const double apq = A[ipq];
-              A[packed(p1, p1)] -= t * apq;
-              A[packed(q1, q1)] += t * apq;
-              A[ipq] = 0.0;
-              continue;
-            }
-            const double c2 = js.c[k2], s2 = js.s[k2];
-            const double m00 = A[packed(p1, p2)];
-            const double m01 = q2 >= 0 ? A[packed(p1, q2)] : 0.0;
-            const double m10 = q1 >= 0 ? A[packed(q1, p2)] : 0.0;
-            const double m11 = (q1 >= 0 && q2 >= 0) ? A[packed(q1, q2)] : 0.0;
-            const double x00 = c1 * m00 - s1 * m10, x01 = c1 * m01 - s1 * m11;
-            const double x10 = s1 * m00 + c1 * m10, x11 = s1 * m01 + c1 * m11;
-            A[packed(p1, p2)] = x00 * c2 - x01 * s2;
-            if (q2 >= 0) A[packed(p1, q2)] = x00 * s2 + x01 * c2;
-            if (q1 >= 0) A[packed(q1, p2)] = x10 * c2 - x11 * s2;
-            if (q1 >= 0 && q2 >= 0) A[packed(q1, q2)] = x10 * s2 + x11 * c2;
+      // A <- J^T A J on 2x2 blocks (pair k1 rows, pair k2 columns), k2 <= k1; one warp per k1
+      for (int k1 = warp; k1 < npair; k1 += nwarps) {
+        const int p1 = js.p[k1], q1 = js.q[k1];
+        const double c1 = js.c[k1], s1 = js.s[k1];
+        for (int k2 = lane; k2 <= k1; k2 += 32) {
+          const int p2 = js.p[k2], q2 = js.q[k2];
+          if (k1 == k2) {
+            if (q1 < 0) continue;
+            const double t = js.t[k1];
+            const int ipq = packed(q1, p1);
+            const double apq = A[ipq];
+            A[packed(p1, p1)] -= t * apq;
+            A[packed(q1, q1)] += t * apq;
+            A[ipq] = 0.0;
+            continue;
           }
-        }
-      }
-      // Ct rows p, q <- c * row_p - s * row_q, s * row_p + c * row_q; four
-      // independent items per thread are loaded before any is stored
-      {
-        const int total = npair * N;
-        const int stride = blockDim.x;
-        for (int base = threadIdx.x; base < total; base += 4 * stride) {
-          double cp[4], cq[4];
-          int rp[4], rq[4];
-          double cc[4], ss[4];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const int e = base + u * stride;
-            rq[u] = -1;
-            if (e < total) {
-              const int k = e / N, j = e % N;
-              const int q = js.q[k];
-              if (q >= 0) {
-                rp[u] = js.p[k] * N + j;
-                rq[u] = q * N + j;
-                cc[u] = js.c[k];
-                ss[u] = js.s[k];
-                cp[u] = Ct[rp[u]];
-                cq[u] = Ct[rq[u]];
-              }
-            }
-          }
-#pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            if (rq[u] < 0) continue;
-            Ct[rp[u]] = cc[u] * cp[u] - ss[u] * cq[u];
-            Ct[rq[u]] = ss[u] * cp[u] + cc[u] * cq[u];
-          }
+          const double c2 = js.c[k2], s2 = js.s[k2];
+          if (s1 == 0.0 && s2 == 0.0) continue;
+          const double m00 = A[packed(p1, p2)];
+          const double m01 = q2 >= 0 ? A[packed(p1, q2)] : 0.0;
+          const double m10 = q1 >= 0 ? A[packed(q1, p2)] : 0.0;
+          const double m11 = (q1 >= 0 && q2 >= 0) ? A[packed(q1, q2)] : 0.0;
+          const double x00 = c1 * m00 - s1 * m10, x01 = c1 * m01 - s1 * m11;
+          const double x10 = s1 * m00 + c1 * m10, x11 = s1 * m01 + c1 * m11;
+          A[packed(p1, p2)] = x00 * c2 - x01 * s2;
+          if (q2 >= 0) A[packed(p1, q2)] = x00 * s2 + x01 * c2;
+          if (q1 >= 0) A[packed(q1, p2)] = x10 * c2 - x11 * s2;
+          if (q1 >= 0 && q2 >= 0) A[packed(q1, q2)] = x10 * s2 + x11 * c2;
         }
       }
       __syncthreads();
+      ++nrec;
+      ++g_all;
+      if (nrec == cap_rounds) {
+        const ReplayPlan pl = plan_replay(N, npair, nullptr, 0, U, U_bytes, 32);
+        replay_rotations(N, Ne, npair, g0, nrec, rot, Ct, identity, nullptr, pl.T, pl.w, pl.St, pl.rb);
+        identity = false;
+        g0 = g_all;
+        nrec = 0;
+      }
     }
     offmax = cta_max(offmax, red);
-    if (offmax < tol) return sweep + 1;
+    if (offmax < tol) {
+      sweeps = sweep + 1;
+      break;
+    }
   }
-  return -1;
+  // eigenvalues and ranks (A still alive), then the final replay with sorting
+  for (int k = tid; k < N; k += blockDim.x) {
+    const double ek = A[packed(k, k)];
+    int rk = 0;
+    for (int j = 0; j < N; ++j) {
+      const double ej = A[packed(j, j)];
+      rk += (ej < ek || (ej == ek && j < k)) ? 1 : 0;
+    }
+    eps[rk] = ek;
+    rank[k] = rk;
+  }
+  __syncthreads();
+  const ReplayPlan pl = Afree ? plan_replay(N, npair, Afree, Afree_bytes, U, U_bytes, 64)
+                              : plan_replay(N, npair, nullptr, 0, U, U_bytes, 32);
+  replay_rotations(N, Ne, npair, g0, nrec, rot, Ct, identity, rank, pl.T, pl.w, pl.St, pl.rb);
+  return sweeps;
 }
 
 // ---------------------------------------------------------------------------
@@ -539,9 +660,10 @@ struct ScfShared {
   int diis_ok;
   int flag;
   int pad;
+  int rank[2 * kJacobiMaxPairs];
   // phase scratch: GEMM stages, Fock-build warp buffers and Jacobi rotations
   // are never live at the same time
-  union {
+  union __align__(16) {
     double gemm[4 * (kGemmTileA + kGemmTileB)];
     double fockw[(kScfThreads / 32) * kFockWarpScratch];
     JacobiShared js;
@@ -633,11 +755,11 @@ __device__ const double* diis_step(int N, const double* F, const double* P, doub
 
 // Full diagonalisation of Fx (held in F) into orbital-major Ct, sorted by energy.
 // Cold: Ct = I and A = F.  Warm: A = C^T F C from the current Ct.  A is the
-// packed lower triangle, in shared memory or (when it does not fit) in F,
-// which is free once the transform is done.  W1, W2 are scratch.
-__device__ int full_diagonalise(int N, double* F, double* Ct, double* W1, double* W2, double* eps, double* A, bool warm,
-                                int max_sweeps, double tol, ScfShared& sh) {
-  const size_t NN = (size_t)N * N;
+// packed lower triangle, in shared memory (Abytes > 0 reserved there) or, when
+// it does not fit, in F (free once the transform is done).  W1, W2 scratch.
+__device__ int full_diagonalise(int N, double* F, double* Ct, double* W1, double* W2, double* eps, double* A,
+                                size_t A_smem_bytes, bool warm, double* rot, int cap_rounds, int max_sweeps,
+                                double tol, ScfShared& sh) {
   const int tid = threadIdx.x;
   const double* src;
   if (warm) {
@@ -645,13 +767,13 @@ __device__ int full_diagonalise(int N, double* F, double* Ct, double* W1, double
     cta_gemm(N, N, N, 1.0, Ct, N, false, W1, N, false, 0.0, W2, N, sh.gemm);  // C^T F C
     src = W2;
   } else {
-    for (size_t k = tid; k < NN; k += blockDim.x) {
-      const int i = (int)(k / N), j = (int)(k % N);
-      Ct[k] = (i == j) ? 1.0 : 0.0;
-      W2[k] = F[k];
+    src = F;
+    if (A == F) {
+      const size_t NN = (size_t)N * N;
+      for (size_t k = tid; k < NN; k += blockDim.x) W2[k] = F[k];
+      __syncthreads();
+      src = W2;
     }
-    __syncthreads();
-    src = W2;
   }
   for (int e = tid; e < N * (N + 1) / 2; e += blockDim.x) {
     int i = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
@@ -661,22 +783,11 @@ __device__ int full_diagonalise(int N, double* F, double* Ct, double* W1, double
     A[e] = 0.5 * (src[(size_t)i * N + j] + src[(size_t)j * N + i]);
   }
   __syncthreads();
-  const int sweeps = jacobi_packed(N, A, Ct, sh.js, sh.red, max_sweeps, tol);
-  // sort orbitals by energy: rank of each diagonal entry, rows of Ct permuted through W1
-  for (int k = tid; k < N; k += blockDim.x) {
-    const double ek = A[packed(k, k)];
-    int rank = 0;
-    for (int j = 0; j < N; ++j) {
-      const double ej = A[packed(j, j)];
-      rank += (ej < ek || (ej == ek && j < k)) ? 1 : 0;
-    }
-    eps[rank] = ek;
-    for (int j = 0; j < N; ++j) W1[(size_t)rank * N + j] = Ct[(size_t)k * N + j];
-  }
-  __syncthreads();
-  for (size_t e = tid; e < NN; e += blockDim.x) Ct[e] = W1[e];
-  __syncthreads();
-  return sweeps;
+  // replay tiles: the phase-scratch union while A lives; A's shared storage
+  // (when it holds at least 32 columns) for the last replay
+  double* Afree = A_smem_bytes >= sizeof(double) * 32 * (size_t)N ? A : nullptr;
+  return jacobi_diagonalise(N, A, Ct, !warm, rot, cap_rounds, sh.gemm, sizeof(sh.gemm), Afree, A_smem_bytes, sh.rank,
+                            eps, sh.js, sh.red, max_sweeps, tol);
 }
 
 // Occupied-virtual rotation of Ct toward the eigenvectors of F (second order).
@@ -764,8 +875,8 @@ __global__ void __launch_bounds__(kScfThreads) k_scf(const MolDev* __restrict__ 
                                                      const int* __restrict__ hh_pairs, double* jbuf,
                                                      const double* __restrict__ Hall,
                                                      double* Pall, double* Fall, double* Call, double* W1all,
-                                                     double* W2all, double* epsall, double* diisall, MolResult* res,
-                                                     ScfParams sp, int packed_in_smem) {
+                                                     double* W2all, double* epsall, double* diisall, double* rotbuf,
+                                                     MolResult* res, ScfParams sp, int packed_in_smem) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ScfShared& sh = *reinterpret_cast<ScfShared*>(smem_raw);
   double* smemA = reinterpret_cast<double*>(smem_raw + ((sizeof(ScfShared) + 15) / 16) * 16);
@@ -793,6 +904,10 @@ __global__ void __launch_bounds__(kScfThreads) k_scf(const MolDev* __restrict__ 
     double* histE = histF + (size_t)kDiisMax * NN;
     // packed matrix of the Jacobi solver: shared memory when it fits, else F
     double* Apk = packed_in_smem ? smemA : nullptr;
+    const size_t packed_bytes = sizeof(double) * (size_t)N * (N + 1) / 2;
+    // recorded Jacobi rotations: this CTA's slice of the rotation buffer
+    double* rot = rotbuf + (size_t)blockIdx.x * (kRotBudgetBytes / sizeof(double));
+    const int cap_rounds = (int)((kRotBudgetBytes / sizeof(double)) / (2 * ((N + 1) / 2)));
     const int msize = sp.diis_size < 1 ? 1 : (sp.diis_size > kDiisMax ? kDiisMax : sp.diis_size);
     int nhist = 0, head = 0;
     bool have_orbitals = false;
@@ -824,8 +939,9 @@ __global__ void __launch_bounds__(kScfThreads) k_scf(const MolDev* __restrict__ 
       if (need_full) {
         // the first (cold) diagonalisation only has to separate occupied from virtual
         // orbitals; the rotations of the later iterations converge them
-        const int sw = full_diagonalise(N, F, Ct, W1, W2, eps, Apk ? Apk : F, have_orbitals,
-                                        have_orbitals ? sp.jacobi_max_sweeps : 6, have_orbitals ? 1e-10 : 1e-3, sh);
+        const int sw = full_diagonalise(N, F, Ct, W1, W2, eps, Apk ? Apk : F, Apk ? packed_bytes : 0, have_orbitals,
+                                        rot, cap_rounds, have_orbitals ? sp.jacobi_max_sweeps : 6,
+                                        have_orbitals ? 1e-10 : 1e-3, sh);
         if (sw < 0 && have_orbitals) status = kDevJacobiNotConverged;
         nsweeps += sw < 0 ? (have_orbitals ? sp.jacobi_max_sweeps : 6) : sw;
         ++nfull;
@@ -889,6 +1005,8 @@ size_t scf_smem_bytes(int max_nao, int* packed_in_smem) {
 }
 }  // namespace
 
+size_t scf_rotation_bytes_per_cta() { return kRotBudgetBytes; }
+
 int scf_max_grid(int max_nao) {
   int dev = 0, sms = 0, per_sm = 0, in_smem = 0;
   cudaGetDevice(&dev);
@@ -908,8 +1026,8 @@ void launch_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_
   cudaMemsetAsync(b.counter, 0, sizeof(int), s);
   if (grid > b.nmol) grid = b.nmol;
   k_scf<<<grid, kScfThreads, bytes, s>>>(b.mols, b.nmol, b.order, b.counter, b.atoms, b.elems, b.pairs, b.ints,
-                                         b.hh_pairs, b.jbuf, b.H, b.P, b.F, b.C, b.W1, b.W2, b.eps, b.diis, b.res,
-                                         sp, in_smem);
+                                         b.hh_pairs, b.jbuf, b.H, b.P, b.F, b.C, b.W1, b.W2, b.eps, b.diis,
+                                         b.rotbuf, b.res, sp, in_smem);
 }
 
 }  // namespace sgb
