@@ -136,6 +136,31 @@ int32_t sg_batch_calculate(const char* method, int32_t n_molecules, const int32_
                            int32_t max_scf_iterations, uint32_t properties, double* energies, double* gradients,
                            int32_t* iterations, int32_t* converged, char* error_message, int32_t error_capacity);
 
+/* ---- allocation-free single-molecule call ----
+ *
+ * No counterpart in the reference.  Energy (and gradient) of one closed-shell
+ * molecule with every device buffer in one fixed device array of
+ * SG_STATIC_SCRATCH_BYTES (per device context) and every host table in a
+ * fixed host array: the call performs no device or pinned allocation.
+ * Limits: SG_STATIC_MAX_ATOMS atoms and SG_STATIC_MAX_AOS AOs; larger
+ * molecules return SG_ERR_INVALID_ARGUMENT with a message.
+ * The first call on a device (with that device current) does a one-time
+ * set-up: it looks the scratch array up with cudaGetSymbolAddress, uploads
+ * the constant multipole tables and synchronises the stream; make that first
+ * call before any stream capture.  Calls that overlap in time share the
+ * scratch and race: serialise them.  stream is a cudaStream_t (NULL = the
+ * default stream); the call returns after the stream has been synchronised.
+ * Status codes as for sg_batch_results (SG_ERR_NOT_CONVERGED still fills the
+ * outputs). */
+#define SG_STATIC_MAX_ATOMS 64
+#define SG_STATIC_MAX_AOS 256
+#define SG_STATIC_SCRATCH_BYTES (13u * 1024u * 1024u)
+int32_t sg_calculate_static(const char* method, int32_t n_atoms, const int32_t* atomic_numbers,
+                            const double* xyz_bohr, int32_t charge, double self_consistence_criterion,
+                            double density_rmsd_criterion, int32_t max_scf_iterations, uint32_t properties,
+                            void* stream, double* energy, double* gradients, int32_t* iterations, int32_t* converged,
+                            char* error_message, int32_t error_capacity);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,6 +25,8 @@ _lib = None
 SG_PROP_ENERGY = 1
 SG_PROP_GRADIENTS = 2
 SG_ERR_NOT_CONVERGED = 6
+SG_STATIC_MAX_ATOMS = 64
+SG_STATIC_MAX_AOS = 256
 
 _D = ctypes.POINTER(ctypes.c_double)
 _I32 = ctypes.POINTER(ctypes.c_int32)
@@ -92,6 +94,9 @@ def lib():
         "sg_batch_calculate": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _I32, _D, _I32,
                                                 ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_uint32,
                                                 _D, _D, _I32, _I32, ctypes.c_char_p, ctypes.c_int32]),
+        "sg_calculate_static": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _D, ctypes.c_int32,
+                                                 ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_uint32,
+                                                 _VP, _D, _D, _I32, _I32, ctypes.c_char_p, ctypes.c_int32]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -394,3 +399,31 @@ def batch_calculate(method, molecules, charges=None, scc=1e-7, rmsd=1e-5, max_it
         raise SparrowError(rc, msg.value.decode())
     grads = np.split(g.reshape(-1, 3), np.cumsum(n_atoms)[:-1]) if g is not None else None
     return e, grads, it, conv.astype(bool)
+
+
+def calculate_static(method, atomic_numbers, xyz_bohr, charge=0, scc=1e-7, rmsd=1e-5, max_iter=100,
+                     gradients=False, stream=None):
+    """One molecule through the allocation-free entry point (sg_calculate_static).
+
+    All device scratch is a fixed array inside the library (at most
+    SG_STATIC_MAX_ATOMS atoms and SG_STATIC_MAX_AOS AOs); overlapping calls
+    race.  stream: an integer cudaStream_t handle or None for the default
+    stream.  Returns (energy, gradient (n, 3) or None, iterations, converged).
+    """
+    L = lib()
+    Z = np.ascontiguousarray(atomic_numbers, dtype=np.int32)
+    X = np.ascontiguousarray(xyz_bohr, dtype=np.float64).reshape(-1)
+    if X.size != 3 * Z.size:
+        raise ValueError("positions must have 3 entries per atom")
+    e = ctypes.c_double(0.0)
+    it = ctypes.c_int32(0)
+    conv = ctypes.c_int32(0)
+    g = np.zeros(3 * Z.size) if gradients else None
+    msg = ctypes.create_string_buffer(512)
+    props = SG_PROP_ENERGY | (SG_PROP_GRADIENTS if gradients else 0)
+    rc = L.sg_calculate_static(method.encode(), int(Z.size), _iptr(Z), _dptr(X), int(charge), scc, rmsd, max_iter,
+                               props, stream, ctypes.byref(e), _dptr(g) if g is not None else None,
+                               ctypes.byref(it), ctypes.byref(conv), msg, 512)
+    if rc != 0 and rc != SG_ERR_NOT_CONVERGED:
+        raise SparrowError(rc, msg.value.decode())
+    return e.value, (g.reshape(-1, 3) if g is not None else None), it.value, bool(conv.value)
