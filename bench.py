@@ -87,6 +87,35 @@ def cpu_rate(method, mols, target_seconds, procs, rng_seed=12345):
     return count / wall, count, wall, [r[1] for r in res]
 
 
+def plain_gpu_rate(method, mols, target_seconds=8.0, max_count=512, rng_seed=777):
+    """The plain GPU form: one molecule per launch sequence through the
+    Calculator surface (set_structure / calculate), host buffers in and out,
+    one molecule at a time, on a random sample of the batch."""
+    import numpy as np
+    import sparrow_b200
+    rng = np.random.default_rng(rng_seed)
+    order = rng.permutation(len(mols))[:max_count]
+    calc = sparrow_b200.get_calculator(method)
+    calc.settings["self_consistence_criterion"] = SCC
+    calc.settings["density_rmsd_criterion"] = RMSD
+    calc.settings["max_scf_iterations"] = MAX_ITER
+    calc.set_required_properties(["energy", "gradients"])
+    z, x = mols[order[0]]
+    calc.set_structure(z, x)
+    calc.calculate()  # warm-up: module load, pools
+    count, t0 = 0, time.perf_counter()
+    energies = []
+    for i in order:
+        z, x = mols[i]
+        calc.set_structure(z, x)
+        energies.append(calc.calculate().energy)
+        count += 1
+        if time.perf_counter() - t0 > target_seconds:
+            break
+    wall = time.perf_counter() - t0
+    return count / wall, count, wall
+
+
 def host_cores():
     try:
         return len(os.sched_getaffinity(0))
@@ -305,6 +334,15 @@ def run_engine(args, rank, world):
     h2d = hb
     d2h = 8 * args.molecules + 8 * 3 * n_atoms_total + 40 * args.molecules
 
+    # the plain one-molecule-per-launch GPU form on a sample of the same batch
+    plain = None
+    if rank == 0:
+        prate, pcount, pwall = plain_gpu_rate(args.method, mols)
+        plain = {"value": prate, "unit": "solves/s",
+                 "sample": "%d random molecules of the batch, one Calculator.calculate() each (host buffers, "
+                           "energy+gradient), %.1f s wall" % (pcount, pwall),
+                 "batched_device_over_plain": value / world / prate, "batched_e2e_over_plain": e2e_value / world / prate}
+
     # roofline of the SCF kernel (average launch)
     scf_ms = stage_sum[2] / args.steps
     flops = scf_flops(mols, it)
@@ -333,6 +371,7 @@ def run_engine(args, rank, world):
         "gpu_launches": int(launches),
         "roofline": roof,
         "cpu_baseline": cpu,
+        "plain_gpu": plain,
         "clocks": clk,
     }
     if rank == 0:
