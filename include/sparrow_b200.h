@@ -154,7 +154,7 @@ int32_t sg_batch_calculate(const char* method, int32_t n_molecules, const int32_
  * outputs). */
 #define SG_STATIC_MAX_ATOMS 64
 #define SG_STATIC_MAX_AOS 256
-#define SG_STATIC_SCRATCH_BYTES (13u * 1024u * 1024u)
+#define SG_STATIC_SCRATCH_BYTES (14u * 1024u * 1024u)
 int32_t sg_calculate_static(const char* method, int32_t n_atoms, const int32_t* atomic_numbers,
                             const double* xyz_bohr, int32_t charge, double self_consistence_criterion,
                             double density_rmsd_criterion, int32_t max_scf_iterations, uint32_t properties,

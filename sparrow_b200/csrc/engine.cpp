@@ -144,18 +144,19 @@ int Batch::ensure_arena(size_t bytes, std::string& err) {
 int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
   mols_.clear();
   atoms_.clear();
-  pairs_.clear();
+  npairs_ = 0;
+  nhh_ = 0;
   elems_.clear();
   ao_atom_.clear();
   order_.clear();
-  hh_pairs_.clear();
   density_given_ = false;
   if (in.empty()) {
     err = "empty batch";
     return kErrEmptyStructure;
   }
   // element slots
-  std::map<int, int> slot_of;
+  int slot_of[128];
+  for (int& v : slot_of) v = -1;
   for (const auto& m : in) {
     if (m.Z.empty()) {
       err = "molecule without atoms";
@@ -166,7 +167,11 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
       return kErrInvalidArgument;
     }
     for (int z : m.Z) {
-      if (slot_of.count(z)) continue;
+      if (z < 0 || z >= 128) {
+        err = "invalid atomic number " + std::to_string(z);
+        return kErrUnsupportedElement;
+      }
+      if (slot_of[z] >= 0) continue;
       ElemDev e;
       std::string why;
       if (!make_elem(method_, z, e, why)) {
@@ -203,12 +208,14 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
       return kErrInvalidArgument;
     }
     md.atom0 = (int)atoms_.size();
-    md.pair0 = (int)pairs_.size();
+    md.pair0 = (int)npairs_;
     md.ao_base = ao_base;
-    int nao = 0;
+    int nao = 0, heavy = 0;
     double ncore = 0;
+    long long s_sum = 0, s_sq = 0;  // integral block sizes per atom: 1 (s) or 10 (sp)
     for (int a = 0; a < md.nat; ++a) {
-      const ElemDev& e = elems_[slot_of[mol.Z[a]]];
+      const int slot = slot_of[mol.Z[a]];
+      const ElemDev& e = elems_[slot];
       AtomDev ad{};
       ad.x = mol.xyz[3 * a];
       ad.y = mol.xyz[3 * a + 1];
@@ -217,13 +224,17 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
         err = "non-finite position in molecule " + std::to_string(mi);
         return kErrInvalidArgument;
       }
-      ad.slot = slot_of[mol.Z[a]];
+      ad.slot = slot;
       ad.ao0 = nao;
       ad.mol = (int)mi;
       atoms_.push_back(ad);
       for (int k = 0; k < e.nao; ++k) ao_atom_.push_back(md.atom0 + a);
       nao += e.nao;
       ncore += e.core;
+      const int sz = e.nao == 1 ? 1 : 10;
+      s_sum += sz;
+      s_sq += sz * sz;
+      heavy += e.nao == 4 ? 1 : 0;
     }
     md.nao = nao;
     md.nel = (int)std::lround(ncore) - mol.charge;
@@ -237,31 +248,20 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
       err = "molecule " + std::to_string(mi) + " has more than 1024 AOs (batched SCF limit)";
       return kErrInvalidArgument;
     }
+    // pair p of the molecule is (lo, hi) in row-major order over lo < hi; its
+    // integral block follows the blocks of the earlier pairs (sizes 1 x 1,
+    // 1 x 10 or 10 x 10); the device builds the per-pair table
     md.int_off = int_off;
-    for (int a = 0; a < md.nat; ++a)
-      for (int b = a + 1; b < md.nat; ++b) {
-        const int na = elems_[atoms_[md.atom0 + a].slot].nao, nb = elems_[atoms_[md.atom0 + b].slot].nao;
-        PairDev pd{md.atom0 + a, md.atom0 + b, (int)mi, (int)int_off};
-        const double dx = mol.xyz[3 * b] - mol.xyz[3 * a], dy = mol.xyz[3 * b + 1] - mol.xyz[3 * a + 1],
-                     dz = mol.xyz[3 * b + 2] - mol.xyz[3 * a + 2];
-        if (dx * dx + dy * dy + dz * dz < 1e-12) {
-          err = "atoms " + std::to_string(a) + " and " + std::to_string(b) + " of molecule " + std::to_string(mi) +
-                " coincide";
-          return kErrInvalidArgument;
-        }
-        pairs_.push_back(pd);
-        int_off += (na == 1 ? 1 : 10) * (nb == 1 ? 1 : 10);
-        if (int_off > 2000000000LL) {
-          err = "batch too large: more than 2e9 two-centre integrals";
-          return kErrInvalidArgument;
-        }
-      }
-    md.npairs = (int)pairs_.size() - md.pair0;
-    md.hh0 = (int)hh_pairs_.size();
-    for (int k = md.pair0; k < md.pair0 + md.npairs; ++k)
-      if (elems_[atoms_[pairs_[k].a].slot].nao == 4 && elems_[atoms_[pairs_[k].b].slot].nao == 4)
-        hh_pairs_.push_back(k);
-    md.nhh = (int)hh_pairs_.size() - md.hh0;
+    md.npairs = md.nat * (md.nat - 1) / 2;
+    int_off += (s_sum * s_sum - s_sq) / 2;
+    if (int_off > 2000000000LL) {
+      err = "batch too large: more than 2e9 two-centre integrals";
+      return kErrInvalidArgument;
+    }
+    npairs_ += md.npairs;
+    md.hh0 = (int)nhh_;
+    md.nhh = heavy * (heavy - 1) / 2;
+    nhh_ += md.nhh;
     md.mat_off = mat_off;
     md.diis_off = diis_off;
     mat_off += (long long)nao * nao;
@@ -279,7 +279,7 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
   d.method = method_;
   d.nmol = (int)mols_.size();
   d.natoms = (int)atoms_.size();
-  d.npairs = (int)pairs_.size();
+  d.npairs = (int)npairs_;
   d.nao_total = ao_base;
   d.mat_total = mat_off;
   d.diis_total = diis_off;
@@ -293,16 +293,17 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
   };
   const size_t o_mols = take(sizeof(MolDev) * mols_.size());
   const size_t o_atoms = take(sizeof(AtomDev) * atoms_.size());
-  const size_t o_pairs = take(sizeof(PairDev) * std::max<size_t>(pairs_.size(), 1));
   const size_t o_elems = take(sizeof(ElemDev) * elems_.size());
   const size_t o_diat = take(sizeof(DiatomicDev) * diat_.size());
   const size_t o_ao = take(sizeof(int) * ao_atom_.size());
   const size_t o_order = take(sizeof(int) * order_.size());
-  const size_t o_hh = take(sizeof(int) * std::max<size_t>(hh_pairs_.size(), 1));
   const size_t upload_end = off;
+  const size_t o_pairs = take(sizeof(PairDev) * std::max<long long>(npairs_, 1));
+  const size_t o_hh = take(sizeof(int) * std::max<long long>(nhh_, 1));
   const size_t o_counter = take(sizeof(int));
+  const size_t o_flag = take(sizeof(int));
   const size_t o_ints = take(sizeof(double) * std::max<long long>(int_off, 1));
-  const size_t np = std::max<size_t>(pairs_.size(), 1);
+  const size_t np = (size_t)std::max<long long>(npairs_, 1);
   const size_t o_vcore = take(sizeof(double) * 20 * np);
   const size_t o_jbuf = take(sizeof(double) * 20 * np);
   const size_t o_ovl = take(sizeof(double) * 16 * np);
@@ -377,12 +378,10 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
   char* h = static_cast<char*>(pinned_);
   std::memcpy(h + o_mols, mols_.data(), sizeof(MolDev) * mols_.size());
   std::memcpy(h + o_atoms, atoms_.data(), sizeof(AtomDev) * atoms_.size());
-  if (!pairs_.empty()) std::memcpy(h + o_pairs, pairs_.data(), sizeof(PairDev) * pairs_.size());
   std::memcpy(h + o_elems, elems_.data(), sizeof(ElemDev) * elems_.size());
   std::memcpy(h + o_diat, diat_.data(), sizeof(DiatomicDev) * diat_.size());
   std::memcpy(h + o_ao, ao_atom_.data(), sizeof(int) * ao_atom_.size());
   std::memcpy(h + o_order, order_.data(), sizeof(int) * order_.size());
-  if (!hh_pairs_.empty()) std::memcpy(h + o_hh, hh_pairs_.data(), sizeof(int) * hh_pairs_.size());
   cudaError_t e = cudaMemcpyAsync(arena_, pinned_, upload_end, cudaMemcpyHostToDevice, stream_);
   if (e != cudaSuccess) {
     err = cuda_message(e);
@@ -391,9 +390,40 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
   h2d_bytes_ = (long long)upload_end;
   d2h_bytes_ = 0;
   e = cudaMemsetAsync(d.res, 0, sizeof(MolResult) * mols_.size(), stream_);
+  if (e == cudaSuccess) e = cudaMemsetAsync(base + o_flag, 0, sizeof(int), stream_);
   if (e != cudaSuccess) {
     err = cuda_message(e);
     return kErrCuda;
+  }
+  // pair and heavy-pair tables, built on the device; coincident atoms are
+  // reported through the flag (1 + global index of one offending pair)
+  int max_nat = 0;
+  for (const auto& m : mols_) max_nat = std::max(max_nat, m.nat);
+  launch_build_pairs(d, max_nat, reinterpret_cast<int*>(base + o_flag), stream_);
+  int bad = 0;
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, base + o_flag, sizeof(int), cudaMemcpyDeviceToHost, stream_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  if (bad > 0) {
+    const long long pidx = bad - 1;
+    size_t mi = 0;
+    while (mi + 1 < mols_.size() && mols_[mi + 1].pair0 <= pidx) ++mi;
+    const MolDev& m = mols_[mi];
+    long long p = pidx - m.pair0;
+    int lo = 0;
+    while (p >= m.nat - 1 - lo) {
+      p -= m.nat - 1 - lo;
+      ++lo;
+    }
+    const int hi = lo + 1 + (int)p;
+    err = "atoms " + std::to_string(lo) + " and " + std::to_string(hi) + " of molecule " + std::to_string(mi) +
+          " coincide";
+    mols_.clear();
+    return kErrInvalidArgument;
   }
   return kOk;
 }

@@ -89,10 +89,10 @@ class Batch {
   DeviceBatch dev_;
   std::vector<MolDev> mols_;
   std::vector<AtomDev> atoms_;
-  std::vector<PairDev> pairs_;
   std::vector<ElemDev> elems_;
   std::vector<DiatomicDev> diat_;
-  std::vector<int> ao_atom_, order_, hh_pairs_;
+  std::vector<int> ao_atom_, order_;
+  long long npairs_ = 0, nhh_ = 0;  // pair and heavy-pair tables are built on the device
   int scf_grid_ = 0;
   int scf_grid_nao_ = 0;
   int launches_ = 0;

@@ -8,6 +8,10 @@ namespace sgb {
 
 struct LocalTermTable;
 
+// Recorded Jacobi rotations per SCF CTA (device scratch): a cold start of up
+// to six sweeps fits without an intermediate replay for N <= 256.
+constexpr size_t kScfRotationBytesPerCta = size_t(2) << 20;
+
 // Device pointers of one batch (all inside one arena).
 struct DeviceBatch {
   int method = kPM6;
@@ -45,6 +49,9 @@ struct DeviceBatch {
 };
 
 void upload_local_terms(const LocalTermTable& tab, cudaStream_t stream);
+// Per-pair table (atoms, molecule, integral offset) and the heavy-pair list of
+// every molecule; flag receives 1 + the index of a pair of coincident atoms.
+void launch_build_pairs(const DeviceBatch& b, int max_nat, int* flag, cudaStream_t s);
 void launch_pair_values(const DeviceBatch& b, cudaStream_t s);
 void launch_one_electron(const DeviceBatch& b, cudaStream_t s);
 void launch_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s);

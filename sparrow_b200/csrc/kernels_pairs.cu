@@ -100,6 +100,79 @@ __global__ void k_gather_gradient(const MolDev* __restrict__ mols, const AtomDev
   for (int d = 0; d < 3; ++d) grad[(size_t)a * 3 + d] = g[d];
 }
 
+// One CTA per molecule.  Pair p of a molecule with n atoms is (lo, hi), lo <
+// hi, in row-major order: rowstart(l) = l n - l (l + 1) / 2 pairs precede row
+// l.  With block sizes c(a) = 1 (s atom) or 10 (sp atom), suffix sums
+// S(a) = sum_{h >= a} c(h) and R(l) = sum_{l' < l} c(l') S(l' + 1), the
+// integral block of (lo, hi) starts at R(lo) + c(lo) (S(lo + 1) - S(hi))
+// past the molecule's first block, the same order the integral kernel and
+// the oracle use.  Heavy pairs (both atoms sp) are listed in the same order.
+__global__ void __launch_bounds__(256) k_build_pairs(const MolDev* __restrict__ mols,
+                                                     const AtomDev* __restrict__ atoms,
+                                                     const ElemDev* __restrict__ elems, PairDev* __restrict__ pairs,
+                                                     int* __restrict__ hh_pairs, int* __restrict__ flag) {
+  extern __shared__ long long sm_pairs[];
+  const MolDev m = mols[blockIdx.x];
+  const int n = m.nat;
+  long long* R = sm_pairs;                              // [n]
+  int* S = reinterpret_cast<int*>(R + n);              // [n + 1]
+  int* heavy = S + n + 1;                              // [n]
+  __shared__ int nheavy;
+  if (threadIdx.x == 0) {
+    S[n] = 0;
+    for (int a = n - 1; a >= 0; --a) S[a] = S[a + 1] + (elems[atoms[m.atom0 + a].slot].nao == 1 ? 1 : 10);
+    long long r = 0;
+    int h = 0;
+    for (int a = 0; a < n; ++a) {
+      R[a] = r;
+      const int c = S[a] - S[a + 1];
+      r += (long long)c * S[a + 1];
+      if (c == 10) heavy[h++] = a;
+    }
+    nheavy = h;
+  }
+  __syncthreads();
+  const int np = m.npairs;
+  for (int p = threadIdx.x; p < np; p += blockDim.x) {
+    // largest lo with rowstart(lo) <= p
+    const double nn = n - 0.5;
+    int lo = (int)(nn - sqrt(fmax(nn * nn - 2.0 * p, 0.0)));
+    if (lo < 0) lo = 0;
+    while (lo > 0 && (long long)lo * n - (long long)lo * (lo + 1) / 2 > p) --lo;
+    while ((long long)(lo + 1) * n - (long long)(lo + 1) * (lo + 2) / 2 <= p) ++lo;
+    const int hi = p - (lo * n - lo * (lo + 1) / 2) + lo + 1;
+    const int c = S[lo] - S[lo + 1];
+    PairDev pd;
+    pd.a = m.atom0 + lo;
+    pd.b = m.atom0 + hi;
+    pd.mol = blockIdx.x;
+    pd.int_off = (int)(m.int_off + R[lo] + (long long)c * (S[lo + 1] - S[hi]));
+    pairs[m.pair0 + p] = pd;
+    const AtomDev A = atoms[pd.a], B = atoms[pd.b];
+    const double dx = B.x - A.x, dy = B.y - A.y, dz = B.z - A.z;
+    if (dx * dx + dy * dy + dz * dz < 1e-12) atomicCAS(flag, 0, m.pair0 + p + 1);
+  }
+  const int H = nheavy;
+  const int nhh = H * (H - 1) / 2;
+  for (int q = threadIdx.x; q < nhh; q += blockDim.x) {
+    const double hh = H - 0.5;
+    int i = (int)(hh - sqrt(fmax(hh * hh - 2.0 * q, 0.0)));
+    if (i < 0) i = 0;
+    while (i > 0 && i * H - i * (i + 1) / 2 > q) --i;
+    while ((i + 1) * H - (i + 1) * (i + 2) / 2 <= q) ++i;
+    const int j = q - (i * H - i * (i + 1) / 2) + i + 1;
+    const int lo = heavy[i], hi = heavy[j];
+    hh_pairs[m.hh0 + q] = m.pair0 + lo * n - lo * (lo + 1) / 2 + (hi - lo - 1);
+  }
+}
+
+void launch_build_pairs(const DeviceBatch& b, int max_nat, int* flag, cudaStream_t s) {
+  if (b.nmol == 0) return;
+  const size_t smem = sizeof(long long) * max_nat + sizeof(int) * (2 * (size_t)max_nat + 1);
+  cudaFuncSetAttribute(k_build_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_build_pairs<<<b.nmol, 256, smem, s>>>(b.mols, b.atoms, b.elems, b.pairs, b.hh_pairs, flag);
+}
+
 void launch_pair_values(const DeviceBatch& b, cudaStream_t s) {
   if (b.npairs == 0) return;
   int th = 128;

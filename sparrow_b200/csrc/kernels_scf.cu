@@ -36,9 +36,17 @@ namespace sgb {
 constexpr int kScfThreads = 512;
 constexpr int kGemmGroup = 256;       // threads per GEMM tile group
 constexpr int kJacobiMaxPairs = 512;  // supports N <= 1024
-constexpr int kGemmBM = 64, kGemmBN = 64, kGemmBK = 16;
-constexpr size_t kRotBudgetBytes = size_t(1) << 20;  // recorded Jacobi rotations per CTA
-constexpr int kGemmTileA = kGemmBK * (kGemmBM + 1), kGemmTileB = kGemmBK * (kGemmBN + 1);
+constexpr int kGemmBM = 64, kGemmBN = 64, kGemmBK = 8;
+constexpr size_t kRotBudgetBytes = kScfRotationBytesPerCta;
+// shared strides of the GEMM input tiles: k-contiguous rows of 8 (+4 pad) or
+// m/n-contiguous rows of 64 (+8 pad); one stage holds an A and a B tile
+constexpr int kGemmLdK = kGemmBK + 4, kGemmLdMN = kGemmBM + 8;
+constexpr int kGemmStage = 2 * (kGemmBM * kGemmLdK > kGemmBK * kGemmLdMN ? kGemmBM * kGemmLdK : kGemmBK * kGemmLdMN);
+// cp.async pipeline depth of the GEMM (stages in flight per tile group)
+#ifndef SGB_GEMM_STAGES
+#define SGB_GEMM_STAGES 3
+#endif
+constexpr int kGemmStages = SGB_GEMM_STAGES;
 
 // ---------------------------------------------------------------------------
 // CTA helpers
@@ -85,88 +93,115 @@ __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool v
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+template <int kPending>
+__device__ __forceinline__ void cp_async_wait_pending() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(kPending) : "memory");
+}
 
-// C = alpha * op(A) * op(B) + beta * C, row-major, op(X) = X or X^T.  The CTA
-// (512 threads) is split into two groups of 256 that work on different 64x64
-// output tiles; each thread accumulates a 4x4 register tile.  The 64x16 and
-// 16x64 input tiles are double-buffered in shared memory with cp.async so
-// the next k-slice streams in while the current one is multiplied.  smem
-// holds 2 groups x 2 stages x (kGemmTileA + kGemmTileB) doubles.
+// C = alpha * op(A) * op(B) + beta * C, row-major, op(X) = X or X^T, on the
+// FP64 tensor cores (mma.sync m8n8k4 f64).  The CTA (512 threads) is split
+// into two groups of 256 that work on different 64x64 output tiles; in a
+// group each of the 8 warps owns a 16x32 block (2 x 4 MMA tiles, 16
+// accumulators per thread).  The 64x8 / 8x64 input tiles stream through a
+// kGemmStages-deep cp.async ring in shared memory, so the global-load latency
+// of the next slices overlaps the MMAs of the current one.  Their layout follows the global one so the
+// copies stay coalesced: A row-major [m][k] (stride 12) or, when op(A) = A^T,
+// [k][m] (stride 72), and likewise for B; with these strides both the copies
+// and the fragment reads touch every bank twice (two wavefronts per warp).
+__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
 __device__ void cta_gemm(int M, int Nn, int K, double alpha, const double* __restrict__ A, int lda, bool tA,
                          const double* __restrict__ B, int ldb, bool tB, double beta, double* C, int ldc,
                          double* smem) {
   const int grp = threadIdx.x / kGemmGroup, tid = threadIdx.x % kGemmGroup;
-  double* base = smem + grp * 2 * (kGemmTileA + kGemmTileB);
-  const int tx = tid & 15, ty = tid >> 4;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int wm = warp >> 1, wn = warp & 1;
+  double* base = smem + grp * kGemmStages * kGemmStage;
   const int tilesM = (M + kGemmBM - 1) / kGemmBM, tilesN = (Nn + kGemmBN - 1) / kGemmBN;
   const int ntiles = tilesM * tilesN;
   const int nk = (K + kGemmBK - 1) / kGemmBK;
-  // the source address is only formed when in bounds; out-of-bounds slots copy 0 bytes from A/B
+  // shared strides of A(m, k) and B(k, n)
+  const int a_sm = tA ? 1 : kGemmLdK, a_sk = tA ? kGemmLdMN : 1;
+  const int b_sn = tB ? kGemmLdK : 1, b_sk = tB ? 1 : kGemmLdMN;
+  // the source address is only formed when in bounds; out-of-bounds slots copy 0 bytes
   auto load_stage = [&](int stage, int m0, int n0, int k0) {
-    double* smA = base + stage * (kGemmTileA + kGemmTileB);
-    double* smB = smA + kGemmTileA;
+    double* smA = base + stage * kGemmStage;
+    double* smB = smA + kGemmStage / 2;
 #pragma unroll
     for (int r = 0; r < (kGemmBM * kGemmBK) / kGemmGroup; ++r) {
       const int e = tid + r * kGemmGroup;
       int mm, kk;
-      if (!tA) { mm = e / kGemmBK; kk = e % kGemmBK; }
-      else { kk = e / kGemmBM; mm = e % kGemmBM; }
+      if (!tA) { mm = e >> 3; kk = e & 7; }
+      else { kk = e >> 6; mm = e & 63; }
       const int gm = m0 + mm, gk = k0 + kk;
       const bool ok = gm < M && gk < K;
       const double* src = ok ? (tA ? A + (size_t)gk * lda + gm : A + (size_t)gm * lda + gk) : A;
-      cp_async8(&smA[kk * (kGemmBM + 1) + mm], src, ok);
+      cp_async8(&smA[mm * a_sm + kk * a_sk], src, ok);
     }
 #pragma unroll
     for (int r = 0; r < (kGemmBK * kGemmBN) / kGemmGroup; ++r) {
       const int e = tid + r * kGemmGroup;
       int nn, kk;
-      if (!tB) { kk = e / kGemmBN; nn = e % kGemmBN; }
-      else { nn = e / kGemmBK; kk = e % kGemmBK; }
+      if (!tB) { kk = e >> 6; nn = e & 63; }
+      else { nn = e >> 3; kk = e & 7; }
       const int gn = n0 + nn, gk = k0 + kk;
       const bool ok = gn < Nn && gk < K;
       const double* src = ok ? (tB ? B + (size_t)gn * ldb + gk : B + (size_t)gk * ldb + gn) : B;
-      cp_async8(&smB[kk * (kGemmBN + 1) + nn], src, ok);
+      cp_async8(&smB[nn * b_sn + kk * b_sk], src, ok);
     }
     cp_async_commit();
   };
+  const int fr = lane >> 2, fc = lane & 3;  // fragment row / column-in-group
   for (int tile = grp; tile < ntiles; tile += 2) {
     const int m0 = (tile / tilesN) * kGemmBM, n0 = (tile % tilesN) * kGemmBN;
-    double acc[4][4];
+    double acc[2][4][2];
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = 0;
-    load_stage(0, m0, n0, 0);
+      for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+#pragma unroll
+    for (int st = 0; st < kGemmStages - 1; ++st) {
+      if (st < nk) load_stage(st, m0, n0, st * kGemmBK);
+      else cp_async_commit();  // empty group: keeps the group count per slice fixed
+    }
     for (int kt = 0; kt < nk; ++kt) {
-      cp_async_wait_all();
-      group_sync(grp);  // stage kt%2 visible; stage (kt+1)%2 no longer read
-      if (kt + 1 < nk) load_stage((kt + 1) & 1, m0, n0, (kt + 1) * kGemmBK);
-      const double* smA = base + (kt & 1) * (kGemmTileA + kGemmTileB);
-      const double* smB = smA + kGemmTileA;
+      cp_async_wait_pending<kGemmStages - 2>();
+      group_sync(grp);  // slice kt visible; the ring slot of slice kt-1 is no longer read
+      const int nxt = kt + kGemmStages - 1;
+      if (nxt < nk) load_stage(nxt % kGemmStages, m0, n0, nxt * kGemmBK);
+      else cp_async_commit();
+      const double* smA = base + (kt % kGemmStages) * kGemmStage;
+      const double* smB = smA + kGemmStage / 2;
 #pragma unroll
-      for (int kk = 0; kk < kGemmBK; ++kk) {
-        double a[4], b[4];
+      for (int ks = 0; ks < kGemmBK; ks += 4) {
+        double a[2], b[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) a[i] = smA[kk * (kGemmBM + 1) + ty * 4 + i];
+        for (int i = 0; i < 2; ++i) a[i] = smA[(wm * 16 + i * 8 + fr) * a_sm + (ks + fc) * a_sk];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) b[j] = smB[kk * (kGemmBN + 1) + tx + 16 * j];
+        for (int j = 0; j < 4; ++j) b[j] = smB[(wn * 32 + j * 8 + fr) * b_sn + (ks + fc) * b_sk];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < 2; ++i)
 #pragma unroll
-          for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+          for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
       }
     }
     group_sync(grp);  // all reads of the last stage done before the next tile overwrites it
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < 2; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int gm = m0 + ty * 4 + i, gn = n0 + tx + 16 * j;
-        if (gm < M && gn < Nn) {
-          double* c = &C[(size_t)gm * ldc + gn];
-          *c = beta == 0.0 ? alpha * acc[i][j] : alpha * acc[i][j] + beta * (*c);
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int gm = m0 + wm * 16 + i * 8 + fr, gn = n0 + wn * 32 + j * 8 + fc * 2 + h;
+          if (gm < M && gn < Nn) {
+            double* c = &C[(size_t)gm * ldc + gn];
+            *c = beta == 0.0 ? alpha * acc[i][j][h] : alpha * acc[i][j][h] + beta * (*c);
+          }
         }
-      }
   }
   __syncthreads();
 }
@@ -664,39 +699,61 @@ struct ScfShared {
   // phase scratch: GEMM stages, Fock-build warp buffers and Jacobi rotations
   // are never live at the same time
   union __align__(16) {
-    double gemm[4 * (kGemmTileA + kGemmTileB)];
+    double gemm[2 * kGemmStages * kGemmStage];
     double fockw[(kScfThreads / 32) * kFockWarpScratch];
     JacobiShared js;
   };
 };
 
 // Pulay DIIS: store (F, FP - PF) in the ring, extend the B matrix, solve.
-// Returns the extrapolated Fock matrix (F itself or dst).
+// Returns the extrapolated Fock matrix (F itself or dst).  The ring keeps the
+// error vectors E = FP - PF (antisymmetric) as their strict upper triangles
+// and the Fock matrices (symmetric) as their upper triangles, row by row:
+// half the traffic of full matrices, and the dot products <E_i, E_j> are
+// twice the upper-triangle sums (a common factor the extrapolation ignores).
+__device__ __forceinline__ int diis_row_e(int N, int i) { return i * (N - 1) - i * (i - 1) / 2; }
+__device__ __forceinline__ int diis_row_f(int N, int i) { return i * N - i * (i - 1) / 2; }
+
 __device__ const double* diis_step(int N, const double* F, const double* P, double* W, double* dst, double* histF,
                                    double* histE, int msize, int& nhist, int& head, ScfShared& sh) {
-  const size_t NN = (size_t)N * N;
-  const int tid = threadIdx.x;
-  cta_gemm(N, N, N, 1.0, F, N, false, P, N, false, 0.0, W, N, sh.gemm);
+  const int TE = N * (N - 1) / 2, TF = N * (N + 1) / 2;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  cta_gemm(N, N, N, 1.0, F, N, false, P, N, false, 0.0, W, N, sh.gemm);  // W = FP
   const int slot = head;
-  double* eS = histE + (size_t)slot * NN;
-  double* fS = histF + (size_t)slot * NN;
-  for (size_t k = tid; k < NN; k += blockDim.x) {
-    const int i = (int)(k / N), j = (int)(k % N);
-    eS[k] = W[k] - W[(size_t)j * N + i];
-    fS[k] = F[k];
-  }
-  __syncthreads();
   head = (head + 1) % msize;
   if (nhist < msize) ++nhist;
-  for (int j = 0; j < nhist; ++j) {
-    const double* eJ = histE + (size_t)j * NN;
-    double d = 0;
-    for (size_t k = tid; k < NN; k += blockDim.x) d += eS[k] * eJ[k];
-    d = cta_sum(d, sh.red);
-    if (tid == 0) {
-      sh.bmat[slot * kDiisMax + j] = d;
-      sh.bmat[j * kDiisMax + slot] = d;
+  double* eS = histE + (size_t)slot * TE;
+  double* fS = histF + (size_t)slot * TF;
+  // one pass over the upper triangle: store E = W - W^T and F, and accumulate
+  // <E, E_j> for every stored error vector j (the new one is E itself)
+  double d[kDiisMax];
+#pragma unroll
+  for (int j = 0; j < kDiisMax; ++j) d[j] = 0.0;
+  for (int i = warp; i < N; i += nwarps) {
+    const int re = diis_row_e(N, i) - i - 1, rf = diis_row_f(N, i) - i;
+    for (int c = i + lane; c < N; c += 32) {
+      fS[rf + c] = F[i * N + c];
+      if (c == i) continue;
+      const double e = W[i * N + c] - W[c * N + i];
+      eS[re + c] = e;
+#pragma unroll
+      for (int j = 0; j < kDiisMax; ++j)
+        if (j < nhist) d[j] += e * (j == slot ? e : histE[(size_t)j * TE + re + c]);
     }
+  }
+  // CTA reduction of the nhist dot products through the (idle) GEMM scratch
+  double* part = sh.gemm;
+#pragma unroll
+  for (int j = 0; j < kDiisMax; ++j) d[j] = warp_sum(d[j]);
+  if (lane == 0)
+#pragma unroll
+    for (int j = 0; j < kDiisMax; ++j) part[warp * kDiisMax + j] = d[j];
+  __syncthreads();
+  if (tid < nhist) {
+    double b = 0;
+    for (int w = 0; w < nwarps; ++w) b += part[w * kDiisMax + tid];
+    sh.bmat[slot * kDiisMax + tid] = b;
+    sh.bmat[tid * kDiisMax + slot] = b;
   }
   __syncthreads();
   if (nhist < 2) return F;
@@ -744,10 +801,15 @@ __device__ const double* diis_step(int N, const double* F, const double* P, doub
   }
   __syncthreads();
   if (!sh.diis_ok) return F;
-  for (size_t k = tid; k < NN; k += blockDim.x) {
-    double s = 0;
-    for (int i = 0; i < nhist; ++i) s += sh.coef[i] * histF[(size_t)i * NN + k];
-    dst[k] = s;
+  // F' = sum_i c_i F_i from the packed upper triangles, written to both halves
+  for (int i = warp; i < N; i += nwarps) {
+    const int rf = diis_row_f(N, i) - i;
+    for (int c = i + lane; c < N; c += 32) {
+      double v = 0;
+      for (int k = 0; k < nhist; ++k) v += sh.coef[k] * histF[(size_t)k * TF + rf + c];
+      dst[i * N + c] = v;
+      dst[c * N + i] = v;
+    }
   }
   __syncthreads();
   return dst;
@@ -834,30 +896,29 @@ __device__ int ov_rotation(int N, int no, double* F, double* Ct, double* W1, dou
   }
   xmax = cta_max(xmax, sh.red);
   if (xmax > 0.5) return 1;
-  // Yo = X^T X, Yv = X X^T (in W1); corrections into F: Do (no x N), Dv (nv x N)
-  double* Yo = W1;
-  double* Yv = W1 + (size_t)no * no;
-  double* Do = F;
-  double* Dv = F + (size_t)no * N;
-  cta_gemm(no, no, nv, 1.0, X, no, true, X, no, false, 0.0, Yo, no, sh.gemm);
-  cta_gemm(nv, nv, no, 1.0, X, no, false, X, no, true, 0.0, Yv, nv, sh.gemm);
-  // Ct_o' = Ct_o + X^T Ct_v - 1/2 Yo Ct_o ;  Ct_v' = Ct_v - X Ct_o - 1/2 Yv Ct_v
-  cta_gemm(no, N, nv, 1.0, X, no, true, Ct + (size_t)no * N, N, false, 0.0, Do, N, sh.gemm);
-  cta_gemm(no, N, no, -0.5, Yo, no, false, Ct, N, false, 1.0, Do, N, sh.gemm);
-  cta_gemm(nv, N, no, -1.0, X, no, false, Ct, N, false, 0.0, Dv, N, sh.gemm);
-  cta_gemm(nv, N, nv, -0.5, Yv, nv, false, Ct + (size_t)no * N, N, false, 1.0, Dv, N, sh.gemm);
-  for (size_t e = tid; e < NN; e += blockDim.x) Ct[e] += F[e];
+  // Ct <- M Ct with M = I + K + K^2/2, K = [[0, X^T], [-X, 0]] (orbital space):
+  //   M = [[I - X^T X / 2, X^T], [-X, I - X X^T / 2]], assembled in W1
+  cta_gemm(no, no, nv, -0.5, X, no, true, X, no, false, 0.0, W1, N, sh.gemm);
+  cta_gemm(nv, nv, no, -0.5, X, no, false, X, no, true, 0.0, W1 + (size_t)no * N + no, N, sh.gemm);
+  for (int e = tid; e < nv * no; e += blockDim.x) {
+    const int a = e / no, i = e % no;
+    W1[(size_t)i * N + no + a] = X[e];
+    W1[(size_t)(no + a) * N + i] = -X[e];
+  }
+  for (int k = tid; k < N; k += blockDim.x) W1[(size_t)k * N + k] += 1.0;
+  __syncthreads();
+  cta_gemm(N, N, N, 1.0, W1, N, false, Ct, N, false, 0.0, F, N, sh.gemm);
+  for (size_t e = tid; e < NN; e += blockDim.x) Ct[e] = F[e];
   __syncthreads();
   // the second-order rotation is orthogonal up to |K|^4 / 4: re-orthonormalise when needed
   drift += 0.25 * xmax * xmax * xmax * xmax;
   if (drift > 1e-12) {
     // S = Ct Ct^T, Ct <- (3/2 I - 1/2 S) Ct  (Newton-Schulz step for S^-1/2)
-    cta_gemm(N, N, N, 1.0, Ct, N, false, Ct, N, true, 0.0, W1, N, sh.gemm);
-    for (size_t e = tid; e < NN; e += blockDim.x) {
-      const int i = (int)(e / N), j = (int)(e % N);
-      W1[e] = (i == j ? 1.5 : 0.0) - 0.5 * W1[e];
-    }
+    for (size_t e = tid; e < NN; e += blockDim.x) W1[e] = 0.0;
     __syncthreads();
+    for (int k = tid; k < N; k += blockDim.x) W1[(size_t)k * N + k] = 1.5;
+    __syncthreads();
+    cta_gemm(N, N, N, -0.5, Ct, N, false, Ct, N, true, 1.0, W1, N, sh.gemm);
     cta_gemm(N, N, N, 1.0, W1, N, false, Ct, N, false, 0.0, W2, N, sh.gemm);
     for (size_t e = tid; e < NN; e += blockDim.x) Ct[e] = W2[e];
     __syncthreads();

@@ -76,7 +76,7 @@ constexpr StaticLayout static_layout(size_t nat, size_t npair, size_t nao, size_
   L.eps = off; off = al256(off + sizeof(double) * nao);
   L.diis = off; off = al256(off + sizeof(double) * 2 * kDiisMax * nao * nao);
   L.grad = off; off = al256(off + sizeof(double) * 3 * nat);
-  L.rot = off; off = al256(off + (size_t(1) << 20));  // recorded Jacobi rotations of the one SCF CTA
+  L.rot = off; off = al256(off + kScfRotationBytesPerCta);  // recorded Jacobi rotations of the one SCF CTA
   L.res = off; off = al256(off + sizeof(MolResult));
   L.total = off;
   return L;

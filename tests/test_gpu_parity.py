@@ -170,6 +170,33 @@ def test_host_side_errors():
     assert abs(res.energy - ref["energy"]) < E_TOL
 
 
+def test_coincident_atoms_are_rejected():
+    # the pair table is built on the device; a pair of coincident atoms in any
+    # molecule of a batch is reported with its molecule and atom indices
+    Z, xa = geometry.water_cluster(3, seed=2)
+    x = geometry.to_bohr(xa)
+    bad = x.copy()
+    bad[4] = bad[1]
+    with pytest.raises(sparrow_b200.SparrowError) as e:
+        sparrow_b200.batch_calculate("PM6", [(Z, x), (Z, bad)])
+    assert e.value.code == 1
+    assert "atoms 1 and 4 of molecule 1 coincide" in str(e.value)
+
+
+def test_pair_tables_for_mixed_molecules():
+    # molecules with H-only, heavy-only and mixed atom orders exercise every
+    # branch of the device-side pair and integral-offset construction
+    mols = [([1, 1], np.array([[0, 0, 0], [1.4, 0, 0.0]])),
+            ([6, 8], np.array([[0, 0, 0], [2.2, 0.1, 0.0]])),
+            ([1, 6, 1, 8, 1, 1], np.array([[0, 0, -2.0], [0, 0, 0], [1.9, 0, 0.4], [0, 2.3, 0], [-1.8, 0.3, 0.5],
+                                           [0.4, 3.9, 0.2]]))]
+    e, g, it, conv = sparrow_b200.batch_calculate("PM6", mols, rmsd=1e-8, scc=1e-9, gradients=True)
+    for i, (z, x) in enumerate(mols):
+        ref = O.scf("PM6", z, x, rmsd=1e-8, scc=1e-9)
+        assert abs(e[i] - ref["energy"]) < E_TOL
+        assert np.max(np.abs(g[i] - ref["gradient"])) < G_TOL
+
+
 def test_single_atom_and_positions_update():
     c, res = engine_single("PM6", [6], np.zeros((1, 3)))
     ref = O.scf("PM6", [6], np.zeros((1, 3)))
