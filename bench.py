@@ -48,6 +48,8 @@ def parse():
     p.add_argument("--method", default=METHOD)
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the cpu_baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-serving", action="store_true", help="skip the request-server latency leg")
+    p.add_argument("--serving-loads", default="250,500,1000,2000", help="offered loads (req/s) of the serving leg")
     return p.parse_args()
 
 
@@ -114,6 +116,91 @@ def plain_gpu_rate(method, mols, target_seconds=8.0, max_count=512, rng_seed=777
             break
     wall = time.perf_counter() - t0
     return count / wall, count, wall
+
+
+def serving_mix(count, seed=5):
+    """The serving request mix: alkanes C_nH_2n+2 (n ~ U[1,60]) or water
+    clusters (H2O)_n (n ~ U[2,64]), 70 % PM6 and 30 % AM1 (the engine's
+    second NDDO method stands in for the DFTB2 share until DFTB is served)."""
+    import numpy as np
+    from sparrow_b200 import geometry
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        if rng.random() < 0.5:
+            z, x = geometry.alkane(int(rng.integers(1, 61)), rng)
+        else:
+            z, x = geometry.water_cluster(int(rng.integers(2, 65)), seed=int(rng.integers(1 << 30)))
+        out.append((np.ascontiguousarray(z, dtype=np.int32), np.ascontiguousarray(geometry.to_bohr(x)).reshape(-1),
+                    "PM6" if rng.random() < 0.7 else "AM1"))
+    return out
+
+
+def serving_leg(loads=(250, 500, 1000, 2000), seconds=3.0, plain_count=48, seed=5):
+    """Open-loop Poisson arrivals into the request server at each offered load
+    (req/s) for `seconds`; latency = completion - submission, timed by the
+    server.  Beside it, the plain form: the same requests one at a time
+    through one Calculator (closed loop)."""
+    import threading
+    import numpy as np
+    import sparrow_b200
+    pool = serving_mix(2048, seed)
+    out = {"mix": "alkanes n~U[1,60] | (H2O)_n n~U[2,64], 70% PM6 / 30% AM1 (DFTB2 share served as AM1), "
+                  "energy+gradient, 3-384 AOs", "loads": []}
+    rng = np.random.default_rng(seed + 1)
+    with sparrow_b200.Server(device_budget_gb=64.0, slots=8, scc=SCC, rmsd=RMSD, max_iter=MAX_ITER) as srv:
+        # warm-up: every code path and the arena pools
+        for r in [srv.submit(m, z, x) for z, x, m in pool[:64]]:
+            srv.wait(r)
+        for lam in loads:
+            n = int(lam * seconds)
+            gaps = rng.exponential(1.0 / lam, size=n)
+            picks = rng.integers(0, len(pool), size=n)
+            ids = []
+            t0 = time.perf_counter()
+            t_next = t0
+            for k in range(n):
+                t_next += gaps[k]
+                dt = t_next - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                z, x, m = pool[picks[k]]
+                ids.append(srv.submit(m, z, x))
+            t_sub = time.perf_counter() - t0
+            lat = []
+            it = []
+            for r in ids:
+                res = srv.wait(r)
+                lat.append(res.latency_s)
+                it.append(res.iterations)
+            t_all = time.perf_counter() - t0
+            st = srv.stats()
+            lat = np.array(lat) * 1e3
+            out["loads"].append({"offered_rps": lam, "requests": n, "achieved_rps": n / t_all,
+                                 "submit_rps": n / t_sub, "p50_ms": float(np.percentile(lat, 50)),
+                                 "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+                                 "batches_so_far": st["batches"], "max_batch": st["max_batch"]})
+    # plain form: one request at a time through the Calculator surface
+    lat = []
+    calcs = {}
+    for k in range(plain_count):
+        z, x, m = pool[k]
+        c = calcs.get(m)
+        if c is None:
+            c = sparrow_b200.get_calculator(m)
+            c.settings["self_consistence_criterion"] = SCC
+            c.settings["density_rmsd_criterion"] = RMSD
+            c.settings["max_scf_iterations"] = MAX_ITER
+            c.set_required_properties(["energy", "gradients"])
+            calcs[m] = c
+        t0 = time.perf_counter()
+        c.set_structure(z, x)
+        c.calculate()
+        lat.append(time.perf_counter() - t0)
+    lat = np.array(lat[2:]) * 1e3
+    out["plain_gpu"] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                        "throughput_rps": 1e3 / float(lat.mean()), "requests": int(lat.size)}
+    return out
 
 
 def host_cores():
@@ -343,6 +430,10 @@ def run_engine(args, rank, world):
                            "energy+gradient), %.1f s wall" % (pcount, pwall),
                  "batched_device_over_plain": value / world / prate, "batched_e2e_over_plain": e2e_value / world / prate}
 
+    serving = None
+    if rank == 0 and not args.no_serving:
+        serving = serving_leg(loads=tuple(float(v) for v in args.serving_loads.split(",")))
+
     # roofline of the SCF kernel (average launch)
     scf_ms = stage_sum[2] / args.steps
     flops = scf_flops(mols, it)
@@ -372,6 +463,7 @@ def run_engine(args, rank, world):
         "roofline": roof,
         "cpu_baseline": cpu,
         "plain_gpu": plain,
+        "serving": serving,
         "clocks": clk,
     }
     if rank == 0:

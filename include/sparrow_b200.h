@@ -48,6 +48,8 @@ extern "C" {
 #define SG_ERR_NO_RESULTS 9
 #define SG_ERR_UNKNOWN_SETTING 10
 #define SG_ERR_DEVICE 11
+#define SG_ERR_TIMEOUT 12
+#define SG_PENDING 13 /* sg_server_poll: the request is still in flight */
 
 /* required-property mask */
 #define SG_PROP_ENERGY 1u
@@ -135,6 +137,40 @@ int32_t sg_batch_calculate(const char* method, int32_t n_molecules, const int32_
                            double self_consistence_criterion, double density_rmsd_criterion,
                            int32_t max_scf_iterations, uint32_t properties, double* energies, double* gradients,
                            int32_t* iterations, int32_t* converged, char* error_message, int32_t error_capacity);
+
+/* ---- request server: continuous batching on one GPU ----
+ *
+ * No counterpart in the reference (its callers loop over Calculator
+ * instances).  A worker thread keeps up to `slots` batches in flight, each on
+ * its own stream; free slots are refilled at once with the oldest pending
+ * requests of one method, admitted while the estimated device memory of all
+ * in-flight batches stays within device_budget_bytes.  Submission validates
+ * the request (elements, electron count, coincident atoms) and returns its
+ * error at once.  Every function is thread-safe; destroy waits for the
+ * requests in flight. */
+typedef struct sg_server sg_server;
+int32_t sg_server_create(uint64_t device_budget_bytes, int32_t slots, int32_t max_batch,
+                         double self_consistence_criterion, double density_rmsd_criterion,
+                         int32_t max_scf_iterations, sg_server** out);
+void sg_server_destroy(sg_server* s);
+/* thread-local text of the last error of a server call on this thread */
+const char* sg_server_last_error(void);
+int32_t sg_server_submit(sg_server* s, const char* method, int32_t n_atoms, const int32_t* atomic_numbers,
+                         const double* xyz_bohr, int32_t charge, uint32_t properties, int64_t* request_id);
+/* Wait up to timeout_s (< 0: forever) for a request.  Returns SG_OK when the
+ * request is finished (its own status in *status: SG_OK, SG_ERR_NOT_CONVERGED
+ * with results, or an error), SG_ERR_TIMEOUT, or SG_ERR_INVALID_ARGUMENT for
+ * an unknown id.  gradients (3 * n_atoms) is written when requested and
+ * non-NULL; latency_s = completion - submission (seconds). */
+int32_t sg_server_wait(sg_server* s, int64_t request_id, double timeout_s, double* energy, double* gradients,
+                       int32_t* iterations, int32_t* status, double* latency_s);
+/* As sg_server_wait without blocking: SG_PENDING while in flight. */
+int32_t sg_server_poll(sg_server* s, int64_t request_id, double* energy, double* gradients, int32_t* iterations,
+                       int32_t* status, double* latency_s);
+/* Block until every submitted request has finished. */
+int32_t sg_server_drain(sg_server* s);
+/* counters: submitted, completed, batches launched, largest batch */
+int32_t sg_server_stats(sg_server* s, int64_t* submitted, int64_t* completed, int64_t* batches, int64_t* max_batch);
 
 /* ---- allocation-free single-molecule call ----
  *

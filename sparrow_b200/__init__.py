@@ -25,6 +25,8 @@ _lib = None
 SG_PROP_ENERGY = 1
 SG_PROP_GRADIENTS = 2
 SG_ERR_NOT_CONVERGED = 6
+SG_ERR_TIMEOUT = 12
+SG_PENDING = 13
 SG_STATIC_MAX_ATOMS = 64
 SG_STATIC_MAX_AOS = 256
 
@@ -94,6 +96,16 @@ def lib():
         "sg_batch_calculate": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _I32, _D, _I32,
                                                 ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_uint32,
                                                 _D, _D, _I32, _I32, ctypes.c_char_p, ctypes.c_int32]),
+        "sg_server_create": (ctypes.c_int32, [ctypes.c_uint64, ctypes.c_int32, ctypes.c_int32, ctypes.c_double,
+                                              ctypes.c_double, ctypes.c_int32, ctypes.POINTER(_VP)]),
+        "sg_server_destroy": (None, [_VP]),
+        "sg_server_last_error": (ctypes.c_char_p, []),
+        "sg_server_submit": (ctypes.c_int32, [_VP, ctypes.c_char_p, ctypes.c_int32, _I32, _D, ctypes.c_int32,
+                                              ctypes.c_uint32, ctypes.POINTER(ctypes.c_int64)]),
+        "sg_server_wait": (ctypes.c_int32, [_VP, ctypes.c_int64, ctypes.c_double, _D, _D, _I32, _I32, _D]),
+        "sg_server_poll": (ctypes.c_int32, [_VP, ctypes.c_int64, _D, _D, _I32, _I32, _D]),
+        "sg_server_drain": (ctypes.c_int32, [_VP]),
+        "sg_server_stats": (ctypes.c_int32, [_VP] + [ctypes.POINTER(ctypes.c_int64)] * 4),
         "sg_calculate_static": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _D, ctypes.c_int32,
                                                  ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_uint32,
                                                  _VP, _D, _D, _I32, _I32, ctypes.c_char_p, ctypes.c_int32]),
@@ -427,3 +439,99 @@ def calculate_static(method, atomic_numbers, xyz_bohr, charge=0, scc=1e-7, rmsd=
     if rc != 0 and rc != SG_ERR_NOT_CONVERGED:
         raise SparrowError(rc, msg.value.decode())
     return e.value, (g.reshape(-1, 3) if g is not None else None), it.value, bool(conv.value)
+
+
+class ServerResult:
+    """Result of one served request: energy (Hartree), gradients ((n, 3)
+    Hartree/bohr or None), iterations, status (0, or 6 = not converged with
+    results), latency_s (completion - submission)."""
+
+    def __init__(self, energy, gradients, iterations, status, latency_s):
+        self.energy = energy
+        self.gradients = gradients
+        self.iterations = iterations
+        self.status = status
+        self.latency_s = latency_s
+
+    @property
+    def successful_calculation(self):
+        return self.status == 0
+
+
+class Server:
+    """Continuous-batching request server on the current GPU (sg_server_*).
+
+    submit() queues a single point (and gradient); requests that arrive while
+    others run are admitted into free batch slots as memory allows."""
+
+    def __init__(self, device_budget_gb=16.0, slots=2, max_batch=4096, scc=1e-7, rmsd=1e-5, max_iter=100):
+        h = _VP()
+        rc = lib().sg_server_create(int(device_budget_gb * 1e9), slots, max_batch, scc, rmsd, max_iter,
+                                    ctypes.byref(h))
+        if rc != 0:
+            raise SparrowError(rc, lib().sg_server_last_error().decode())
+        self._h = h
+        self._req = {}
+
+    def submit(self, method, atomic_numbers, xyz_bohr, charge=0, gradients=True):
+        Z = np.ascontiguousarray(atomic_numbers, dtype=np.int32)
+        X = np.ascontiguousarray(xyz_bohr, dtype=np.float64).reshape(-1)
+        rid = ctypes.c_int64()
+        props = SG_PROP_ENERGY | (SG_PROP_GRADIENTS if gradients else 0)
+        rc = lib().sg_server_submit(self._h, method.encode(), int(Z.size), _iptr(Z), _dptr(X), int(charge), props,
+                                    ctypes.byref(rid))
+        if rc != 0:
+            raise SparrowError(rc, lib().sg_server_last_error().decode())
+        self._req[rid.value] = (int(Z.size), gradients)
+        return rid.value
+
+    def _result(self, rid, fn, *args):
+        n, grads = self._req[rid]
+        e = ctypes.c_double()
+        it = ctypes.c_int32()
+        st = ctypes.c_int32()
+        lat = ctypes.c_double()
+        g = np.zeros(3 * n) if grads else None
+        rc = fn(self._h, rid, *args, ctypes.byref(e), _dptr(g) if g is not None else None, ctypes.byref(it),
+                ctypes.byref(st), ctypes.byref(lat))
+        if rc in (SG_PENDING, SG_ERR_TIMEOUT):
+            return None
+        if rc != 0:
+            raise SparrowError(rc, lib().sg_server_last_error().decode())
+        del self._req[rid]
+        if st.value not in (0, SG_ERR_NOT_CONVERGED):
+            raise SparrowError(st.value, lib().sg_server_last_error().decode())
+        return ServerResult(e.value, g.reshape(-1, 3) if g is not None else None, it.value, st.value, lat.value)
+
+    def wait(self, rid, timeout=None):
+        """Block until request rid is done (None on timeout)."""
+        return self._result(rid, lib().sg_server_wait, -1.0 if timeout is None else float(timeout))
+
+    def poll(self, rid):
+        """The result of request rid, or None while it is in flight."""
+        return self._result(rid, lib().sg_server_poll)
+
+    def drain(self):
+        lib().sg_server_drain(self._h)
+
+    def stats(self):
+        v = [ctypes.c_int64() for _ in range(4)]
+        lib().sg_server_stats(self._h, *[ctypes.byref(x) for x in v])
+        return dict(zip(("submitted", "completed", "batches", "max_batch"), (x.value for x in v)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().sg_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -14,6 +14,7 @@
 #include "../../include/sparrow_b200.h"
 #include "engine.h"
 #include "params.h"
+#include "server.h"
 
 namespace sgb {
 
@@ -518,6 +519,121 @@ int32_t sg_batch_calculate(const char* method, int32_t n_mol, const int32_t* n_a
     errmsg[errcap - 1] = 0;
   }
   return rc;
+}
+
+struct sg_server {
+  std::unique_ptr<sgb::Server> impl;
+};
+
+namespace {
+thread_local std::string g_server_error;
+
+int32_t server_result(const sgb::ServerResult& r, double* energy, double* gradients, int32_t* iterations,
+                      int32_t* status, double* latency_s) {
+  if (energy) *energy = r.energy;
+  if (gradients && !r.gradient.empty()) std::memcpy(gradients, r.gradient.data(), sizeof(double) * r.gradient.size());
+  if (iterations) *iterations = r.iterations;
+  if (status) *status = r.status;
+  if (latency_s) *latency_s = r.t_done - r.t_submit;
+  g_server_error = r.error;
+  return SG_OK;
+}
+}  // namespace
+
+int32_t sg_server_create(uint64_t budget, int32_t slots, int32_t max_batch, double scc, double rmsd, int32_t max_iter,
+                         sg_server** out) {
+  if (!out) return SG_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (!(scc > 0) || !(rmsd > 0) || max_iter < 1 || slots < 1 || max_batch < 1) {
+    g_server_error = "server settings must be positive";
+    return SG_ERR_INVALID_ARGUMENT;
+  }
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    g_server_error = "no CUDA device";
+    return SG_ERR_CUDA;
+  }
+  sgb::ScfParams sp;
+  sp.scc = scc;
+  sp.rmsd = rmsd;
+  sp.max_iter = max_iter;
+  auto* s = new sg_server;
+  s->impl.reset(new sgb::Server((size_t)budget, slots, max_batch, sp));
+  *out = s;
+  return SG_OK;
+}
+
+void sg_server_destroy(sg_server* s) { delete s; }
+
+const char* sg_server_last_error(void) { return g_server_error.c_str(); }
+
+int32_t sg_server_submit(sg_server* s, const char* method, int32_t n, const int32_t* Z, const double* xyz,
+                         int32_t charge, uint32_t props, int64_t* id) {
+  if (!s || !id) return SG_ERR_INVALID_ARGUMENT;
+  sgb::Method m;
+  if (!method || !sgb::parse_method(method, m)) {
+    g_server_error = std::string("unknown method '") + (method ? method : "") + "'";
+    return SG_ERR_UNKNOWN_METHOD;
+  }
+  if (n <= 0 || !Z || !xyz) {
+    g_server_error = "empty molecular structure";
+    return SG_ERR_EMPTY_STRUCTURE;
+  }
+  sgb::MoleculeInput mol;
+  mol.Z.assign(Z, Z + n);
+  mol.xyz.assign(xyz, xyz + 3 * (size_t)n);
+  mol.charge = charge;
+  std::string err;
+  const long long r = s->impl->submit(m, std::move(mol), (props & SG_PROP_GRADIENTS) != 0, err);
+  if (r < 0) {
+    g_server_error = err;
+    return (int32_t)(-r);
+  }
+  *id = r;
+  return SG_OK;
+}
+
+int32_t sg_server_wait(sg_server* s, int64_t id, double timeout_s, double* energy, double* gradients,
+                       int32_t* iterations, int32_t* status, double* latency_s) {
+  if (!s) return SG_ERR_INVALID_ARGUMENT;
+  sgb::ServerResult r;
+  const int rc = s->impl->wait(id, r, timeout_s);
+  if (rc == 1) return SG_ERR_TIMEOUT;
+  if (rc != 0) {
+    g_server_error = "unknown request id";
+    return SG_ERR_INVALID_ARGUMENT;
+  }
+  return server_result(r, energy, gradients, iterations, status, latency_s);
+}
+
+int32_t sg_server_poll(sg_server* s, int64_t id, double* energy, double* gradients, int32_t* iterations,
+                       int32_t* status, double* latency_s) {
+  if (!s) return SG_ERR_INVALID_ARGUMENT;
+  sgb::ServerResult r;
+  const int rc = s->impl->poll(id, r);
+  if (rc == 1) return SG_PENDING;
+  if (rc != 0) {
+    g_server_error = "unknown request id";
+    return SG_ERR_INVALID_ARGUMENT;
+  }
+  return server_result(r, energy, gradients, iterations, status, latency_s);
+}
+
+int32_t sg_server_drain(sg_server* s) {
+  if (!s) return SG_ERR_INVALID_ARGUMENT;
+  s->impl->drain();
+  return SG_OK;
+}
+
+int32_t sg_server_stats(sg_server* s, int64_t* submitted, int64_t* completed, int64_t* batches, int64_t* max_batch) {
+  if (!s) return SG_ERR_INVALID_ARGUMENT;
+  const sgb::ServerStats st = s->impl->stats();
+  if (submitted) *submitted = st.submitted;
+  if (completed) *completed = st.completed;
+  if (batches) *batches = st.batches;
+  if (max_batch) *max_batch = st.max_batch;
+  return SG_OK;
 }
 
 }  // extern "C"

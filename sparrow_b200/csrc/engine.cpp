@@ -141,7 +141,7 @@ int Batch::ensure_arena(size_t bytes, std::string& err) {
   return kOk;
 }
 
-int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
+int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool check_pairs) {
   mols_.clear();
   atoms_.clear();
   npairs_ = 0;
@@ -400,8 +400,15 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err) {
   int max_nat = 0;
   for (const auto& m : mols_) max_nat = std::max(max_nat, m.nat);
   launch_build_pairs(d, max_nat, reinterpret_cast<int*>(base + o_flag), stream_);
-  int bad = 0;
   e = cudaGetLastError();
+  if (!check_pairs) {
+    if (e != cudaSuccess) {
+      err = cuda_message(e);
+      return kErrCuda;
+    }
+    return kOk;
+  }
+  int bad = 0;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, base + o_flag, sizeof(int), cudaMemcpyDeviceToHost, stream_);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
   if (e != cudaSuccess) {

@@ -37,6 +37,8 @@ enum Status : int {
   kErrNoResults = 9,
   kErrUnknownSetting = 10,
   kErrDevice = 11,
+  kErrTimeout = 12,
+  kPending = 13,
 };
 
 // A batch resident on the device: descriptors, integrals, matrices, results.
@@ -48,7 +50,10 @@ class Batch {
   Batch& operator=(const Batch&) = delete;
 
   // Host-side setup and upload of a set of molecules.  Returns a Status.
-  int setup(const std::vector<MoleculeInput>& mols, std::string& err);
+  // check_pairs: wait for the device-built pair table and report coincident
+  // atoms as an error (a caller that validated the geometries itself, like
+  // the request server, passes false and setup does not block).
+  int setup(const std::vector<MoleculeInput>& mols, std::string& err, bool check_pairs = true);
   // Replace positions (same atoms, same order) and upload them.
   int set_positions(const double* xyz_bohr_all, std::string& err);
   // Optional start densities (one N x N matrix per molecule, concatenated).
@@ -62,6 +67,7 @@ class Batch {
   int fetch_orbital_energies(int mol, std::vector<double>& eps, std::string& err);
 
   cudaStream_t stream() const { return stream_; }
+  Method method() const { return method_; }
   int n_molecules() const { return (int)mols_.size(); }
   int n_atoms() const { return (int)atoms_.size(); }
   long long device_bytes() const { return arena_bytes_; }
