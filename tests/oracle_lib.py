@@ -144,3 +144,76 @@ def charge_separations(ns, np_, zs, zp):
     out = np.zeros(2)
     lib().oracle_charge_separations(ns, np_, zs, zp, out.ctypes.data_as(_D))
     return out
+
+
+# ---------------------------------------------------------------------------
+# DFTB2 / DFTB3 oracle (oracle/liboracle_dftb.so)
+# ---------------------------------------------------------------------------
+LIB_DFTB = os.path.join(ROOT, "oracle", "liboracle_dftb.so")
+_dlib = None
+
+
+def dftb_lib():
+    global _dlib
+    if _dlib is None:
+        if not os.path.exists(LIB_DFTB):
+            subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+        L = ctypes.CDLL(LIB_DFTB)
+        L.dftb_oracle_last_error.restype = ctypes.c_char_p
+        L.dftb_oracle_scf.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _I, _D, ctypes.c_int,
+                                      ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D, _D, _D,
+                                      ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+        L.dftb_oracle_matrices.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _I, _D, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _I]
+        _dlib = L
+    return _dlib
+
+
+DFTB_DEFAULT_SET = {2: "mio-1-1", 3: "3ob-3-1"}
+
+
+def dftb_scf(order, Z, xyz_bohr, charge=0, parameters=None, scc=1e-7, rmsd=1e-8, max_iter=1000, gradient=True,
+             want_density=False):
+    """Converged restricted DFTB2/DFTB3: dict(energy, gradient, e_el, e_rep, iterations, converged, nao, nocc,
+    charges, eps[, P])."""
+    Z, x = _arr(Z, xyz_bohr)
+    n = len(Z)
+    params = parameters or DFTB_DEFAULT_SET[order]
+    e = ctypes.c_double()
+    g = np.zeros(x.size)
+    info = np.zeros(8)
+    q = np.zeros(n)
+    eps = np.zeros(4 * n)
+    P = np.zeros(16 * n * n) if want_density else None
+    rc = dftb_lib().dftb_oracle_scf(params.encode(), order, n, Z.ctypes.data_as(_I), x.ctypes.data_as(_D),
+                                    int(charge), scc, rmsd, max_iter, 1 if gradient else 0, ctypes.byref(e),
+                                    g.ctypes.data_as(_D), info.ctypes.data_as(_D), q.ctypes.data, eps.ctypes.data,
+                                    P.ctypes.data if P is not None else None)
+    if rc not in (0, 3):
+        raise RuntimeError(dftb_lib().dftb_oracle_last_error().decode())
+    nao = int(info[4])
+    out = dict(energy=e.value, gradient=g.reshape(-1, 3), e_el=info[0], e_rep=info[1], iterations=int(info[2]),
+               converged=bool(info[3]), nao=nao, nocc=int(info[5]), charges=q, eps=eps[:nao])
+    if P is not None:
+        out["P"] = P[:nao * nao].reshape(nao, nao)
+    return out
+
+
+def dftb_matrices(order, Z, xyz_bohr, parameters=None):
+    """H0, S (N x N), gamma (nat x nat) and Gamma (nat x nat, DFTB3) at a geometry."""
+    Z, x = _arr(Z, xyz_bohr)
+    n = len(Z)
+    params = parameters or DFTB_DEFAULT_SET[order]
+    N = 4 * n
+    H0 = np.zeros(N * N)
+    S = np.zeros(N * N)
+    gam = np.zeros(n * n)
+    Gam = np.zeros(n * n)
+    nao = ctypes.c_int()
+    rc = dftb_lib().dftb_oracle_matrices(params.encode(), order, n, Z.ctypes.data_as(_I), x.ctypes.data_as(_D),
+                                         H0.ctypes.data, S.ctypes.data, gam.ctypes.data, Gam.ctypes.data,
+                                         ctypes.byref(nao))
+    if rc != 0:
+        raise RuntimeError(dftb_lib().dftb_oracle_last_error().decode())
+    N = nao.value
+    return H0[:N * N].reshape(N, N), S[:N * N].reshape(N, N), gam.reshape(n, n), Gam.reshape(n, n)
