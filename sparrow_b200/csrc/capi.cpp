@@ -18,6 +18,19 @@
 
 namespace sgb {
 
+// "METHOD" or, for DFTB, "METHOD:parameter-set" (e.g. "DFTB3:3ob-2-1").
+bool parse_method_spec(const char* spec, Method& m, std::string& set) {
+  std::string s(spec);
+  const size_t c = s.find(':');
+  set.clear();
+  if (c != std::string::npos) {
+    set = s.substr(c + 1);
+    s = s.substr(0, c);
+  }
+  if (!parse_method(s, m)) return false;
+  return set.empty() || is_dftb(m);
+}
+
 struct Settings {
   int charge = 0;
   int multiplicity = 1;
@@ -65,8 +78,11 @@ class Calculator {
       error = "empty molecular structure";
       return kErrEmptyStructure;
     }
-    if (!settings_.parameters.empty()) {
-      error = "method_parameters: only the embedded parameter sets are available";
+    if (is_dftb(method_)) {
+      // DFTB: the setting names an embedded Slater-Koster set (empty = the method's default)
+      batch_->set_dftb_parameters(settings_.parameters);
+    } else if (!settings_.parameters.empty()) {
+      error = "method_parameters: only the embedded NDDO parameters are available";
       return kErrInvalidArgument;
     }
     if (settings_.multiplicity != 1 || settings_.spin_mode == "unrestricted") {
@@ -390,7 +406,8 @@ int32_t sg_batch_create(const char* method, int32_t n_mol, const int32_t* n_atom
   if (!out) return SG_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   Method m;
-  if (!method || !parse_method(method, m)) {
+  std::string set;
+  if (!method || !parse_method_spec(method, m, set)) {
     g_create_error = "unknown method";
     return SG_ERR_UNKNOWN_METHOD;
   }
@@ -402,6 +419,7 @@ int32_t sg_batch_create(const char* method, int32_t n_mol, const int32_t* n_atom
   }
   std::unique_ptr<sg_batch> b(new sg_batch);
   b->impl.reset(new Batch(m));
+  b->impl->set_dftb_parameters(set);
   int rc = b->impl->setup(mols, err);
   if (rc) {
     g_create_error = err;
@@ -572,8 +590,9 @@ int32_t sg_server_submit(sg_server* s, const char* method, int32_t n, const int3
                          int32_t charge, uint32_t props, int64_t* id) {
   if (!s || !id) return SG_ERR_INVALID_ARGUMENT;
   sgb::Method m;
-  if (!method || !sgb::parse_method(method, m)) {
-    g_server_error = std::string("unknown method '") + (method ? method : "") + "'";
+  std::string set;
+  if (!method || !sgb::parse_method_spec(method, m, set) || !set.empty()) {
+    g_server_error = std::string("unknown method '") + (method ? method : "") + "' (the server uses the default sets)";
     return SG_ERR_UNKNOWN_METHOD;
   }
   if (n <= 0 || !Z || !xyz) {

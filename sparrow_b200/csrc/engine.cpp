@@ -8,6 +8,7 @@
 
 #include "nddo_math.cuh"
 #include "params.h"
+#include "dftb_params.h"
 
 namespace sgb {
 
@@ -174,7 +175,18 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
       if (slot_of[z] >= 0) continue;
       ElemDev e;
       std::string why;
-      if (!make_elem(method_, z, e, why)) {
+      if (is_dftb(method_)) {
+        // DFTB: orbitals and core charge from the parameter set (records built below)
+        const char* set = dftb_set_.empty() ? dftb_default_set(method_) : dftb_set_.c_str();
+        e = ElemDev();
+        e.Z = z;
+        e.nao = dftb_n_aos(set, z);
+        e.core = dftb_core_charge(set, z);
+        if (e.nao == 0 || e.core < 0) {
+          err = std::string("no ") + set + " s/p parameters for element Z=" + std::to_string(z);
+          return kErrUnsupportedElement;
+        }
+      } else if (!make_elem(method_, z, e, why)) {
         err = why;
         return kErrUnsupportedElement;
       }
@@ -187,7 +199,14 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
     }
   }
   diat_.assign(kMaxElementSlots * kMaxElementSlots, DiatomicDev());
-  for (size_t i = 0; i < elems_.size(); ++i)
+  DftbPrepared dftb;
+  if (is_dftb(method_)) {
+    std::vector<int> zs;
+    for (const auto& e : elems_) zs.push_back(e.Z);
+    const std::string set = dftb_set_.empty() ? dftb_default_set(method_) : dftb_set_;
+    if (!dftb_prepare(set, method_ == kDFTB3 ? 3 : 2, zs, dftb, err)) return kErrUnsupportedElement;
+  }
+  for (size_t i = 0; i < elems_.size() && !is_dftb(method_); ++i)
     for (size_t j = 0; j < elems_.size(); ++j) {
       DiatomicDev d = make_diatomic(method_, elems_[i].Z, elems_[j].Z);
       if (method_ == kPM6 && !d.present) {
@@ -197,7 +216,7 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
       }
       diat_[i * kMaxElementSlots + j] = d;
     }
-  long long int_off = 0, mat_off = 0, diis_off = 0;
+  long long int_off = 0, mat_off = 0, diis_off = 0, gam_off = 0;
   int ao_base = 0, max_nao = 0;
   for (size_t mi = 0; mi < in.size(); ++mi) {
     const auto& mol = in[mi];
@@ -264,6 +283,8 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
     nhh_ += md.nhh;
     md.mat_off = mat_off;
     md.diis_off = diis_off;
+    md.gam_off = gam_off;
+    gam_off += (long long)md.nat * md.nat;
     mat_off += (long long)nao * nao;
     diis_off += 2LL * kDiisMax * nao * nao;
     ao_base += nao;
@@ -297,16 +318,26 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
   const size_t o_diat = take(sizeof(DiatomicDev) * diat_.size());
   const size_t o_ao = take(sizeof(int) * ao_atom_.size());
   const size_t o_order = take(sizeof(int) * order_.size());
+  // DFTB records, tables and splines (in the upload region)
+  const bool dftb_batch = is_dftb(method_);
+  size_t o_delems = 0, o_dpairs = 0, o_dtable = 0, o_dspl = 0;
+  if (dftb_batch) {
+    o_delems = take(sizeof(DftbElemDev) * kMaxElementSlots);
+    o_dpairs = take(sizeof(DftbPairDev) * dftb.pairs.size());
+    o_dtable = take(sizeof(double) * std::max<size_t>(dftb.table.size(), 1));
+    o_dspl = take(sizeof(DftbSplineDev) * std::max<size_t>(dftb.splines.size(), 1));
+  }
   const size_t upload_end = off;
   const size_t o_pairs = take(sizeof(PairDev) * std::max<long long>(npairs_, 1));
   const size_t o_hh = take(sizeof(int) * std::max<long long>(nhh_, 1));
   const size_t o_counter = take(sizeof(int));
   const size_t o_flag = take(sizeof(int));
-  const size_t o_ints = take(sizeof(double) * std::max<long long>(int_off, 1));
   const size_t np = (size_t)std::max<long long>(npairs_, 1);
-  const size_t o_vcore = take(sizeof(double) * 20 * np);
-  const size_t o_jbuf = take(sizeof(double) * 20 * np);
-  const size_t o_ovl = take(sizeof(double) * 16 * np);
+  const size_t npn = dftb_batch ? 1 : np;  // NDDO-only per-pair buffers
+  const size_t o_ints = take(sizeof(double) * (dftb_batch ? 1 : std::max<long long>(int_off, 1)));
+  const size_t o_vcore = take(sizeof(double) * 20 * npn);
+  const size_t o_jbuf = take(sizeof(double) * 20 * npn);
+  const size_t o_ovl = take(sizeof(double) * 16 * npn);
   const size_t o_erep = take(sizeof(double) * np);
   const size_t o_gpair = take(sizeof(double) * 3 * np);
   const size_t mat_bytes = sizeof(double) * (size_t)mat_off;
@@ -322,6 +353,13 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
   const int grid_eff = std::min<int>(scf_grid_, (int)mols_.size());
   const size_t o_rot = take(scf_rotation_bytes_per_cta() * (size_t)grid_eff);
   const size_t o_res = take(sizeof(MolResult) * mols_.size());
+  const size_t mat_dftb = dftb_batch ? mat_bytes : sizeof(double);
+  const size_t o_S = take(mat_dftb), o_X = take(mat_dftb), o_Pp = take(mat_dftb);
+  const size_t gam_bytes = sizeof(double) * (dftb_batch ? std::max<long long>(gam_off, 1) : 1);
+  const size_t o_gam = take(gam_bytes);
+  const size_t o_Gam = take(method_ == kDFTB3 ? gam_bytes : sizeof(double));
+  const size_t o_qat = take(sizeof(double) * (dftb_batch ? atoms_.size() : 1));
+  const size_t o_shift = take(sizeof(double) * 4 * (dftb_batch ? atoms_.size() : 1));
   int rc = ensure_arena(off, err);
   if (rc) return rc;
   rc = ensure_terms(stream_, err);
@@ -354,6 +392,21 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
   d.rotbuf = reinterpret_cast<double*>(base + o_rot);
   d.scf_grid = grid_eff;
   d.res = reinterpret_cast<MolResult*>(base + o_res);
+  d.S = reinterpret_cast<double*>(base + o_S);
+  d.X = reinterpret_cast<double*>(base + o_X);
+  d.Pp = reinterpret_cast<double*>(base + o_Pp);
+  d.gam = reinterpret_cast<double*>(base + o_gam);
+  d.Gam = reinterpret_cast<double*>(base + o_Gam);
+  d.qat = reinterpret_cast<double*>(base + o_qat);
+  d.ashift = reinterpret_cast<double*>(base + o_shift);
+  if (dftb_batch) {
+    d.dftb_order = method_ == kDFTB3 ? 3 : 2;
+    d.gam_total = gam_off;
+    d.delems = reinterpret_cast<DftbElemDev*>(base + o_delems);
+    d.dpairs = reinterpret_cast<DftbPairDev*>(base + o_dpairs);
+    d.dtable = reinterpret_cast<double*>(base + o_dtable);
+    d.dsplines = reinterpret_cast<DftbSplineDev*>(base + o_dspl);
+  }
   dev_ = d;
 
   // stage the descriptors in pinned memory and upload them with one copy
@@ -382,6 +435,14 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
   std::memcpy(h + o_diat, diat_.data(), sizeof(DiatomicDev) * diat_.size());
   std::memcpy(h + o_ao, ao_atom_.data(), sizeof(int) * ao_atom_.size());
   std::memcpy(h + o_order, order_.data(), sizeof(int) * order_.size());
+  if (dftb_batch) {
+    std::memset(h + o_delems, 0, sizeof(DftbElemDev) * kMaxElementSlots);
+    std::memcpy(h + o_delems, dftb.elems.data(), sizeof(DftbElemDev) * dftb.elems.size());
+    std::memcpy(h + o_dpairs, dftb.pairs.data(), sizeof(DftbPairDev) * dftb.pairs.size());
+    if (!dftb.table.empty()) std::memcpy(h + o_dtable, dftb.table.data(), sizeof(double) * dftb.table.size());
+    if (!dftb.splines.empty())
+      std::memcpy(h + o_dspl, dftb.splines.data(), sizeof(DftbSplineDev) * dftb.splines.size());
+  }
   cudaError_t e = cudaMemcpyAsync(arena_, pinned_, upload_end, cudaMemcpyHostToDevice, stream_);
   if (e != cudaSuccess) {
     err = cuda_message(e);
@@ -484,18 +545,33 @@ int Batch::run(const ScfParams& sp, bool gradient, std::string& err) {
     if (!ev) cudaEventCreate(&ev);
   launches_ = 0;
   cudaEventRecord(stage_ev_[0], stream_);
-  launch_pair_values(dev_, stream_);
-  launches_ += dev_.npairs > 0 ? 1 : 0;
-  cudaEventRecord(stage_ev_[1], stream_);
-  launch_one_electron(dev_, stream_);
-  launches_ += 1;
-  cudaEventRecord(stage_ev_[2], stream_);
-  launch_scf(dev_, sp, dev_.scf_grid, stream_);
-  launches_ += 1;
-  cudaEventRecord(stage_ev_[3], stream_);
-  if (gradient) {
-    launch_gradient(dev_, stream_);
+  if (is_dftb(method_)) {
+    // pair and on-site terms (+ start density) | SCC loop | gradient
+    launch_dftb_setup(dev_, stream_);
     launches_ += dev_.npairs > 0 ? 2 : 1;
+    cudaEventRecord(stage_ev_[1], stream_);
+    cudaEventRecord(stage_ev_[2], stream_);
+    launch_dftb_scf(dev_, sp, dev_.scf_grid, stream_);
+    launches_ += 1;
+    cudaEventRecord(stage_ev_[3], stream_);
+    if (gradient) {
+      launch_dftb_gradient(dev_, stream_);
+      launches_ += dev_.npairs > 0 ? 2 : 1;
+    }
+  } else {
+    launch_pair_values(dev_, stream_);
+    launches_ += dev_.npairs > 0 ? 1 : 0;
+    cudaEventRecord(stage_ev_[1], stream_);
+    launch_one_electron(dev_, stream_);
+    launches_ += 1;
+    cudaEventRecord(stage_ev_[2], stream_);
+    launch_scf(dev_, sp, dev_.scf_grid, stream_);
+    launches_ += 1;
+    cudaEventRecord(stage_ev_[3], stream_);
+    if (gradient) {
+      launch_gradient(dev_, stream_);
+      launches_ += dev_.npairs > 0 ? 2 : 1;
+    }
   }
   cudaEventRecord(stage_ev_[4], stream_);
   stages_recorded_ = true;

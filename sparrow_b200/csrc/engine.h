@@ -68,6 +68,10 @@ class Batch {
 
   cudaStream_t stream() const { return stream_; }
   Method method() const { return method_; }
+  // DFTB parameter set (embedded sets: mio-1-1, 3ob-3-1, 3ob-2-1); empty =
+  // the method's default.  Takes effect at the next setup().
+  void set_dftb_parameters(const std::string& set) { dftb_set_ = set; }
+  const std::string& dftb_parameters() const { return dftb_set_; }
   int n_molecules() const { return (int)mols_.size(); }
   int n_atoms() const { return (int)atoms_.size(); }
   long long device_bytes() const { return arena_bytes_; }
@@ -99,6 +103,7 @@ class Batch {
   std::vector<DiatomicDev> diat_;
   std::vector<int> ao_atom_, order_;
   long long npairs_ = 0, nhh_ = 0;  // pair and heavy-pair tables are built on the device
+  std::string dftb_set_;
   int scf_grid_ = 0;
   int scf_grid_nao_ = 0;
   int launches_ = 0;

@@ -24,7 +24,8 @@ constexpr int kMaxAtomsPerMolecule = 4096;
 constexpr int kDiisMax = 6;          // Pulay subspace size
 constexpr int kMaxElementSlots = 16; // distinct elements in one batch
 
-enum Method : int { kMNDO = 0, kAM1 = 1, kPM6 = 2 };
+enum Method : int { kMNDO = 0, kAM1 = 1, kPM6 = 2, kDFTB2 = 3, kDFTB3 = 4 };
+inline bool is_dftb(int m) { return m == kDFTB2 || m == kDFTB3; }
 
 struct ElemDev {
   int Z = 0;
@@ -73,6 +74,7 @@ struct MolDev {
   long long mat_off;   // N*N matrices (H, P, F, C, scratch) at this offset
   long long diis_off;  // DIIS history
   long long int_off;   // first integral of the molecule
+  long long gam_off;  // DFTB: offset of the molecule's nat x nat gamma blocks
 };
 
 // Per-molecule result record written by the SCF kernel.

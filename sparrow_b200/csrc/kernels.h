@@ -7,6 +7,9 @@
 namespace sgb {
 
 struct LocalTermTable;
+struct DftbElemDev;
+struct DftbPairDev;
+struct DftbSplineDev;
 
 // Recorded Jacobi rotations per SCF CTA (device scratch): a cold start of up
 // to six sweeps fits without an intermediate replay for N <= 256.
@@ -46,6 +49,20 @@ struct DeviceBatch {
   double* grad = nullptr;           // [natoms * 3]
   MolResult* res = nullptr;         // [nmol]
   int use_guess = 1;                // 0: P already holds a start density
+  // DFTB (H holds H0)
+  int dftb_order = 0;               // 2 or 3 for DFTB batches
+  long long gam_total = 0;
+  double* S = nullptr;              // [mat_total] overlap
+  double* X = nullptr;              // [mat_total] S^-1/2
+  double* Pp = nullptr;             // [mat_total] density in the orthogonal basis
+  double* gam = nullptr;            // [gam_total] gamma (nat x nat per molecule)
+  double* Gam = nullptr;            // [gam_total] Gamma (DFTB3)
+  double* qat = nullptr;            // [natoms] Mulliken charges
+  double* ashift = nullptr;         // [natoms * 4] atom shift terms
+  DftbElemDev* delems = nullptr;    // [kMaxElementSlots]
+  DftbPairDev* dpairs = nullptr;    // [kMaxElementSlots^2]
+  double* dtable = nullptr;         // completed Slater-Koster tables
+  DftbSplineDev* dsplines = nullptr;
 };
 
 void upload_local_terms(const LocalTermTable& tab, cudaStream_t stream);
@@ -56,6 +73,11 @@ void launch_pair_values(const DeviceBatch& b, cudaStream_t s);
 void launch_one_electron(const DeviceBatch& b, cudaStream_t s);
 void launch_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s);
 void launch_gradient(const DeviceBatch& b, cudaStream_t s);
+void launch_gather_gradient(const DeviceBatch& b, cudaStream_t s);
+// DFTB: pair and on-site terms (+ start density), SCC loop, gradient
+void launch_dftb_setup(const DeviceBatch& b, cudaStream_t s);
+void launch_dftb_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s);
+void launch_dftb_gradient(const DeviceBatch& b, cudaStream_t s);
 int scf_max_grid(int max_nao);
 size_t scf_rotation_bytes_per_cta();
 

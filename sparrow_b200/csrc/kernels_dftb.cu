@@ -1,0 +1,490 @@
+// DFTB2 / DFTB3 kernels: Slater-Koster pair blocks, on-site terms, the
+// persistent self-consistent-charge kernel and the nuclear gradient.
+//
+// Reference behaviour followed (paths relative to
+// src/Sparrow/Sparrow/Implementations/Dftb/):
+//   H0, S                  Utils/ZeroOrderMatricesCalculator.cpp:56-232
+//   gamma, gamma^h, Gamma  Utils/SecondOrderFock.cpp:53-113, Utils/ThirdOrderFock.cpp:55-155
+//   charges, Fock          Utils/ScfFock.cpp:50-103 (Mulliken q = Z - N),
+//                          SecondOrderFock.cpp:115-145, ThirdOrderFock.cpp:157-200
+//   energy                 SecondOrderFock.cpp:178-195, ThirdOrderFock.cpp:228-255
+//   density guess          Utils/DensityGuess.cpp:22-40
+//   gradient               ZeroOrderMatricesCalculator.cpp:431-460,
+//                          SecondOrderFock.cpp:148-176, ThirdOrderFock.cpp:202-226
+// The self-consistent-charge Fock matrix is F = H0 + S o (s_a + s_b): every
+// density-dependent term of DFTB2 and DFTB3 is a per-atom shift s_a, so one
+// iteration costs an N^2 pass plus the atom-matrix products.  The
+// generalised eigenproblem is solved in the Loewdin basis, X = S^-1/2 from a
+// coupled Newton-Schulz iteration (GEMMs only), with the same DIIS, Jacobi
+// cold start and occupied-virtual rotation as the NDDO kernel.  The
+// energy-weighted density of the gradient is W = 1/2 P F P.
+#include <cuda_runtime.h>
+
+#include "dftb_math.cuh"
+#include "kernels.h"
+#include "scf_core.cuh"
+
+namespace sgb {
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Pair terms: S / H0 off-diagonal blocks, gamma (Gamma) entries, repulsion
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_dftb_pairs(const PairDev* __restrict__ pairs, int npairs,
+                                                    const AtomDev* __restrict__ atoms, const MolDev* __restrict__ mols,
+                                                    const DftbElemDev* __restrict__ el,
+                                                    const DftbPairDev* __restrict__ pp, const double* __restrict__ table,
+                                                    const DftbSplineDev* __restrict__ spl, int order, double* H0all,
+                                                    double* Sall, double* gam, double* Gam, double* erep) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npairs) return;
+  const PairDev pr = pairs[p];
+  const AtomDev A = atoms[pr.a], B = atoms[pr.b];
+  const MolDev m = mols[pr.mol];
+  const DftbElemDev ea = el[A.slot], eb = el[B.slot];
+  const bool flip = ea.Z > eb.Z;  // the atom of lower Z comes first in the tables
+  const double R[3] = {B.x - A.x, B.y - A.y, B.z - A.z};
+  const double dist = sqrt(R[0] * R[0] + R[1] * R[1] + R[2] * R[2]);
+  const double Rf[3] = {flip ? -R[0] : R[0], flip ? -R[1] : R[1], flip ? -R[2] : R[2]};
+  const DftbPairDev& pf = flip ? pp[B.slot * kMaxElementSlots + A.slot] : pp[A.slot * kMaxElementSlots + B.slot];
+  double me[2][4][4];
+  dftb_blocks<double>(pf, table, flip ? eb.nao : ea.nao, flip ? ea.nao : eb.nao, Rf, me);
+  const int N = m.nao;
+  double* H0 = H0all + m.mat_off;
+  double* S = Sall + m.mat_off;
+  for (int i = 0; i < ea.nao; ++i)
+    for (int j = 0; j < eb.nao; ++j) {
+      const double s = flip ? me[0][j][i] : me[0][i][j];
+      const double h = flip ? me[1][j][i] : me[1][i][j];
+      const size_t u = A.ao0 + i, v = B.ao0 + j;
+      S[u * N + v] = S[v * N + u] = s;
+      H0[u * N + v] = H0[v * N + u] = h;
+    }
+  const int ia = pr.a - m.atom0, ib = pr.b - m.atom0, nat = m.nat;
+  const DftbPairDev& pab = pp[A.slot * kMaxElementSlots + B.slot];
+  if (order == 3) {
+    double o[6];
+    dftb_gamma3(ea, eb, pab, dist, o);
+    gam[m.gam_off + (size_t)ia * nat + ib] = gam[m.gam_off + (size_t)ib * nat + ia] = o[0];
+    Gam[m.gam_off + (size_t)ia * nat + ib] = o[2];
+    Gam[m.gam_off + (size_t)ib * nat + ia] = o[4];
+  } else {
+    double g, dg;
+    dftb_gamma2(ea, eb, pab, dist, g, dg);
+    gam[m.gam_off + (size_t)ia * nat + ib] = gam[m.gam_off + (size_t)ib * nat + ia] = g;
+  }
+  double E, dE;
+  dftb_repulsion(pab, spl, dist, E, dE);
+  erep[p] = E;
+}
+
+// ---------------------------------------------------------------------------
+// On-site blocks, gamma_aa (Gamma_aa), start density, repulsion energy
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_dftb_onsite(const MolDev* __restrict__ mols, const AtomDev* __restrict__ atoms,
+                                                     const DftbElemDev* __restrict__ el,
+                                                     const int* __restrict__ ao_atom, const double* __restrict__ erep,
+                                                     int order, double* H0all, double* Sall, double* gam, double* Gam,
+                                                     double* Pall, MolResult* res, int write_guess) {
+  __shared__ double red[32];
+  const MolDev m = mols[blockIdx.x];
+  const int N = m.nao, nat = m.nat;
+  double* H0 = H0all + m.mat_off;
+  double* S = Sall + m.mat_off;
+  for (int a = threadIdx.x; a < nat; a += blockDim.x) {
+    const AtomDev A = atoms[m.atom0 + a];
+    const DftbElemDev e = el[A.slot];
+    for (int i = 0; i < e.nao; ++i)
+      for (int j = 0; j < e.nao; ++j) {
+        const size_t u = A.ao0 + i, v = A.ao0 + j;
+        H0[u * N + v] = i == j ? (i == 0 ? e.es : e.ep) : 0.0;
+        S[u * N + v] = i == j ? 1.0 : 0.0;
+      }
+    gam[m.gam_off + (size_t)a * nat + a] = e.U;
+    if (order == 3) Gam[m.gam_off + (size_t)a * nat + a] = 0.5 * e.hd;
+  }
+  if (write_guess) {
+    // neutral atoms: the core charge spread over the atom's orbitals
+    double* P = Pall + m.mat_off;
+    for (int k = threadIdx.x; k < N * N; k += blockDim.x) {
+      const int i = k / N, j = k % N;
+      double v = 0.0;
+      if (i == j) {
+        const AtomDev A = atoms[ao_atom[m.ao_base + i]];
+        const DftbElemDev e = el[A.slot];
+        v = e.occ / e.nao;
+      }
+      P[k] = v;
+    }
+  }
+  double s = 0;
+  for (int k = threadIdx.x; k < m.npairs; k += blockDim.x) s += erep[m.pair0 + k];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    res[blockIdx.x].e_rep = t;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Persistent self-consistent-charge kernel
+// ---------------------------------------------------------------------------
+// X = S^-1/2 by the coupled Newton-Schulz iteration Y <- Y T, Z <- T Z with
+// T = (3 I - Z Y) / 2, Y0 = S / c, Z0 = I, c a Gershgorin bound on the largest
+// eigenvalue of S; Z converges quadratically to (S / c)^-1/2.  Buffers:
+// Y in {y0, y1}, Z in {X, z1}, T in t.  Returns the iterations used, or -1.
+__device__ int inverse_sqrt(int N, const double* S, double* X, double* y0, double* y1, double* z1, double* t,
+                            ScfShared& sh) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const int NN = N * N;
+  double c = 0;
+  for (int i = warp; i < N; i += nwarps) {
+    double r = 0;
+    for (int j = lane; j < N; j += 32) r += fabs(S[(size_t)i * N + j]);
+    c = fmax(c, warp_sum(r));
+  }
+  c = cta_max(c, sh.red);
+  const double ic = 1.0 / c;
+  for (int k = tid; k < NN; k += blockDim.x) {
+    y0[k] = S[k] * ic;
+    X[k] = (k % (N + 1) == 0) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  double *Y = y0, *Yn = y1, *Z = X, *Zn = z1;
+  int it = 0, extra = -1;
+  for (; it < 100; ++it) {
+    for (int k = tid; k < NN; k += blockDim.x) t[k] = (k % (N + 1) == 0) ? 1.5 : 0.0;
+    __syncthreads();
+    cta_gemm(N, N, N, -0.5, Z, N, false, Y, N, false, 1.0, t, N, sh.gemm);  // T = 3/2 I - 1/2 Z Y
+    double err = 0;
+    for (int k = tid; k < NN; k += blockDim.x) err = fmax(err, fabs(t[k] - ((k % (N + 1) == 0) ? 1.0 : 0.0)));
+    err = cta_max(err, sh.red);
+    cta_gemm(N, N, N, 1.0, Y, N, false, t, N, false, 0.0, Yn, N, sh.gemm);
+    cta_gemm(N, N, N, 1.0, t, N, false, Z, N, false, 0.0, Zn, N, sh.gemm);
+    double* s1 = Y;
+    Y = Yn;
+    Yn = s1;
+    double* s2 = Z;
+    Z = Zn;
+    Zn = s2;
+    if (!isfinite(err)) return -1;
+    if (extra < 0 && err < 1e-10) extra = 2;  // two more quadratic steps reach rounding level
+    if (extra >= 0 && extra-- == 0) break;
+  }
+  const double sc = sqrt(ic);
+  for (int k = tid; k < NN; k += blockDim.x) X[k] = Z[k] * sc;
+  __syncthreads();
+  return it < 100 ? it + 1 : -1;
+}
+
+// Mulliken charges, atom shifts and the per-atom energy terms for the AO
+// density P.  Shift layout per atom: {s_a, V_a, A_a, unused} with
+// V_a = -sum_i gamma_ai q_i, A_a = sum_i Gamma_ai q_i (DFTB3) and
+// s_a = V_a / 2 + (2 q_a A_a + sum_i Gamma_ia q_i^2) / 6.  Returns
+// sum_a (-1/2 q_a V_a - 1/3 q_a^2 A_a), i.e. E2 (+ E3).  pop: N scratch.
+__device__ double charges_and_shifts(const MolDev& m, int order, const AtomDev* atoms, const DftbElemDev* el,
+                                     const double* P, const double* S, const double* gm, const double* Gm, double* pop,
+                                     double* q, double* sh4, double* red) {
+  const int N = m.nao, nat = m.nat;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  for (int i = warp; i < N; i += nwarps) {
+    double s = 0;
+    for (int j = lane; j < N; j += 32) s += P[(size_t)i * N + j] * S[(size_t)i * N + j];
+    s = warp_sum(s);
+    if (lane == 0) pop[i] = s;
+  }
+  __syncthreads();
+  for (int a = tid; a < nat; a += blockDim.x) {
+    const AtomDev A = atoms[m.atom0 + a];
+    const DftbElemDev e = el[A.slot];
+    double n = 0;
+    for (int k = 0; k < e.nao; ++k) n += pop[A.ao0 + k];
+    q[a] = e.occ - n;
+  }
+  __syncthreads();
+  double e23 = 0;
+  for (int a = warp; a < nat; a += nwarps) {
+    double V = 0, Aa = 0, Ba = 0;
+    for (int i = lane; i < nat; i += 32) {
+      V -= gm[(size_t)a * nat + i] * q[i];
+      if (order == 3) {
+        Aa += Gm[(size_t)a * nat + i] * q[i];
+        Ba += Gm[(size_t)i * nat + a] * q[i] * q[i];
+      }
+    }
+    V = warp_sum(V);
+    Aa = warp_sum(Aa);
+    Ba = warp_sum(Ba);
+    if (lane == 0) {
+      const double qa = q[a];
+      sh4[4 * a + 0] = 0.5 * V + (order == 3 ? (2.0 * qa * Aa + Ba) / 6.0 : 0.0);
+      sh4[4 * a + 1] = V;
+      sh4[4 * a + 2] = Aa;
+      e23 += -0.5 * qa * V - (order == 3 ? qa * qa * Aa / 3.0 : 0.0);
+    }
+  }
+  return cta_sum(e23, red);
+}
+
+// F = H0 + S o (s_a + s_b) (warp per row); returns sum H0 o P.
+__device__ double dftb_fock(const MolDev& m, const int* ao_atom, const double* H0, const double* S, const double* P,
+                            const double* sh4, double* F, double* red) {
+  const int N = m.nao;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  double eb = 0;
+  for (int i = warp; i < N; i += nwarps) {
+    const double si = sh4[4 * (ao_atom[m.ao_base + i] - m.atom0)];
+    for (int j = lane; j < N; j += 32) {
+      const size_t k = (size_t)i * N + j;
+      const double sj = sh4[4 * (ao_atom[m.ao_base + j] - m.atom0)];
+      F[k] = H0[k] + S[k] * (si + sj);
+      eb += H0[k] * P[k];
+    }
+  }
+  return cta_sum(eb, red);
+}
+
+__global__ void __launch_bounds__(kScfThreads) k_dftb_scf(
+    const MolDev* __restrict__ mols, int nmol, const int* __restrict__ order_list, int* counter,
+    const AtomDev* __restrict__ atoms, const DftbElemDev* __restrict__ el, const int* __restrict__ ao_atom,
+    const double* __restrict__ H0all, const double* __restrict__ Sall, double* Xall, double* Pall, double* Ppall,
+    double* Fall, double* Call, double* W1all, double* W2all, double* epsall, double* diisall, double* rotbuf,
+    const double* __restrict__ gamall, const double* __restrict__ Gamall, double* qall, double* shall,
+    MolResult* res, ScfParams sp, int packed_in_smem, int order) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ScfShared& sh = *reinterpret_cast<ScfShared*>(smem_raw);
+  double* smemA = reinterpret_cast<double*>(smem_raw + ((sizeof(ScfShared) + 15) / 16) * 16);
+  const int tid = threadIdx.x;
+  while (true) {
+    if (tid == 0) sh.mol = atomicAdd(counter, 1);
+    __syncthreads();
+    const int slot = sh.mol;
+    __syncthreads();
+    if (slot >= nmol) break;
+    const int mi = order_list[slot];
+    const MolDev m = mols[mi];
+    const int N = m.nao, no = m.nocc;
+    const size_t NN = (size_t)N * N;
+    const double* H0 = H0all + m.mat_off;
+    const double* S = Sall + m.mat_off;
+    double* X = Xall + m.mat_off;
+    double* P = Pall + m.mat_off;
+    double* Pp = Ppall + m.mat_off;
+    double* F = Fall + m.mat_off;
+    double* Ct = Call + m.mat_off;
+    double* W1 = W1all + m.mat_off;
+    double* W2 = W2all + m.mat_off;
+    double* eps = epsall + m.ao_base;
+    double* histF = diisall + m.diis_off;
+    double* histE = histF + (size_t)kDiisMax * NN;
+    const double* gm = gamall + m.gam_off;
+    const double* Gm = Gamall + (order == 3 ? m.gam_off : 0);
+    double* q = qall + m.atom0;
+    double* sh4 = shall + 4 * (size_t)m.atom0;
+    double* Apk = packed_in_smem ? smemA : nullptr;
+    const size_t packed_bytes = sizeof(double) * (size_t)N * (N + 1) / 2;
+    double* rot = rotbuf + (size_t)blockIdx.x * (kRotBudgetBytes / sizeof(double));
+    const int cap_rounds = (int)((kRotBudgetBytes / sizeof(double)) / (2 * ((N + 1) / 2)));
+    const int msize = sp.diis_size < 1 ? 1 : (sp.diis_size > kDiisMax ? kDiisMax : sp.diis_size);
+    int status = kDevOk;
+
+    // Loewdin orthogonaliser (W1, F, Ct, W2 serve as Newton-Schulz buffers)
+    const int ns_it = inverse_sqrt(N, S, X, W1, F, Ct, W2, sh);
+    if (ns_it < 0) status = kDevNonFinite;
+
+    int nhist = 0, head = 0, it = 0, converged = 0, nfull = 0, nsweeps = 0;
+    bool have_orbitals = false;
+    double drift = 0, Eold = 0, last_dE = 0, last_rms = 0;
+    for (it = 1; it <= sp.max_iter && status == kDevOk; ++it) {
+      const double e23 = charges_and_shifts(m, order, atoms, el, P, S, gm, Gm, W2, q, sh4, sh.red);
+      const double eb = dftb_fock(m, ao_atom, H0, S, P, sh4, F, sh.red);
+      const double E = eb + e23;
+      // F' = X F X
+      cta_gemm(N, N, N, 1.0, F, N, false, X, N, false, 0.0, W1, N, sh.gemm);
+      cta_gemm(N, N, N, 1.0, X, N, false, W1, N, false, 0.0, F, N, sh.gemm);
+      if (have_orbitals) {
+        const double* Fx = diis_step(N, F, Pp, W1, W2, histF, histE, msize, nhist, head, sh);
+        if (Fx != F) {
+          for (size_t k = tid; k < NN; k += blockDim.x) F[k] = W2[k];
+          __syncthreads();
+        }
+      }
+      int need_full = !have_orbitals;
+      if (have_orbitals) need_full = ov_rotation(N, no, F, Ct, W1, W2, eps, drift, sh);
+      if (need_full) {
+        const int sw = full_diagonalise(N, F, Ct, W1, W2, eps, Apk ? Apk : F, Apk ? packed_bytes : 0, have_orbitals,
+                                        rot, cap_rounds, have_orbitals ? sp.jacobi_max_sweeps : 6,
+                                        have_orbitals ? 1e-10 : 1e-3, sh);
+        if (sw < 0 && have_orbitals) status = kDevJacobiNotConverged;
+        nsweeps += sw < 0 ? (have_orbitals ? sp.jacobi_max_sweeps : 6) : sw;
+        ++nfull;
+        have_orbitals = true;
+        drift = 0;
+      }
+      // P' = 2 C'_occ C'_occ^T, P = X P' X
+      cta_gemm(N, N, no, 2.0, Ct, N, true, Ct, N, false, 0.0, Pp, N, sh.gemm);
+      cta_gemm(N, N, N, 1.0, X, N, false, Pp, N, false, 0.0, W1, N, sh.gemm);
+      cta_gemm(N, N, N, 1.0, W1, N, false, X, N, false, 0.0, W2, N, sh.gemm);
+      double d2 = 0;
+      for (size_t k = tid; k < NN; k += blockDim.x) {
+        const double d = W2[k] - P[k];
+        d2 += d * d;
+        P[k] = W2[k];
+      }
+      d2 = cta_sum(d2, sh.red);
+      const double rms = sqrt(d2 / (double)NN);
+      last_rms = rms;
+      last_dE = it > 1 ? fabs(E - Eold) : 0.0;
+      const bool dE_ok = it > 1 && fabs(E - Eold) < sp.scc;
+      Eold = E;
+      if (!isfinite(E) || !isfinite(rms)) {
+        status = kDevNonFinite;
+        break;
+      }
+      if (dE_ok && rms < sp.rmsd) {
+        converged = 1;
+        break;
+      }
+      __syncthreads();
+    }
+    if (it > sp.max_iter) it = sp.max_iter;
+    __syncthreads();
+    // final charges, Fock matrix and energy of the converged density; W = 1/2 P F P into W1
+    const double e23 = charges_and_shifts(m, order, atoms, el, P, S, gm, Gm, W2, q, sh4, sh.red);
+    const double eb = dftb_fock(m, ao_atom, H0, S, P, sh4, F, sh.red);
+    cta_gemm(N, N, N, 1.0, F, N, false, P, N, false, 0.0, W2, N, sh.gemm);
+    cta_gemm(N, N, N, 0.5, P, N, false, W2, N, false, 0.0, W1, N, sh.gemm);
+    if (tid == 0) {
+      MolResult& r = res[mi];
+      r.e_el = eb + e23;
+      r.energy = r.e_el + r.e_rep;
+      r.iterations = it;
+      r.converged = converged;
+      r.status = status;
+      r.last_dE = last_dE;
+      r.last_rmsd = last_rms;
+      r.full_diag = nfull;
+      r.jacobi_sweeps = nsweeps;
+      r.cycles[0] = ns_it;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Nuclear gradient per pair (dE/dR_b, R = R_b - R_a)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(64) k_dftb_gradient(const PairDev* __restrict__ pairs, int npairs,
+                                                      const AtomDev* __restrict__ atoms,
+                                                      const MolDev* __restrict__ mols,
+                                                      const DftbElemDev* __restrict__ el,
+                                                      const DftbPairDev* __restrict__ pp,
+                                                      const double* __restrict__ table,
+                                                      const DftbSplineDev* __restrict__ spl, int order,
+                                                      const double* __restrict__ Pall, const double* __restrict__ Wall,
+                                                      const double* __restrict__ qall,
+                                                      const double* __restrict__ shall, double* __restrict__ gpair) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npairs) return;
+  const PairDev pr = pairs[p];
+  const AtomDev A = atoms[pr.a], B = atoms[pr.b];
+  const MolDev m = mols[pr.mol];
+  const DftbElemDev ea = el[A.slot], eb = el[B.slot];
+  const bool flip = ea.Z > eb.Z;
+  const double R[3] = {B.x - A.x, B.y - A.y, B.z - A.z};
+  const double dist = sqrt(R[0] * R[0] + R[1] * R[1] + R[2] * R[2]);
+  const double Rf[3] = {flip ? -R[0] : R[0], flip ? -R[1] : R[1], flip ? -R[2] : R[2]};
+  const DftbPairDev& pf = flip ? pp[B.slot * kMaxElementSlots + A.slot] : pp[A.slot * kMaxElementSlots + B.slot];
+  Dual3 me[2][4][4];
+  const int nz = dftb_blocks<Dual3>(pf, table, flip ? eb.nao : ea.nao, flip ? ea.nao : eb.nao, Rf, me);
+  const int N = m.nao;
+  const double* P = Pall + m.mat_off;
+  const double* W = Wall + m.mat_off;
+  const double sab = shall[4 * (size_t)pr.a] + shall[4 * (size_t)pr.b];
+  const double sgn = flip ? -1.0 : 1.0;  // blocks were differentiated with respect to -R when flipped
+  double d[3] = {0, 0, 0};
+  if (nz)
+    for (int i = 0; i < ea.nao; ++i)
+      for (int j = 0; j < eb.nao; ++j) {
+        const Dual3& s = flip ? me[0][j][i] : me[0][i][j];
+        const Dual3& h = flip ? me[1][j][i] : me[1][i][j];
+        const size_t u = A.ao0 + i, v = B.ao0 + j;
+        const double Puv = P[u * N + v];
+        const double Wm = W[u * N + v] - sab * Puv;
+        d[0] += 2.0 * sgn * (Puv * h.dx - Wm * s.dx);
+        d[1] += 2.0 * sgn * (Puv * h.dy - Wm * s.dy);
+        d[2] += 2.0 * sgn * (Puv * h.dz - Wm * s.dz);
+      }
+  const double qa = qall[pr.a], qb = qall[pr.b];
+  const DftbPairDev& pab = pp[A.slot * kMaxElementSlots + B.slot];
+  double coef;
+  if (order == 3) {
+    double o[6];
+    dftb_gamma3(ea, eb, pab, dist, o);
+    // the reference's pair term: q_a q_b gamma' + q_a q_b / 3 (q_b Gamma_ba' - q_a Gamma_ab')
+    coef = qa * qb * o[1] + (qa * qb / 3.0) * (qb * o[5] - qa * o[3]);
+  } else {
+    double g, dg;
+    dftb_gamma2(ea, eb, pab, dist, g, dg);
+    coef = qa * qb * dg;
+  }
+  double E, dE;
+  dftb_repulsion(pab, spl, dist, E, dE);
+  coef += dE;
+  for (int k = 0; k < 3; ++k) gpair[(size_t)p * 3 + k] = d[k] + coef * R[k] / dist;
+}
+
+size_t dftb_smem_bytes(int max_nao, int* packed_in_smem) {
+  const size_t base = ((sizeof(ScfShared) + 15) / 16) * 16;
+  const size_t pk = sizeof(double) * (size_t)max_nao * (max_nao + 1) / 2;
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (base + pk <= (size_t)optin) {
+    *packed_in_smem = 1;
+    return base + pk;
+  }
+  *packed_in_smem = 0;
+  return base;
+}
+
+}  // namespace
+
+void launch_dftb_setup(const DeviceBatch& b, cudaStream_t s) {
+  if (b.npairs > 0) {
+    const int th = 128;
+    k_dftb_pairs<<<(b.npairs + th - 1) / th, th, 0, s>>>(b.pairs, b.npairs, b.atoms, b.mols, b.delems, b.dpairs,
+                                                         b.dtable, b.dsplines, b.dftb_order, b.H, b.S, b.gam, b.Gam,
+                                                         b.erep);
+  }
+  k_dftb_onsite<<<b.nmol, 256, 0, s>>>(b.mols, b.atoms, b.delems, b.ao_atom, b.erep, b.dftb_order, b.H, b.S, b.gam,
+                                       b.Gam, b.P, b.res, b.use_guess);
+}
+
+void launch_dftb_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s) {
+  if (b.nmol == 0) return;
+  int in_smem = 0;
+  const size_t bytes = dftb_smem_bytes(b.max_nao, &in_smem);
+  cudaFuncSetAttribute(k_dftb_scf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaMemsetAsync(b.counter, 0, sizeof(int), s);
+  if (grid > b.nmol) grid = b.nmol;
+  k_dftb_scf<<<grid, kScfThreads, bytes, s>>>(b.mols, b.nmol, b.order, b.counter, b.atoms, b.delems, b.ao_atom, b.H,
+                                              b.S, b.X, b.P, b.Pp, b.F, b.C, b.W1, b.W2, b.eps, b.diis, b.rotbuf,
+                                              b.gam, b.Gam, b.qat, b.ashift, b.res, sp, in_smem, b.dftb_order);
+}
+
+void launch_dftb_gradient(const DeviceBatch& b, cudaStream_t s) {
+  if (b.npairs > 0) {
+    const int th = 64;
+    k_dftb_gradient<<<(b.npairs + th - 1) / th, th, 0, s>>>(b.pairs, b.npairs, b.atoms, b.mols, b.delems, b.dpairs,
+                                                            b.dtable, b.dsplines, b.dftb_order, b.P, b.W1, b.qat,
+                                                            b.ashift, b.gpair);
+  }
+  launch_gather_gradient(b, s);
+}
+
+}  // namespace sgb

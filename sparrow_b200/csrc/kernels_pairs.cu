@@ -186,7 +186,11 @@ void launch_gradient(const DeviceBatch& b, cudaStream_t s) {
     k_pair_gradient<<<(b.npairs + th - 1) / th, th, 0, s>>>(b.pairs, b.npairs, b.atoms, b.elems, b.diat, b.mols,
                                                              b.method, b.P, b.gpair);
   }
-  int th = 128;
+  launch_gather_gradient(b, s);
+}
+
+void launch_gather_gradient(const DeviceBatch& b, cudaStream_t s) {
+  const int th = 128;
   k_gather_gradient<<<(b.natoms + th - 1) / th, th, 0, s>>>(b.mols, b.atoms, b.natoms, b.gpair, b.grad);
 }
 

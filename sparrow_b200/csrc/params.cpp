@@ -1,4 +1,5 @@
 #include "params.h"
+#include "dftb_params.h"
 
 #include <algorithm>
 #include <cctype>
@@ -106,13 +107,24 @@ bool parse_method(const std::string& name, Method& m) {
   if (t == "PM6") m = kPM6;
   else if (t == "AM1") m = kAM1;
   else if (t == "MNDO") m = kMNDO;
+  else if (t == "DFTB2") m = kDFTB2;
+  else if (t == "DFTB3") m = kDFTB3;
   else return false;
   return true;
 }
 
-const char* method_name(Method m) { return m == kPM6 ? "PM6" : (m == kAM1 ? "AM1" : "MNDO"); }
+const char* method_name(Method m) {
+  switch (m) {
+    case kPM6: return "PM6";
+    case kAM1: return "AM1";
+    case kDFTB2: return "DFTB2";
+    case kDFTB3: return "DFTB3";
+    default: return "MNDO";
+  }
+}
 
 int engine_n_aos(Method m, int Z) {
+  if (is_dftb(m)) return dftb_n_aos(dftb_default_set(m), Z);
   const NddoRawAtomic* r = raw_for(m, Z);
   if (!r) return 0;
   int n = Z == 1 ? 1 : (m == kPM6 ? pm6_n_aos(Z) : 4);

@@ -6,6 +6,7 @@
 #include <map>
 
 #include "params.h"
+#include "dftb_params.h"
 
 namespace sgb {
 
@@ -20,7 +21,9 @@ double core_charge(Method m, int z) {
   auto it = cache.find(key);
   if (it != cache.end()) return it->second;
   double c = -1;
-  if (engine_n_aos(m, z) > 0) {
+  if (is_dftb(m)) {
+    if (engine_n_aos(m, z) > 0) c = dftb_core_charge(dftb_default_set(m), z);
+  } else if (engine_n_aos(m, z) > 0) {
     ElemDev e;
     std::string why;
     if (make_elem(m, z, e, why)) c = e.core;
