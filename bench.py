@@ -120,8 +120,7 @@ def plain_gpu_rate(method, mols, target_seconds=8.0, max_count=512, rng_seed=777
 
 def serving_mix(count, seed=5):
     """The serving request mix: alkanes C_nH_2n+2 (n ~ U[1,60]) or water
-    clusters (H2O)_n (n ~ U[2,64]), 70 % PM6 and 30 % AM1 (the engine's
-    second NDDO method stands in for the DFTB2 share until DFTB is served)."""
+    clusters (H2O)_n (n ~ U[2,64]), 70 % PM6 and 30 % DFTB2 (mio-1-1)."""
     import numpy as np
     from sparrow_b200 import geometry
     rng = np.random.default_rng(seed)
@@ -132,7 +131,7 @@ def serving_mix(count, seed=5):
         else:
             z, x = geometry.water_cluster(int(rng.integers(2, 65)), seed=int(rng.integers(1 << 30)))
         out.append((np.ascontiguousarray(z, dtype=np.int32), np.ascontiguousarray(geometry.to_bohr(x)).reshape(-1),
-                    "PM6" if rng.random() < 0.7 else "AM1"))
+                    "PM6" if rng.random() < 0.7 else "DFTB2"))
     return out
 
 
@@ -145,7 +144,7 @@ def serving_leg(loads=(250, 500, 1000, 2000), seconds=3.0, plain_count=48, seed=
     import numpy as np
     import sparrow_b200
     pool = serving_mix(2048, seed)
-    out = {"mix": "alkanes n~U[1,60] | (H2O)_n n~U[2,64], 70% PM6 / 30% AM1 (DFTB2 share served as AM1), "
+    out = {"mix": "alkanes n~U[1,60] | (H2O)_n n~U[2,64], 70% PM6 / 30% DFTB2 (mio-1-1), "
                   "energy+gradient, 3-384 AOs", "loads": []}
     rng = np.random.default_rng(seed + 1)
     with sparrow_b200.Server(device_budget_gb=64.0, slots=8, scc=SCC, rmsd=RMSD, max_iter=MAX_ITER) as srv:
