@@ -21,7 +21,8 @@ def _mix(count, seed):
             z, x = geometry.alkane(int(rng.integers(1, 14)), rng)
         else:
             z, x = geometry.water_cluster(int(rng.integers(2, 9)), seed=int(rng.integers(1 << 30)))
-        mols.append((np.asarray(z, np.int32), geometry.to_bohr(x), "PM6" if rng.random() < 0.7 else "AM1"))
+        r = rng.random()
+        mols.append((np.asarray(z, np.int32), geometry.to_bohr(x), "PM6" if r < 0.6 else ("DFTB2" if r < 0.85 else "AM1")))
     return mols
 
 
@@ -80,7 +81,10 @@ def test_served_results_match_oracle_and_clients_overlap():
         for t in threads:
             t.join()
     for i, (z, x, m) in enumerate(mols):
-        ref = O.scf(m, z, x, scc=1e-9, rmsd=1e-8)
+        if m == "DFTB2":
+            ref = O.dftb_scf(2, z, x, scc=1e-10, rmsd=1e-9)
+        else:
+            ref = O.scf(m, z, x, scc=1e-9, rmsd=1e-8)
         assert abs(results[i].energy - ref["energy"]) < E_TOL
         assert np.max(np.abs(results[i].gradients - ref["gradient"])) < G_TOL
         assert results[i].latency_s > 0
