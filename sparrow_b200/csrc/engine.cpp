@@ -301,6 +301,7 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
   d.nmol = (int)mols_.size();
   d.natoms = (int)atoms_.size();
   d.npairs = (int)npairs_;
+  d.nhh_total = (int)nhh_;
   d.nao_total = ao_base;
   d.mat_total = mat_off;
   d.diis_total = diis_off;

@@ -33,6 +33,7 @@ struct DeviceBatch {
   double* vcore = nullptr;          // [npairs * 20]
   double* jbuf = nullptr;           // [npairs * 20] per-pair Coulomb vectors of the Fock build
   int* hh_pairs = nullptr;          // [n_hh] global pair indices of s/p-s/p pairs
+  int nhh_total = 0;
   double* ovl = nullptr;            // [npairs * 16]
   double* erep = nullptr;           // [npairs]
   double* H = nullptr;              // [mat_total]

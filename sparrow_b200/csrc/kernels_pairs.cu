@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include "kernels.h"
+#include "nddo_grad.cuh"
 #include "nddo_math.cuh"
 
 namespace sgb {
@@ -60,24 +61,259 @@ __global__ void __launch_bounds__(128) k_pair_values(const PairDev* __restrict__
   erep[p] = E;
 }
 
-// Per pair: dE/dR_AB (R_AB = pos_B - pos_A) at density P.
-__global__ void __launch_bounds__(64) k_pair_gradient(const PairDev* __restrict__ pairs, int npairs,
-                                                       const AtomDev* __restrict__ atoms,
-                                                       const ElemDev* __restrict__ elems,
-                                                       const DiatomicDev* __restrict__ diat,
-                                                       const MolDev* __restrict__ mols, int method,
-                                                       const double* __restrict__ Pall, double* __restrict__ gpair) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
+// Pair gradient, reverse mode (see nddo_grad.cuh), for pairs with at least
+// one s-only atom: one thread per pair, 10-vectors only.  Heavy pairs (both
+// atoms s/p) return at once; k_pair_gradient_heavy handles them.
+__global__ void __launch_bounds__(128) k_pair_gradient_light(const PairDev* __restrict__ pairs, int npairs,
+                                                             const AtomDev* __restrict__ atoms,
+                                                             const ElemDev* __restrict__ elems,
+                                                             const DiatomicDev* __restrict__ diat,
+                                                             const MolDev* __restrict__ mols, int method,
+                                                             const double* __restrict__ Pall,
+                                                             double* __restrict__ gpair) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npairs) return;
   const PairDev pr = pairs[p];
   const AtomDev a = atoms[pr.a], b = atoms[pr.b];
+  const ElemDev& A = elems[a.slot];
+  const ElemDev& B = elems[b.slot];
+  const int nA = A.nao, nB = B.nao;
+  if (nA == 4 && nB == 4) return;
   const MolDev m = mols[pr.mol];
-  double g[3];
-  pair_gradient(c_local_terms, method, elems[a.slot], elems[b.slot], diat[a.slot * kMaxElementSlots + b.slot],
-                b.x - a.x, b.y - a.y, b.z - a.z, Pall + m.mat_off, m.nao, a.ao0, b.ao0, g);
+  const int N = m.nao;
+  const double* P = Pall + m.mat_off;
+  const double X = b.x - a.x, Y = b.y - a.y, Z = b.z - a.z;
+  const double R = sqrt(X * X + Y * Y + Z * Z);
+  double PA[4][4] = {}, PB[4][4] = {}, PAB[4][4] = {};
+  for (int i = 0; i < nA; ++i)
+    for (int j = 0; j < nA; ++j) PA[i][j] = P[(size_t)(a.ao0 + i) * N + a.ao0 + j];
+  for (int i = 0; i < nB; ++i)
+    for (int j = 0; j < nB; ++j) PB[i][j] = P[(size_t)(b.ao0 + i) * N + b.ao0 + j];
+  for (int i = 0; i < nA; ++i)
+    for (int j = 0; j < nB; ++j) PAB[i][j] = P[(size_t)(a.ao0 + i) * N + b.ao0 + j];
+  double g[3] = {0, 0, 0};
+  double adjA[4][4] = {}, adjB[4][4] = {};
+  double dR = 0;
+  RotGrad ra, rb;
+  const bool rotate = nA == 4 || nB == 4;
+  if (rotate) {
+    rotation_grad(Dual3(X, 1, 0, 0), Dual3(Y, 0, 1, 0), Dual3(Z, 0, 0, 1), ra);
+    rotation_grad(Dual3(-X, -1, 0, 0), Dual3(-Y, 0, -1, 0), Dual3(-Z, 0, 0, -1), rb);
+  }
+  // two-centre term
+  if (!rotate) {
+    double L, dL;
+    local_ss(c_local_terms, R, A, B, false, 0.0, L, dL);
+    dR += density_factor(PA, PB, PAB, 0, 0) * dL;
+  } else {
+    double L[10], dL[10];
+    if (nB == 1) local_column(c_local_terms, R, A, B, false, 0.0, L, dL);
+    else local_row(c_local_terms, R, A, B, L, dL);
+    for (int g2 = 0; g2 < 10; ++g2) {
+      const double Fg = nB == 1 ? density_factor(PA, PB, PAB, g2, 0) : density_factor(PA, PB, PAB, 0, g2);
+      if (Fg == 0.0) continue;
+      for (int k = 0; k < 5; ++k) {
+        const int q = axis_index(k);
+        if (L[q] == 0.0 && dL[q] == 0.0) continue;
+        w_adjoint(ra.r, g2, q, Fg * L[q], adjA);
+        dR += Fg * w_entry(ra.r, g2, q) * dL[q];
+      }
+    }
+  }
+  // core attraction: A's orbitals against B's core (frame A->B), B's against A's (frame B->A)
+  for (int side = 0; side < 2; ++side) {
+    const ElemDev& O = side ? B : A;    // orbitals
+    const ElemDev& C = side ? A : B;    // core
+    const double (*PO)[4] = side ? PB : PA;
+    const RotGrad& rg = side ? rb : ra;
+    double(*adj)[4] = side ? adjB : adjA;
+    if (O.nao == 1) {
+      double L, dL;
+      local_ss(c_local_terms, R, O, C, true, C.pcore, L, dL);
+      dR += -C.core * PO[0][0] * dL;
+    } else {
+      double L[10], dL[10];
+      local_column(c_local_terms, R, O, C, true, C.pcore, L, dL);
+      for (int g2 = 0; g2 < 10; ++g2) {
+        const double f = -C.core * atom_factor(PO, g2);
+        if (f == 0.0) continue;
+        for (int k = 0; k < 5; ++k) {
+          const int q = axis_index(k);
+          if (L[q] == 0.0 && dL[q] == 0.0) continue;
+          w_adjoint(rg.r, g2, q, f * L[q], adj);
+          dR += f * w_entry(rg.r, g2, q) * dL[q];
+        }
+      }
+    }
+  }
+  // overlap (resonance integrals)
+  {
+    double f[4][4] = {};
+    for (int i = 0; i < nA; ++i)
+      for (int j = 0; j < nB; ++j)
+        f[i][j] = ((i == 0 ? A.betaS : A.betaP) + (j == 0 ? B.betaS : B.betaP)) * PAB[i][j];
+    const double Rv[3] = {X, Y, Z};
+    for (int la = 0; la < (nA == 4 ? 2 : 1); ++la)
+      for (int lb = 0; lb < (nB == 4 ? 2 : 1); ++lb)
+        for (int i = 0; i < 6; ++i)
+          for (int j = 0; j < 6; ++j) overlap_primitive_grad(A, B, Rv, la, lb, i, j, f, g);
+  }
+  // core repulsion
+  {
+    double E, dE;
+    core_repulsion(method, A, B, diat[a.slot * kMaxElementSlots + b.slot], R, E, dE);
+    dR += dE;
+  }
+  g[0] += dR * X / R;
+  g[1] += dR * Y / R;
+  g[2] += dR * Z / R;
+  if (rotate) {
+    add_rotation_gradient(ra, adjA, g);
+    add_rotation_gradient(rb, adjB, g);
+  }
   gpair[(size_t)p * 3 + 0] = g[0];
   gpair[(size_t)p * 3 + 1] = g[1];
   gpair[(size_t)p * 3 + 2] = g[2];
+}
+
+// Pair gradient, reverse mode, for pairs of two s/p atoms: one warp per pair
+// with the 10 x 10 blocks in shared memory.  Lanes split the 21 unique local
+// integrals, the 100-entry matrices and products, the rotation adjoints and
+// the 144 primitive pairs of the overlap; each lane's partial gradient is
+// summed across the warp at the end.
+constexpr int kGradWarps = 4;
+struct HeavyGradShared {
+  double L[100], dL[100], W[100], F[100], T1[100], T2[100];
+  double Lc[10], dLc[10], Lcb[10], dLcb[10];
+  double PA[4][4], PB[4][4], PAB[4][4];
+  RotGrad ra, rb;
+};
+
+__global__ void __launch_bounds__(kGradWarps * 32) k_pair_gradient_heavy(
+    const int* __restrict__ hh, int nhh, const PairDev* __restrict__ pairs, const AtomDev* __restrict__ atoms,
+    const ElemDev* __restrict__ elems, const DiatomicDev* __restrict__ diat, const MolDev* __restrict__ mols, int method,
+    const double* __restrict__ Pall, double* __restrict__ gpair) {
+  __shared__ HeavyGradShared shm[kGradWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = blockIdx.x * kGradWarps + warp;
+  if (w >= nhh) return;  // uniform per warp
+  HeavyGradShared& s = shm[warp];
+  const int p = hh[w];
+  const PairDev pr = pairs[p];
+  const AtomDev a = atoms[pr.a], b = atoms[pr.b];
+  const ElemDev& A = elems[a.slot];
+  const ElemDev& B = elems[b.slot];
+  const MolDev m = mols[pr.mol];
+  const int N = m.nao;
+  const double* P = Pall + m.mat_off;
+  const double X = b.x - a.x, Y = b.y - a.y, Z = b.z - a.z;
+  const double R = sqrt(X * X + Y * Y + Z * Z);
+  const LocalTermTable& tab = c_local_terms;
+  if (lane < 16) {
+    const int i = lane >> 2, j = lane & 3;
+    s.PA[i][j] = P[(size_t)(a.ao0 + i) * N + a.ao0 + j];
+    s.PB[i][j] = P[(size_t)(b.ao0 + i) * N + b.ao0 + j];
+    s.PAB[i][j] = P[(size_t)(a.ao0 + i) * N + b.ao0 + j];
+  }
+  if (lane == 30) rotation_grad(Dual3(X, 1, 0, 0), Dual3(Y, 0, 1, 0), Dual3(Z, 0, 0, 1), s.ra);
+  if (lane == 31) rotation_grad(Dual3(-X, -1, 0, 0), Dual3(-Y, 0, -1, 0), Dual3(-Z, 0, 0, -1), s.rb);
+  for (int k = lane; k < 100; k += 32) s.L[k] = s.dL[k] = 0.0;
+  if (lane < 10) s.Lc[lane] = s.dLc[lane] = s.Lcb[lane] = s.dLcb[lane] = 0.0;
+  __syncwarp();
+  if (lane < kLocalUnique) {
+    const int r = tab.row[lane], c = tab.col[lane];
+    double v, d;
+    local_entry(tab, lane, R, A, B, false, 0.0, v, d);
+    s.L[r * 10 + c] = v;
+    s.dL[r * 10 + c] = d;
+    if (c == 0) {
+      local_entry(tab, lane, R, A, B, true, B.pcore, v, d);
+      s.Lc[r] = v;
+      s.dLc[r] = d;
+      local_entry(tab, lane, R, B, A, true, A.pcore, v, d);
+      s.Lcb[r] = v;
+      s.dLcb[r] = d;
+    }
+  }
+  __syncwarp();
+  if (lane == 0) {
+    local_copies(10, 10, reinterpret_cast<double(*)[10]>(s.L), reinterpret_cast<double(*)[10]>(s.dL));
+    s.Lc[5] = s.Lc[2];
+    s.dLc[5] = s.dLc[2];
+    s.Lcb[5] = s.Lcb[2];
+    s.dLcb[5] = s.dLcb[2];
+  }
+  for (int k = lane; k < 100; k += 32) {
+    s.W[k] = w_entry(s.ra.r, k / 10, k % 10);
+    s.F[k] = density_factor(s.PA, s.PB, s.PAB, k / 10, k % 10);
+  }
+  __syncwarp();
+  // T1 = F W, T2 = F^T W
+  for (int k = lane; k < 100; k += 32) {
+    const int r = k / 10, c = k % 10;
+    double t1 = 0, t2 = 0;
+    for (int l = 0; l < 10; ++l) {
+      t1 += s.F[r * 10 + l] * s.W[l * 10 + c];
+      t2 += s.F[l * 10 + r] * s.W[l * 10 + c];
+    }
+    s.T1[k] = t1;
+    s.T2[k] = t2;
+  }
+  __syncwarp();
+  double adjA[4][4] = {}, adjB[4][4] = {};
+  double dR = 0, g[3] = {0, 0, 0};
+  // two-centre: dE/dW[p][q] = sum_j T1[p][j] L[q][j] + sum_a T2[p][a] L[a][q];
+  // dE/dL[x][y] = sum_g W[g][x] T1[g][y]
+  for (int k = lane; k < 100; k += 32) {
+    const int pp = k / 10, qq = k % 10;
+    double adw = 0;
+    for (int j = 0; j < 10; ++j) adw += s.T1[pp * 10 + j] * s.L[qq * 10 + j] + s.T2[pp * 10 + j] * s.L[j * 10 + qq];
+    if (adw != 0.0) w_adjoint(s.ra.r, pp, qq, adw, adjA);
+    if (s.dL[k] != 0.0) {
+      double mm = 0;
+      for (int g2 = 0; g2 < 10; ++g2) mm += s.W[g2 * 10 + pp] * s.T1[g2 * 10 + qq];
+      dR += s.dL[k] * mm;
+    }
+  }
+  // core attraction (both sides), 10 orbital pairs x 5 axis entries each
+  for (int k = lane; k < 100; k += 32) {
+    const int side = k / 50, g2 = (k % 50) / 5, q = axis_index(k % 5);
+    const double* Lv = side ? s.Lcb : s.Lc;
+    const double* dLv = side ? s.dLcb : s.dLc;
+    if (Lv[q] == 0.0 && dLv[q] == 0.0) continue;
+    const double f = -(side ? A.core : B.core) * atom_factor(side ? s.PB : s.PA, g2);
+    if (f == 0.0) continue;
+    const RotGrad& rg = side ? s.rb : s.ra;
+    w_adjoint(rg.r, g2, q, f * Lv[q], side ? adjB : adjA);
+    dR += f * w_entry(rg.r, g2, q) * dLv[q];
+  }
+  // overlap: 2 x 2 shells x 6 x 6 primitives
+  {
+    double f[4][4];
+    for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < 4; ++j)
+        f[i][j] = ((i == 0 ? A.betaS : A.betaP) + (j == 0 ? B.betaS : B.betaP)) * s.PAB[i][j];
+    const double Rv[3] = {X, Y, Z};
+    for (int k = lane; k < 144; k += 32)
+      overlap_primitive_grad(A, B, Rv, k / 72, (k / 36) % 2, (k / 6) % 6, k % 6, f, g);
+  }
+  if (lane == 0) {
+    double E, dE;
+    core_repulsion(method, A, B, diat[a.slot * kMaxElementSlots + b.slot], R, E, dE);
+    dR += dE;
+  }
+  g[0] += dR * X / R;
+  g[1] += dR * Y / R;
+  g[2] += dR * Z / R;
+  add_rotation_gradient(s.ra, adjA, g);
+  add_rotation_gradient(s.rb, adjB, g);
+  for (int k = 0; k < 3; ++k)
+    for (int o = 16; o > 0; o >>= 1) g[k] += __shfl_xor_sync(0xffffffffu, g[k], o);
+  if (lane == 0) {
+    gpair[(size_t)p * 3 + 0] = g[0];
+    gpair[(size_t)p * 3 + 1] = g[1];
+    gpair[(size_t)p * 3 + 2] = g[2];
+  }
 }
 
 // Atom gradient: sum of the pair gradients (+ for the second atom of a pair,
@@ -182,9 +418,13 @@ void launch_pair_values(const DeviceBatch& b, cudaStream_t s) {
 
 void launch_gradient(const DeviceBatch& b, cudaStream_t s) {
   if (b.npairs > 0) {
-    int th = 64;
-    k_pair_gradient<<<(b.npairs + th - 1) / th, th, 0, s>>>(b.pairs, b.npairs, b.atoms, b.elems, b.diat, b.mols,
-                                                             b.method, b.P, b.gpair);
+    const int th = 128;
+    k_pair_gradient_light<<<(b.npairs + th - 1) / th, th, 0, s>>>(b.pairs, b.npairs, b.atoms, b.elems, b.diat, b.mols,
+                                                                   b.method, b.P, b.gpair);
+  }
+  if (b.nhh_total > 0) {
+    k_pair_gradient_heavy<<<(b.nhh_total + kGradWarps - 1) / kGradWarps, kGradWarps * 32, 0, s>>>(
+        b.hh_pairs, b.nhh_total, b.pairs, b.atoms, b.elems, b.diat, b.mols, b.method, b.P, b.gpair);
   }
   launch_gather_gradient(b, s);
 }

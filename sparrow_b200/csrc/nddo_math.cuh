@@ -113,6 +113,23 @@ SGB_HD void local_entry(const LocalTermTable& tab, int e, double R, const ElemDe
   }
 }
 
+// Entries of the local dA x dB block that the reference copies by symmetry
+// about the bond axis (Local2c2eMatrix.cpp:91-149).
+SGB_HD void local_copies(int dA, int dB, double L[10][10], double dL[10][10]) {
+  if (dB == 10) { L[0][5] = L[0][2]; dL[0][5] = dL[0][2]; }
+  if (dA == 10) { L[5][0] = L[2][0]; dL[5][0] = dL[2][0]; }
+  if (dA == 10 && dB == 10) {
+    const int cp[10][4] = {{3, 3, 1, 1}, {3, 8, 1, 7}, {5, 2, 2, 5}, {5, 5, 2, 2}, {5, 6, 2, 6},
+                           {5, 9, 2, 9}, {6, 5, 6, 2}, {8, 3, 7, 1}, {8, 8, 7, 7}, {9, 5, 9, 2}};
+    for (int k = 0; k < 10; ++k) {
+      L[cp[k][0]][cp[k][1]] = L[cp[k][2]][cp[k][3]];
+      dL[cp[k][0]][cp[k][1]] = dL[cp[k][2]][cp[k][3]];
+    }
+    L[4][4] = 0.5 * (L[2][2] - L[2][5]);
+    dL[4][4] = 0.5 * (dL[2][2] - dL[2][5]);
+  }
+}
+
 // Fill the local dA x dB block (dA, dB in {1, 10}) the way the reference does.
 SGB_HD void local_block(const LocalTermTable& tab, int dA, int dB, double R, const ElemDev& A, const ElemDev& B,
                         bool coreB, double rhoCoreB, double L[10][10], double dL[10][10]) {
@@ -123,19 +140,7 @@ SGB_HD void local_block(const LocalTermTable& tab, int dA, int dB, double R, con
     if (i >= dA || j >= dB) continue;
     local_entry(tab, e, R, A, B, coreB, rhoCoreB, L[i][j], dL[i][j]);
   }
-  // entries that the reference copies by symmetry about the bond axis
-  if (dB == 10) { L[0][5] = L[0][2]; dL[0][5] = dL[0][2]; }
-  if (dA == 10) { L[5][0] = L[2][0]; dL[5][0] = dL[2][0]; }
-  if (dA == 10 && dB == 10) {
-    const int cp[11][4] = {{3, 3, 1, 1}, {3, 8, 1, 7}, {5, 2, 2, 5}, {5, 5, 2, 2}, {5, 6, 2, 6}, {5, 9, 2, 9},
-                           {6, 5, 6, 2}, {8, 3, 7, 1}, {8, 8, 7, 7}, {9, 5, 9, 2}, {0, 0, 0, 0}};
-    for (int k = 0; k < 10; ++k) {
-      L[cp[k][0]][cp[k][1]] = L[cp[k][2]][cp[k][3]];
-      dL[cp[k][0]][cp[k][1]] = dL[cp[k][2]][cp[k][3]];
-    }
-    L[4][4] = 0.5 * (L[2][2] - L[2][5]);
-    dL[4][4] = 0.5 * (dL[2][2] - dL[2][5]);
-  }
+  local_copies(dA, dB, L, dL);
 }
 
 // Rotation coefficients rot[global][local] for s, x, y, z given the pair
@@ -358,78 +363,6 @@ SGB_HD void core_repulsion(int method, const ElemDev& A, const ElemDev& B, const
     E += gs / R * ZZ / ev;
     dE += (dgs / R - gs / (R * R)) * ZZ / ev;
   }
-}
-
-// dE/dR_AB of one pair (R_AB = pos_B - pos_A) for the symmetric density P
-// (N x N, row-major; the pair's AOs start at oa and ob).  Contributions
-// (OneElectronMatrix.cpp:136-229, TwoElectronMatrix.cpp:168-241, repulsion):
-//   sum over ordered AO quadruples of (mn|ls)' [P_mn P_ls - 1/2 P_ml P_ns]
-//   + sum_mn P_mn V'_mn on both atoms + sum (beta_m + beta_n) P_mn S'_mn + E_rep'
-SGB_HD void pair_gradient(const LocalTermTable& tab, int method, const ElemDev& A, const ElemDev& B,
-                          const DiatomicDev& AB, double Xv, double Yv, double Zv, const double* P, int N, int oa,
-                          int ob, double g[3]) {
-  const Dual3 X(Xv, 1, 0, 0), Y(Yv, 0, 1, 0), Z(Zv, 0, 0, 1);
-  const int nA = A.nao, nB = B.nao;
-  double g0 = 0, g1 = 0, g2 = 0;
-  {
-    Dual3 G[10][10];
-    global_block<Dual3>(tab, A, B, X, Y, Z, G);
-    for (int mu = 0; mu < nA; ++mu)
-      for (int nu = 0; nu < nA; ++nu)
-        for (int la = 0; la < nB; ++la)
-          for (int si = 0; si < nB; ++si) {
-            double f = P[(oa + mu) * N + oa + nu] * P[(ob + la) * N + ob + si] -
-                       0.5 * P[(oa + mu) * N + ob + la] * P[(oa + nu) * N + ob + si];
-            const Dual3& I = G[pair_index(mu, nu)][pair_index(la, si)];
-            g0 += f * I.dx;
-            g1 += f * I.dy;
-            g2 += f * I.dz;
-          }
-  }
-  {
-    Dual3 V[10];
-    core_vector<Dual3>(tab, A, B, X, Y, Z, V);
-    for (int mu = 0; mu < nA; ++mu)
-      for (int nu = 0; nu < nA; ++nu) {
-        double f = P[(oa + mu) * N + oa + nu];
-        const Dual3& v = V[pair_index(mu, nu)];
-        g0 += f * v.dx;
-        g1 += f * v.dy;
-        g2 += f * v.dz;
-      }
-    const Dual3 Xr(-Xv, -1, 0, 0), Yr(-Yv, 0, -1, 0), Zr(-Zv, 0, 0, -1);
-    core_vector<Dual3>(tab, B, A, Xr, Yr, Zr, V);
-    for (int mu = 0; mu < nB; ++mu)
-      for (int nu = 0; nu < nB; ++nu) {
-        double f = P[(ob + mu) * N + ob + nu];
-        const Dual3& v = V[pair_index(mu, nu)];
-        g0 += f * v.dx;
-        g1 += f * v.dy;
-        g2 += f * v.dz;
-      }
-  }
-  {
-    Dual3 R[3] = {X, Y, Z};
-    Dual3 S[4][4];
-    overlap_block<Dual3>(A, B, R, S);
-    for (int mu = 0; mu < nA; ++mu)
-      for (int nu = 0; nu < nB; ++nu) {
-        double f = ((mu == 0 ? A.betaS : A.betaP) + (nu == 0 ? B.betaS : B.betaP)) * P[(oa + mu) * N + ob + nu];
-        g0 += f * S[mu][nu].dx;
-        g1 += f * S[mu][nu].dy;
-        g2 += f * S[mu][nu].dz;
-      }
-  }
-  {
-    double Rabs = sqrt(Xv * Xv + Yv * Yv + Zv * Zv), E, dE;
-    core_repulsion(method, A, B, AB, Rabs, E, dE);
-    g0 += dE * Xv / Rabs;
-    g1 += dE * Yv / Rabs;
-    g2 += dE * Zv / Rabs;
-  }
-  g[0] = g0;
-  g[1] = g1;
-  g[2] = g2;
 }
 
 }  // namespace sgb

@@ -293,6 +293,7 @@ extern "C" int32_t sg_calculate_static(const char* method, int32_t n_atoms, cons
   d.nmol = 1;
   d.natoms = n_atoms;
   d.npairs = npairs;
+  d.nhh_total = nhh;
   d.nao_total = nao;
   d.mat_total = (long long)nao * nao;
   d.diis_total = 2LL * kDiisMax * nao * nao;
