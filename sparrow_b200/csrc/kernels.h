@@ -75,6 +75,9 @@ void launch_one_electron(const DeviceBatch& b, cudaStream_t s);
 void launch_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s);
 void launch_gradient(const DeviceBatch& b, cudaStream_t s);
 void launch_gather_gradient(const DeviceBatch& b, cudaStream_t s);
+// Fock matrix F = H + G(P) of the batch's single (large) molecule over the
+// whole GPU; *energy (device) receives the electronic energy of P.
+void launch_fock_grid(const DeviceBatch& b, const double* P, double* F, double* energy, cudaStream_t s);
 // DFTB: pair and on-site terms (+ start density), SCC loop, gradient
 void launch_dftb_setup(const DeviceBatch& b, cudaStream_t s);
 void launch_dftb_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s);

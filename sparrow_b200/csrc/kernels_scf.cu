@@ -126,16 +126,16 @@ __constant__ int c_pair_nu[10] = {0, 1, 1, 2, 2, 2, 3, 3, 3, 3};
 // pair owns its block).  s/p-s/p pairs are handled by a warp each, pairs with
 // an s-only atom by a thread each.
 // Phase 2: diagonal blocks F_AA = H_AA + G_1c(P_AA) + sum of the partners' J_A.
-__device__ double build_fock(const MolDev& m, const AtomDev* __restrict__ atoms, const ElemDev* __restrict__ elems,
+// Fock build, phase 1a: pairs with at most one s/p atom, pair k0, k0 + kstep, ...
+// (one thread each).  Writes the off-diagonal F blocks and the per-pair
+// Coulomb vectors; returns this thread's share of sum P (H + F).
+__device__ double fock_light_pairs(const MolDev& m, const AtomDev* __restrict__ atoms, const ElemDev* __restrict__ elems,
                              const PairDev* __restrict__ pairs, const double* __restrict__ ints,
                              const int* __restrict__ hh_pairs, double* __restrict__ jbuf,
-                             const double* __restrict__ H, const double* __restrict__ P, double* F, double* red,
-                             double* wscratch) {
+                             const double* __restrict__ H, const double* __restrict__ P, double* F, int k0, int kstep) {
   const int N = m.nao;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   double e = 0;
-  // phase 1a: pairs with at most one s/p atom, one thread each
-  for (int k = tid; k < m.npairs; k += blockDim.x) {
+  for (int k = k0; k < m.npairs; k += kstep) {
     const int pi = m.pair0 + k;
     const PairDev pr = pairs[pi];
     const AtomDev aA = atoms[pr.a], aB = atoms[pr.b];
@@ -189,13 +189,23 @@ __device__ double build_fock(const MolDev& m, const AtomDev* __restrict__ atoms,
       e += P[ixh] * (h + f);
     }
   }
-  // phase 1b: s/p-s/p pairs, one warp each
-  double* ws = wscratch + (size_t)warp * kFockWarpScratch;
+  return e;
+}
+
+// Fock build, phase 1b: s/p-s/p pairs h0, h0 + hstep, ... of the molecule's
+// heavy-pair list, one warp each (ws: this warp's kFockWarpScratch doubles).
+__device__ double fock_heavy_pairs(const MolDev& m, const AtomDev* __restrict__ atoms, const ElemDev* __restrict__ elems,
+                             const PairDev* __restrict__ pairs, const double* __restrict__ ints,
+                             const int* __restrict__ hh_pairs, double* __restrict__ jbuf,
+                             const double* __restrict__ H, const double* __restrict__ P, double* F, double* ws, int h0, int hstep) {
+  const int N = m.nao;
+  const int lane = threadIdx.x & 31;
+  double e = 0;
   double* Wsm = ws;
   double* Pab = ws + 100;
   double* pvA = ws + 116;
   double* pvB = ws + 126;
-  for (int h = warp; h < m.nhh; h += nwarps) {
+  for (int h = h0; h < m.nhh; h += hstep) {
     const int pi = hh_pairs[m.hh0 + h];
     const PairDev pr = pairs[pi];
     const int oa = atoms[pr.a].ao0, ob = atoms[pr.b].ao0;
@@ -237,9 +247,18 @@ __device__ double build_fock(const MolDev& m, const AtomDev* __restrict__ atoms,
     }
     __syncwarp();
   }
-  __syncthreads();
-  // phase 2: diagonal blocks
-  for (int idx = tid; idx < m.nat * 10; idx += blockDim.x) {
+  return e;
+}
+
+// Fock build, phase 2 (after every pair of the molecule is done): one-centre
+// blocks for entries i0, i0 + istep, ... of (atom, orbital pair).
+__device__ double fock_diagonal(const MolDev& m, const AtomDev* __restrict__ atoms, const ElemDev* __restrict__ elems,
+                             const PairDev* __restrict__ pairs, const double* __restrict__ ints,
+                             const int* __restrict__ hh_pairs, double* __restrict__ jbuf,
+                             const double* __restrict__ H, const double* __restrict__ P, double* F, int i0, int istep) {
+  const int N = m.nao;
+  double e = 0;
+  for (int idx = i0; idx < m.nat * 10; idx += istep) {
     const int a = idx / 10, p = idx % 10;
     const AtomDev aA = atoms[m.atom0 + a];
     const ElemDev& eA = elems[aA.slot];
@@ -262,6 +281,20 @@ __device__ double build_fock(const MolDev& m, const AtomDev* __restrict__ atoms,
     if (mu != nu) F[(size_t)(aA.ao0 + nu) * N + aA.ao0 + mu] = f;
     e += (mu == nu ? 0.5 : 1.0) * P[i1] * (h + f);
   }
+  return e;
+}
+
+__device__ double build_fock(const MolDev& m, const AtomDev* __restrict__ atoms, const ElemDev* __restrict__ elems,
+                             const PairDev* __restrict__ pairs, const double* __restrict__ ints,
+                             const int* __restrict__ hh_pairs, double* __restrict__ jbuf,
+                             const double* __restrict__ H, const double* __restrict__ P, double* F, double* red,
+                             double* wscratch) {
+  const int tid = threadIdx.x, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  double e = fock_light_pairs(m, atoms, elems, pairs, ints, hh_pairs, jbuf, H, P, F, tid, blockDim.x);
+  e += fock_heavy_pairs(m, atoms, elems, pairs, ints, hh_pairs, jbuf, H, P, F, wscratch + (size_t)warp * kFockWarpScratch,
+                        warp, nwarps);
+  __syncthreads();
+  e += fock_diagonal(m, atoms, elems, pairs, ints, hh_pairs, jbuf, H, P, F, tid, blockDim.x);
   __syncthreads();
   return cta_sum(e, red);
 }
@@ -428,6 +461,72 @@ void launch_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_
   k_scf<<<grid, kScfThreads, bytes, s>>>(b.mols, b.nmol, b.order, b.counter, b.atoms, b.elems, b.pairs, b.ints,
                                          b.hh_pairs, b.jbuf, b.H, b.P, b.F, b.C, b.W1, b.W2, b.eps, b.diis,
                                          b.rotbuf, b.res, sp, in_smem);
+}
+
+}  // namespace sgb
+
+// ---------------------------------------------------------------------------
+// Whole-GPU Fock build of one large molecule (the large-molecule SCF path):
+// the pair phases over the full grid (threads for pairs with hydrogen, warps
+// for s/p pairs), then the one-centre phase in a second launch; sum P (H + F)
+// is accumulated into *energy.
+// ---------------------------------------------------------------------------
+namespace sgb {
+namespace {
+
+__device__ void block_add(double v, double* red, double* out) {
+  v = warp_sum(v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += red[i];
+    atomicAdd(out, s);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_fock_pairs_grid(const MolDev* __restrict__ mols, const AtomDev* __restrict__ atoms,
+                                                         const ElemDev* __restrict__ elems,
+                                                         const PairDev* __restrict__ pairs,
+                                                         const double* __restrict__ ints, const int* __restrict__ hh,
+                                                         double* jbuf, const double* __restrict__ H,
+                                                         const double* __restrict__ P, double* F, double* energy) {
+  __shared__ double red[32];
+  __shared__ double ws[8 * kFockWarpScratch];
+  const MolDev m = mols[0];
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
+  const int gwarp = gtid >> 5, gwarps = gthreads >> 5;
+  double e = fock_light_pairs(m, atoms, elems, pairs, ints, hh, jbuf, H, P, F, gtid, gthreads);
+  e += fock_heavy_pairs(m, atoms, elems, pairs, ints, hh, jbuf, H, P, F, ws + (threadIdx.x >> 5) * kFockWarpScratch,
+                        gwarp, gwarps);
+  block_add(e, red, energy);
+}
+
+__global__ void __launch_bounds__(256) k_fock_diag_grid(const MolDev* __restrict__ mols, const AtomDev* __restrict__ atoms,
+                                                        const ElemDev* __restrict__ elems,
+                                                        const PairDev* __restrict__ pairs,
+                                                        const double* __restrict__ ints, const int* __restrict__ hh,
+                                                        double* jbuf, const double* __restrict__ H,
+                                                        const double* __restrict__ P, double* F, double* energy) {
+  __shared__ double red[32];
+  const MolDev m = mols[0];
+  const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gthreads = gridDim.x * blockDim.x;
+  const double e = fock_diagonal(m, atoms, elems, pairs, ints, hh, jbuf, H, P, F, gtid, gthreads);
+  block_add(e, red, energy);
+}
+
+}  // namespace
+
+void launch_fock_grid(const DeviceBatch& b, const double* P, double* F, double* energy, cudaStream_t s) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaMemsetAsync(energy, 0, sizeof(double), s);
+  k_fock_pairs_grid<<<sms * 8, 256, 0, s>>>(b.mols, b.atoms, b.elems, b.pairs, b.ints, b.hh_pairs, b.jbuf, b.H, P, F,
+                                            energy);
+  k_fock_diag_grid<<<sms * 8, 256, 0, s>>>(b.mols, b.atoms, b.elems, b.pairs, b.ints, b.hh_pairs, b.jbuf, b.H, P, F,
+                                           energy);
 }
 
 }  // namespace sgb
