@@ -74,7 +74,9 @@ int32_t sg_get_n_atoms(const sg_calculator* h, int32_t* n_atoms);
 
 /* Settings keys follow the reference: "molecular_charge", "spin_multiplicity",
  * "spin_mode", "self_consistence_criterion", "density_rmsd_criterion",
- * "max_scf_iterations", "scf_mixer", "method_parameters". */
+ * "max_scf_iterations", "scf_mixer", "method_parameters", and one of this
+ * engine: "scf_path" = "auto" | "batched" | "large" | "large_mixed" (see
+ * sg_batch_set_scf_path). */
 int32_t sg_set_setting_int(sg_calculator* h, const char* key, int64_t value);
 int32_t sg_set_setting_double(sg_calculator* h, const char* key, double value);
 int32_t sg_set_setting_string(sg_calculator* h, const char* key, const char* value);
@@ -105,6 +107,15 @@ void sg_batch_destroy(sg_batch* b);
 const char* sg_batch_last_error(const sg_batch* b);
 int32_t sg_batch_set_scf(sg_batch* b, double self_consistence_criterion, double density_rmsd_criterion,
                          int32_t max_scf_iterations);
+/* SCF path: 0 automatic (a single NDDO molecule of more than 1024 AOs runs
+ * the large-molecule path, everything else the batched persistent kernel),
+ * 1 batched kernel, 2 large-molecule path in FP64 (grid-wide Fock build,
+ * DIIS, SP2 purification on FP64 GEMMs), 3 large-molecule path with the SP2
+ * products in split-BF16 on the tensor cores until rms(dP) < 1e-5, then FP64.
+ * Paths 2 and 3 take a batch of one NDDO molecule.  On the large path the
+ * scf_stats report iterations with mixed-precision purification as
+ * full_diagonalisations and the SP2 steps as jacobi_sweeps. */
+int32_t sg_batch_set_scf_path(sg_batch* b, int32_t path);
 int32_t sg_batch_set_positions(sg_batch* b, const double* xyz_bohr);
 /* enqueue integrals -> SCF -> (gradient) on the device; asynchronous */
 int32_t sg_batch_run(sg_batch* b, uint32_t properties);

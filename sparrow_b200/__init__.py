@@ -81,6 +81,7 @@ def lib():
         "sg_batch_destroy": (None, [_VP]),
         "sg_batch_last_error": (ctypes.c_char_p, [_VP]),
         "sg_batch_set_scf": (ctypes.c_int32, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int32]),
+        "sg_batch_set_scf_path": (ctypes.c_int32, [_VP, ctypes.c_int32]),
         "sg_batch_set_positions": (ctypes.c_int32, [_VP, _D]),
         "sg_batch_run": (ctypes.c_int32, [_VP, ctypes.c_uint32]),
         "sg_batch_results": (ctypes.c_int32, [_VP, _D, _D, _I32, _I32]),
@@ -308,7 +309,9 @@ class Batch:
     copies the energies / gradients back.
     """
 
-    def __init__(self, method, molecules, charges=None, scc=1e-7, rmsd=1e-5, max_iter=100):
+    SCF_PATHS = {"auto": 0, "batched": 1, "large": 2, "large_mixed": 3}
+
+    def __init__(self, method, molecules, charges=None, scc=1e-7, rmsd=1e-5, max_iter=100, scf_path="auto"):
         L = lib()
         self.n_atoms, Z, X = _flatten(molecules)
         ch = None if charges is None else np.ascontiguousarray(charges, dtype=np.int32)
@@ -320,7 +323,16 @@ class Batch:
         self._h = h
         self.n_molecules = len(molecules)
         self._check(L.sg_batch_set_scf(h, scc, rmsd, max_iter))
+        self.set_scf_path(scf_path)
         self._props = SG_PROP_ENERGY
+
+    def set_scf_path(self, path):
+        """"auto", "batched", "large" (one NDDO molecule, grid-wide FP64 SCF with
+        SP2 purification) or "large_mixed" (split-BF16 purification products
+        until rms(dP) < 1e-5, then FP64)."""
+        if path not in self.SCF_PATHS:
+            raise ValueError(f"unknown scf_path {path!r}")
+        self._check(lib().sg_batch_set_scf_path(self._h, self.SCF_PATHS[path]))
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:

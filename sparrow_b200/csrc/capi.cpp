@@ -40,6 +40,7 @@ struct Settings {
   int max_iter = 100;
   std::string mixer = "diis";
   std::string parameters;
+  std::string scf_path = "auto";  // auto | batched | large | large_mixed
 };
 
 class Calculator {
@@ -99,6 +100,10 @@ class Calculator {
     in[0].xyz = xyz_;
     in[0].charge = settings_.charge;
     int rc = batch_->setup(in, error);
+    if (rc) return rc;
+    const std::string& sp_name = settings_.scf_path;
+    rc = batch_->set_scf_path(sp_name == "batched" ? 1 : sp_name == "large" ? 2 : sp_name == "large_mixed" ? 3 : 0,
+                              error);
     if (rc) return rc;
     if (!state_.empty()) {
       rc = batch_->set_start_density(state_.data(), error);
@@ -314,6 +319,10 @@ int32_t sg_set_setting_string(sg_calculator* h, const char* key, const char* v) 
     s.mixer = val == "diis" ? "diis" : "none";
   } else if (k == "method_parameters") {
     s.parameters = val;
+  } else if (k == "scf_path") {
+    if (val != "auto" && val != "batched" && val != "large" && val != "large_mixed")
+      return fail(h, SG_ERR_INVALID_ARGUMENT, "unknown scf_path '" + val + "' (auto, batched, large, large_mixed)");
+    s.scf_path = val;
   } else
     return fail(h, SG_ERR_UNKNOWN_SETTING, "unknown string setting '" + k + "'");
   return SG_OK;
@@ -439,6 +448,11 @@ int32_t sg_batch_set_scf(sg_batch* b, double scc, double rmsd, int32_t max_iter)
   b->sp.rmsd = rmsd;
   b->sp.max_iter = max_iter;
   return SG_OK;
+}
+
+int32_t sg_batch_set_scf_path(sg_batch* b, int32_t path) {
+  if (!b) return SG_ERR_INVALID_ARGUMENT;
+  return b->impl->set_scf_path(path, b->error);
 }
 
 int32_t sg_batch_set_positions(sg_batch* b, const double* xyz) {

@@ -98,6 +98,7 @@ Batch::~Batch() {
   if (stream_) cudaStreamSynchronize(stream_);
   pool_give(false, arena_, arena_bytes_);
   pool_give(true, pinned_, pinned_bytes_);
+  if (large_scratch_) cudaFree(large_scratch_);
   for (auto& e : stage_ev_)
     if (e) cudaEventDestroy(e);
   for (auto& e : user_ev_)
@@ -263,8 +264,9 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
       return kErrOddElectrons;
     }
     md.nocc = md.nel / 2;
-    if (nao > 1024) {
-      err = "molecule " + std::to_string(mi) + " has more than 1024 AOs (batched SCF limit)";
+    if (nao > 1024 && (in.size() > 1 || is_dftb(method_))) {
+      err = "molecule " + std::to_string(mi) + " has more than 1024 AOs: the batched SCF limit (a single NDDO "
+            "molecule of that size runs the large-molecule path)";
       return kErrInvalidArgument;
     }
     // pair p of the molecule is (lo, hi) in row-major order over lo < hi; its
@@ -497,6 +499,19 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
   return kOk;
 }
 
+int Batch::set_scf_path(int path, std::string& err) {
+  if (path < 0 || path > 3) {
+    err = "SCF path must be 0 (automatic), 1 (batched), 2 (large, FP64) or 3 (large, mixed precision)";
+    return kErrInvalidArgument;
+  }
+  if (path >= 2 && (is_dftb(method_) || mols_.size() > 1)) {
+    err = "the large-molecule SCF path takes one NDDO molecule";
+    return kErrInvalidArgument;
+  }
+  scf_path_ = path;
+  return kOk;
+}
+
 int Batch::set_positions(const double* xyz, std::string& err) {
   if (mols_.empty()) {
     err = "no structure";
@@ -560,14 +575,51 @@ int Batch::run(const ScfParams& sp, bool gradient, std::string& err) {
       launches_ += dev_.npairs > 0 ? 2 : 1;
     }
   } else {
+    const int N = mols_[0].nao;
+    const bool large = mols_.size() == 1 && (scf_path_ >= 2 || (scf_path_ == 0 && N > 1024));
+    if (scf_path_ >= 2 && mols_.size() > 1) {
+      err = "the large-molecule SCF path takes one NDDO molecule";
+      return kErrInvalidArgument;
+    }
+    if (!large && mols_[0].nao > 1024) {
+      err = "more than 1024 AOs needs the large-molecule SCF path";
+      return kErrInvalidArgument;
+    }
+    if (large) {
+      const size_t need = large_scf_scratch_bytes(N);
+      if (large_scratch_bytes_ < need) {
+        if (large_scratch_) {
+          cudaStreamSynchronize(stream_);
+          cudaFree(large_scratch_);
+          large_scratch_ = nullptr;
+          large_scratch_bytes_ = 0;
+        }
+        cudaError_t e = cudaMalloc(&large_scratch_, need);
+        if (e != cudaSuccess) {
+          cudaGetLastError();
+          large_scratch_ = nullptr;
+          err = "device allocation of " + std::to_string(need) + " bytes failed: " + cudaGetErrorString(e);
+          return e == cudaErrorMemoryAllocation ? kErrOutOfMemory : kErrCuda;
+        }
+        large_scratch_bytes_ = need;
+      }
+    }
+    dev_.large = large ? 1 : 0;
+    dev_.large_scratch = large ? large_scratch_ : nullptr;
     launch_pair_values(dev_, stream_);
     launches_ += dev_.npairs > 0 ? 1 : 0;
     cudaEventRecord(stage_ev_[1], stream_);
     launch_one_electron(dev_, stream_);
     launches_ += 1;
     cudaEventRecord(stage_ev_[2], stream_);
-    launch_scf(dev_, sp, dev_.scf_grid, stream_);
-    launches_ += 1;
+    if (large) {
+      // host-driven: returns when the SCF is done
+      const int rc = run_large_scf(dev_, mols_[0], sp, scf_path_ == 3 ? 1 : 0, stream_, &launches_, err);
+      if (rc != kOk) return rc;
+    } else {
+      launch_scf(dev_, sp, dev_.scf_grid, stream_);
+      launches_ += 1;
+    }
     cudaEventRecord(stage_ev_[3], stream_);
     if (gradient) {
       launch_gradient(dev_, stream_);

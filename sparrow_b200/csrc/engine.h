@@ -72,6 +72,14 @@ class Batch {
   // the method's default.  Takes effect at the next setup().
   void set_dftb_parameters(const std::string& set) { dftb_set_ = set; }
   const std::string& dftb_parameters() const { return dftb_set_; }
+  // SCF path: 0 automatic (one NDDO molecule of more than 1024 AOs runs the
+  // large-molecule path, anything else the batched kernel), 1 batched
+  // kernel, 2 large-molecule path in FP64, 3 large-molecule path with
+  // mixed-precision purification.  Paths 2 and 3 take one NDDO molecule.
+  int set_scf_path(int path, std::string& err);
+  int scf_path() const { return scf_path_; }
+  // Path taken by the last run(): 1 batched kernel, 2 / 3 large-molecule
+  bool last_run_large() const { return dev_.large != 0; }
   int n_molecules() const { return (int)mols_.size(); }
   int n_atoms() const { return (int)atoms_.size(); }
   long long device_bytes() const { return arena_bytes_; }
@@ -104,6 +112,9 @@ class Batch {
   std::vector<int> ao_atom_, order_;
   long long npairs_ = 0, nhh_ = 0;  // pair and heavy-pair tables are built on the device
   std::string dftb_set_;
+  int scf_path_ = 0;
+  void* large_scratch_ = nullptr;
+  size_t large_scratch_bytes_ = 0;
   int scf_grid_ = 0;
   int scf_grid_nao_ = 0;
   int launches_ = 0;

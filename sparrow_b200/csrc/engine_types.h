@@ -110,6 +110,7 @@ enum DeviceStatus : int {
   kDevJacobiNotConverged = 1,
   kDevDiisSingular = 2,
   kDevNonFinite = 3,
+  kDevSp2NotConverged = 4,  // large-molecule path: SP2 purification did not settle
 };
 
 }  // namespace sgb

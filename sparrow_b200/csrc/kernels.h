@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <string>
+
 #include "engine_types.h"
 
 namespace sgb {
@@ -50,6 +52,8 @@ struct DeviceBatch {
   double* grad = nullptr;           // [natoms * 3]
   MolResult* res = nullptr;         // [nmol]
   int use_guess = 1;                // 0: P already holds a start density
+  int large = 0;                    // 1: one molecule over the whole GPU (large-molecule path)
+  void* large_scratch = nullptr;    // [large_scf_scratch_bytes(nao)] when large
   // DFTB (H holds H0)
   int dftb_order = 0;               // 2 or 3 for DFTB batches
   long long gam_total = 0;
@@ -82,6 +86,15 @@ void launch_fock_grid(const DeviceBatch& b, const double* P, double* F, double* 
 void launch_dftb_setup(const DeviceBatch& b, cudaStream_t s);
 void launch_dftb_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s);
 void launch_dftb_gradient(const DeviceBatch& b, cudaStream_t s);
+// Large-molecule SCF of the batch's single molecule m (host-driven grid
+// kernels, SP2 density): precision 0 FP64, 1 mixed (split-BF16 SP2 products
+// until rms(dP) < 1e-5, then FP64).  Synchronises the stream a few times per
+// iteration; fills res[0] (full_diag: iterations with mixed-precision SP2,
+// jacobi_sweeps: SP2 steps in total) and adds its kernel launches to
+// *launches.  Returns a Status.
+int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, int precision, cudaStream_t s,
+                  int* launches, std::string& err);
+size_t large_scf_scratch_bytes(long long nao);
 int scf_max_grid(int max_nao);
 size_t scf_rotation_bytes_per_cta();
 

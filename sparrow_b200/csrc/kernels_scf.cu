@@ -42,22 +42,15 @@ namespace sgb {
 //   two atoms:  1/2 (beta_mu + beta_nu) S_mu,nu
 // start density (NDDODensityGuess.cpp:31-66): S * n_el / (2N) between atoms,
 // zero within an atom off the diagonal, core charge / n_AO on the diagonal.
-__global__ void __launch_bounds__(kScfThreads) k_one_electron(const MolDev* __restrict__ mols,
-                                                              const AtomDev* __restrict__ atoms,
-                                                              const ElemDev* __restrict__ elems,
-                                                              const PairDev* __restrict__ pairs,
-                                                              const int* __restrict__ ao_atom,
-                                                              const double* __restrict__ vcore,
-                                                              const double* __restrict__ ovl,
-                                                              const double* __restrict__ erep, double* Hall,
-                                                              double* Pall, MolResult* res, int write_guess) {
-  __shared__ double red[32];
-  const MolDev m = mols[blockIdx.x];
+// Entries idx0, idx0 + step, ... of H (and of the start density when
+// write_guess) of molecule m.
+__device__ void one_electron_range(const MolDev& m, const AtomDev* __restrict__ atoms,
+                                   const ElemDev* __restrict__ elems, const int* __restrict__ ao_atom,
+                                   const double* __restrict__ vcore, const double* __restrict__ ovl, double* H,
+                                   double* P, int write_guess, long long idx0, long long step) {
   const int N = m.nao;
-  double* H = Hall + m.mat_off;
-  double* P = Pall + m.mat_off;
-  for (int idx = threadIdx.x; idx < N * N; idx += blockDim.x) {
-    const int i = idx / N, j = idx % N;
+  for (long long idx = idx0; idx < (long long)N * N; idx += step) {
+    const int i = (int)(idx / N), j = (int)(idx % N);
     const int A = ao_atom[m.ao_base + i], B = ao_atom[m.ao_base + j];
     const AtomDev aA = atoms[A], aB = atoms[B];
     const ElemDev& eA = elems[aA.slot];
@@ -84,16 +77,60 @@ __global__ void __launch_bounds__(kScfThreads) k_one_electron(const MolDev* __re
     H[idx] = h;
     if (write_guess) P[idx] = p;
   }
+}
+
+__global__ void __launch_bounds__(kScfThreads) k_one_electron(const MolDev* __restrict__ mols,
+                                                              const AtomDev* __restrict__ atoms,
+                                                              const ElemDev* __restrict__ elems,
+                                                              const int* __restrict__ ao_atom,
+                                                              const double* __restrict__ vcore,
+                                                              const double* __restrict__ ovl,
+                                                              const double* __restrict__ erep, double* Hall,
+                                                              double* Pall, MolResult* res, int write_guess) {
+  __shared__ double red[32];
+  const MolDev m = mols[blockIdx.x];
+  one_electron_range(m, atoms, elems, ao_atom, vcore, ovl, Hall + m.mat_off, Pall + m.mat_off, write_guess,
+                     threadIdx.x, blockDim.x);
   double e = 0;
   for (int k = threadIdx.x; k < m.npairs; k += blockDim.x) e += erep[m.pair0 + k];
   e = cta_sum(e, red);
   if (threadIdx.x == 0) res[blockIdx.x].e_rep = e;
 }
 
+// The same for the single molecule of a batch over the whole grid; e_rep is
+// accumulated into res[0].e_rep (zeroed by the launcher).
+__global__ void __launch_bounds__(256) k_one_electron_grid(const MolDev* __restrict__ mols,
+                                                           const AtomDev* __restrict__ atoms,
+                                                           const ElemDev* __restrict__ elems,
+                                                           const int* __restrict__ ao_atom,
+                                                           const double* __restrict__ vcore,
+                                                           const double* __restrict__ ovl,
+                                                           const double* __restrict__ erep, double* H, double* P,
+                                                           MolResult* res, int write_guess) {
+  __shared__ double red[32];
+  const MolDev m = mols[0];
+  const long long gtid = blockIdx.x * (long long)blockDim.x + threadIdx.x, gthreads = (long long)gridDim.x * blockDim.x;
+  one_electron_range(m, atoms, elems, ao_atom, vcore, ovl, H + m.mat_off, P + m.mat_off, write_guess, gtid, gthreads);
+  double e = 0;
+  for (long long k = gtid; k < m.npairs; k += gthreads) e += erep[m.pair0 + k];
+  e = cta_sum(e, red);
+  if (threadIdx.x == 0) atomicAdd(&res[0].e_rep, e);
+}
+
 void launch_one_electron(const DeviceBatch& b, cudaStream_t s) {
   if (b.nmol == 0) return;
-  k_one_electron<<<b.nmol, kScfThreads, 0, s>>>(b.mols, b.atoms, b.elems, b.pairs, b.ao_atom, b.vcore, b.ovl,
-                                                b.erep, b.H, b.P, b.res, b.use_guess);
+  if (b.large) {
+    // one large molecule: spread H over the whole GPU
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaMemsetAsync(&b.res[0].e_rep, 0, sizeof(double), s);
+    k_one_electron_grid<<<sms * 4, 256, 0, s>>>(b.mols, b.atoms, b.elems, b.ao_atom, b.vcore, b.ovl, b.erep, b.H,
+                                                b.P, b.res, b.use_guess);
+    return;
+  }
+  k_one_electron<<<b.nmol, kScfThreads, 0, s>>>(b.mols, b.atoms, b.elems, b.ao_atom, b.vcore, b.ovl, b.erep, b.H,
+                                                b.P, b.res, b.use_guess);
 }
 
 // ---------------------------------------------------------------------------
