@@ -116,6 +116,10 @@ int32_t sg_batch_set_scf(sg_batch* b, double self_consistence_criterion, double 
  * scf_stats report iterations with mixed-precision purification as
  * full_diagonalisations and the SP2 steps as jacobi_sweeps. */
 int32_t sg_batch_set_scf_path(sg_batch* b, int32_t path);
+/* SCF path 3: rms(dP) below which the purification switches from split-BF16
+ * to FP64 (default 1e-5; also when the mixed densities stop halving below
+ * 1e-4) */
+int32_t sg_batch_set_mixed_switch(sg_batch* b, double density_rmsd);
 int32_t sg_batch_set_positions(sg_batch* b, const double* xyz_bohr);
 /* enqueue integrals -> SCF -> (gradient) on the device; asynchronous */
 int32_t sg_batch_run(sg_batch* b, uint32_t properties);

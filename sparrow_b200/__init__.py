@@ -82,6 +82,7 @@ def lib():
         "sg_batch_last_error": (ctypes.c_char_p, [_VP]),
         "sg_batch_set_scf": (ctypes.c_int32, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int32]),
         "sg_batch_set_scf_path": (ctypes.c_int32, [_VP, ctypes.c_int32]),
+        "sg_batch_set_mixed_switch": (ctypes.c_int32, [_VP, ctypes.c_double]),
         "sg_batch_set_positions": (ctypes.c_int32, [_VP, _D]),
         "sg_batch_run": (ctypes.c_int32, [_VP, ctypes.c_uint32]),
         "sg_batch_results": (ctypes.c_int32, [_VP, _D, _D, _I32, _I32]),
@@ -333,6 +334,10 @@ class Batch:
         if path not in self.SCF_PATHS:
             raise ValueError(f"unknown scf_path {path!r}")
         self._check(lib().sg_batch_set_scf_path(self._h, self.SCF_PATHS[path]))
+
+    def set_mixed_switch(self, rmsd):
+        """rms(dP) below which "large_mixed" purifies in FP64 (default 1e-5)."""
+        self._check(lib().sg_batch_set_mixed_switch(self._h, rmsd))
 
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:

@@ -455,6 +455,12 @@ int32_t sg_batch_set_scf_path(sg_batch* b, int32_t path) {
   return b->impl->set_scf_path(path, b->error);
 }
 
+int32_t sg_batch_set_mixed_switch(sg_batch* b, double rmsd) {
+  if (!b || !(rmsd > 0) || !std::isfinite(rmsd)) return SG_ERR_INVALID_ARGUMENT;
+  b->sp.mixed_switch_rmsd = rmsd;
+  return SG_OK;
+}
+
 int32_t sg_batch_set_positions(sg_batch* b, const double* xyz) {
   if (!b || !xyz) return SG_ERR_INVALID_ARGUMENT;
   return b->impl->set_positions(xyz, b->error);

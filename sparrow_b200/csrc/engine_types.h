@@ -102,6 +102,9 @@ struct ScfParams {
   int diis_size = kDiisMax;
   int jacobi_max_sweeps = 30;
   int pad = 0;
+  // large-molecule mixed-precision path: purification switches from split-BF16
+  // to FP64 once rms(Delta P) falls below this (or stops halving below 1e-4)
+  double mixed_switch_rmsd = 1e-5;
 };
 
 // Device failure codes (MolResult::status)

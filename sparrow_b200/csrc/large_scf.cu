@@ -11,12 +11,15 @@
 //                  (e_max - e_min) from Gershgorin bounds, then X <- X^2 or
 //                  2X - X^2, whichever trace is closer to n_occ, until X is
 //                  idempotent; P = 2X.  Only matrix products: no eigensolver.
-// Precision: FP64 throughout, or "mixed": the SP2 products run on the tensor
-// cores as six BF16 GEMMs of a three-term split (X = X1 + X2 + X3, keeping
-// X1X1 + X1X2 + X2X1 + X1X3 + X2X2 + X3X1) with FP32 accumulation.  FP64
+// Precision: FP64 throughout (X X as a symmetric rank-k update, half the
+// flops of a GEMM), or "mixed": the SP2 products run on the tensor cores from
+// a three-term BF16 split (X = X1 + X2 + X3, keeping X1X1 + X1X2 + X2X1 +
+// X1X3 + X2X2 + X3X1, as one GEMM of K = 4N by symmetry) with FP32
+// accumulation.  FP64
 // stays for the Fock build, DIIS, energy and gradient, and once the density
-// change falls below 1e-5 the remaining iterations run SP2 in FP64 (the
-// residual correction), so the converged density is the FP64 one.
+// change falls below a switch threshold (1e-5 by default) the remaining
+// iterations run SP2 in FP64 (the residual correction), so the converged
+// density is the FP64 one.
 // GEMMs use cuBLAS (plain library GEMMs); the rest are the kernels below.
 #include <cublas_v2.h>
 #include <cuda_bf16.h>
@@ -66,19 +69,20 @@ __device__ __forceinline__ double key_to_double(unsigned long long u) {
   return __longlong_as_double((long long)((u & 0x8000000000000000ull) ? (u & 0x7fffffffffffffffull) : ~u));
 }
 
-// Block sums of (a, b) added into out[0], out[1].
+// Block sums of (a, b) added into out[0], out[1] (1-D or 2-D blocks).
 __device__ void block_add2(double a, double b, double* out) {
   __shared__ double r0[kLT / 32], r1[kLT / 32];
+  const int t = threadIdx.y * blockDim.x + threadIdx.x, nw = (blockDim.x * blockDim.y) >> 5;
   a = lw_sum(a);
   b = lw_sum(b);
-  if ((threadIdx.x & 31) == 0) {
-    r0[threadIdx.x >> 5] = a;
-    r1[threadIdx.x >> 5] = b;
+  if ((t & 31) == 0) {
+    r0[t >> 5] = a;
+    r1[t >> 5] = b;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (t == 0) {
     double x = 0, y = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+    for (int w = 0; w < nw; ++w) {
       x += r0[w];
       y += r1[w];
     }
@@ -108,26 +112,72 @@ __global__ void __launch_bounds__(kLT) k_sp2_init(const double* __restrict__ F, 
 // One SP2 step from the product X2 = X X: with n_occ the target trace,
 // X <- X2 when |tr(X2) - n_occ| < |2 tr(X) - tr(X2) - n_occ|, else 2X - X2
 // (tr(X), tr(X2) in cur[0], cur[1]); the traces of the new X go to next.
-template <typename T>
-__global__ void __launch_bounds__(kLT) k_sp2_step(double* X, const T* __restrict__ X2, int N, double nocc,
-                                                  const double* __restrict__ cur, double* next) {
+// Only the upper triangle (column >= row) of X2 holds the product (a
+// symmetric rank-k update); 32 x 32 tiles (block 32 x 8), lower tiles read
+// their mirror tile through shared memory.
+__global__ void __launch_bounds__(kLT) k_sp2_step_upper(double* X, const double* __restrict__ X2, int N, double nocc,
+                                                        const double* __restrict__ cur, double* next) {
+  __shared__ double tile[32][33];
   const double tr = cur[0], tr2 = cur[1];
   const int square = fabs(tr2 - nocc) < fabs(2.0 * tr - tr2 - nocc);
+  const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32, tx = threadIdx.x, ty = threadIdx.y;
+  const bool mirror = blockIdx.y > blockIdx.x;
+  if (mirror) {
+    for (int r = ty; r < 32; r += 8) {
+      const int i = j0 + r, j = i0 + tx;  // tile (j0.., i0..) of the upper triangle
+      tile[r][tx] = (i < N && j < N) ? X2[(size_t)i * N + j] : 0.0;
+    }
+    __syncthreads();
+  }
   double t = 0, t2 = 0;
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < (size_t)N * N; k += (size_t)gridDim.x * blockDim.x) {
-    const double x2 = (double)X2[k];
+  for (int r = ty; r < 32; r += 8) {
+    const int i = i0 + r, j = j0 + tx;
+    if (i >= N || j >= N) continue;
+    const size_t k = (size_t)i * N + j;
+    // diagonal tiles: the strictly lower entries come from their mirror
+    const double x2 = mirror ? tile[tx][r] : (j >= i ? X2[k] : X2[(size_t)j * N + i]);
     const double x = square ? x2 : 2.0 * X[k] - x2;
     X[k] = x;
     t2 += x * x;
-    if (k % (N + 1) == 0) t += x;
+    if (i == j) t += x;
+  }
+  block_add2(t, t2, next);
+}
+
+// The same step when the product is X X = A + A^T (A in FP32 from the
+// split-BF16 GEMM); 32 x 32 tiles (block 32 x 8), the mirror tile of A read
+// through shared memory.
+__global__ void __launch_bounds__(kLT) k_sp2_step_sym(double* X, const float* __restrict__ A, int N, double nocc,
+                                                      const double* __restrict__ cur, double* next) {
+  __shared__ float tile[32][33];
+  const double tr = cur[0], tr2 = cur[1];
+  const int square = fabs(tr2 - nocc) < fabs(2.0 * tr - tr2 - nocc);
+  const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32, tx = threadIdx.x, ty = threadIdx.y;
+  for (int r = ty; r < 32; r += 8) {
+    const int i = j0 + r, j = i0 + tx;
+    tile[r][tx] = (i < N && j < N) ? A[(size_t)i * N + j] : 0.0f;
+  }
+  __syncthreads();
+  double t = 0, t2 = 0;
+  for (int r = ty; r < 32; r += 8) {
+    const int i = i0 + r, j = j0 + tx;
+    if (i >= N || j >= N) continue;
+    const size_t k = (size_t)i * N + j;
+    const double x2 = (double)A[k] + (double)tile[tx][r];
+    const double x = square ? x2 : 2.0 * X[k] - x2;
+    X[k] = x;
+    t2 += x * x;
+    if (i == j) t += x;
   }
   block_add2(t, t2, next);
 }
 
 // Three-term BF16 split X = X1 + X2 + X3 (each term the rounding of the
-// remainder), written as L = [X1 X2 X3] and R = [X1 X1 X1 X2 X2] (blocks of
-// n entries) so that X X ~ L[:, 0:3n] R1^T + L[:, 0:2n] R2^T + X1 X3 in three
-// GEMMs (X and every term are symmetric).
+// remainder).  With every term symmetric,
+//   X1 X1 + X1 X2 + X2 X1 + X1 X3 + X3 X1 + X2 X2 = A + A^T,
+//   A = X1 (X1 / 2) + X1 X2 + X1 X3 + X2 (X2 / 2) = L R^T,
+// L = [X1 X1 X1 X2], R = [X1/2 X2 X3 X2/2] (blocks of n entries): one GEMM
+// with K = 4N (halving is exact in BF16).
 __global__ void __launch_bounds__(kLT) k_split3(const double* __restrict__ X, size_t n, __nv_bfloat16* L,
                                                 __nv_bfloat16* R) {
   for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
@@ -136,14 +186,15 @@ __global__ void __launch_bounds__(kLT) k_split3(const double* __restrict__ X, si
     const double r1 = x - (double)__bfloat162float(a);
     const __nv_bfloat16 b = __double2bfloat16(r1);
     const double r2 = r1 - (double)__bfloat162float(b);
+    const __nv_bfloat16 half = __float2bfloat16(0.5f);
     L[k] = a;
-    L[n + k] = b;
-    L[2 * n + k] = __double2bfloat16(r2);
-    R[k] = a;
-    R[n + k] = a;
-    R[2 * n + k] = a;
-    R[3 * n + k] = b;
-    R[4 * n + k] = b;
+    L[n + k] = a;
+    L[2 * n + k] = a;
+    L[3 * n + k] = b;
+    R[k] = __hmul(a, half);
+    R[n + k] = b;
+    R[2 * n + k] = __double2bfloat16(r2);
+    R[3 * n + k] = __hmul(b, half);
   }
 }
 
@@ -295,7 +346,7 @@ bool diis_solve(const double* bm, int n, double* coef) {
 
 size_t large_scf_scratch_bytes(long long nao) {
   const size_t NN = (size_t)nao * nao;
-  return kStateBytes + align256(3 * NN * 2) + align256(5 * NN * 2) + align256(NN * 4);
+  return kStateBytes + align256(4 * NN * 2) + align256(4 * NN * 2) + align256(NN * 4);
 }
 
 namespace {
@@ -324,14 +375,16 @@ const char* blas_message(cublasStatus_t st) {
   }
 }
 
-// SP2 stop rule on the idempotency measure e_j = tr(X_j) - tr(X_j^2) of the
-// j-th iterate (hp holds the trace pairs): e_j below 1e-14 N, or, once every
-// eigenvalue is within about 0.1 of 0 or 1 (e_j < 0.1), no decrease against
-// two steps before (the rounding floor of the working precision).
+// SP2 stop rule on the idempotency measure e_j = tr(X_j) - tr(X_j^2) =
+// sum lambda (1 - lambda) of the j-th iterate (hp holds the trace pairs),
+// which bounds every eigenvalue's distance from 0 or 1: e_j below 1e-12 N
+// (the step already queued behind X_j squares that distance away), or, once
+// every eigenvalue is within about 0.1 of 0 or 1 (e_j < 0.1), no decrease
+// against two steps before (the rounding floor of the working precision).
 bool sp2_converged(const double* hp, int j, int N) {
   const double e = std::fabs(hp[2 * j] - hp[2 * j + 1]);
   if (!std::isfinite(e)) return true;
-  if (e < 1e-14 * N) return true;
+  if (e < 1e-12 * N) return true;
   return j >= 2 && e < 0.1 && e >= std::fabs(hp[2 * (j - 2)] - hp[2 * (j - 2) + 1]);
 }
 
@@ -357,8 +410,8 @@ int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, in
   char* scr = static_cast<char*>(b.large_scratch);
   double* st = reinterpret_cast<double*>(scr);
   __nv_bfloat16* L = reinterpret_cast<__nv_bfloat16*>(scr + kStateBytes);
-  __nv_bfloat16* R = reinterpret_cast<__nv_bfloat16*>(scr + kStateBytes + align256(3 * NN * 2));
-  float* C32 = reinterpret_cast<float*>(scr + kStateBytes + align256(3 * NN * 2) + align256(5 * NN * 2));
+  __nv_bfloat16* R = reinterpret_cast<__nv_bfloat16*>(scr + kStateBytes + align256(4 * NN * 2));
+  float* C32 = reinterpret_cast<float*>(scr + kStateBytes + align256(4 * NN * 2) + align256(4 * NN * 2));
   double* histF = b.diis;
   double* histE = b.diis + (size_t)kDiisMax * NN;
   double* X = b.C;
@@ -377,7 +430,7 @@ int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, in
   const int msize = sp.diis_size < 1 ? 1 : (sp.diis_size > kDiisMax ? kDiisMax : sp.diis_size);
   double bmat[kDiisMax * kDiisMax] = {};
   int nhist = 0, head = 0, nl = 0;
-  double Eold = 0, last_dE = 0, last_rms = 0;
+  double Eold = 0, last_dE = 0, last_rms = 0, prev_rms = 1e300;
   int it = 0, converged = 0, status = kDevOk, sp2_total = 0, mixed_iters = 0;
   bool mixed = precision == 1;
   const dim3 tgrid((N + 31) / 32, (N + 31) / 32), tblock(32, 8);
@@ -430,20 +483,15 @@ int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, in
       double* cur = st + kSlotTraces + 2 * k;
       if (use_mixed) {
         k_split3<<<grid, kLT, 0, s>>>(X, NN, L, R);
-        // X1 X1 + X2 X1 + X3 X1, then + X1 X2 + X2 X2, then + X1 X3
-        bs = cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_T, N, N, 3 * N, &onef, L, CUDA_R_16BF, N, R, CUDA_R_16BF, N,
+        bs = cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_T, N, N, 4 * N, &onef, L, CUDA_R_16BF, N, R, CUDA_R_16BF, N,
                           &zerof, C32, CUDA_R_32F, N, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT);
-        if (bs == CUBLAS_STATUS_SUCCESS)
-          bs = cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_T, N, N, 2 * N, &onef, L, CUDA_R_16BF, N, R + 3 * NN,
-                            CUDA_R_16BF, N, &onef, C32, CUDA_R_32F, N, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT);
-        if (bs == CUBLAS_STATUS_SUCCESS)
-          bs = cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_N, N, N, N, &onef, L, CUDA_R_16BF, N, L + 2 * NN, CUDA_R_16BF,
-                            N, &onef, C32, CUDA_R_32F, N, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT);
-        k_sp2_step<float><<<grid, kLT, 0, s>>>(X, C32, N, nocc, cur, cur + 2);
+        k_sp2_step_sym<<<tgrid, tblock, 0, s>>>(X, C32, N, nocc, cur, cur + 2);
         nl += 2;
       } else {
-        bs = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, N, N, N, &one, X, N, X, N, &zero, X2, N);
-        k_sp2_step<double><<<grid, kLT, 0, s>>>(X, X2, N, nocc, cur, cur + 2);
+        // X X = X X^T: half the flops of a GEMM; the column-major lower
+        // triangle is the row-major upper one
+        bs = cublasDsyrk(h, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, N, N, &one, X, N, &zero, X2, N);
+        k_sp2_step_upper<<<tgrid, tblock, 0, s>>>(X, X2, N, nocc, cur, cur + 2);
         ++nl;
       }
       if (bs != CUBLAS_STATUS_SUCCESS) {
@@ -486,7 +534,9 @@ int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, in
     // the residual correction: once the mixed density is this close, the
     // remaining purifications run in FP64 (convergence is only accepted on
     // an FP64 density)
-    if (mixed && rms < 1e-5) mixed = false;
+    // (or when the mixed densities stop improving: the precision floor)
+    if (mixed && (rms < sp.mixed_switch_rmsd || (rms < 1e-4 && rms > 0.5 * prev_rms))) mixed = false;
+    prev_rms = rms;
     if (dE_ok && rms < sp.rmsd && !use_mixed) {
       converged = 1;
       break;
