@@ -16,7 +16,9 @@ inputs resident in HBM; `e2e` is the same metric through sg_batch_calculate
 from host buffers (host setup, H2D copies, kernels, D2H of energies and
 gradients); `roofline` is the dominant kernel (the persistent SCF kernel)
 against the measured FP64 GEMM rate; `cpu_baseline` is the oracle on a
-bounded random sample of the same molecules.
+bounded random sample of the same molecules.  Side legs (rank 0): the plain
+one-molecule-per-launch GPU form, the request server's p50/p99 latency, and
+the large-molecule path on (H2O)_256/512/1024 in FP64 and mixed precision.
 """
 import argparse
 import json
@@ -49,6 +51,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0, help="target CPU time of the cpu_baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-serving", action="store_true", help="skip the request-server latency leg")
+    p.add_argument("--no-large", action="store_true", help="skip the large-molecule (water cluster) leg")
     p.add_argument("--serving-loads", default="250,500,1000,2000", help="offered loads (req/s) of the serving leg")
     return p.parse_args()
 
@@ -200,6 +203,53 @@ def serving_leg(loads=(250, 500, 1000, 2000), seconds=3.0, plain_count=48, seed=
     out["plain_gpu"] = {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                         "throughput_rps": 1e3 / float(lat.mean()), "requests": int(lat.size)}
     return out
+
+
+def large_leg(sizes=(256, 512, 1024), seed=0):
+    """Mixed-precision PM6 on large water clusters (the large-molecule path):
+    per size the FP64 path and the split-BF16 path (energy + gradient), device
+    ms of the SCF stage, wall ms of run + results, and the energy error of the
+    mixed path against the FP64 GPU path and, where the oracle's fixture
+    exists (tests/golden/large_water_pm6_<n>.json), of both against the
+    oracle."""
+    import numpy as np
+    import sparrow_b200
+    from sparrow_b200 import geometry
+    rows = []
+    warm = True
+    for n in sizes:
+        Z, xa = geometry.water_cluster(n, seed=seed)
+        x = geometry.to_bohr(xa)
+        gold = None
+        gp = os.path.join(ROOT, "tests", "golden", "large_water_pm6_%d.json" % n)
+        if os.path.exists(gp):
+            with open(gp) as f:
+                gold = json.load(f)
+        row = {"waters": n, "nao": 6 * n, "atoms": 3 * n}
+        for path in ("large", "large_mixed"):
+            reps = 2 if warm else 1  # the first run of the process pays cuBLAS module loading
+            for _ in range(reps):
+                b = sparrow_b200.Batch("PM6", [(Z, x)], scc=SCC, rmsd=RMSD, max_iter=MAX_ITER, scf_path=path)
+                t0 = time.perf_counter()
+                b.run(gradients=True)
+                e, g, it, conv = b.results()
+                wall = time.perf_counter() - t0
+                st = b.stage_times()
+                nm, ns, _ = b.scf_stats()
+                del b
+            r = {"energy": float(e[0]), "converged": bool(conv[0]), "iterations": int(it[0]),
+                 "mixed_iterations": int(nm[0]), "sp2_steps": int(ns[0]), "scf_ms": float(st[2]),
+                 "total_device_ms": float(sum(st)), "wall_ms": wall * 1e3}
+            if gold is not None:
+                r["dE_vs_oracle"] = float(e[0]) - gold["energy"]
+                r["max_dgrad_vs_oracle"] = float(np.max(np.abs(g[0].reshape(-1) - np.array(gold["gradient"]))))
+            row[path] = r
+        warm = False
+        row["dE_mixed_vs_fp64"] = row["large_mixed"]["energy"] - row["large"]["energy"]
+        row["speedup_mixed_over_fp64"] = row["large"]["total_device_ms"] / row["large_mixed"]["total_device_ms"]
+        rows.append(row)
+    return {"workload": "PM6 (H2O)_n, n in %s, seed %d, one molecule over the whole GPU, energy+gradient, "
+                        "rms dP 1e-8" % (list(sizes), seed), "sizes": rows}
 
 
 def host_cores():
@@ -433,6 +483,10 @@ def run_engine(args, rank, world):
     if rank == 0 and not args.no_serving:
         serving = serving_leg(loads=tuple(float(v) for v in args.serving_loads.split(",")))
 
+    large = None
+    if rank == 0 and not args.no_large:
+        large = large_leg()
+
     # roofline of the SCF kernel (average launch)
     scf_ms = stage_sum[2] / args.steps
     flops = scf_flops(mols, it)
@@ -463,6 +517,7 @@ def run_engine(args, rank, world):
         "cpu_baseline": cpu,
         "plain_gpu": plain,
         "serving": serving,
+        "large_molecules": large,
         "clocks": clk,
     }
     if rank == 0:

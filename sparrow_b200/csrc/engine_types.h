@@ -95,13 +95,18 @@ struct MolResult {
   long long cycles[5];
 };
 
+#ifndef SGB_COLD_SWEEPS
+#define SGB_COLD_SWEEPS 3
+#endif
 struct ScfParams {
   double scc = 1e-7;   // |Delta E| criterion (Hartree)
   double rmsd = 1e-5;  // rms(Delta P) criterion
   int max_iter = 100;
   int diis_size = kDiisMax;
   int jacobi_max_sweeps = 30;
-  int pad = 0;
+  // cap on the sweeps of the first (cold) diagonalisation, which only has to
+  // separate occupied from virtual orbitals
+  int cold_sweeps = SGB_COLD_SWEEPS;
   // large-molecule mixed-precision path: purification switches from split-BF16
   // to FP64 once rms(Delta P) falls below this (or stops halving below 1e-4)
   double mixed_switch_rmsd = 1e-5;

@@ -317,10 +317,10 @@ __global__ void __launch_bounds__(kScfThreads) k_dftb_scf(
       if (have_orbitals) need_full = ov_rotation(N, no, F, Ct, W1, W2, eps, drift, sh);
       if (need_full) {
         const int sw = full_diagonalise(N, F, Ct, W1, W2, eps, Apk ? Apk : F, Apk ? packed_bytes : 0, have_orbitals,
-                                        rot, cap_rounds, have_orbitals ? sp.jacobi_max_sweeps : 6,
+                                        rot, cap_rounds, have_orbitals ? sp.jacobi_max_sweeps : sp.cold_sweeps,
                                         have_orbitals ? 1e-10 : 1e-3, sh);
         if (sw < 0 && have_orbitals) status = kDevJacobiNotConverged;
-        nsweeps += sw < 0 ? (have_orbitals ? sp.jacobi_max_sweeps : 6) : sw;
+        nsweeps += sw < 0 ? (have_orbitals ? sp.jacobi_max_sweeps : sp.cold_sweeps) : sw;
         ++nfull;
         have_orbitals = true;
         drift = 0;

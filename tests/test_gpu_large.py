@@ -94,3 +94,24 @@ def test_large_path_rejects_batches_and_dftb():
         sparrow_b200.Batch("DFTB2", mols[:1], scf_path="large")
     with pytest.raises(ValueError):
         sparrow_b200.Batch("PM6", mols[:1], scf_path="fast")
+
+
+def _fixtures():
+    import glob
+    import os
+    return sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "large_water_pm6_*.json")))
+
+
+@pytest.mark.parametrize("fixture", _fixtures())
+def test_large_clusters_match_oracle_fixture(fixture):
+    # the oracle's converged (H2O)_256 / (H2O)_512 PM6 energies and gradients
+    # (tests/golden/make_large_water_golden.py), FP64 and mixed-precision paths
+    import json
+    gold = json.load(open(fixture))
+    Z, xa = geometry.water_cluster(gold["waters"], seed=gold["seed"])
+    x = geometry.to_bohr(xa)
+    for path in ("large", "large_mixed"):
+        _, e, g, it, conv = run_one("PM6", Z, x, path)
+        assert conv
+        assert abs(e - gold["energy"]) < E_TOL, path
+        assert np.max(np.abs(g.reshape(-1) - np.array(gold["gradient"]))) < G_TOL, path
