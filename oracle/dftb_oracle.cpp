@@ -20,6 +20,9 @@
 //   density guess    Utils/DensityGuess.cpp:22-40
 //   gradient         ZeroOrderMatricesCalculator.cpp:431-460, SecondOrderFock.cpp:148-176,
 //                    ThirdOrderFock.cpp:202-226
+//   TD-DFTB          Utils/DipoleUtils/TransitionChargesCalculator.h:138-165,
+//                    TimeDependent/LinearResponse/TDDFTBSigmaVectorEvaluator.cpp:40-110,
+//                    TDDFTBEigenvalueSolver.h:150-197, DipoleUtils/DFTBDipoleMatrixCalculator.cpp:60-84
 // The SCF driver, DIIS and the generalised eigensolver live in the
 // reference's un-vendored dependency (scine_utilities); they are restated from
 // the standard algorithms (Loewdin orthogonalisation, Householder + QL, Pulay
@@ -94,7 +97,8 @@ constexpr double kDistFudge = 1.0, kDeltaR = 1e-5;
 struct Elem {
   int Z = 0, nao = 0;
   double es = 0, ep = 0, U = 0, occ = 0, hd = 0;
-  bool has_hd = false;
+  double w = 0;  // atomically resolved spin constant (W_pp for p elements, W_ss for s)
+  bool has_hd = false, has_w = false;
 };
 
 struct Pair {
@@ -232,6 +236,8 @@ bool load(const char* set_name, const std::vector<int>& Zs, int order, Params& P
     e.occ = r.fs + r.fp + r.fd;
     e.hd = r.hubbard_derivative;
     e.has_hd = r.has_hubbard_derivative != 0;
+    e.w = e.nao == 1 ? r.wss : r.wpp;  // SKAtom.h:94-102
+    e.has_w = r.has_spin != 0;
     P.have[r.Z] = true;
   }
   for (int z : Zs) {
@@ -747,6 +753,104 @@ bool setup(const char* set, int order, int nat, const int* Z, const double* xyz,
   return true;
 }
 
+// Linear-response TD-DFTB (restricted reference, singlets or triplets, the
+// full Casida form, not TDA) for the nroots lowest excitations.
+//   transition charges (TransitionChargesCalculator.h:138-165):
+//     q_A^{ia} = 1/2 sum_{mu on A} (C_mu,i (SC)_mu,a + C_mu,a (SC)_mu,i)
+//   Casida matrix (TDDFTBSigmaVectorEvaluator.cpp:40-110, factor 4 for a
+//   restricted reference, TDDFTBSigmaVectorEvaluator.h:118-120):
+//     Omega_{ia,jb} = delta Delta_ia^2 + 4 sqrt(Delta_ia) K_{ia,jb} sqrt(Delta_jb)
+//     K = q^T gamma q (singlets), q^T diag(W_A) q (triplets)
+//   omega_I = sqrt(eigenvalue), c_ia = sqrt(Delta_ia / omega_I) F_ia
+//   (TDDFTBEigenvalueSolver.h:150-197)
+//   transition dipole (DFTBDipoleMatrixCalculator.cpp:60-84 for the MO dipole
+//   matrix D_ia = sum_A q_A^{ia} R_A; the restricted singlet factor sqrt(2)
+//   of the spin-adapted transition density, restated for the un-vendored
+//   Utils::TransitionDipoleCalculator): mu_I = sqrt(2) sum_ia c_ia D_ia.
+// The eigenproblem is solved densely (the reference's Davidson lives in the
+// un-vendored scine_utilities; converged eigenpairs do not depend on it).
+bool tddftb(const Mol& M, const State& st, int triplet, int nroots, std::vector<double>& omega,
+            std::vector<double>& dip) {
+  const int N = M.nao, no = M.nocc, nv = N - no, nat = M.nat;
+  const int dim = no * nv;
+  if (dim == 0) {
+    g_error = "no occupied-virtual transitions";
+    return false;
+  }
+  if (nroots > dim) nroots = dim;
+  const auto SC = matmul(N, st.S, st.C);
+  std::vector<int> atom_of(N);
+  for (int a = 0; a < nat; ++a)
+    for (int i = 0; i < M.nao_of[a]; ++i) atom_of[M.ao0[a] + i] = a;
+  // q[k][A] with k = i * nv + a
+  std::vector<double> q((size_t)dim * nat, 0.0), delta(dim);
+  for (int i = 0; i < no; ++i)
+    for (int a = 0; a < nv; ++a) {
+      const int k = i * nv + a, av = no + a;
+      delta[k] = st.eps[av] - st.eps[i];
+      for (int mu = 0; mu < N; ++mu) {
+        const double v = 0.5 * (st.C[(size_t)mu * N + i] * SC[(size_t)mu * N + av] +
+                                st.C[(size_t)mu * N + av] * SC[(size_t)mu * N + i]);
+        q[(size_t)k * nat + atom_of[mu]] += v;
+      }
+    }
+  // coupling matrix of the atoms
+  std::vector<double> G((size_t)nat * nat, 0.0);
+  for (int A = 0; A < nat; ++A)
+    for (int B = 0; B < nat; ++B) {
+      if (triplet) {
+        if (A == B) {
+          const Elem& e = M.P.elem[M.Z[A]];
+          if (!e.has_w) {
+            g_error = "no spin constant for element Z=" + std::to_string(M.Z[A]);
+            return false;
+          }
+          G[(size_t)A * nat + A] = e.w;
+        }
+      } else {
+        G[(size_t)A * nat + B] = st.gam[(size_t)A * nat + B];
+      }
+    }
+  std::vector<double> qG((size_t)dim * nat, 0.0);
+  for (int k = 0; k < dim; ++k)
+    for (int B = 0; B < nat; ++B) {
+      double s = 0;
+      for (int A = 0; A < nat; ++A) s += q[(size_t)k * nat + A] * G[(size_t)A * nat + B];
+      qG[(size_t)k * nat + B] = s;
+    }
+  std::vector<double> Om((size_t)dim * dim);
+  for (int k = 0; k < dim; ++k)
+    for (int l = 0; l <= k; ++l) {
+      double s = 0;
+      for (int B = 0; B < nat; ++B) s += qG[(size_t)k * nat + B] * q[(size_t)l * nat + B];
+      double v = 4.0 * std::sqrt(delta[k]) * s * std::sqrt(delta[l]);
+      if (k == l) v += delta[k] * delta[k];
+      Om[(size_t)k * dim + l] = Om[(size_t)l * dim + k] = v;
+    }
+  std::vector<double> w, V;
+  if (!oracle_la::eigh(dim, Om, w, V)) {
+    g_error = "Casida diagonalisation failed";
+    return false;
+  }
+  omega.assign(nroots, 0.0);
+  dip.assign(3 * (size_t)nroots, 0.0);
+  for (int I = 0; I < nroots; ++I) {
+    if (!(w[I] > 0)) {
+      g_error = "non-positive Casida eigenvalue";
+      return false;
+    }
+    const double om = std::sqrt(w[I]);
+    omega[I] = om;
+    if (triplet) continue;
+    for (int k = 0; k < dim; ++k) {
+      const double c = std::sqrt(delta[k] / om) * V[(size_t)k * dim + I];
+      for (int A = 0; A < nat; ++A)
+        for (int x = 0; x < 3; ++x) dip[3 * I + x] += std::sqrt(2.0) * c * q[(size_t)k * nat + A] * M.pos[3 * A + x];
+    }
+  }
+  return true;
+}
+
 }  // namespace dftb_oracle
 
 extern "C" {
@@ -801,6 +905,33 @@ int dftb_oracle_scf(const char* set, int order, int nat, const int* Z, const dou
     std::memcpy(grad, g.data(), sizeof(double) * g.size());
   }
   return st.converged ? 0 : 3;
+}
+
+// TD-DFTB excitations of a converged restricted DFTB reference: omega
+// (nroots, Hartree) and, for singlets, the transition dipoles (3 * nroots,
+// e bohr).  info[4] = ground-state energy, nao, nocc, transitions.
+int dftb_oracle_tddftb(const char* set, int order, int nat, const int* Z, const double* xyz, int charge, double scc,
+                       double rmsd, int max_iter, int triplet, int nroots, double* omega, double* dip, double* info) {
+  using namespace dftb_oracle;
+  Mol M;
+  if (!setup(set, order, nat, Z, xyz, charge, M)) return 1;
+  State st;
+  if (!scf(M, st, scc, rmsd, max_iter)) return 2;
+  if (!st.converged) {
+    g_error = "reference SCF did not converge";
+    return 3;
+  }
+  std::vector<double> om, dp;
+  if (!tddftb(M, st, triplet, nroots, om, dp)) return 4;
+  std::memcpy(omega, om.data(), sizeof(double) * om.size());
+  if (dip) std::memcpy(dip, dp.data(), sizeof(double) * dp.size());
+  if (info) {
+    info[0] = st.e_el + st.e_rep;
+    info[1] = M.nao;
+    info[2] = M.nocc;
+    info[3] = (double)M.nocc * (M.nao - M.nocc);
+  }
+  return 0;
 }
 
 }  // extern "C"

@@ -12,6 +12,8 @@ struct DftbElemRaw {
   double fs, fp, fd;     // occupations of the neutral atom
   double hubbard_derivative;
   int has_hubbard_derivative;
+  double wss, wpp;       // spin constants (spin.dat) for triplet excitations
+  int has_spin;
 };
 
 struct DftbPairRaw {

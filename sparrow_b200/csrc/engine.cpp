@@ -551,11 +551,15 @@ int Batch::set_start_density(const double* P, std::string& err) {
   return cudaStreamSynchronize(stream_) == cudaSuccess ? kOk : kErrCuda;
 }
 
-int Batch::run(const ScfParams& sp, bool gradient, std::string& err) {
+int Batch::run(const ScfParams& sp_in, bool gradient, std::string& err) {
   if (mols_.empty()) {
     err = "no structure";
     return kErrEmptyStructure;
   }
+  // From a given (converged) start density the first diagonalisation is
+  // already the answer: give it the sweeps to resolve the orbitals fully.
+  ScfParams sp = sp_in;
+  if (density_given_) sp.cold_sweeps = std::max(sp.cold_sweeps, 6);
   dev_.use_guess = density_given_ ? 0 : 1;
   for (auto& ev : stage_ev_)
     if (!ev) cudaEventCreate(&ev);

@@ -165,6 +165,9 @@ def dftb_lib():
                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.dftb_oracle_matrices.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _I, _D, ctypes.c_void_p,
                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _I]
+        L.dftb_oracle_tddftb.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _I, _D, ctypes.c_int,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         _D, ctypes.c_void_p, _D]
         _dlib = L
     return _dlib
 
@@ -217,3 +220,23 @@ def dftb_matrices(order, Z, xyz_bohr, parameters=None):
         raise RuntimeError(dftb_lib().dftb_oracle_last_error().decode())
     N = nao.value
     return H0[:N * N].reshape(N, N), S[:N * N].reshape(N, N), gam.reshape(n, n), Gam.reshape(n, n)
+
+
+def dftb_tddftb(order, Z, xyz_bohr, nroots=8, triplet=False, charge=0, parameters=None, scc=1e-9, rmsd=1e-9,
+                max_iter=1000):
+    """TD-DFTB excitation energies (Hartree, ascending) and singlet transition dipoles (nroots x 3, e bohr)."""
+    Z, x = _arr(Z, xyz_bohr)
+    n = len(Z)
+    params = parameters or DFTB_DEFAULT_SET[order]
+    om = np.zeros(nroots)
+    dip = np.zeros(3 * nroots)
+    info = np.zeros(4)
+    rc = dftb_lib().dftb_oracle_tddftb(params.encode(), order, n, Z.ctypes.data_as(_I), x.ctypes.data_as(_D),
+                                       int(charge), scc, rmsd, max_iter, 1 if triplet else 0, nroots,
+                                       om.ctypes.data_as(_D), dip.ctypes.data, info.ctypes.data_as(_D))
+    if rc != 0:
+        raise RuntimeError(dftb_lib().dftb_oracle_last_error().decode())
+    nt = int(info[3])
+    k = min(nroots, nt)
+    return dict(omega=om[:k], dipoles=dip[:3 * k].reshape(k, 3), energy=info[0], nao=int(info[1]),
+                nocc=int(info[2]), transitions=nt)
