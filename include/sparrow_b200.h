@@ -94,6 +94,15 @@ int32_t sg_get_scf_info(const sg_calculator* h, int32_t* iterations, int32_t* co
 int32_t sg_get_orbital_energies(const sg_calculator* h, double* eps);
 /* density matrix (n_aos x n_aos, row-major) of the last calculation, and a
  * start density for the next one (warm start) */
+/* Linear-response TD-DFTB on the converged DFTB2 / DFTB3 reference of the
+ * last sg_calculate (replaces TDDFTBCalculator::calculate,
+ * Implementations/Dftb/TimeDependent/LinearResponse/TDDFTBCalculator.cpp:124-158,
+ * restricted singlets or triplets, full TD-DFTB, no basis pruning): the
+ * nroots (1..16) lowest excitation energies omega (Hartree, ascending) and,
+ * for singlets, the transition dipoles (nroots x 3, e bohr; zero for
+ * triplets; dipoles may be NULL).  SG_ERR_NOT_CONVERGED when the Davidson
+ * solver did not reach its residual tolerance (1e-8). */
+int32_t sg_calculate_excitations(sg_calculator* h, int32_t nroots, int32_t triplet, double* omega, double* dipoles);
 int32_t sg_get_density(const sg_calculator* h, double* P);
 int32_t sg_set_density(sg_calculator* h, const double* P);
 
@@ -120,6 +129,14 @@ int32_t sg_batch_set_scf_path(sg_batch* b, int32_t path);
  * to FP64 (default 1e-5; also when the mixed densities stop halving below
  * 1e-4) */
 int32_t sg_batch_set_mixed_switch(sg_batch* b, double density_rmsd);
+/* TD-DFTB of every molecule of a DFTB batch after sg_batch_run: omega
+ * [n_molecules * nroots], dipoles [n_molecules * nroots * 3] (may be NULL),
+ * status [n_molecules] (0 ok, 1 not converged, 2 orbital diagonalisation,
+ * 3 non-positive eigenvalue, 4 reference not converged; may be NULL).  The
+ * call overwrites the batch's orbital scratch; gradients of the preceding
+ * run stay valid. */
+int32_t sg_batch_excitations(sg_batch* b, int32_t nroots, int32_t triplet, double* omega, double* dipoles,
+                             int32_t* status);
 int32_t sg_batch_set_positions(sg_batch* b, const double* xyz_bohr);
 /* enqueue integrals -> SCF -> (gradient) on the device; asynchronous */
 int32_t sg_batch_run(sg_batch* b, uint32_t properties);

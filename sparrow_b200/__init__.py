@@ -75,6 +75,8 @@ def lib():
         "sg_get_scf_info": (ctypes.c_int32, [_VP, _I32, _I32, _I32, _I32]),
         "sg_get_orbital_energies": (ctypes.c_int32, [_VP, _D]),
         "sg_get_density": (ctypes.c_int32, [_VP, _D]),
+        "sg_calculate_excitations": (ctypes.c_int32, [_VP, ctypes.c_int32, ctypes.c_int32, _D, _VP]),
+        "sg_batch_excitations": (ctypes.c_int32, [_VP, ctypes.c_int32, ctypes.c_int32, _D, _VP, _VP]),
         "sg_set_density": (ctypes.c_int32, [_VP, _D]),
         "sg_batch_create": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _I32, _D, _I32,
                                              ctypes.POINTER(_VP)]),
@@ -264,6 +266,15 @@ class Calculator:
         self._nao = nao.value
         return Results(e.value, grad, rc == 0 and bool(conv.value), it.value, nao.value, nocc.value)
 
+    def excitations(self, nroots=8, triplet=False):
+        """TD-DFTB on the last DFTB2/DFTB3 calculation: (omega [nroots] Hartree,
+        transition dipoles [nroots, 3] e bohr)."""
+        om = np.zeros(nroots)
+        dp = np.zeros(3 * nroots)
+        self._check(lib().sg_calculate_excitations(self._h, nroots, 1 if triplet else 0, _dptr(om),
+                                                   dp.ctypes.data_as(_VP)))
+        return om, dp.reshape(nroots, 3)
+
     def density(self):
         n = self._nao
         P = np.zeros(n * n)
@@ -369,6 +380,19 @@ class Batch:
         if g is not None:
             grads = np.split(g.reshape(-1, 3), np.cumsum(self.n_atoms)[:-1])
         return e, grads, it, conv.astype(bool)
+
+    def excitations(self, nroots=8, triplet=False):
+        """TD-DFTB of every molecule after run() on a DFTB batch: omega [n, nroots]
+        (Hartree), transition dipoles [n, nroots, 3] (e bohr), status [n]
+        (0 ok, 1 Davidson not converged, 2-4 failures)."""
+        n = self.n_molecules
+        om = np.zeros(n * nroots)
+        dp = np.zeros(3 * n * nroots)
+        st = np.zeros(n, dtype=np.int32)
+        self._check(lib().sg_batch_excitations(self._h, nroots, 1 if triplet else 0, _dptr(om),
+                                               dp.ctypes.data_as(_VP), st.ctypes.data_as(_VP)),
+                    allow=(SG_ERR_NOT_CONVERGED,))
+        return om.reshape(n, nroots), dp.reshape(n, nroots, 3), st
 
     @property
     def launches(self):

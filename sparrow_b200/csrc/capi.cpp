@@ -131,6 +131,32 @@ class Calculator {
     return kOk;
   }
 
+  // TD-DFTB on the converged DFTB reference of the last calculate()
+  int excitations(int nroots, bool triplet, double* omega, double* dip) {
+    if (!have_result_ || !result_.converged) {
+      error = "TD-DFTB needs a converged reference calculation";
+      return kErrNoResults;
+    }
+    int rc = batch_->run_tddftb(nroots, triplet, 1e-8, 200, error);
+    if (rc) return rc;
+    std::vector<double> om, dp;
+    std::vector<int> info;
+    rc = batch_->fetch_tddftb(om, dp, info, error);
+    if (rc) return rc;
+    std::memcpy(omega, om.data(), sizeof(double) * om.size());
+    if (dip) std::memcpy(dip, dp.data(), sizeof(double) * dp.size());
+    return td_status(info[1], error);
+  }
+  static int td_status(int st, std::string& error) {
+    if (st == 0) return kOk;
+    if (st == 1) {
+      error = "TD-DFTB Davidson did not converge";
+      return kErrNotConverged;
+    }
+    error = "TD-DFTB device failure code " + std::to_string(st);
+    return kErrDevice;
+  }
+
   bool have_result() const { return have_result_; }
   bool have_gradient() const { return have_gradient_; }
   const MoleculeOutput& result() const { return result_; }
@@ -397,6 +423,11 @@ int32_t sg_get_orbital_energies(const sg_calculator* h, double* eps) {
   return SG_OK;
 }
 
+int32_t sg_calculate_excitations(sg_calculator* h, int32_t nroots, int32_t triplet, double* omega, double* dipoles) {
+  if (!h || !omega) return SG_ERR_INVALID_ARGUMENT;
+  return h->impl->excitations(nroots, triplet != 0, omega, dipoles);
+}
+
 int32_t sg_get_density(const sg_calculator* h, double* P) {
   if (!h || !P) return SG_ERR_INVALID_ARGUMENT;
   if (!h->impl->have_result()) return SG_ERR_NO_RESULTS;
@@ -459,6 +490,25 @@ int32_t sg_batch_set_mixed_switch(sg_batch* b, double rmsd) {
   if (!b || !(rmsd > 0) || !std::isfinite(rmsd)) return SG_ERR_INVALID_ARGUMENT;
   b->sp.mixed_switch_rmsd = rmsd;
   return SG_OK;
+}
+
+int32_t sg_batch_excitations(sg_batch* b, int32_t nroots, int32_t triplet, double* omega, double* dipoles,
+                             int32_t* status) {
+  if (!b || !omega) return SG_ERR_INVALID_ARGUMENT;
+  int rc = b->impl->run_tddftb(nroots, triplet != 0, 1e-8, 200, b->error);
+  if (rc) return rc;
+  std::vector<double> om, dp;
+  std::vector<int> info;
+  rc = b->impl->fetch_tddftb(om, dp, info, b->error);
+  if (rc) return rc;
+  std::memcpy(omega, om.data(), sizeof(double) * om.size());
+  if (dipoles) std::memcpy(dipoles, dp.data(), sizeof(double) * dp.size());
+  int worst = 0;
+  for (size_t i = 0; i < info.size() / 2; ++i) {
+    if (status) status[i] = info[2 * i + 1];
+    if (info[2 * i + 1] > worst) worst = info[2 * i + 1];
+  }
+  return Calculator::td_status(worst, b->error);
 }
 
 int32_t sg_batch_set_positions(sg_batch* b, const double* xyz) {

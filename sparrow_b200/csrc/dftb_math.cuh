@@ -28,6 +28,9 @@ constexpr int kDftbCols = 10;  // completed integral columns per table row
 struct DftbElemDev {
   int Z, nao;
   double es, ep, U, occ, hd;
+  double w;    // atomically resolved spin constant (W_pp, or W_ss for s-only atoms)
+  int has_w;   // spin constant available (triplet excitations)
+  int pad;
 };
 
 // Parameters of an ordered element pair (file Z1-Z2): its completed integral

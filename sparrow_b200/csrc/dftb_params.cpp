@@ -84,6 +84,9 @@ bool dftb_prepare(const std::string& set, int order, const std::vector<int>& Zs,
     d.U = e->us;
     d.occ = e->fs + e->fp + e->fd;
     d.hd = e->hubbard_derivative;
+    d.w = nao == 1 ? e->wss : e->wpp;  // SKAtom.h:94-102
+    d.has_w = e->has_spin;
+    d.pad = 0;
   }
   out.pairs.assign(kMaxElementSlots * kMaxElementSlots, DftbPairDev());
   out.table.clear();

@@ -99,6 +99,7 @@ Batch::~Batch() {
   pool_give(false, arena_, arena_bytes_);
   pool_give(true, pinned_, pinned_bytes_);
   if (large_scratch_) cudaFree(large_scratch_);
+  if (td_scratch_) cudaFree(td_scratch_);
   for (auto& e : stage_ev_)
     if (e) cudaEventDestroy(e);
   for (auto& e : user_ev_)
@@ -152,6 +153,8 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
   ao_atom_.clear();
   order_.clear();
   density_given_ = false;
+  stages_recorded_ = false;
+  td_roots_ = 0;
   if (in.empty()) {
     err = "empty batch";
     return kErrEmptyStructure;
@@ -672,6 +675,111 @@ int Batch::fetch(std::vector<MoleculeOutput>& out, bool gradient, std::string& e
     else
       o.gradient.clear();
   }
+  return kOk;
+}
+
+int Batch::run_tddftb(int nroots, bool triplet, double tol, int max_iter, std::string& err) {
+  if (mols_.empty()) {
+    err = "no structure";
+    return kErrEmptyStructure;
+  }
+  if (!is_dftb(method_)) {
+    err = "TD-DFTB needs a DFTB2 or DFTB3 reference";
+    return kErrInvalidArgument;
+  }
+  if (!stages_recorded_) {
+    err = "TD-DFTB needs a converged reference: run the batch first";
+    return kErrNoResults;
+  }
+  if (nroots < 1 || nroots > 16 || !(tol > 0) || max_iter < 1) {
+    err = "TD-DFTB: 1 <= nroots <= 16, tol > 0, max_iter >= 1";
+    return kErrInvalidArgument;
+  }
+  // per-molecule scratch blocks, then the result arrays
+  std::vector<long long> off(mols_.size());
+  long long total = 0;
+  for (size_t i = 0; i < mols_.size(); ++i) {
+    const MolDev& m = mols_[i];
+    const int dim = m.nocc * (m.nao - m.nocc);
+    const int k = nroots < dim ? nroots : dim;
+    off[i] = total;
+    total += dim > 0 ? td_block_doubles(dim, m.nat, k) : 0;
+    total = (total + 31) & ~31LL;
+  }
+  const size_t n = mols_.size();
+  const size_t need = sizeof(double) * (size_t)total + sizeof(long long) * n + sizeof(double) * n * nroots * 4 +
+                      sizeof(int) * 2 * n + 4 * 256;
+  if (td_scratch_bytes_ < need) {
+    if (td_scratch_) {
+      cudaStreamSynchronize(stream_);
+      cudaFree(td_scratch_);
+      td_scratch_ = nullptr;
+      td_scratch_bytes_ = 0;
+    }
+    cudaError_t e = cudaMalloc(&td_scratch_, need);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      td_scratch_ = nullptr;
+      err = "device allocation of " + std::to_string(need) + " bytes failed: " + cudaGetErrorString(e);
+      return e == cudaErrorMemoryAllocation ? kErrOutOfMemory : kErrCuda;
+    }
+    td_scratch_bytes_ = need;
+  }
+  char* p = static_cast<char*>(td_scratch_);
+  double* td = reinterpret_cast<double*>(p);
+  size_t o = align_up(sizeof(double) * (size_t)total);
+  long long* d_off = reinterpret_cast<long long*>(p + o);
+  o = align_up(o + sizeof(long long) * n);
+  td_omega_ = reinterpret_cast<double*>(p + o);
+  o = align_up(o + sizeof(double) * n * nroots);
+  td_dip_ = reinterpret_cast<double*>(p + o);
+  o = align_up(o + sizeof(double) * n * nroots * 3);
+  td_info_ = reinterpret_cast<int*>(p + o);
+  td_roots_ = nroots;
+  cudaError_t e = cudaMemcpyAsync(d_off, off.data(), sizeof(long long) * n, cudaMemcpyHostToDevice, stream_);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  // the copy reads the host vector: wait before it goes out of scope
+  e = cudaStreamSynchronize(stream_);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  h2d_bytes_ += (long long)(sizeof(long long) * n);
+  launch_tddftb(dev_, td, d_off, nroots, triplet ? 1 : 0, tol, max_iter, td_omega_, td_dip_, td_info_, dev_.scf_grid,
+                stream_);
+  launches_ += 1;
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  return kOk;
+}
+
+int Batch::fetch_tddftb(std::vector<double>& omega, std::vector<double>& dip, std::vector<int>& info, std::string& err) {
+  if (!td_roots_) {
+    err = "no TD-DFTB run";
+    return kErrNoResults;
+  }
+  const size_t n = mols_.size();
+  omega.resize(n * td_roots_);
+  dip.resize(n * td_roots_ * 3);
+  info.resize(2 * n);
+  cudaError_t e = cudaMemcpyAsync(omega.data(), td_omega_, sizeof(double) * omega.size(), cudaMemcpyDeviceToHost,
+                                  stream_);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dip.data(), td_dip_, sizeof(double) * dip.size(), cudaMemcpyDeviceToHost, stream_);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(info.data(), td_info_, sizeof(int) * info.size(), cudaMemcpyDeviceToHost, stream_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  d2h_bytes_ += (long long)(sizeof(double) * (omega.size() + dip.size()) + sizeof(int) * info.size());
   return kOk;
 }
 

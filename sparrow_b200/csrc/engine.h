@@ -65,6 +65,15 @@ class Batch {
   int fetch_density(int mol, std::vector<double>& P, std::string& err);
   int fetch_raw_results(std::vector<MolResult>& r, std::string& err);
   int fetch_orbital_energies(int mol, std::vector<double>& eps, std::string& err);
+  // Linear-response TD-DFTB (DFTB2 / DFTB3 batches, after run()): the nroots
+  // (<= 16) lowest singlet (or triplet) excitations of every molecule.
+  // Asynchronous on stream(); overwrites the orbital scratch (the gradient of
+  // the preceding run() stays valid).  tol: Davidson residual norm.
+  int run_tddftb(int nroots, bool triplet, double tol, int max_iter, std::string& err);
+  // omega [nmol * nroots] (Hartree), dipoles [nmol * nroots * 3] (e bohr,
+  // zero for triplets), info [nmol * 2] (Davidson iterations, status).
+  int fetch_tddftb(std::vector<double>& omega, std::vector<double>& dipoles, std::vector<int>& info, std::string& err);
+  int tddftb_roots() const { return td_roots_; }
 
   cudaStream_t stream() const { return stream_; }
   Method method() const { return method_; }
@@ -113,6 +122,12 @@ class Batch {
   long long npairs_ = 0, nhh_ = 0;  // pair and heavy-pair tables are built on the device
   std::string dftb_set_;
   int scf_path_ = 0;
+  void* td_scratch_ = nullptr;
+  size_t td_scratch_bytes_ = 0;
+  int td_roots_ = 0;
+  double* td_omega_ = nullptr;
+  double* td_dip_ = nullptr;
+  int* td_info_ = nullptr;
   void* large_scratch_ = nullptr;
   size_t large_scratch_bytes_ = 0;
   int scf_grid_ = 0;

@@ -95,6 +95,28 @@ void launch_dftb_gradient(const DeviceBatch& b, cudaStream_t s);
 int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, int precision, cudaStream_t s,
                   int* launches, std::string& err);
 size_t large_scf_scratch_bytes(long long nao);
+// TD-DFTB per-molecule scratch: subspace size and doubles of the block of a
+// molecule with dim occupied-virtual transitions, nat atoms and k roots.
+#ifdef __CUDACC__
+#define SGB_TD_HD __host__ __device__
+#else
+#define SGB_TD_HD
+#endif
+SGB_TD_HD inline int td_subspace(int dim, int k) {
+  int m = 6 * k;
+  if (m > 64) m = 64;
+  if (m < 2 * k) m = 2 * k;
+  return m < dim ? m : dim;
+}
+SGB_TD_HD inline long long td_block_doubles(int dim, int nat, int k) {
+  const long long mm = td_subspace(dim, k);
+  return (long long)nat * dim + 4LL * dim + 2 * mm * dim + 2LL * k * dim + 2LL * nat * mm + mm * mm;
+}
+// TD-DFTB of every molecule of a converged DFTB batch: td (device scratch,
+// td_off[mol] doubles per molecule), omega [nmol * nroots], dip
+// [nmol * nroots * 3], info [nmol * 2] (Davidson iterations, status).
+void launch_tddftb(const DeviceBatch& b, double* td, const long long* td_off, int nroots, int triplet, double tol,
+                   int max_iter, double* omega, double* dip, int* info, int grid, cudaStream_t s);
 int scf_max_grid(int max_nao);
 size_t scf_rotation_bytes_per_cta();
 

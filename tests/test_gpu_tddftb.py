@@ -1,0 +1,101 @@
+"""TD-DFTB on the GPU (through the C-ABI) against the TD-DFTB oracle and the
+reference's known answers.
+
+Tolerances: excitation energies 1e-6 Hartree against the oracle (the
+reference's own test asserts 1e-3 eV, also checked); transition dipoles 1e-5
+e bohr against the oracle, compared up to the arbitrary sign of each
+eigenvector.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import sparrow_b200
+from sparrow_b200 import geometry
+from tests import oracle_lib as O
+
+pytestmark = pytest.mark.gpu
+
+W_TOL = 1e-6
+MU_TOL = 1e-5
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "tddftb_known_answers.json")))
+SYM = {"H": 1, "C": 6, "N": 7, "O": 8}
+
+
+def _aligned_dipole_error(a, b):
+    err = 0.0
+    for i in range(len(a)):
+        s = 1.0 if np.dot(a[i], b[i]) >= 0 else -1.0
+        err = max(err, float(np.max(np.abs(a[i] - s * b[i]))))
+    return err
+
+
+@pytest.mark.parametrize("spin", ["singlet", "triplet"])
+def test_methane_matches_reference_and_oracle(spin):
+    rec = next(t for t in GOLD["tests"] if t.get("spin") == spin)
+    Z = [SYM[e] for e in rec["elements"]]
+    x = np.array(rec["xyz_angstrom"]) * O.bohr_per_angstrom()
+    c = sparrow_b200.get_calculator("DFTB2")
+    c.set_structure(Z, x)
+    c.settings["method_parameters"] = rec["parameters"]
+    c.settings["density_rmsd_criterion"] = 1e-9
+    c.settings["self_consistence_criterion"] = 1e-9
+    assert c.calculate().successful_calculation
+    n = len(rec["energies_ev"])
+    om, mu = c.excitations(n, triplet=spin == "triplet")
+    ev = O.ev_per_hartree()
+    assert np.max(np.abs(om * ev - np.array(rec["energies_ev"]))) < rec["tolerance_ev"]
+    ref = O.dftb_tddftb(2, Z, x, nroots=n, triplet=spin == "triplet", parameters=rec["parameters"])
+    assert np.max(np.abs(om - ref["omega"])) < W_TOL
+    if spin == "singlet":
+        assert _aligned_dipole_error(mu, ref["dipoles"]) < MU_TOL
+    else:
+        assert np.all(mu == 0.0)
+
+
+@pytest.mark.parametrize("method,order", [("DFTB3", 3), ("DFTB2", 2)])
+def test_polyene_batch_matches_oracle(method, order):
+    mols = [(z, geometry.to_bohr(x)) for z, x in geometry.polyene_batch(6, seed=11, k_min=5, k_max=9)]
+    b = sparrow_b200.Batch(method, mols, scc=1e-9, rmsd=1e-9, max_iter=200)
+    b.run()
+    e, _, _, conv = b.results()
+    assert conv.all()
+    om, mu, st = b.excitations(8)
+    assert (st == 0).all()
+    for i, (Z, x) in enumerate(mols):
+        ref = O.dftb_tddftb(order, Z, x, nroots=8)
+        assert abs(e[i] - ref["energy"]) < 1e-6, i
+        assert np.max(np.abs(om[i] - ref["omega"])) < W_TOL, i
+        assert _aligned_dipole_error(mu[i], ref["dipoles"]) < MU_TOL, i
+
+
+def test_batch_equals_single_molecule():
+    mols = [(z, geometry.to_bohr(x)) for z, x in geometry.polyene_batch(4, seed=12, k_min=5, k_max=12)]
+    b = sparrow_b200.Batch("DFTB3", mols, scc=1e-9, rmsd=1e-9)
+    b.run()
+    om, mu, st = b.excitations(8)
+    b1 = sparrow_b200.Batch("DFTB3", mols[2:3], scc=1e-9, rmsd=1e-9)
+    b1.run()
+    om1, mu1, st1 = b1.excitations(8)
+    assert (st == 0).all() and st1[0] == 0
+    assert np.max(np.abs(om[2] - om1[0])) < 1e-9
+    assert _aligned_dipole_error(mu[2], mu1[0]) < 1e-7
+
+
+def test_excitations_need_a_dftb_reference():
+    mols = [(np.array([1, 1]), np.array([[0, 0, 0], [0, 0, 1.4]], float))]
+    b = sparrow_b200.Batch("PM6", mols)
+    b.run()
+    with pytest.raises(sparrow_b200.SparrowError):
+        b.excitations(4)
+    d = sparrow_b200.Batch("DFTB2", mols)
+    with pytest.raises(sparrow_b200.SparrowError):
+        d.excitations(4)  # not run yet
+    d.run()
+    with pytest.raises(sparrow_b200.SparrowError):
+        d.excitations(0)
+    om, mu, st = d.excitations(4)  # H2: one transition
+    ref = O.dftb_tddftb(2, [1, 1], mols[0][1], nroots=4)
+    assert st[0] == 0 and abs(om[0, 0] - ref["omega"][0]) < W_TOL and np.all(om[0, 1:] == 0)
