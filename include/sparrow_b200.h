@@ -137,6 +137,9 @@ int32_t sg_batch_set_mixed_switch(sg_batch* b, double density_rmsd);
  * run stay valid. */
 int32_t sg_batch_excitations(sg_batch* b, int32_t nroots, int32_t triplet, double* omega, double* dipoles,
                              int32_t* status);
+/* SM cycles per molecule of the last sg_batch_excitations: canonical
+ * orbitals, transition charges, Davidson (3 per molecule) */
+int32_t sg_batch_excitation_cycles(sg_batch* b, int64_t* cycles3);
 int32_t sg_batch_set_positions(sg_batch* b, const double* xyz_bohr);
 /* enqueue integrals -> SCF -> (gradient) on the device; asynchronous */
 int32_t sg_batch_run(sg_batch* b, uint32_t properties);

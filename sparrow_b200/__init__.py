@@ -77,6 +77,7 @@ def lib():
         "sg_get_density": (ctypes.c_int32, [_VP, _D]),
         "sg_calculate_excitations": (ctypes.c_int32, [_VP, ctypes.c_int32, ctypes.c_int32, _D, _VP]),
         "sg_batch_excitations": (ctypes.c_int32, [_VP, ctypes.c_int32, ctypes.c_int32, _D, _VP, _VP]),
+        "sg_batch_excitation_cycles": (ctypes.c_int32, [_VP, _VP]),
         "sg_set_density": (ctypes.c_int32, [_VP, _D]),
         "sg_batch_create": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _I32, _D, _I32,
                                              ctypes.POINTER(_VP)]),
@@ -393,6 +394,13 @@ class Batch:
                                                dp.ctypes.data_as(_VP), st.ctypes.data_as(_VP)),
                     allow=(SG_ERR_NOT_CONVERGED,))
         return om.reshape(n, nroots), dp.reshape(n, nroots, 3), st
+
+    def excitation_cycles(self):
+        """SM cycles per molecule of the last excitations(): canonical orbitals,
+        transition charges, Davidson ([n, 3])."""
+        c = np.zeros(3 * self.n_molecules, dtype=np.int64)
+        self._check(lib().sg_batch_excitation_cycles(self._h, c.ctypes.data_as(_VP)))
+        return c.reshape(-1, 3)
 
     @property
     def launches(self):

@@ -503,12 +503,30 @@ int32_t sg_batch_excitations(sg_batch* b, int32_t nroots, int32_t triplet, doubl
   if (rc) return rc;
   std::memcpy(omega, om.data(), sizeof(double) * om.size());
   if (dipoles) std::memcpy(dipoles, dp.data(), sizeof(double) * dp.size());
-  int worst = 0;
+  // per-molecule outcomes go to status; the return code is the worst of them,
+  // a reference that did not converge counting as not converged
+  int failed = 0, unconverged = 0;
   for (size_t i = 0; i < info.size() / 2; ++i) {
-    if (status) status[i] = info[2 * i + 1];
-    if (info[2 * i + 1] > worst) worst = info[2 * i + 1];
+    const int st = info[2 * i + 1];
+    if (status) status[i] = st;
+    if (st == 1 || st == 4) ++unconverged;
+    else if (st != 0) ++failed;
   }
-  return Calculator::td_status(worst, b->error);
+  if (failed) return Calculator::td_status(2, b->error);
+  if (unconverged) {
+    b->error = std::to_string(unconverged) + " molecule(s) without converged excitations (see status)";
+    return SG_ERR_NOT_CONVERGED;
+  }
+  return SG_OK;
+}
+
+int32_t sg_batch_excitation_cycles(sg_batch* b, int64_t* cycles3) {
+  if (!b || !cycles3) return SG_ERR_INVALID_ARGUMENT;
+  std::vector<long long> c;
+  const int rc = b->impl->fetch_tddftb_cycles(c, b->error);
+  if (rc) return rc;
+  for (size_t i = 0; i < c.size(); ++i) cycles3[i] = c[i];
+  return SG_OK;
 }
 
 int32_t sg_batch_set_positions(sg_batch* b, const double* xyz) {

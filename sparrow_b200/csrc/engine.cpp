@@ -708,7 +708,7 @@ int Batch::run_tddftb(int nroots, bool triplet, double tol, int max_iter, std::s
   }
   const size_t n = mols_.size();
   const size_t need = sizeof(double) * (size_t)total + sizeof(long long) * n + sizeof(double) * n * nroots * 4 +
-                      sizeof(int) * 2 * n + 4 * 256;
+                      sizeof(int) * 2 * n + sizeof(long long) * 3 * n + 5 * 256;
   if (td_scratch_bytes_ < need) {
     if (td_scratch_) {
       cudaStreamSynchronize(stream_);
@@ -735,6 +735,8 @@ int Batch::run_tddftb(int nroots, bool triplet, double tol, int max_iter, std::s
   td_dip_ = reinterpret_cast<double*>(p + o);
   o = align_up(o + sizeof(double) * n * nroots * 3);
   td_info_ = reinterpret_cast<int*>(p + o);
+  o = align_up(o + sizeof(int) * 2 * n);
+  td_cycles_ = reinterpret_cast<long long*>(p + o);
   td_roots_ = nroots;
   cudaError_t e = cudaMemcpyAsync(d_off, off.data(), sizeof(long long) * n, cudaMemcpyHostToDevice, stream_);
   if (e != cudaSuccess) {
@@ -748,8 +750,8 @@ int Batch::run_tddftb(int nroots, bool triplet, double tol, int max_iter, std::s
     return kErrCuda;
   }
   h2d_bytes_ += (long long)(sizeof(long long) * n);
-  launch_tddftb(dev_, td, d_off, nroots, triplet ? 1 : 0, tol, max_iter, td_omega_, td_dip_, td_info_, dev_.scf_grid,
-                stream_);
+  launch_tddftb(dev_, td, d_off, nroots, triplet ? 1 : 0, tol, max_iter, td_omega_, td_dip_, td_info_, td_cycles_,
+                dev_.scf_grid, stream_);
   launches_ += 1;
   e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -780,6 +782,22 @@ int Batch::fetch_tddftb(std::vector<double>& omega, std::vector<double>& dip, st
     return kErrCuda;
   }
   d2h_bytes_ += (long long)(sizeof(double) * (omega.size() + dip.size()) + sizeof(int) * info.size());
+  return kOk;
+}
+
+int Batch::fetch_tddftb_cycles(std::vector<long long>& cycles, std::string& err) {
+  if (!td_roots_) {
+    err = "no TD-DFTB run";
+    return kErrNoResults;
+  }
+  cycles.resize(3 * mols_.size());
+  cudaError_t e = cudaMemcpyAsync(cycles.data(), td_cycles_, sizeof(long long) * cycles.size(), cudaMemcpyDeviceToHost,
+                                  stream_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
   return kOk;
 }
 

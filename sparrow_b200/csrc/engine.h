@@ -73,6 +73,9 @@ class Batch {
   // omega [nmol * nroots] (Hartree), dipoles [nmol * nroots * 3] (e bohr,
   // zero for triplets), info [nmol * 2] (Davidson iterations, status).
   int fetch_tddftb(std::vector<double>& omega, std::vector<double>& dipoles, std::vector<int>& info, std::string& err);
+  // SM cycles per molecule of the last TD-DFTB run: canonical orbitals,
+  // transition charges, Davidson (3 per molecule)
+  int fetch_tddftb_cycles(std::vector<long long>& cycles, std::string& err);
   int tddftb_roots() const { return td_roots_; }
 
   cudaStream_t stream() const { return stream_; }
@@ -128,6 +131,7 @@ class Batch {
   double* td_omega_ = nullptr;
   double* td_dip_ = nullptr;
   int* td_info_ = nullptr;
+  long long* td_cycles_ = nullptr;
   void* large_scratch_ = nullptr;
   size_t large_scratch_bytes_ = 0;
   int scf_grid_ = 0;

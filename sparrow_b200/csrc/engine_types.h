@@ -95,9 +95,6 @@ struct MolResult {
   long long cycles[5];
 };
 
-#ifndef SGB_COLD_SWEEPS
-#define SGB_COLD_SWEEPS 3
-#endif
 struct ScfParams {
   double scc = 1e-7;   // |Delta E| criterion (Hartree)
   double rmsd = 1e-5;  // rms(Delta P) criterion
@@ -105,8 +102,10 @@ struct ScfParams {
   int diis_size = kDiisMax;
   int jacobi_max_sweeps = 30;
   // cap on the sweeps of the first (cold) diagonalisation, which only has to
-  // separate occupied from virtual orbitals
-  int cold_sweeps = SGB_COLD_SWEEPS;
+  // separate occupied from virtual orbitals; 0 = the method's default (NDDO
+  // 3: the rotations converge the rest cheaper than more sweeps; DFTB 6: the
+  // small gaps of conjugated chains need the better start)
+  int cold_sweeps = 0;
   // large-molecule mixed-precision path: purification switches from split-BF16
   // to FP64 once rms(Delta P) falls below this (or stops halving below 1e-4)
   double mixed_switch_rmsd = 1e-5;

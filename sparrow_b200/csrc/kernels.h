@@ -114,9 +114,10 @@ SGB_TD_HD inline long long td_block_doubles(int dim, int nat, int k) {
 }
 // TD-DFTB of every molecule of a converged DFTB batch: td (device scratch,
 // td_off[mol] doubles per molecule), omega [nmol * nroots], dip
-// [nmol * nroots * 3], info [nmol * 2] (Davidson iterations, status).
+// [nmol * nroots * 3], info [nmol * 2] (Davidson iterations, status), cycles
+// [nmol * 3] (SM cycles: canonical orbitals, transition charges, Davidson).
 void launch_tddftb(const DeviceBatch& b, double* td, const long long* td_off, int nroots, int triplet, double tol,
-                   int max_iter, double* omega, double* dip, int* info, int grid, cudaStream_t s);
+                   int max_iter, double* omega, double* dip, int* info, long long* cycles, int grid, cudaStream_t s);
 int scf_max_grid(int max_nao);
 size_t scf_rotation_bytes_per_cta();
 

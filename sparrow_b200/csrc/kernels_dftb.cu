@@ -290,6 +290,7 @@ __global__ void __launch_bounds__(kScfThreads) k_dftb_scf(
     double* rot = rotbuf + (size_t)blockIdx.x * (kRotBudgetBytes / sizeof(double));
     const int cap_rounds = (int)((kRotBudgetBytes / sizeof(double)) / (2 * ((N + 1) / 2)));
     const int msize = sp.diis_size < 1 ? 1 : (sp.diis_size > kDiisMax ? kDiisMax : sp.diis_size);
+    const int cold_sweeps = sp.cold_sweeps > 0 ? sp.cold_sweeps : 6;
     int status = kDevOk;
 
     // Loewdin orthogonaliser (W1, F, Ct, W2 serve as Newton-Schulz buffers)
@@ -317,10 +318,10 @@ __global__ void __launch_bounds__(kScfThreads) k_dftb_scf(
       if (have_orbitals) need_full = ov_rotation(N, no, F, Ct, W1, W2, eps, drift, sh);
       if (need_full) {
         const int sw = full_diagonalise(N, F, Ct, W1, W2, eps, Apk ? Apk : F, Apk ? packed_bytes : 0, have_orbitals,
-                                        rot, cap_rounds, have_orbitals ? sp.jacobi_max_sweeps : sp.cold_sweeps,
+                                        rot, cap_rounds, have_orbitals ? sp.jacobi_max_sweeps : cold_sweeps,
                                         have_orbitals ? 1e-10 : 1e-3, sh);
         if (sw < 0 && have_orbitals) status = kDevJacobiNotConverged;
-        nsweeps += sw < 0 ? (have_orbitals ? sp.jacobi_max_sweeps : sp.cold_sweeps) : sw;
+        nsweeps += sw < 0 ? (have_orbitals ? sp.jacobi_max_sweeps : cold_sweeps) : sw;
         ++nfull;
         have_orbitals = true;
         drift = 0;

@@ -379,6 +379,7 @@ __global__ void __launch_bounds__(kScfThreads) k_scf(const MolDev* __restrict__ 
     double* rot = rotbuf + (size_t)blockIdx.x * (kRotBudgetBytes / sizeof(double));
     const int cap_rounds = (int)((kRotBudgetBytes / sizeof(double)) / (2 * ((N + 1) / 2)));
     const int msize = sp.diis_size < 1 ? 1 : (sp.diis_size > kDiisMax ? kDiisMax : sp.diis_size);
+    const int cold_sweeps = sp.cold_sweeps > 0 ? sp.cold_sweeps : 3;
     int nhist = 0, head = 0;
     bool have_orbitals = false;
     double drift = 0;
@@ -410,10 +411,10 @@ __global__ void __launch_bounds__(kScfThreads) k_scf(const MolDev* __restrict__ 
         // the first (cold) diagonalisation only has to separate occupied from virtual
         // orbitals; the rotations of the later iterations converge them
         const int sw = full_diagonalise(N, F, Ct, W1, W2, eps, Apk ? Apk : F, Apk ? packed_bytes : 0, have_orbitals,
-                                        rot, cap_rounds, have_orbitals ? sp.jacobi_max_sweeps : sp.cold_sweeps,
+                                        rot, cap_rounds, have_orbitals ? sp.jacobi_max_sweeps : cold_sweeps,
                                         have_orbitals ? 1e-10 : 1e-3, sh);
         if (sw < 0 && have_orbitals) status = kDevJacobiNotConverged;
-        nsweeps += sw < 0 ? (have_orbitals ? sp.jacobi_max_sweeps : sp.cold_sweeps) : sw;
+        nsweeps += sw < 0 ? (have_orbitals ? sp.jacobi_max_sweeps : cold_sweeps) : sw;
         ++nfull;
         have_orbitals = true;
         drift = 0;

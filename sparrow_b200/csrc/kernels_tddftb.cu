@@ -182,7 +182,7 @@ __global__ void __launch_bounds__(kScfThreads) k_tddftb(
     const double* __restrict__ Xall, double* Fall, double* Call, double* W1all, double* W2all, double* epsall,
     double* rotbuf, const double* __restrict__ gamall, const MolResult* __restrict__ res, double* td,
     const long long* __restrict__ td_off, int nroots, int triplet, double tol, int max_iter, double* omega_out,
-    double* dip_out, int* info, int packed_in_smem) {
+    double* dip_out, int* info, long long* cycles, int packed_in_smem) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ScfShared& sh = *reinterpret_cast<ScfShared*>(smem_raw);
   unsigned char* after = smem_raw + ((sizeof(ScfShared) + 15) / 16) * 16;
@@ -224,6 +224,7 @@ __global__ void __launch_bounds__(kScfThreads) k_tddftb(
     double* eps = epsall + m.ao_base;
     const double* gm = gamall + m.gam_off;
     int status = kTdOk;
+    const long long c0 = clock64();
 
     // 1. canonical orbitals of F' = X F X, C = X C'^T (AO rows, orbital columns) in W1, SC in W2
     cta_gemm(N, N, N, 1.0, F, N, false, X, N, false, 0.0, W1, N, sh.gemm);
@@ -241,6 +242,7 @@ __global__ void __launch_bounds__(kScfThreads) k_tddftb(
     cta_gemm(N, N, N, 1.0, S, N, false, W1, N, false, 0.0, W2, N, sh.gemm);
     const double* C = W1;
     const double* SC = W2;
+    const long long c1 = clock64();
 
     // per-molecule scratch
     double* hT = td + td_off[mi];                 // [nat][dim]  q sqrt(Delta)
@@ -277,6 +279,8 @@ __global__ void __launch_bounds__(kScfThreads) k_tddftb(
       D[2 * (size_t)dim + kk] = dz;
     }
     __syncthreads();
+
+    const long long c2 = clock64();
 
     // 3. start vectors: unit vectors of the m0 smallest Delta
     const int m0 = 2 * k < mmax ? 2 * k : mmax;
@@ -509,6 +513,9 @@ __global__ void __launch_bounds__(kScfThreads) k_tddftb(
     if (tid == 0) {
       info[2 * mi] = iter;
       info[2 * mi + 1] = status;
+      cycles[3 * mi + 0] = c1 - c0;
+      cycles[3 * mi + 1] = c2 - c1;
+      cycles[3 * mi + 2] = clock64() - c2;
     }
     __syncthreads();
   }
@@ -529,7 +536,7 @@ size_t tddftb_smem_bytes(int max_nao, int* packed_in_smem) {
 }  // namespace
 
 void launch_tddftb(const DeviceBatch& b, double* td, const long long* td_off, int nroots, int triplet, double tol,
-                   int max_iter, double* omega, double* dip, int* info, int grid, cudaStream_t s) {
+                   int max_iter, double* omega, double* dip, int* info, long long* cycles, int grid, cudaStream_t s) {
   if (b.nmol == 0) return;
   int in_smem = 0;
   const size_t bytes = tddftb_smem_bytes(b.max_nao, &in_smem);
@@ -538,7 +545,7 @@ void launch_tddftb(const DeviceBatch& b, double* td, const long long* td_off, in
   if (grid > b.nmol) grid = b.nmol;
   k_tddftb<<<grid, kScfThreads, bytes, s>>>(b.mols, b.nmol, b.order, b.counter, b.atoms, b.delems, b.S, b.X, b.F, b.C,
                                             b.W1, b.W2, b.eps, b.rotbuf, b.gam, b.res, td, td_off, nroots, triplet, tol,
-                                            max_iter, omega, dip, info, in_smem);
+                                            max_iter, omega, dip, info, cycles, in_smem);
 }
 
 }  // namespace sgb
