@@ -18,7 +18,8 @@ gradients); `roofline` is the dominant kernel (the persistent SCF kernel)
 against the measured FP64 GEMM rate; `cpu_baseline` is the oracle on a
 bounded random sample of the same molecules.  Side legs (rank 0): the plain
 one-molecule-per-launch GPU form, the request server's p50/p99 latency, and
-the large-molecule path on (H2O)_256/512/1024 in FP64 and mixed precision.
+the large-molecule path on (H2O)_256/512/1024 in FP64 and mixed precision,
+and DFTB3 + TD-DFTB excitations over 1024 polyenes.
 """
 import argparse
 import json
@@ -52,6 +53,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-serving", action="store_true", help="skip the request-server latency leg")
     p.add_argument("--no-large", action="store_true", help="skip the large-molecule (water cluster) leg")
+    p.add_argument("--no-tddftb", action="store_true", help="skip the DFTB3 + TD-DFTB polyene leg")
+    p.add_argument("--no-plain", action="store_true", help="skip the plain one-molecule-per-launch GPU leg")
     p.add_argument("--serving-loads", default="250,500,1000,2000", help="offered loads (req/s) of the serving leg")
     return p.parse_args()
 
@@ -250,6 +253,55 @@ def large_leg(sizes=(256, 512, 1024), seed=0):
         rows.append(row)
     return {"workload": "PM6 (H2O)_n, n in %s, seed %d, one molecule over the whole GPU, energy+gradient, "
                         "rms dP 1e-8" % (list(sizes), seed), "sizes": rows}
+
+
+def tddftb_leg(count=1024, seed=6, nroots=8, cpu_seconds=10.0):
+    """DFTB3 (3ob-3-1) ground state plus TD-DFTB for the lowest singlets over a
+    batch of polyenes C_2kH_2k+2, k ~ U[5,40]: device ms of the SCF and of the
+    excitations, molecules/s, Davidson outcome; the CPU oracle (dense Casida)
+    on a bounded sample of the smallest molecules of the batch, with the
+    largest excitation-energy difference of the GPU on that sample."""
+    import numpy as np
+    import sparrow_b200
+    from sparrow_b200 import geometry
+    mols = [(z, geometry.to_bohr(x)) for z, x in geometry.polyene_batch(count, seed=seed)]
+    out = {"workload": "%d polyenes C_2kH_2k+2, k~U[5,40], seed %d, DFTB3 3ob-3-1, rms dP 1e-8, %d lowest singlets "
+                       "(full TD-DFTB, Davidson residual 1e-8)" % (count, seed, nroots)}
+    for rep in range(2):  # the first pass pays module loading
+        b = sparrow_b200.Batch("DFTB3", mols, scc=1e-7, rmsd=1e-8, max_iter=200)
+        b.record_event(0)
+        b.run()
+        b.record_event(1)
+        e, _, it, conv = b.results()
+        b.record_event(2)
+        om, mu, st = b.excitations(nroots)
+        b.record_event(3)
+        scf_ms, td_ms = b.elapsed_ms(0, 1), b.elapsed_ms(2, 3)
+    cyc = b.excitation_cycles().astype(float)
+    out.update({"scf_ms": scf_ms, "tddftb_ms": td_ms, "molecules_per_s": count / ((scf_ms + td_ms) / 1e3),
+                "scf_converged": int(conv.sum()), "mean_scf_iterations": float(it.mean()),
+                "excitations_ok": int((st == 0).sum()),
+                "tddftb_cycle_share": {"canonical_orbitals": float(cyc[:, 0].sum() / cyc.sum()),
+                                       "transition_charges": float(cyc[:, 1].sum() / cyc.sum()),
+                                       "davidson": float(cyc[:, 2].sum() / cyc.sum())}})
+    # CPU oracle on the smallest molecules, within the time budget
+    from tests import oracle_lib as O
+    order = sorted(range(count), key=lambda i: len(mols[i][0]))
+    t0 = time.perf_counter()
+    done, dmax = 0, 0.0
+    for i in order:
+        if time.perf_counter() - t0 > cpu_seconds:
+            break
+        r = O.dftb_tddftb(3, mols[i][0], mols[i][1], nroots=nroots)
+        dmax = max(dmax, float(np.max(np.abs(r["omega"] - om[i][:len(r["omega"])]))))
+        done += 1
+    wall = time.perf_counter() - t0
+    out["cpu_baseline"] = {"value": done / wall, "unit": "molecules/s", "cores": 1, "kind": "port",
+                           "sample": "the %d smallest polyenes of the batch (%d-%d atoms), oracle DFTB3 SCF + dense "
+                                     "Casida diagonalisation, %.1f s wall" % (
+                                         done, len(mols[order[0]][0]), len(mols[order[max(done - 1, 0)]][0]), wall),
+                           "max_abs_domega_gpu_vs_oracle_hartree": dmax}
+    return out
 
 
 def host_cores():
@@ -472,12 +524,13 @@ def run_engine(args, rank, world):
 
     # the plain one-molecule-per-launch GPU form on a sample of the same batch
     plain = None
-    if rank == 0:
+    if rank == 0 and not args.no_plain:
         prate, pcount, pwall = plain_gpu_rate(args.method, mols)
         plain = {"value": prate, "unit": "solves/s",
                  "sample": "%d random molecules of the batch, one Calculator.calculate() each (host buffers, "
                            "energy+gradient), %.1f s wall" % (pcount, pwall),
                  "batched_device_over_plain": value / world / prate, "batched_e2e_over_plain": e2e_value / world / prate}
+
 
     serving = None
     if rank == 0 and not args.no_serving:
@@ -486,6 +539,9 @@ def run_engine(args, rank, world):
     large = None
     if rank == 0 and not args.no_large:
         large = large_leg()
+    tddftb = None
+    if rank == 0 and not args.no_tddftb:
+        tddftb = tddftb_leg()
 
     # roofline of the SCF kernel (average launch)
     scf_ms = stage_sum[2] / args.steps
@@ -518,6 +574,7 @@ def run_engine(args, rank, world):
         "plain_gpu": plain,
         "serving": serving,
         "large_molecules": large,
+        "tddftb": tddftb,
         "clocks": clk,
     }
     if rank == 0:
