@@ -178,7 +178,6 @@ __device__ double fock_light_pairs(const MolDev& m, const AtomDev* __restrict__ 
     const AtomDev aA = atoms[pr.a], aB = atoms[pr.b];
     const int nA = elems[aA.slot].nao, nB = elems[aB.slot].nao;
     if (nA == 4 && nB == 4) continue;
-    const int dA = nA == 1 ? 1 : 10, dB = nB == 1 ? 1 : 10;
     const int oa = aA.ao0, ob = aB.ao0;
     const double* W = ints + pr.int_off;
     double* jb = jbuf + (size_t)pi * 20;

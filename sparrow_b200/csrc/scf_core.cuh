@@ -333,7 +333,7 @@ __device__ int jacobi_diagonalise(int N, double* A, double* Ct, bool cold, doubl
                                   JacobiShared& js, double* red, int max_sweeps, double tol) {
   const int Ne = N + (N & 1);
   const int npair = Ne / 2;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  const int tid = threadIdx.x;
   long long g_all = 0, g0 = 0;
   int nrec = 0;
   bool identity = cold;
@@ -366,11 +366,17 @@ __device__ int jacobi_diagonalise(int N, double* A, double* Ct, bool cold, doubl
         rc[npair + k] = s;
       }
       __syncthreads();
-      // A <- J^T A J on 2x2 blocks (pair k1 rows, pair k2 columns), k2 <= k1; one warp per k1
-      for (int k1 = warp; k1 < npair; k1 += nwarps) {
+      // A <- J^T A J on 2x2 blocks (pair k1 rows, pair k2 columns), k2 <= k1:
+      // the triangle of blocks is flattened over the CTA so every lane works
+      const int nblk = npair * (npair + 1) / 2;
+      for (int b = tid; b < nblk; b += blockDim.x) {
+        int k1 = (int)((sqrtf(8.0f * (float)b + 1.0f) - 1.0f) * 0.5f);
+        while (k1 * (k1 + 1) / 2 > b) --k1;
+        while ((k1 + 1) * (k1 + 2) / 2 <= b) ++k1;
+        const int k2 = b - k1 * (k1 + 1) / 2;
         const int p1 = js.p[k1], q1 = js.q[k1];
         const double c1 = js.c[k1], s1 = js.s[k1];
-        for (int k2 = lane; k2 <= k1; k2 += 32) {
+        {
           const int p2 = js.p[k2], q2 = js.q[k2];
           if (k1 == k2) {
             if (q1 < 0) continue;
