@@ -14,9 +14,10 @@
 //   dipole matrix       Utils/DipoleUtils/DFTBDipoleMatrixCalculator.cpp:60-84
 //                       D_ia = sum_A q_A^{ia} R_A; mu_I = sqrt(2) sum_ia c_ia D_ia
 // Per molecule:
-//   1. canonical orbitals: F' = X F X of the converged Fock matrix, a warm
-//      Jacobi diagonalisation in the basis of the SCF's last orbitals (the
-//      rotation-based SCF keeps them only close to canonical), C = X C'.
+//   1. canonical orbitals: F' = X F X of the converged Fock matrix, Jacobi
+//      diagonalisations of its occupied and virtual blocks in the basis of the
+//      SCF's last orbitals (the rotation-based SCF keeps them only close to
+//      canonical; the occupied-virtual block vanishes at convergence), C = X C'.
 //   2. SC, the transition charges and dipole vectors of every occupied-virtual
 //      pair, h = q sqrt(Delta).
 //   3. block Davidson for the lowest n_roots eigenpairs of the symmetric
@@ -182,12 +183,12 @@ __global__ void __launch_bounds__(kScfThreads) k_tddftb(
     const double* __restrict__ Xall, double* Fall, double* Call, double* W1all, double* W2all, double* epsall,
     double* rotbuf, const double* __restrict__ gamall, const MolResult* __restrict__ res, double* td,
     const long long* __restrict__ td_off, int nroots, int triplet, double tol, int max_iter, double* omega_out,
-    double* dip_out, int* info, long long* cycles, int packed_in_smem) {
+    double* dip_out, int* info, long long* cycles, size_t region_bytes) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ScfShared& sh = *reinterpret_cast<ScfShared*>(smem_raw);
   unsigned char* after = smem_raw + ((sizeof(ScfShared) + 15) / 16) * 16;
   TdShared& ts = *reinterpret_cast<TdShared*>(after);  // after the canonicalisation
-  double* smemA = reinterpret_cast<double*>(after);     // packed Jacobi matrix during it
+  double* smemA = reinterpret_cast<double*>(after);     // packed Jacobi blocks during it
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5, nt = blockDim.x;
   while (true) {
     if (tid == 0) sh.mol = atomicAdd(counter, 1);
@@ -226,16 +227,35 @@ __global__ void __launch_bounds__(kScfThreads) k_tddftb(
     int status = kTdOk;
     const long long c0 = clock64();
 
-    // 1. canonical orbitals of F' = X F X, C = X C'^T (AO rows, orbital columns) in W1, SC in W2
+    // 1. canonical orbitals of F' = X F X.  At self-consistency the
+    //    occupied-virtual block of F' in the SCF's orbitals vanishes, so the
+    //    occupied and the virtual blocks are diagonalised separately (a
+    //    quarter of the work of one full diagonalisation, and blocks that fit
+    //    shared memory); then C = X C'^T (AO rows, orbital columns) in W1, SC in W2
     cta_gemm(N, N, N, 1.0, F, N, false, X, N, false, 0.0, W1, N, sh.gemm);
     cta_gemm(N, N, N, 1.0, X, N, false, W1, N, false, 0.0, F, N, sh.gemm);
-    {
+    for (int blk = 0; blk < 2; ++blk) {
+      const int r0 = blk ? no : 0, n = blk ? nv : no;
+      if (n == 0) continue;
+      double* Cb = Ct + (size_t)r0 * N;
+      cta_gemm(n, N, N, 1.0, Cb, N, false, F, N, false, 0.0, W1, N, sh.gemm);  // C_b F'
+      cta_gemm(n, n, N, 1.0, W1, N, false, Cb, N, true, 0.0, W2, n, sh.gemm);  // C_b F' C_b^T
+      const size_t pk_bytes = sizeof(double) * (size_t)n * (n + 1) / 2;
+      const bool in_smem = pk_bytes <= region_bytes;
+      double* A = in_smem ? smemA : W1;
+      for (int e = tid; e < n * (n + 1) / 2; e += nt) {
+        int i = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+        while ((i + 1) * (i + 2) / 2 <= e) ++i;
+        while (i * (i + 1) / 2 > e) --i;
+        const int j = e - i * (i + 1) / 2;
+        A[e] = 0.5 * (W2[(size_t)i * n + j] + W2[(size_t)j * n + i]);
+      }
+      __syncthreads();
       double* rot = rotbuf + (size_t)blockIdx.x * (kRotBudgetBytes / sizeof(double));
-      const int cap_rounds = (int)((kRotBudgetBytes / sizeof(double)) / (2 * ((N + 1) / 2)));
-      double* Apk = packed_in_smem ? smemA : nullptr;
-      const size_t packed_bytes = sizeof(double) * (size_t)N * (N + 1) / 2;
-      const int sw = full_diagonalise(N, F, Ct, W1, W2, eps, Apk ? Apk : F, Apk ? packed_bytes : 0, true, rot,
-                                      cap_rounds, 30, 1e-12, sh);
+      const int cap_rounds = (int)((kRotBudgetBytes / sizeof(double)) / (2 * ((n + 1) / 2)));
+      double* Afree = in_smem && region_bytes >= sizeof(double) * 32 * (size_t)n ? smemA : nullptr;
+      const int sw = jacobi_diagonalise(n, A, Cb, false, rot, cap_rounds, sh.gemm, sizeof(sh.gemm), Afree,
+                                        Afree ? region_bytes : 0, sh.rank, eps + r0, sh.js, sh.red, 30, 1e-12, N, N);
       if (sw < 0) status = kTdOrbitals;
     }
     cta_gemm(N, N, N, 1.0, X, N, false, Ct, N, true, 0.0, W1, N, sh.gemm);
@@ -521,15 +541,17 @@ __global__ void __launch_bounds__(kScfThreads) k_tddftb(
   }
 }
 
-size_t tddftb_smem_bytes(int max_nao, int* packed_in_smem) {
+// ScfShared, then one region for the packed Jacobi blocks of the
+// canonicalisation and, afterwards, the Davidson state: all the opt-in shared
+// memory that is left (at least the Davidson state).
+size_t tddftb_smem_bytes(size_t* region_bytes) {
   const size_t base = ((sizeof(ScfShared) + 15) / 16) * 16;
-  const size_t pk = sizeof(double) * (size_t)max_nao * (max_nao + 1) / 2;
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  const size_t td = sizeof(TdShared);
-  *packed_in_smem = base + pk <= (size_t)optin ? 1 : 0;
-  const size_t region = *packed_in_smem && pk > td ? pk : td;
+  size_t region = (size_t)optin > base ? (((size_t)optin - base) / 16) * 16 : 0;
+  if (region < sizeof(TdShared)) region = sizeof(TdShared);
+  *region_bytes = region;
   return base + region;
 }
 
@@ -538,14 +560,14 @@ size_t tddftb_smem_bytes(int max_nao, int* packed_in_smem) {
 void launch_tddftb(const DeviceBatch& b, double* td, const long long* td_off, int nroots, int triplet, double tol,
                    int max_iter, double* omega, double* dip, int* info, long long* cycles, int grid, cudaStream_t s) {
   if (b.nmol == 0) return;
-  int in_smem = 0;
-  const size_t bytes = tddftb_smem_bytes(b.max_nao, &in_smem);
+  size_t region = 0;
+  const size_t bytes = tddftb_smem_bytes(&region);
   cudaFuncSetAttribute(k_tddftb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   cudaMemsetAsync(b.counter, 0, sizeof(int), s);
   if (grid > b.nmol) grid = b.nmol;
   k_tddftb<<<grid, kScfThreads, bytes, s>>>(b.mols, b.nmol, b.order, b.counter, b.atoms, b.delems, b.S, b.X, b.F, b.C,
                                             b.W1, b.W2, b.eps, b.rotbuf, b.gam, b.res, td, td_off, nroots, triplet, tol,
-                                            max_iter, omega, dip, info, cycles, in_smem);
+                                            max_iter, omega, dip, info, cycles, region);
 }
 
 }  // namespace sgb

@@ -231,21 +231,22 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
 }
 __device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
-// Replay nrec recorded rounds (the first is global round g0) onto Ct.
-// Ct is processed in tiles of w AO columns (w a power of two, T laid out
+// Replay nrec recorded rounds (the first is global round g0) onto the N rows
+// of Ct (ncols AO columns, row stride ldc).  Ct is processed in tiles of w AO columns (w a power of two, T laid out
 // [row][w]); the rounds' (c, s) are streamed into the staging buffer St in
 // chunks of rb rounds, double-buffered with cp.async.  cold: Ct is the
 // identity and is not read.  rank: when non-null, row k of the result is
 // written to row rank[k] (eigenvalue order).
 __device__ void replay_rotations(int N, int Ne, int npair, long long g0, int nrec, const double* __restrict__ rot,
-                                 double* Ct, bool cold, const int* rank, double* T, int w, double* St, int rb) {
+                                 double* Ct, bool cold, const int* rank, double* T, int w, double* St, int rb,
+                                 int ncols, int ldc) {
   const int tid = threadIdx.x, bd = blockDim.x;
   const int lw = __ffs(w) - 1;
   const int jj = tid & (w - 1), k_first = tid >> lw, k_step = bd >> lw;
   const int round_doubles = 2 * npair;  // a multiple of 2: 16-byte chunks
   const int nchunk = (nrec + rb - 1) / rb;
-  for (int j0 = 0; j0 < N; j0 += w) {
-    const int wj = min(w, N - j0);
+  for (int j0 = 0; j0 < ncols; j0 += w) {
+    const int wj = min(w, ncols - j0);
     auto stage = [&](int c) {
       const int g = c * rb, n = min(rb, nrec - g);
       const double* src = rot + (size_t)g * round_doubles;
@@ -256,7 +257,7 @@ __device__ void replay_rotations(int N, int Ne, int npair, long long g0, int nre
     cp_async_commit();
     for (int e = tid; e < N * w; e += bd) {
       const int k = e >> lw, j = e & (w - 1);
-      T[e] = (j >= wj) ? 0.0 : cold ? (k == j0 + j ? 1.0 : 0.0) : Ct[(size_t)k * N + j0 + j];
+      T[e] = (j >= wj) ? 0.0 : cold ? (k == j0 + j ? 1.0 : 0.0) : Ct[(size_t)k * ldc + j0 + j];
     }
     for (int c = 0; c < nchunk; ++c) {
       if (c + 1 < nchunk) stage(c + 1);
@@ -288,7 +289,7 @@ __device__ void replay_rotations(int N, int Ne, int npair, long long g0, int nre
     __syncthreads();
     for (int e = tid; e < N * w; e += bd) {
       const int k = e >> lw, j = e & (w - 1);
-      if (j < wj) Ct[(size_t)(rank ? rank[k] : k) * N + j0 + j] = T[e];
+      if (j < wj) Ct[(size_t)(rank ? rank[k] : k) * ldc + j0 + j] = T[e];
     }
     __syncthreads();
   }
@@ -325,12 +326,16 @@ __device__ ReplayPlan plan_replay(int N, int npair, double* tile, size_t tile_by
 }
 
 // Diagonalise the packed A; Ct <- Ct J (all rotations), sorted by eigenvalue
-// into eps / rows of Ct.  Returns the sweep count (-1 if not converged).
+// into eps / rows of Ct (N rows of ncols entries, row stride ldc; both
+// default to N).  Returns the sweep count (-1 if not converged).
 // U: the shared phase-scratch region (tiles and staging while A is alive);
 // Afree: A's shared storage, reused as the tile of the last replay (or null).
 __device__ int jacobi_diagonalise(int N, double* A, double* Ct, bool cold, double* rot, int cap_rounds,
                                   double* U, size_t U_bytes, double* Afree, size_t Afree_bytes, int* rank, double* eps,
-                                  JacobiShared& js, double* red, int max_sweeps, double tol) {
+                                  JacobiShared& js, double* red, int max_sweeps, double tol, int ncols = -1,
+                                  int ldc = -1) {
+  if (ncols < 0) ncols = N;
+  if (ldc < 0) ldc = N;
   const int Ne = N + (N & 1);
   const int npair = Ne / 2;
   const int tid = threadIdx.x;
@@ -407,7 +412,7 @@ __device__ int jacobi_diagonalise(int N, double* A, double* Ct, bool cold, doubl
       ++g_all;
       if (nrec == cap_rounds) {
         const ReplayPlan pl = plan_replay(N, npair, nullptr, 0, U, U_bytes, 32);
-        replay_rotations(N, Ne, npair, g0, nrec, rot, Ct, identity, nullptr, pl.T, pl.w, pl.St, pl.rb);
+        replay_rotations(N, Ne, npair, g0, nrec, rot, Ct, identity, nullptr, pl.T, pl.w, pl.St, pl.rb, ncols, ldc);
         identity = false;
         g0 = g_all;
         nrec = 0;
@@ -433,7 +438,7 @@ __device__ int jacobi_diagonalise(int N, double* A, double* Ct, bool cold, doubl
   __syncthreads();
   const ReplayPlan pl = Afree ? plan_replay(N, npair, Afree, Afree_bytes, U, U_bytes, 64)
                               : plan_replay(N, npair, nullptr, 0, U, U_bytes, 32);
-  replay_rotations(N, Ne, npair, g0, nrec, rot, Ct, identity, rank, pl.T, pl.w, pl.St, pl.rb);
+  replay_rotations(N, Ne, npair, g0, nrec, rot, Ct, identity, rank, pl.T, pl.w, pl.St, pl.rb, ncols, ldc);
   return sweeps;
 }
 
