@@ -438,6 +438,34 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------
+# replicas: one rank per GPU, molecules sharded by rank (seeded per rank), no
+# data-path collective; the process group only carries the barriers and the
+# max-over-ranks of the timings
+# ----------------------------------------------------------------------------
+def init_ranks(world, timeout_s=300):
+    """torch.distributed process group for world > 1 (NCCL with GPUs, gloo without), else None."""
+    if world <= 1:
+        return None
+    import datetime
+    import torch
+    import torch.distributed as td
+    td.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                          timeout=datetime.timedelta(seconds=timeout_s))
+    return td
+
+
+def reduce_max(dist, v):
+    """Maximum of v over the ranks (v itself without a process group)."""
+    if dist is None:
+        return v
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_engine(args, rank, world):
     import numpy as np
     import sparrow_b200
@@ -452,25 +480,14 @@ def run_engine(args, rank, world):
                "sample": "%d random molecules of the batch, oracle (C++ FP64 restatement of the reference path), "
                          "molecule-parallel over %d processes, %.1f s wall" % (count, procs, wall)}
 
-    dist = None
-    if world > 1:
-        import torch
-        import torch.distributed as td
-        td.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
-                              timeout=__import__("datetime").timedelta(seconds=300))
-        dist = td
+    dist = init_ranks(world)
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
     def max_over_ranks(v):
-        if dist is None:
-            return v
-        import torch
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(dist, v)
 
     peak = None
     if rank == 0:
