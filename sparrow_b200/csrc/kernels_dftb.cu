@@ -248,7 +248,7 @@ __device__ double dftb_fock(const MolDev& m, const int* ao_atom, const double* H
   return cta_sum(eb, red);
 }
 
-__global__ void __launch_bounds__(kScfThreads) k_dftb_scf(
+__global__ void __launch_bounds__(kScfThreads, 1) k_dftb_scf(
     const MolDev* __restrict__ mols, int nmol, const int* __restrict__ order_list, int* counter,
     const AtomDev* __restrict__ atoms, const DftbElemDev* __restrict__ el, const int* __restrict__ ao_atom,
     const double* __restrict__ H0all, const double* __restrict__ Sall, double* Xall, double* Pall, double* Ppall,
@@ -327,9 +327,9 @@ __global__ void __launch_bounds__(kScfThreads) k_dftb_scf(
         drift = 0;
       }
       // P' = 2 C'_occ C'_occ^T, P = X P' X
-      cta_gemm(N, N, no, 2.0, Ct, N, true, Ct, N, false, 0.0, Pp, N, sh.gemm);
+      cta_gemm(N, N, no, 2.0, Ct, N, true, Ct, N, false, 0.0, Pp, N, sh.gemm, true);
       cta_gemm(N, N, N, 1.0, X, N, false, Pp, N, false, 0.0, W1, N, sh.gemm);
-      cta_gemm(N, N, N, 1.0, W1, N, false, X, N, false, 0.0, W2, N, sh.gemm);
+      cta_gemm(N, N, N, 1.0, W1, N, false, X, N, false, 0.0, W2, N, sh.gemm, true);
       double d2 = 0;
       for (size_t k = tid; k < NN; k += blockDim.x) {
         const double d = W2[k] - P[k];
@@ -358,7 +358,7 @@ __global__ void __launch_bounds__(kScfThreads) k_dftb_scf(
     const double e23 = charges_and_shifts(m, order, atoms, el, P, S, gm, Gm, W2, q, sh4, sh.red);
     const double eb = dftb_fock(m, ao_atom, H0, S, P, sh4, F, sh.red);
     cta_gemm(N, N, N, 1.0, F, N, false, P, N, false, 0.0, W2, N, sh.gemm);
-    cta_gemm(N, N, N, 0.5, P, N, false, W2, N, false, 0.0, W1, N, sh.gemm);
+    cta_gemm(N, N, N, 0.5, P, N, false, W2, N, false, 0.0, W1, N, sh.gemm, true);
     if (tid == 0) {
       MolResult& r = res[mi];
       r.e_el = eb + e23;

@@ -335,7 +335,7 @@ __device__ double build_fock(const MolDev& m, const AtomDev* __restrict__ atoms,
   return cta_sum(e, red);
 }
 
-__global__ void __launch_bounds__(kScfThreads) k_scf(const MolDev* __restrict__ mols, int nmol,
+__global__ void __launch_bounds__(kScfThreads, 1) k_scf(const MolDev* __restrict__ mols, int nmol,
                                                      const int* __restrict__ order, int* counter,
                                                      const AtomDev* __restrict__ atoms,
                                                      const ElemDev* __restrict__ elems,
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(kScfThreads) k_scf(const MolDev* __restrict__ 
       long long t4 = clock64();
       cyc[3] += t4 - t3;
       // new density P = 2 C_occ C_occ^T = 2 Ct_o^T Ct_o into W1, rms change against P
-      cta_gemm(N, N, no, 2.0, Ct, N, true, Ct, N, false, 0.0, W1, N, sh.gemm);
+      cta_gemm(N, N, no, 2.0, Ct, N, true, Ct, N, false, 0.0, W1, N, sh.gemm, true);
       double d2 = 0;
       for (size_t k = tid; k < NN; k += blockDim.x) {
         const double d = W1[k] - P[k];

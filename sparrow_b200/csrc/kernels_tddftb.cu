@@ -177,7 +177,7 @@ enum TdStatus : int {
   kTdNoReference = 4,       // the DFTB reference did not converge
 };
 
-__global__ void __launch_bounds__(kScfThreads) k_tddftb(
+__global__ void __launch_bounds__(kScfThreads, 1) k_tddftb(
     const MolDev* __restrict__ mols, int nmol, const int* __restrict__ order_list, int* counter,
     const AtomDev* __restrict__ atoms, const DftbElemDev* __restrict__ el, const double* __restrict__ Sall,
     const double* __restrict__ Xall, double* Fall, double* Call, double* W1all, double* W2all, double* epsall,

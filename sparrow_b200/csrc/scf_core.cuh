@@ -92,15 +92,17 @@ __device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, dou
                : "d"(a), "d"(b));
 }
 
-__device__ void cta_gemm(int M, int Nn, int K, double alpha, const double* __restrict__ A, int lda, bool tA,
+// sym: the result is known to be symmetric (M == Nn): only the tiles on or
+// above the diagonal are computed, off-diagonal tiles are mirrored.
+__device__ __forceinline__ void cta_gemm(int M, int Nn, int K, double alpha, const double* __restrict__ A, int lda, bool tA,
                          const double* __restrict__ B, int ldb, bool tB, double beta, double* C, int ldc,
-                         double* smem) {
+                         double* smem, bool sym = false) {
   const int grp = threadIdx.x / kGemmGroup, tid = threadIdx.x % kGemmGroup;
   const int lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1;
   double* base = smem + grp * kGemmStages * kGemmStage;
   const int tilesM = (M + kGemmBM - 1) / kGemmBM, tilesN = (Nn + kGemmBN - 1) / kGemmBN;
-  const int ntiles = tilesM * tilesN;
+  const int ntiles = sym ? tilesM * (tilesM + 1) / 2 : tilesM * tilesN;
   const int nk = (K + kGemmBK - 1) / kGemmBK;
   // shared strides of A(m, k) and B(k, n)
   const int a_sm = tA ? 1 : kGemmLdK, a_sk = tA ? kGemmLdMN : 1;
@@ -135,7 +137,17 @@ __device__ void cta_gemm(int M, int Nn, int K, double alpha, const double* __res
   };
   const int fr = lane >> 2, fc = lane & 3;  // fragment row / column-in-group
   for (int tile = grp; tile < ntiles; tile += 2) {
-    const int m0 = (tile / tilesN) * kGemmBM, n0 = (tile % tilesN) * kGemmBN;
+    int tm = tile / tilesN, tn = tile % tilesN;
+    if (sym) {  // tile-th upper tile, row-major over (tm, tn >= tm)
+      int t = tile;
+      tm = 0;
+      while (t >= tilesM - tm) {
+        t -= tilesM - tm;
+        ++tm;
+      }
+      tn = tm + t;
+    }
+    const int m0 = tm * kGemmBM, n0 = tn * kGemmBN;
     double acc[2][4][2];
 #pragma unroll
     for (int i = 0; i < 2; ++i)
@@ -177,7 +189,9 @@ __device__ void cta_gemm(int M, int Nn, int K, double alpha, const double* __res
           const int gm = m0 + wm * 16 + i * 8 + fr, gn = n0 + wn * 32 + j * 8 + fc * 2 + h;
           if (gm < M && gn < Nn) {
             double* c = &C[(size_t)gm * ldc + gn];
-            *c = beta == 0.0 ? alpha * acc[i][j][h] : alpha * acc[i][j][h] + beta * (*c);
+            const double v = beta == 0.0 ? alpha * acc[i][j][h] : alpha * acc[i][j][h] + beta * (*c);
+            *c = v;
+            if (sym && tn > tm) C[(size_t)gn * ldc + gm] = v;
           }
         }
   }
@@ -586,7 +600,7 @@ __device__ int full_diagonalise(int N, double* F, double* Ct, double* W1, double
   const double* src;
   if (warm) {
     cta_gemm(N, N, N, 1.0, F, N, false, Ct, N, true, 0.0, W1, N, sh.gemm);  // F C
-    cta_gemm(N, N, N, 1.0, Ct, N, false, W1, N, false, 0.0, W2, N, sh.gemm);  // C^T F C
+    cta_gemm(N, N, N, 1.0, Ct, N, false, W1, N, false, 0.0, W2, N, sh.gemm, true);  // C^T F C
     src = W2;
   } else {
     src = F;
@@ -658,8 +672,8 @@ __device__ int ov_rotation(int N, int no, double* F, double* Ct, double* W1, dou
   if (xmax > 0.5) return 1;
   // Ct <- M Ct with M = I + K + K^2/2, K = [[0, X^T], [-X, 0]] (orbital space):
   //   M = [[I - X^T X / 2, X^T], [-X, I - X X^T / 2]], assembled in W1
-  cta_gemm(no, no, nv, -0.5, X, no, true, X, no, false, 0.0, W1, N, sh.gemm);
-  cta_gemm(nv, nv, no, -0.5, X, no, false, X, no, true, 0.0, W1 + (size_t)no * N + no, N, sh.gemm);
+  cta_gemm(no, no, nv, -0.5, X, no, true, X, no, false, 0.0, W1, N, sh.gemm, true);
+  cta_gemm(nv, nv, no, -0.5, X, no, false, X, no, true, 0.0, W1 + (size_t)no * N + no, N, sh.gemm, true);
   for (int e = tid; e < nv * no; e += blockDim.x) {
     const int a = e / no, i = e % no;
     W1[(size_t)i * N + no + a] = X[e];
@@ -678,7 +692,7 @@ __device__ int ov_rotation(int N, int no, double* F, double* Ct, double* W1, dou
     __syncthreads();
     for (int k = tid; k < N; k += blockDim.x) W1[(size_t)k * N + k] = 1.5;
     __syncthreads();
-    cta_gemm(N, N, N, -0.5, Ct, N, false, Ct, N, true, 1.0, W1, N, sh.gemm);
+    cta_gemm(N, N, N, -0.5, Ct, N, false, Ct, N, true, 1.0, W1, N, sh.gemm, true);
     cta_gemm(N, N, N, 1.0, W1, N, false, Ct, N, false, 0.0, W2, N, sh.gemm);
     for (size_t e = tid; e < NN; e += blockDim.x) Ct[e] = W2[e];
     __syncthreads();
