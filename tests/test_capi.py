@@ -73,3 +73,14 @@ def test_clone_keeps_settings_and_structure():
     d = c.clone()
     assert d.settings["self_consistence_criterion"] == pytest.approx(1e-9)
     assert np.allclose(d.positions, c.positions)
+
+
+def test_excitation_entry_points_check_their_arguments():
+    # argument checks happen on the host, before any device work
+    L = sparrow_b200.lib()
+    om = np.zeros(4)
+    om_p = om.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    assert L.sg_calculate_excitations(None, 4, 0, om_p, None) == 1
+    assert L.sg_batch_excitations(None, 4, 0, om_p, None, None) == 1
+    assert L.sg_batch_set_scf_path(None, 2) == 1
+    assert L.sg_batch_set_mixed_switch(None, 1e-5) == 1
