@@ -496,7 +496,11 @@ __device__ const double* diis_step(int N, const double* F, const double* P, doub
   const int slot = head;
   head = (head + 1) % msize;
   if (nhist < msize) ++nhist;
-  double* eS = histE + (size_t)slot * TE;
+  // the error vectors only enter the B matrix: they are kept in FP32 (half
+  // the ring traffic; relative precision 6e-8 at any magnitude), the Fock
+  // matrices that are combined stay FP64
+  float* hE = reinterpret_cast<float*>(histE);
+  float* eS = hE + (size_t)slot * TE;
   double* fS = histF + (size_t)slot * TF;
   // one pass over the upper triangle: store E = W - W^T and F, and accumulate
   // <E, E_j> for every stored error vector j (the new one is E itself)
@@ -508,11 +512,12 @@ __device__ const double* diis_step(int N, const double* F, const double* P, doub
     for (int c = i + lane; c < N; c += 32) {
       fS[rf + c] = F[i * N + c];
       if (c == i) continue;
-      const double e = W[i * N + c] - W[c * N + i];
-      eS[re + c] = e;
+      const float ef = (float)(W[i * N + c] - W[c * N + i]);
+      eS[re + c] = ef;
+      const double e = (double)ef;
 #pragma unroll
       for (int j = 0; j < kDiisMax; ++j)
-        if (j < nhist) d[j] += e * (j == slot ? e : histE[(size_t)j * TE + re + c]);
+        if (j < nhist) d[j] += e * (j == slot ? e : (double)hE[(size_t)j * TE + re + c]);
     }
   }
   // CTA reduction of the nhist dot products through the (idle) GEMM scratch
