@@ -614,7 +614,7 @@ int Batch::run(const ScfParams& sp_in, bool gradient, std::string& err) {
     dev_.large = large ? 1 : 0;
     dev_.large_scratch = large ? large_scratch_ : nullptr;
     launch_pair_values(dev_, stream_);
-    launches_ += dev_.npairs > 0 ? 1 : 0;
+    launches_ += (dev_.npairs > 0 ? 1 : 0) + (dev_.nhh_total > 0 ? 1 : 0);
     cudaEventRecord(stage_ev_[1], stream_);
     launch_one_electron(dev_, stream_);
     launches_ += 1;

@@ -21,18 +21,12 @@ void upload_local_terms(const LocalTermTable& tab, cudaStream_t stream) {
   cudaMemcpyToSymbolAsync(c_local_terms, &tab, sizeof(LocalTermTable), 0, cudaMemcpyHostToDevice, stream);
 }
 
-__global__ void __launch_bounds__(128) k_pair_values(const PairDev* __restrict__ pairs, int npairs,
-                                                      const AtomDev* __restrict__ atoms,
-                                                      const ElemDev* __restrict__ elems,
-                                                      const DiatomicDev* __restrict__ diat, int method,
-                                                      double* __restrict__ ints, double* __restrict__ vcore,
-                                                      double* __restrict__ ovl, double* __restrict__ erep) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= npairs) return;
-  const PairDev pr = pairs[p];
-  const AtomDev a = atoms[pr.a], b = atoms[pr.b];
-  const ElemDev& A = elems[a.slot];
-  const ElemDev& B = elems[b.slot];
+// Values of pair p (see the file comment).
+__device__ __forceinline__ void pair_values_one(int p, const PairDev& pr, const AtomDev& a, const AtomDev& b,
+                                                const ElemDev& A, const ElemDev& B,
+                                                const DiatomicDev* __restrict__ diat, int method,
+                                                double* __restrict__ ints, double* __restrict__ vcore,
+                                                double* __restrict__ ovl, double* __restrict__ erep) {
   const double X = b.x - a.x, Y = b.y - a.y, Z = b.z - a.z;
   const int dA = A.nao == 1 ? 1 : 10, dB = B.nao == 1 ? 1 : 10;
 
@@ -59,6 +53,42 @@ __global__ void __launch_bounds__(128) k_pair_values(const PairDev* __restrict__
   double E, dE;
   core_repulsion(method, A, B, diat[a.slot * kMaxElementSlots + b.slot], sqrt(X * X + Y * Y + Z * Z), E, dE);
   erep[p] = E;
+}
+
+// Pairs with at least one s-only atom, one thread each.  s/p-s/p pairs cost
+// two orders of magnitude more and sit in the same rows of the pair table
+// (heavy atoms first): they go to k_pair_values_heavy, so that no warp waits
+// on one of them while its other lanes idle.
+__global__ void __launch_bounds__(128) k_pair_values(const PairDev* __restrict__ pairs, int npairs,
+                                                      const AtomDev* __restrict__ atoms,
+                                                      const ElemDev* __restrict__ elems,
+                                                      const DiatomicDev* __restrict__ diat, int method,
+                                                      double* __restrict__ ints, double* __restrict__ vcore,
+                                                      double* __restrict__ ovl, double* __restrict__ erep) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npairs) return;
+  const PairDev pr = pairs[p];
+  const AtomDev a = atoms[pr.a], b = atoms[pr.b];
+  const ElemDev& A = elems[a.slot];
+  const ElemDev& B = elems[b.slot];
+  if (A.nao == 4 && B.nao == 4) return;
+  pair_values_one(p, pr, a, b, A, B, diat, method, ints, vcore, ovl, erep);
+}
+
+// The s/p-s/p pairs (the heavy-pair list), one thread each.
+__global__ void __launch_bounds__(128) k_pair_values_heavy(const int* __restrict__ hh, int nhh,
+                                                            const PairDev* __restrict__ pairs,
+                                                            const AtomDev* __restrict__ atoms,
+                                                            const ElemDev* __restrict__ elems,
+                                                            const DiatomicDev* __restrict__ diat, int method,
+                                                            double* __restrict__ ints, double* __restrict__ vcore,
+                                                            double* __restrict__ ovl, double* __restrict__ erep) {
+  const int h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= nhh) return;
+  const int p = hh[h];
+  const PairDev pr = pairs[p];
+  const AtomDev a = atoms[pr.a], b = atoms[pr.b];
+  pair_values_one(p, pr, a, b, elems[a.slot], elems[b.slot], diat, method, ints, vcore, ovl, erep);
 }
 
 // Pair gradient, reverse mode (see nddo_grad.cuh), for pairs with at least
@@ -414,6 +444,10 @@ void launch_pair_values(const DeviceBatch& b, cudaStream_t s) {
   int th = 128;
   k_pair_values<<<(b.npairs + th - 1) / th, th, 0, s>>>(b.pairs, b.npairs, b.atoms, b.elems, b.diat, b.method,
                                                          b.ints, b.vcore, b.ovl, b.erep);
+  if (b.nhh_total > 0)
+    k_pair_values_heavy<<<(b.nhh_total + th - 1) / th, th, 0, s>>>(b.hh_pairs, b.nhh_total, b.pairs, b.atoms,
+                                                                   b.elems, b.diat, b.method, b.ints, b.vcore,
+                                                                   b.ovl, b.erep);
 }
 
 void launch_gradient(const DeviceBatch& b, cudaStream_t s) {
