@@ -50,6 +50,7 @@ extern "C" {
 #define SG_ERR_DEVICE 11
 #define SG_ERR_TIMEOUT 12
 #define SG_PENDING 13 /* sg_server_poll: the request is still in flight */
+#define SG_ERR_PARAMETERS 14 /* a parameter file is missing or malformed */
 
 /* required-property mask */
 #define SG_PROP_ENERGY 1u
@@ -76,7 +77,16 @@ int32_t sg_get_n_atoms(const sg_calculator* h, int32_t* n_atoms);
  * "spin_mode", "self_consistence_criterion", "density_rmsd_criterion",
  * "max_scf_iterations", "scf_mixer", "method_parameters", and one of this
  * engine: "scf_path" = "auto" | "batched" | "large" | "large_mixed" (see
- * sg_batch_set_scf_path). */
+ * sg_batch_set_scf_path).
+ * "method_parameters" (empty = the embedded default) is read at sg_calculate,
+ * as the reference's method wrappers read it at initialize()
+ * (Implementations/Nddo/Pm6/Wrapper/PM6MethodWrapper.cpp:62-75,
+ * Implementations/Dftb/Utils/DFTBCommon.cpp:112-120): for MNDO / AM1 / PM6 the
+ * path of a parameters.json file in the layout of Nddo/Parameters.cpp:76-93;
+ * for DFTB2 / DFTB3 an embedded set name (mio-1-1, 3ob-3-1, 3ob-2-1) or a
+ * directory of Slater-Koster files X-Y.skf with optional hubbard.dat and
+ * spin.dat (Dftb/ParameterSet.cpp:69-133).  A missing or malformed file makes
+ * sg_calculate return SG_ERR_PARAMETERS. */
 int32_t sg_set_setting_int(sg_calculator* h, const char* key, int64_t value);
 int32_t sg_set_setting_double(sg_calculator* h, const char* key, double value);
 int32_t sg_set_setting_string(sg_calculator* h, const char* key, const char* value);
@@ -106,9 +116,32 @@ int32_t sg_calculate_excitations(sg_calculator* h, int32_t nroots, int32_t tripl
 int32_t sg_get_density(const sg_calculator* h, double* P);
 int32_t sg_set_density(sg_calculator* h, const double* P);
 
+/* ---- parameter queries (host only, no device use) ---- */
+/* Runtime (atomic-unit) parameters of element Z under a method spec as for
+ * sg_batch_create, as the engine uploads them.
+ * NDDO, SG_NDDO_ELEMENT_VALUES doubles: nao, core charge, U_ss, U_pp, beta_s,
+ *   beta_p, alpha, D_sp1, D_pp2, rho_ss0, rho_sp1, rho_pp0, rho_pp2, pcore,
+ *   g_ss, g_sp, g_pp, g_p2, h_sp, h_pp, STO-6G s exponents[6], s coefficients[6],
+ *   p exponents[6], p coefficients[6], Gaussian term count, a[4], b[4], c[4]
+ *   (RawParameterProcessor.cpp:67-188 of Implementations/Nddo/Utils/ParameterUtils).
+ * DFTB, SG_DFTB_ELEMENT_VALUES doubles: nao, occupation, e_s, e_p, Hubbard U,
+ *   Hubbard derivative, spin constant W, has W (Dftb/Utils/SKAtom.cpp:16-70).
+ * Returns SG_ERR_PARAMETERS for an unreadable parameter source and
+ * SG_ERR_UNSUPPORTED_ELEMENT when it has no s/p record for Z. */
+#define SG_NDDO_ELEMENT_VALUES 57
+#define SG_DFTB_ELEMENT_VALUES 8
+int32_t sg_element_parameters(const char* method, int32_t Z, double* out, int32_t n_out, char* errmsg,
+                              int32_t errcap);
+/* PM6 diatomic core-repulsion pair (alpha_AB in 1/bohr, or 1/bohr^2 for X-H
+ * with X in C, N, O; x_AB) under a method spec. */
+int32_t sg_diatomic_parameters(const char* method, int32_t Z1, int32_t Z2, double* alpha_x, char* errmsg,
+                               int32_t errcap);
+
 /* ---- batches: many independent molecules per device launch sequence ---- */
 /* Molecule i has n_atoms[i] atoms; atomic_numbers / xyz_bohr are the
- * concatenation over molecules; charges may be NULL (all neutral). */
+ * concatenation over molecules; charges may be NULL (all neutral).  method is
+ * "METHOD" or "METHOD:parameters" with parameters as for "method_parameters"
+ * (e.g. "DFTB3:3ob-2-1", "PM6:/data/pm6.json"). */
 int32_t sg_batch_create(const char* method, int32_t n_molecules, const int32_t* n_atoms,
                         const int32_t* atomic_numbers, const double* xyz_bohr, const int32_t* charges,
                         sg_batch** out);

@@ -200,7 +200,18 @@ static double klopman_var2(double D, double shift) {
   return guess;
 }
 
+// Parameter records that replace a method's published set (a parameter file
+// read by the test), per method; empty = the published set.
+std::vector<NddoRawAtomic> g_override_atomic[3];
+std::vector<NddoRawDiatomic> g_override_diatomic[3];
+bool g_override[3] = {false, false, false};
+
 const NddoRawAtomic* find_raw(Method m, int Z) {
+  if (g_override[(int)m]) {
+    for (const auto& r : g_override_atomic[(int)m])
+      if (r.Z == Z) return &r;
+    return nullptr;
+  }
   const NddoRawAtomic* tab = m == kPM6 ? kPM6Atomic : (m == kAM1 ? kAM1Atomic : kMNDOAtomic);
   size_t n = m == kPM6 ? sizeof(kPM6Atomic) / sizeof(kPM6Atomic[0])
                        : (m == kAM1 ? sizeof(kAM1Atomic) / sizeof(kAM1Atomic[0]) : sizeof(kMNDOAtomic) / sizeof(kMNDOAtomic[0]));
@@ -512,8 +523,10 @@ struct PairParams { double alphaAB = 0, xAB = 0; bool found = false; };
 
 static PairParams pm6_pair(const Element& A, const Element& B) {
   PairParams pp;
-  for (int i = 0; i < kPM6NumDiatomic; ++i) {
-    const NddoRawDiatomic& d = kPM6Diatomic[i];
+  const bool own = g_override[(int)kPM6];
+  const int count = own ? (int)g_override_diatomic[(int)kPM6].size() : kPM6NumDiatomic;
+  for (int i = 0; i < count; ++i) {
+    const NddoRawDiatomic& d = own ? g_override_diatomic[(int)kPM6][i] : kPM6Diatomic[i];
     if ((d.z1 == A.Z && d.z2 == B.Z) || (d.z1 == B.Z && d.z2 == A.Z)) {
       bool xh = (A.Z == 1 && (B.Z == 8 || B.Z == 7 || B.Z == 6)) || (B.Z == 1 && (A.Z == 8 || A.Z == 7 || A.Z == 6));
       pp.alphaAB = xh ? d.exponent * kAngstromPerBohr * kAngstromPerBohr : d.exponent * kAngstromPerBohr;
@@ -1001,6 +1014,19 @@ using namespace oracle;
 extern "C" {
 
 const char* oracle_last_error() { return g_err.c_str(); }
+
+// Replace the published records of a method by caller-given ones (n_atomic < 0:
+// back to the published set).  The records carry the STO-6G expansions.
+int oracle_set_parameters(const char* method, const NddoRawAtomic* atomic, int n_atomic,
+                          const NddoRawDiatomic* diatomic, int n_diatomic) {
+  Method m;
+  if (!parse_method(method, m)) return 1;
+  const int k = (int)m;
+  g_override[k] = n_atomic >= 0;
+  g_override_atomic[k].assign(atomic, atomic + (n_atomic > 0 ? n_atomic : 0));
+  g_override_diatomic[k].assign(diatomic, diatomic + (n_diatomic > 0 ? n_diatomic : 0));
+  return 0;
+}
 
 double oracle_ev_per_hartree() { return kEvPerHartree; }
 double oracle_bohr_per_angstrom() { return kBohrPerAngstrom; }

@@ -16,7 +16,8 @@ import os
 
 import numpy as np
 
-__all__ = ["Calculator", "Batch", "Results", "get_calculator", "batch_calculate", "library_path", "SparrowError"]
+__all__ = ["Calculator", "Batch", "Results", "get_calculator", "batch_calculate", "library_path", "SparrowError",
+           "element_parameters", "diatomic_parameters"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libsparrow_b200.so")
@@ -27,6 +28,9 @@ SG_PROP_GRADIENTS = 2
 SG_ERR_NOT_CONVERGED = 6
 SG_ERR_TIMEOUT = 12
 SG_PENDING = 13
+SG_ERR_PARAMETERS = 14
+SG_NDDO_ELEMENT_VALUES = 57
+SG_DFTB_ELEMENT_VALUES = 8
 SG_STATIC_MAX_ATOMS = 64
 SG_STATIC_MAX_AOS = 256
 
@@ -111,6 +115,10 @@ def lib():
         "sg_server_poll": (ctypes.c_int32, [_VP, ctypes.c_int64, _D, _D, _I32, _I32, _D]),
         "sg_server_drain": (ctypes.c_int32, [_VP]),
         "sg_server_stats": (ctypes.c_int32, [_VP] + [ctypes.POINTER(ctypes.c_int64)] * 4),
+        "sg_element_parameters": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _D, ctypes.c_int32,
+                                                   ctypes.c_char_p, ctypes.c_int32]),
+        "sg_diatomic_parameters": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, _D,
+                                                    ctypes.c_char_p, ctypes.c_int32]),
         "sg_calculate_static": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _D, ctypes.c_int32,
                                                  ctypes.c_double, ctypes.c_double, ctypes.c_int32, ctypes.c_uint32,
                                                  _VP, _D, _D, _I32, _I32, ctypes.c_char_p, ctypes.c_int32]),
@@ -439,6 +447,45 @@ class Batch:
     @property
     def stream(self):
         return lib().sg_batch_stream(self._h)
+
+
+def element_parameters(method, Z):
+    """Runtime (atomic-unit) parameters of element Z as the engine uploads them.
+
+    method is "METHOD" or "METHOD:parameters" (a parameters.json path for
+    MNDO/AM1/PM6; an embedded set name or a Slater-Koster directory for DFTB).
+    NDDO: dict with nao, core, Uss, Upp, betaS, betaP, alpha, D (D_sp1, D_pp2),
+    rho (ss0, sp1, pp0, pp2), pcore, gss, gsp, gpp, gp2, hsp, hpp, s_exp,
+    s_coef, p_exp, p_coef, gauss (list of (a, b, c)).  DFTB: dict with nao,
+    occupation, es, ep, U, hubbard_derivative, W, has_W.  Host only.
+    """
+    L = lib()
+    out = np.zeros(max(SG_NDDO_ELEMENT_VALUES, SG_DFTB_ELEMENT_VALUES))
+    err = ctypes.create_string_buffer(512)
+    rc = L.sg_element_parameters(method.encode(), int(Z), _dptr(out), out.size, err, 512)
+    if rc != 0:
+        raise SparrowError(rc, err.value.decode())
+    if method.split(":")[0].upper().startswith("DFTB"):
+        keys = ["nao", "occupation", "es", "ep", "U", "hubbard_derivative", "W", "has_W"]
+        return dict(zip(keys, out[:SG_DFTB_ELEMENT_VALUES].tolist()))
+    v = out
+    ng = int(v[44])
+    return {"nao": int(v[0]), "core": v[1], "Uss": v[2], "Upp": v[3], "betaS": v[4], "betaP": v[5], "alpha": v[6],
+            "D": v[7:9].copy(), "rho": v[9:13].copy(), "pcore": v[13], "gss": v[14], "gsp": v[15], "gpp": v[16],
+            "gp2": v[17], "hsp": v[18], "hpp": v[19], "s_exp": v[20:26].copy(), "s_coef": v[26:32].copy(),
+            "p_exp": v[32:38].copy(), "p_coef": v[38:44].copy(),
+            "gauss": [(v[45 + k], v[49 + k], v[53 + k]) for k in range(ng)], "vector": v[:20].copy()}
+
+
+def diatomic_parameters(method, Z1, Z2):
+    """PM6 diatomic core-repulsion pair (alpha_AB in atomic units, x_AB).  Host only."""
+    L = lib()
+    out = np.zeros(2)
+    err = ctypes.create_string_buffer(512)
+    rc = L.sg_diatomic_parameters(method.encode(), int(Z1), int(Z2), _dptr(out), err, 512)
+    if rc != 0:
+        raise SparrowError(rc, err.value.decode())
+    return float(out[0]), float(out[1])
 
 
 def batch_calculate(method, molecules, charges=None, scc=1e-7, rmsd=1e-5, max_iter=100, gradients=False):

@@ -12,13 +12,16 @@
 #include <vector>
 
 #include "../../include/sparrow_b200.h"
+#include "dftb_params.h"
 #include "engine.h"
 #include "params.h"
 #include "server.h"
 
 namespace sgb {
 
-// "METHOD" or, for DFTB, "METHOD:parameter-set" (e.g. "DFTB3:3ob-2-1").
+// "METHOD" or "METHOD:parameters": for DFTB an embedded set name or a
+// directory of Slater-Koster files (e.g. "DFTB3:3ob-2-1"), for NDDO the path
+// of a parameters.json file (e.g. "PM6:/data/pm6-refit.json").
 bool parse_method_spec(const char* spec, Method& m, std::string& set) {
   std::string s(spec);
   const size_t c = s.find(':');
@@ -27,8 +30,7 @@ bool parse_method_spec(const char* spec, Method& m, std::string& set) {
     set = s.substr(c + 1);
     s = s.substr(0, c);
   }
-  if (!parse_method(s, m)) return false;
-  return set.empty() || is_dftb(m);
+  return parse_method(s, m);
 }
 
 struct Settings {
@@ -79,13 +81,9 @@ class Calculator {
       error = "empty molecular structure";
       return kErrEmptyStructure;
     }
-    if (is_dftb(method_)) {
-      // DFTB: the setting names an embedded Slater-Koster set (empty = the method's default)
-      batch_->set_dftb_parameters(settings_.parameters);
-    } else if (!settings_.parameters.empty()) {
-      error = "method_parameters: only the embedded NDDO parameters are available";
-      return kErrInvalidArgument;
-    }
+    // DFTB: an embedded set name or a Slater-Koster directory; NDDO: a
+    // parameters.json path; empty = the method's embedded default
+    batch_->set_parameters(settings_.parameters);
     if (settings_.multiplicity != 1 || settings_.spin_mode == "unrestricted") {
       error = "only restricted closed-shell singlets are supported";
       return kErrInvalidArgument;
@@ -169,7 +167,7 @@ class Calculator {
     }
     int n = 0;
     for (int z : Z_) {
-      int k = engine_n_aos(method_, z);
+      int k = aos_of(z);
       if (!k) {
         error = "unsupported element";
         return kErrUnsupportedElement;
@@ -181,8 +179,16 @@ class Calculator {
   }
   int n_aos() const {
     int n = 0;
-    for (int z : Z_) n += engine_n_aos(method_, z);
+    for (int z : Z_) n += aos_of(z);
     return n;
+  }
+  // AOs of element Z under the current parameter source
+  int aos_of(int z) const {
+    const std::string& src = settings_.parameters;
+    if (is_dftb(method_)) return dftb_n_aos(src.empty() ? dftb_default_set(method_) : src.c_str(), z);
+    std::string unused;
+    auto set = src.empty() ? nullptr : nddo_parameter_set(method_, src, unused);
+    return engine_n_aos(method_, z, set.get());
   }
   std::unique_ptr<Calculator> clone() const {
     std::unique_ptr<Calculator> c(new Calculator(method_));
@@ -459,7 +465,7 @@ int32_t sg_batch_create(const char* method, int32_t n_mol, const int32_t* n_atom
   }
   std::unique_ptr<sg_batch> b(new sg_batch);
   b->impl.reset(new Batch(m));
-  b->impl->set_dftb_parameters(set);
+  b->impl->set_parameters(set);
   int rc = b->impl->setup(mols, err);
   if (rc) {
     g_create_error = err;
@@ -744,3 +750,101 @@ int32_t sg_server_stats(sg_server* s, int64_t* submitted, int64_t* completed, in
 }
 
 }  // extern "C"
+
+namespace {
+
+void copy_message(const std::string& s, char* errmsg, int32_t errcap) {
+  if (errmsg && errcap > 0) {
+    std::strncpy(errmsg, s.c_str(), (size_t)errcap - 1);
+    errmsg[errcap - 1] = 0;
+  }
+}
+
+}  // namespace
+
+int32_t sg_element_parameters(const char* method, int32_t Z, double* out, int32_t n_out, char* errmsg,
+                              int32_t errcap) {
+  using namespace sgb;
+  Method m;
+  std::string src;
+  if (!method || !parse_method_spec(method, m, src)) {
+    copy_message("unknown method", errmsg, errcap);
+    return SG_ERR_UNKNOWN_METHOD;
+  }
+  if (!out || n_out < (is_dftb(m) ? SG_DFTB_ELEMENT_VALUES : SG_NDDO_ELEMENT_VALUES)) {
+    copy_message("output buffer too small", errmsg, errcap);
+    return SG_ERR_INVALID_ARGUMENT;
+  }
+  std::string err;
+  if (is_dftb(m)) {
+    const std::string set = src.empty() ? dftb_default_set(m) : src;
+    if (!dftb_parameter_set(set, err)) {
+      copy_message(err, errmsg, errcap);
+      return SG_ERR_PARAMETERS;
+    }
+    DftbPrepared p;
+    if (!dftb_prepare(set, m == kDFTB3 ? 3 : 2, {Z}, p, err)) {
+      copy_message(err, errmsg, errcap);
+      return SG_ERR_UNSUPPORTED_ELEMENT;
+    }
+    const DftbElemDev& e = p.elems[0];
+    const double v[SG_DFTB_ELEMENT_VALUES] = {(double)e.nao, e.occ, e.es, e.ep, e.U, e.hd, e.w, (double)e.has_w};
+    std::memcpy(out, v, sizeof(v));
+    return SG_OK;
+  }
+  std::shared_ptr<const NddoParamSet> set;
+  if (!src.empty()) {
+    set = nddo_parameter_set(m, src, err);
+    if (!set) {
+      copy_message(err, errmsg, errcap);
+      return SG_ERR_PARAMETERS;
+    }
+  }
+  ElemDev e;
+  if (!make_elem(m, Z, e, err, set.get())) {
+    copy_message(err, errmsg, errcap);
+    return SG_ERR_UNSUPPORTED_ELEMENT;
+  }
+  double* o = out;
+  const double head[20] = {(double)e.nao, e.core, e.Uss, e.Upp,  e.betaS,  e.betaP,  e.alpha,
+                           e.D[1],        e.D[3], e.rho[0], e.rho[1], e.rho[2], e.rho[3], e.pcore,
+                           e.gss,         e.gsp,  e.gpp,  e.gp2,    e.hsp,    e.hpp};
+  std::memcpy(o, head, sizeof(head));
+  o += 20;
+  for (const double* a : {e.s_exp, e.s_coef, e.p_exp, e.p_coef}) {
+    std::memcpy(o, a, 6 * sizeof(double));
+    o += 6;
+  }
+  *o++ = e.n_gauss;
+  for (const double* a : {e.ga, e.gb, e.gc}) {
+    std::memcpy(o, a, 4 * sizeof(double));
+    o += 4;
+  }
+  return SG_OK;
+}
+
+int32_t sg_diatomic_parameters(const char* method, int32_t Z1, int32_t Z2, double* alpha_x, char* errmsg,
+                               int32_t errcap) {
+  using namespace sgb;
+  Method m;
+  std::string src;
+  if (!method || !parse_method_spec(method, m, src) || is_dftb(m)) {
+    copy_message("unknown NDDO method", errmsg, errcap);
+    return SG_ERR_UNKNOWN_METHOD;
+  }
+  if (!alpha_x) return SG_ERR_INVALID_ARGUMENT;
+  std::string err;
+  std::shared_ptr<const NddoParamSet> set;
+  if (!src.empty() && !(set = nddo_parameter_set(m, src, err))) {
+    copy_message(err, errmsg, errcap);
+    return SG_ERR_PARAMETERS;
+  }
+  const DiatomicDev d = make_diatomic(m, Z1, Z2, set.get());
+  if (!d.present) {
+    copy_message("no diatomic parameters for the pair", errmsg, errcap);
+    return SG_ERR_UNSUPPORTED_ELEMENT;
+  }
+  alpha_x[0] = d.alpha;
+  alpha_x[1] = d.x;
+  return SG_OK;
+}

@@ -1,8 +1,11 @@
 #include "dftb_params.h"
 
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include "dftb_raw.h"
+#include "param_files.h"
 
 namespace sgb {
 
@@ -10,51 +13,59 @@ namespace sgb {
 
 namespace {
 
-const DftbSetRaw* find_set(const char* name) {
-  for (const auto& s : kDftbSetRaw)
-    if (!std::strcmp(s.name, name)) return &s;
-  return nullptr;
+int n_aos_of(int Z) { return Z <= 2 ? 1 : (Z <= 10 ? 4 : 9); }
+
+std::shared_ptr<const DftbSetData> set_or_null(const char* name) {
+  std::string unused;
+  return dftb_parameter_set(name, unused);
 }
 
-const DftbElemRaw* find_elem(const DftbSetRaw* s, int Z) {
-  for (int i = 0; i < s->n_elem; ++i)
-    if (kDftbElemRaw[s->elem0 + i].Z == Z) return &kDftbElemRaw[s->elem0 + i];
-  return nullptr;
-}
+}  // namespace
 
-const DftbPairRaw* find_pair(const DftbSetRaw* s, int z1, int z2) {
-  for (int i = 0; i < s->n_pair; ++i) {
-    const DftbPairRaw& p = kDftbPairRaw[s->pair0 + i];
-    if (p.z1 == z1 && p.z2 == z2) return &p;
+std::shared_ptr<const DftbSetData> dftb_embedded_set(const std::string& name) {
+  static std::mutex mu;
+  static std::map<std::string, std::shared_ptr<const DftbSetData>> sets;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = sets.find(name);
+  if (it != sets.end()) return it->second;
+  for (const auto& s : kDftbSetRaw) {
+    if (name != s.name) continue;
+    auto d = std::make_shared<DftbSetData>();
+    d->name = s.name;
+    d->elems.assign(kDftbElemRaw + s.elem0, kDftbElemRaw + s.elem0 + s.n_elem);
+    for (int i = 0; i < s.n_pair; ++i) {
+      DftbPairRaw p = kDftbPairRaw[s.pair0 + i];
+      const int row0 = (int)(d->table.size() / 8), spline0 = (int)d->splines.size();
+      for (int r = 0; r < p.rows; ++r) d->table.insert(d->table.end(), kDftbTable[p.row0 + r], kDftbTable[p.row0 + r] + 8);
+      d->splines.insert(d->splines.end(), kDftbSplineRaw + p.spline0, kDftbSplineRaw + p.spline0 + p.n_spline);
+      p.row0 = row0;
+      p.spline0 = spline0;
+      d->pairs.push_back(p);
+    }
+    sets[name] = d;
+    return d;
   }
   return nullptr;
 }
 
-int n_aos_of(int Z) { return Z <= 2 ? 1 : (Z <= 10 ? 4 : 9); }
-
-}  // namespace
-
 const char* dftb_default_set(Method m) { return m == kDFTB3 ? "3ob-3-1" : "mio-1-1"; }
 
 int dftb_n_aos(const char* set, int Z) {
-  const DftbSetRaw* s = find_set(set);
-  if (!s || !find_elem(s, Z)) return 0;
+  auto s = set_or_null(set);
+  if (!s || !s->find_elem(Z)) return 0;
   const int n = n_aos_of(Z);
   return n <= 4 ? n : 0;
 }
 
 double dftb_core_charge(const char* set, int Z) {
-  const DftbSetRaw* s = find_set(set);
-  const DftbElemRaw* e = s ? find_elem(s, Z) : nullptr;
+  auto s = set_or_null(set);
+  const DftbElemRaw* e = s ? s->find_elem(Z) : nullptr;
   return e ? e->fs + e->fp + e->fd : -1.0;
 }
 
 bool dftb_prepare(const std::string& set, int order, const std::vector<int>& Zs, DftbPrepared& out, std::string& err) {
-  const DftbSetRaw* s = find_set(set.c_str());
-  if (!s) {
-    err = "unknown DFTB parameter set '" + set + "' (embedded: mio-1-1, 3ob-3-1, 3ob-2-1)";
-    return false;
-  }
+  auto s = dftb_parameter_set(set, err);
+  if (!s) return false;
   const int n = (int)Zs.size();
   if (n > kMaxElementSlots) {
     err = "more than 16 distinct elements in one batch";
@@ -62,7 +73,7 @@ bool dftb_prepare(const std::string& set, int order, const std::vector<int>& Zs,
   }
   out.elems.assign(n, DftbElemDev());
   for (int i = 0; i < n; ++i) {
-    const DftbElemRaw* e = find_elem(s, Zs[i]);
+    const DftbElemRaw* e = s->find_elem(Zs[i]);
     if (!e) {
       err = "no " + set + " parameters for element Z=" + std::to_string(Zs[i]);
       return false;
@@ -93,8 +104,8 @@ bool dftb_prepare(const std::string& set, int order, const std::vector<int>& Zs,
   out.splines.clear();
   for (int i = 0; i < n; ++i)
     for (int j = 0; j < n; ++j) {
-      const DftbPairRaw* r = find_pair(s, Zs[i], Zs[j]);
-      const DftbPairRaw* v = find_pair(s, Zs[j], Zs[i]);
+      const DftbPairRaw* r = s->find_pair(Zs[i], Zs[j]);
+      const DftbPairRaw* v = s->find_pair(Zs[j], Zs[i]);
       if (!r || !v) {
         err = "no " + set + " Slater-Koster file for the element pair Z=" + std::to_string(Zs[i]) + ", Z=" +
               std::to_string(Zs[j]);
@@ -111,8 +122,8 @@ bool dftb_prepare(const std::string& set, int order, const std::vector<int>& Zs,
       // s-p overlap and Hamiltonian integrals with opposite sign
       p.table_off = (long long)out.table.size();
       for (int row = 0; row < r->rows; ++row) {
-        const double* a = kDftbTable[r->row0 + row];
-        const double* b = row < v->rows ? kDftbTable[v->row0 + row] : nullptr;
+        const double* a = s->table.data() + (size_t)(r->row0 + row) * 8;
+        const double* b = row < v->rows ? s->table.data() + (size_t)(v->row0 + row) * 8 : nullptr;
         for (int c = 0; c < 8; ++c) out.table.push_back(a[c]);
         out.table.push_back(b ? -b[2] : 0.0);
         out.table.push_back(b ? -b[3] : 0.0);
@@ -162,7 +173,7 @@ bool dftb_prepare(const std::string& set, int order, const std::vector<int>& Zs,
       p.c5 = r->c5;
       p.spline_off = (int)out.splines.size();
       for (int k = 0; k < r->n_spline; ++k) {
-        const DftbSplineRaw& q = kDftbSplineRaw[r->spline0 + k];
+        const DftbSplineRaw& q = s->splines[r->spline0 + k];
         out.splines.push_back(DftbSplineDev{q.start, q.end, q.c0, q.c1, q.c2, q.c3});
       }
     }

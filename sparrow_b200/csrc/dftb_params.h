@@ -9,6 +9,7 @@
 // parameter, table completion from the reverse pair, tail coefficients and
 // gamma terms per ordered pair.
 #pragma once
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -16,6 +17,11 @@
 #include "engine_types.h"
 
 namespace sgb {
+
+struct DftbSetData;
+
+// An embedded parameter set (mio-1-1, 3ob-3-1, 3ob-2-1) by name, or nullptr.
+std::shared_ptr<const DftbSetData> dftb_embedded_set(const std::string& name);
 
 // Default parameter set of a DFTB method (DFTB2: mio-1-1, DFTB3: 3ob-3-1).
 const char* dftb_default_set(Method m);
@@ -31,7 +37,8 @@ struct DftbPrepared {
   std::vector<DftbSplineDev> splines;   // repulsion splines
 };
 
-// Records for the elements Zs (slot i = Zs[i]).  order 3 requires Hubbard
+// Records for the elements Zs (slot i = Zs[i]).  set is an embedded set name
+// or a directory of Slater-Koster files.  order 3 requires Hubbard
 // derivatives.  Returns false and sets err when a parameter is missing.
 bool dftb_prepare(const std::string& set, int order, const std::vector<int>& Zs, DftbPrepared& out, std::string& err);
 

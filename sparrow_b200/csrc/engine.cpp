@@ -159,6 +159,13 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
     err = "empty batch";
     return kErrEmptyStructure;
   }
+  nddo_set_.reset();
+  if (!is_dftb(method_) && !param_source_.empty()) {
+    nddo_set_ = nddo_parameter_set(method_, param_source_, err);
+    if (!nddo_set_) return kErrParameters;
+  }
+  if (is_dftb(method_) && !dftb_parameter_set(param_source_.empty() ? dftb_default_set(method_) : param_source_, err))
+    return kErrParameters;
   // element slots
   int slot_of[128];
   for (int& v : slot_of) v = -1;
@@ -181,7 +188,7 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
       std::string why;
       if (is_dftb(method_)) {
         // DFTB: orbitals and core charge from the parameter set (records built below)
-        const char* set = dftb_set_.empty() ? dftb_default_set(method_) : dftb_set_.c_str();
+        const char* set = param_source_.empty() ? dftb_default_set(method_) : param_source_.c_str();
         e = ElemDev();
         e.Z = z;
         e.nao = dftb_n_aos(set, z);
@@ -190,7 +197,7 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
           err = std::string("no ") + set + " s/p parameters for element Z=" + std::to_string(z);
           return kErrUnsupportedElement;
         }
-      } else if (!make_elem(method_, z, e, why)) {
+      } else if (!make_elem(method_, z, e, why, nddo_set_.get())) {
         err = why;
         return kErrUnsupportedElement;
       }
@@ -207,12 +214,12 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
   if (is_dftb(method_)) {
     std::vector<int> zs;
     for (const auto& e : elems_) zs.push_back(e.Z);
-    const std::string set = dftb_set_.empty() ? dftb_default_set(method_) : dftb_set_;
+    const std::string set = param_source_.empty() ? dftb_default_set(method_) : param_source_;
     if (!dftb_prepare(set, method_ == kDFTB3 ? 3 : 2, zs, dftb, err)) return kErrUnsupportedElement;
   }
   for (size_t i = 0; i < elems_.size() && !is_dftb(method_); ++i)
     for (size_t j = 0; j < elems_.size(); ++j) {
-      DiatomicDev d = make_diatomic(method_, elems_[i].Z, elems_[j].Z);
+      DiatomicDev d = make_diatomic(method_, elems_[i].Z, elems_[j].Z, nddo_set_.get());
       if (method_ == kPM6 && !d.present) {
         err = "no PM6 diatomic parameters for the element pair Z=" + std::to_string(elems_[i].Z) + ", Z=" +
               std::to_string(elems_[j].Z);

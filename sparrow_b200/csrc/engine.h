@@ -2,11 +2,13 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <memory>
 #include <string>
 #include <vector>
 
 #include "engine_types.h"
 #include "kernels.h"
+#include "param_files.h"
 
 namespace sgb {
 
@@ -39,6 +41,7 @@ enum Status : int {
   kErrDevice = 11,
   kErrTimeout = 12,
   kPending = 13,
+  kErrParameters = 14,  // a parameter file is missing or malformed
 };
 
 // A batch resident on the device: descriptors, integrals, matrices, results.
@@ -80,10 +83,12 @@ class Batch {
 
   cudaStream_t stream() const { return stream_; }
   Method method() const { return method_; }
-  // DFTB parameter set (embedded sets: mio-1-1, 3ob-3-1, 3ob-2-1); empty =
-  // the method's default.  Takes effect at the next setup().
-  void set_dftb_parameters(const std::string& set) { dftb_set_ = set; }
-  const std::string& dftb_parameters() const { return dftb_set_; }
+  // Parameter source, the reference's "method_parameters" setting; empty =
+  // the method's embedded default.  DFTB: an embedded set name (mio-1-1,
+  // 3ob-3-1, 3ob-2-1) or a directory of Slater-Koster files; NDDO: the path of
+  // a parameters.json file.  Takes effect at the next setup().
+  void set_parameters(const std::string& source) { param_source_ = source; }
+  const std::string& parameters() const { return param_source_; }
   // SCF path: 0 automatic (one NDDO molecule of more than 1024 AOs runs the
   // large-molecule path, anything else the batched kernel), 1 batched
   // kernel, 2 large-molecule path in FP64, 3 large-molecule path with
@@ -123,7 +128,8 @@ class Batch {
   std::vector<DiatomicDev> diat_;
   std::vector<int> ao_atom_, order_;
   long long npairs_ = 0, nhh_ = 0;  // pair and heavy-pair tables are built on the device
-  std::string dftb_set_;
+  std::string param_source_;
+  std::shared_ptr<const NddoParamSet> nddo_set_;  // resolved NDDO source (nullptr: embedded)
   int scf_path_ = 0;
   void* td_scratch_ = nullptr;
   size_t td_scratch_bytes_ = 0;

@@ -1,5 +1,6 @@
 #include "params.h"
 #include "dftb_params.h"
+#include "param_files.h"
 
 #include <algorithm>
 #include <cctype>
@@ -23,7 +24,8 @@ const NddoRawAtomic* lookup(const NddoRawAtomic (&tab)[N], int Z) {
   return nullptr;
 }
 
-const NddoRawAtomic* raw_for(Method m, int Z) {
+const NddoRawAtomic* raw_for(Method m, int Z, const NddoParamSet* set) {
+  if (set) return set->find(Z);
   switch (m) {
     case kPM6: return lookup(kPM6Atomic, Z);
     case kAM1: return lookup(kAM1Atomic, Z);
@@ -123,21 +125,37 @@ const char* method_name(Method m) {
   }
 }
 
-int engine_n_aos(Method m, int Z) {
+const NddoRawAtomic* nddo_embedded_atomic(Method m, size_t& count) {
+  switch (m) {
+    case kPM6: count = sizeof(kPM6Atomic) / sizeof(kPM6Atomic[0]); return kPM6Atomic;
+    case kAM1: count = sizeof(kAM1Atomic) / sizeof(kAM1Atomic[0]); return kAM1Atomic;
+    default: count = sizeof(kMNDOAtomic) / sizeof(kMNDOAtomic[0]); return kMNDOAtomic;
+  }
+}
+
+const NddoRawDiatomic* nddo_embedded_diatomic(Method m, size_t& count) {
+  count = m == kPM6 ? (size_t)kPM6NumDiatomic : 0;
+  return kPM6Diatomic;
+}
+
+int nddo_shell_n(int Z, int l) { return l == 0 ? shell_n_s(Z) : shell_n_p(Z); }
+
+int engine_n_aos(Method m, int Z, const NddoParamSet* set) {
   if (is_dftb(m)) return dftb_n_aos(dftb_default_set(m), Z);
-  const NddoRawAtomic* r = raw_for(m, Z);
+  const NddoRawAtomic* r = raw_for(m, Z, set);
   if (!r) return 0;
   int n = Z == 1 ? 1 : (m == kPM6 ? pm6_n_aos(Z) : 4);
   return (n == 1 || n == 4) ? n : 0;
 }
 
-bool make_elem(Method m, int Z, ElemDev& e, std::string& err) {
-  const NddoRawAtomic* r = raw_for(m, Z);
+bool make_elem(Method m, int Z, ElemDev& e, std::string& err, const NddoParamSet* set) {
+  const NddoRawAtomic* r = raw_for(m, Z, set);
   if (!r) {
-    err = std::string("no ") + method_name(m) + " parameters for element Z=" + std::to_string(Z);
+    err = std::string("no ") + method_name(m) + " parameters for element Z=" + std::to_string(Z) +
+          (set && !set->source.empty() ? " in '" + set->source + "'" : std::string());
     return false;
   }
-  int nao = engine_n_aos(m, Z);
+  int nao = engine_n_aos(m, Z, set);
   if (nao == 0) {
     err = std::string(method_name(m)) + " gives element Z=" + std::to_string(Z) +
           " a d shell; this engine covers s/p elements only";
@@ -189,11 +207,14 @@ bool make_elem(Method m, int Z, ElemDev& e, std::string& err) {
   return true;
 }
 
-DiatomicDev make_diatomic(Method m, int Z1, int Z2) {
+DiatomicDev make_diatomic(Method m, int Z1, int Z2, const NddoParamSet* set) {
   DiatomicDev d;
   if (m != kPM6) return d;
-  for (int i = 0; i < kPM6NumDiatomic; ++i) {
-    const NddoRawDiatomic& r = kPM6Diatomic[i];
+  size_t count = 0;
+  const NddoRawDiatomic* tab = set ? set->diatomic.data() : nddo_embedded_diatomic(m, count);
+  if (set) count = set->diatomic.size();
+  for (size_t i = 0; i < count; ++i) {
+    const NddoRawDiatomic& r = tab[i];
     if ((r.z1 == Z1 && r.z2 == Z2) || (r.z1 == Z2 && r.z2 == Z1)) {
       bool xh = (Z1 == 1 && (Z2 == 6 || Z2 == 7 || Z2 == 8)) || (Z2 == 1 && (Z1 == 6 || Z1 == 7 || Z1 == 8));
       d.alpha = xh ? r.exponent * kAngstromPerBohr * kAngstromPerBohr : r.exponent * kAngstromPerBohr;

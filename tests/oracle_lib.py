@@ -125,6 +125,22 @@ def energy_at_density(method, Z, xyz_bohr, P):
     return e.value, g.reshape(-1, 3)
 
 
+def set_parameters(method, records=None):
+    """Make the oracle use caller-given raw records for a method (the output of
+    tests.param_sets.oracle_records), or its published set again (None)."""
+    L = lib()
+    L.oracle_set_parameters.argtypes = [ctypes.c_char_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                        ctypes.c_int]
+    if records is None:
+        rc = L.oracle_set_parameters(method.encode(), None, -1, None, 0)
+    else:
+        arr, n, darr, nd = records
+        rc = L.oracle_set_parameters(method.encode(), ctypes.cast(arr, ctypes.c_void_p), n,
+                                     ctypes.cast(darr, ctypes.c_void_p), nd)
+    if rc != 0:
+        raise RuntimeError("oracle_set_parameters failed")
+
+
 def element_params(method, Z):
     out = np.zeros(20)
     rc = lib().oracle_element_params(method.encode(), Z, out.ctypes.data_as(_D))

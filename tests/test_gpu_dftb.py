@@ -85,10 +85,10 @@ def test_dftb_errors_and_warm_start():
     assert ei.value.code == 3
     Z, x = geometry.water_cluster(3, seed=5)
     c.set_structure(Z, geometry.to_bohr(x))
-    c.settings["method_parameters"] = "no-such-set"
+    c.settings["method_parameters"] = "no-such-set"  # neither an embedded set nor a directory
     with pytest.raises(sparrow_b200.SparrowError) as ei:
         c.calculate()
-    assert ei.value.code == 3
+    assert ei.value.code == sparrow_b200.SG_ERR_PARAMETERS
     c.settings["method_parameters"] = ""
     r1 = c.calculate()
     P = c.density()
