@@ -770,12 +770,16 @@ static void build_one_electron(Molecule& M) {
   }
 }
 
-// Full two-electron matrix G(P) (TwoElectronMatrix.cpp:82-166, written for the
-// full symmetric matrix: G_mn = sum_ls P_ls [(mn|ls) - 1/2 (ml|ns)]).
-static void build_G(const Molecule& M, const std::vector<double>& P, std::vector<double>& G) {
+// Full two-electron matrix (TwoElectronMatrix.cpp:82-166, written for the
+// full symmetric matrix): G_mn = sum_ls [Pc_ls (mn|ls) - xf Px_ls (ml|ns)].
+// Restricted: Pc = Px = P, xf = 1/2.  Unrestricted, spin s
+// (TwoElectronMatrix.cpp:98-103, 142-161): Pc = P_alpha + P_beta, Px = P_s, xf = 1.
+static void build_G(const Molecule& M, const std::vector<double>& Pc, const std::vector<double>& Px, double xf,
+                    std::vector<double>& G) {
   int N = M.nao;
   G.assign((size_t)N * N, 0);
-  auto Pm = [&](int i, int j) { return P[(size_t)i * N + j]; };
+  auto Pm = [&](int i, int j) { return Pc[(size_t)i * N + j]; };
+  auto Xm = [&](int i, int j) { return Px[(size_t)i * N + j]; };
   auto Gm = [&](int i, int j) -> double& { return G[(size_t)i * N + j]; };
   for (int a = 0; a < M.nat; ++a) {
     const Element& e = M.el[a];
@@ -785,7 +789,7 @@ static void build_G(const Molecule& M, const std::vector<double>& P, std::vector
         double s = 0;
         for (int k = 0; k < e.nao; ++k)
           for (int l = 0; l < e.nao; ++l)
-            s += Pm(o + k, o + l) * (one_center(e, i, j, k, l) - 0.5 * one_center(e, i, k, j, l));
+            s += Pm(o + k, o + l) * one_center(e, i, j, k, l) - xf * Xm(o + k, o + l) * one_center(e, i, k, j, l);
         Gm(o + i, o + j) += s;
       }
   }
@@ -811,11 +815,15 @@ static void build_G(const Molecule& M, const std::vector<double>& P, std::vector
       for (int la = 0; la < B.nao; ++la) {
         double s = 0;
         for (int nu = 0; nu < A.nao; ++nu)
-          for (int si = 0; si < B.nao; ++si) s += Pm(oa + nu, ob + si) * I(mu, nu, la, si);
-        Gm(oa + mu, ob + la) -= 0.5 * s;
-        Gm(ob + la, oa + mu) -= 0.5 * s;
+          for (int si = 0; si < B.nao; ++si) s += Xm(oa + nu, ob + si) * I(mu, nu, la, si);
+        Gm(oa + mu, ob + la) -= xf * s;
+        Gm(ob + la, oa + mu) -= xf * s;
       }
   }
+}
+
+static void build_G(const Molecule& M, const std::vector<double>& P, std::vector<double>& G) {
+  build_G(M, P, P, 0.5, G);
 }
 
 static double electronic_energy(const std::vector<double>& P, const std::vector<double>& H, const std::vector<double>& G) {
@@ -929,13 +937,156 @@ static bool run_scf(Molecule& M, const ScfSettings& st, ScfResult& r, const std:
   return true;
 }
 
+// Unrestricted SCF (spin densities P_a, P_b; the reference's unrestricted
+// branches of FockMatrix.cpp:108-150 and NDDOElectronicEnergyCalculator.cpp:68-90):
+//   F_s = H + G_s,  G_s = sum [(P_a + P_b)(mn|ls) - P_s (ml|ns)]
+//   E_el = 1/2 sum [(P_a + P_b) H + P_a F_a + P_b F_b]
+// Pulay DIIS on the stacked commutators (F_a P_a - P_a F_a, F_b P_b - P_b F_b)
+// with one set of coefficients for both Fock matrices; start P_a = P_b = P0 / 2
+// from the restricted guess; P_s = sum over the n_s lowest orbitals of F_s;
+// convergence on |dE| and the larger of the two rms density changes.
+struct ScfResultU {
+  double Eel = 0, Erep = 0, Etot = 0;
+  int iterations = 0;
+  bool converged = false;
+  std::vector<double> Pa, Pb, epsa, epsb;
+};
+
+static double uhf_energy(const Molecule& M, const std::vector<double>& Pa, const std::vector<double>& Pb,
+                         const std::vector<double>& Ga, const std::vector<double>& Gb) {
+  double e = 0;
+  for (size_t k = 0; k < Pa.size(); ++k) e += (Pa[k] + Pb[k]) * M.H[k] + 0.5 * (Pa[k] * Ga[k] + Pb[k] * Gb[k]);
+  return e;
+}
+
+static bool run_uhf(Molecule& M, int na, int nb, const ScfSettings& st, ScfResultU& r) {
+  const int N = M.nao;
+  const size_t NN = (size_t)N * N;
+  std::vector<double> P0(NN, 0);
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j) P0[(size_t)i * N + j] = M.S[(size_t)i * N + j] * M.nel / (2.0 * N);
+  for (int a = 0; a < M.nat; ++a)
+    for (int k = 0; k < M.el[a].nao; ++k)
+      P0[(size_t)(M.ao0[a] + k) * N + M.ao0[a] + k] = M.el[a].core / M.el[a].nao;
+  std::vector<double> Pa(NN), Pb(NN);
+  for (size_t k = 0; k < NN; ++k) Pa[k] = Pb[k] = 0.5 * P0[k];
+  std::vector<double> PT(NN), Ga, Gb, Fa(NN), Fb(NN), w, C;
+  std::vector<std::vector<double>> hFa, hFb, hE;
+  auto commutator = [&](const std::vector<double>& F, const std::vector<double>& P, double* out) {
+    std::vector<double> FP(NN, 0);
+    for (int i = 0; i < N; ++i)
+      for (int k = 0; k < N; ++k) {
+        const double f = F[(size_t)i * N + k];
+        if (f == 0) continue;
+        for (int j = 0; j < N; ++j) FP[(size_t)i * N + j] += f * P[(size_t)k * N + j];
+      }
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j) out[(size_t)i * N + j] = FP[(size_t)i * N + j] - FP[(size_t)j * N + i];
+  };
+  auto occupied_density = [&](const std::vector<double>& Fx, int n, std::vector<double>& Pn) -> bool {
+    if (!eigh(N, Fx, w, C)) return false;
+    Pn.assign(NN, 0);
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j) {
+        double t = 0;
+        for (int o = 0; o < n; ++o) t += C[(size_t)i * N + o] * C[(size_t)j * N + o];
+        Pn[(size_t)i * N + j] = t;
+      }
+    return true;
+  };
+  double Eold = 0;
+  bool have_old = false;
+  int it;
+  for (it = 1; it <= st.max_iter; ++it) {
+    for (size_t k = 0; k < NN; ++k) PT[k] = Pa[k] + Pb[k];
+    build_G(M, PT, Pa, 1.0, Ga);
+    build_G(M, PT, Pb, 1.0, Gb);
+    for (size_t k = 0; k < NN; ++k) {
+      Fa[k] = M.H[k] + Ga[k];
+      Fb[k] = M.H[k] + Gb[k];
+    }
+    const double E = uhf_energy(M, Pa, Pb, Ga, Gb);
+    std::vector<double> err(2 * NN);
+    commutator(Fa, Pa, err.data());
+    commutator(Fb, Pb, err.data() + NN);
+    hFa.push_back(Fa);
+    hFb.push_back(Fb);
+    hE.push_back(err);
+    if ((int)hE.size() > st.diis_size) {
+      hFa.erase(hFa.begin());
+      hFb.erase(hFb.begin());
+      hE.erase(hE.begin());
+    }
+    std::vector<double> Fxa = Fa, Fxb = Fb;
+    const int m = (int)hE.size();
+    if (m >= 2) {
+      std::vector<double> B((size_t)(m + 1) * (m + 1), 0), rhs(m + 1, 0);
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j <= i; ++j) {
+          double t = 0;
+          for (size_t k = 0; k < err.size(); ++k) t += hE[i][k] * hE[j][k];
+          B[i * (m + 1) + j] = B[j * (m + 1) + i] = t;
+        }
+      for (int i = 0; i < m; ++i) B[i * (m + 1) + m] = B[m * (m + 1) + i] = -1;
+      rhs[m] = -1;
+      if (solve_dense(m + 1, B, rhs)) {
+        std::fill(Fxa.begin(), Fxa.end(), 0.0);
+        std::fill(Fxb.begin(), Fxb.end(), 0.0);
+        for (int i = 0; i < m; ++i)
+          for (size_t k = 0; k < NN; ++k) {
+            Fxa[k] += rhs[i] * hFa[i][k];
+            Fxb[k] += rhs[i] * hFb[i][k];
+          }
+      }
+    }
+    std::vector<double> Pna, Pnb;
+    if (!occupied_density(Fxa, na, Pna) || !occupied_density(Fxb, nb, Pnb)) return false;
+    double da = 0, db = 0;
+    for (size_t k = 0; k < NN; ++k) {
+      da += (Pna[k] - Pa[k]) * (Pna[k] - Pa[k]);
+      db += (Pnb[k] - Pb[k]) * (Pnb[k] - Pb[k]);
+    }
+    const double rms = std::sqrt(std::max(da, db) / (double)NN);
+    Pa.swap(Pna);
+    Pb.swap(Pnb);
+    const bool dE_ok = have_old && std::fabs(E - Eold) < st.scc;
+    Eold = E;
+    have_old = true;
+    if (dE_ok && rms < st.rmsd) {
+      r.converged = true;
+      break;
+    }
+  }
+  r.iterations = std::min(it, st.max_iter);
+  for (size_t k = 0; k < NN; ++k) PT[k] = Pa[k] + Pb[k];
+  build_G(M, PT, Pa, 1.0, Ga);
+  build_G(M, PT, Pb, 1.0, Gb);
+  r.Eel = uhf_energy(M, Pa, Pb, Ga, Gb);
+  r.Erep = M.Erep;
+  r.Etot = r.Eel + r.Erep;
+  for (size_t k = 0; k < NN; ++k) {
+    Fa[k] = M.H[k] + Ga[k];
+    Fb[k] = M.H[k] + Gb[k];
+  }
+  eigh(N, Fa, r.epsa, C);
+  eigh(N, Fb, r.epsb, C);
+  r.Pa = Pa;
+  r.Pb = Pb;
+  return true;
+}
+
 // ---------------------------------------------------------------------------
 // Nuclear gradient (OneElectronMatrix.cpp:136-229, TwoElectronMatrix.cpp:168-241)
 // ---------------------------------------------------------------------------
-static void gradient(const Molecule& M, const std::vector<double>& P, std::vector<double>& grad) {
+// P is the total density; Pa, Pb the spin densities entering the exchange
+// products (restricted: both P/2).
+static void gradient(const Molecule& M, const std::vector<double>& P, const std::vector<double>& Pa,
+                     const std::vector<double>& Pb, std::vector<double>& grad) {
   int N = M.nao;
   grad.assign(3 * M.nat, 0);
   auto Pm = [&](int i, int j) { return P[(size_t)i * N + j]; };
+  auto Am = [&](int i, int j) { return Pa[(size_t)i * N + j]; };
+  auto Bm = [&](int i, int j) { return Pb[(size_t)i * N + j]; };
   for (int a = 0; a < M.nat; ++a)
     for (int b = a + 1; b < M.nat; ++b) {
       const Element &A = M.el[a], &B = M.el[b];
@@ -951,7 +1102,8 @@ static void gradient(const Molecule& M, const std::vector<double>& P, std::vecto
         for (int nu = 0; nu < A.nao; ++nu)
           for (int la = 0; la < B.nao; ++la)
             for (int si = 0; si < B.nao; ++si) {
-              double f = Pm(oa + mu, oa + nu) * Pm(ob + la, ob + si) - 0.5 * Pm(oa + mu, ob + la) * Pm(oa + nu, ob + si);
+              double f = Pm(oa + mu, oa + nu) * Pm(ob + la, ob + si) -
+                         (Am(oa + mu, ob + la) * Am(oa + nu, ob + si) + Bm(oa + mu, ob + la) * Bm(oa + nu, ob + si));
               const D3& I = G[pidx(mu, nu)][pidx(la, si)];
               for (int d = 0; d < 3; ++d) g[d] += f * I.g[d];
             }
@@ -993,6 +1145,12 @@ static void gradient(const Molecule& M, const std::vector<double>& P, std::vecto
         grad[3 * a + d] -= g[d];
       }
     }
+}
+
+static void gradient(const Molecule& M, const std::vector<double>& P, std::vector<double>& grad) {
+  std::vector<double> half(P.size());
+  for (size_t k = 0; k < P.size(); ++k) half[k] = 0.5 * P[k];
+  gradient(M, P, half, half, grad);
 }
 
 static bool parse_method(const char* s, Method& m) {
@@ -1136,6 +1294,49 @@ int oracle_scf(const char* method, int nat, const int* Z, const double* xyz_bohr
   if (want_gradient && grad) {
     std::vector<double> g;
     gradient(M, r.P, g);
+    std::memcpy(grad, g.data(), sizeof(double) * g.size());
+  }
+  return 0;
+}
+
+// Unrestricted single point with spin multiplicity mult (n_a - n_b = mult - 1).
+// info[8] = {E_el, E_rep, iterations, converged, nao, n_alpha, n_beta, nel};
+// eps_a / eps_b (N each) optional.
+int oracle_scf_uhf(const char* method, int nat, const int* Z, const double* xyz_bohr, int charge, int mult,
+                   double scc, double rmsd, int max_iter, int want_gradient, double* energy, double* grad,
+                   double* info, double* eps_a, double* eps_b) {
+  Method m;
+  if (!parse_method(method, m)) { g_err = "unknown method"; return 1; }
+  Molecule M;
+  int rc = setup(M, m, nat, Z, xyz_bohr, charge, g_err);
+  if (rc && rc != 3) return rc;
+  const int na2 = M.nel + mult - 1;
+  if (mult < 1 || na2 % 2 != 0 || M.nel - (mult - 1) < 0) {
+    g_err = "electron count and spin multiplicity do not match";
+    return 3;
+  }
+  const int na = na2 / 2, nb = M.nel - na;
+  if (na > M.nao) { g_err = "more alpha electrons than orbitals"; return 3; }
+  build_pairs(M);
+  build_one_electron(M);
+  ScfSettings st;
+  st.scc = scc;
+  st.rmsd = rmsd;
+  st.max_iter = max_iter;
+  ScfResultU r;
+  if (!run_uhf(M, na, nb, st, r)) { g_err = "eigensolver failed"; return 5; }
+  *energy = r.Etot;
+  if (info) {
+    double v[8] = {r.Eel, r.Erep, (double)r.iterations, r.converged ? 1.0 : 0.0, (double)M.nao, (double)na,
+                   (double)nb, (double)M.nel};
+    std::memcpy(info, v, sizeof(v));
+  }
+  if (eps_a) std::memcpy(eps_a, r.epsa.data(), sizeof(double) * r.epsa.size());
+  if (eps_b) std::memcpy(eps_b, r.epsb.data(), sizeof(double) * r.epsb.size());
+  if (want_gradient && grad) {
+    std::vector<double> PT(r.Pa.size()), g;
+    for (size_t k = 0; k < PT.size(); ++k) PT[k] = r.Pa[k] + r.Pb[k];
+    gradient(M, PT, r.Pa, r.Pb, g);
     std::memcpy(grad, g.data(), sizeof(double) * g.size());
   }
   return 0;

@@ -82,6 +82,29 @@ def scf(method, Z, xyz_bohr, charge=0, scc=1e-7, rmsd=1e-8, max_iter=1000, gradi
     return out
 
 
+def scf_uhf(method, Z, xyz_bohr, multiplicity, charge=0, scc=1e-9, rmsd=1e-9, max_iter=1000, gradient=True):
+    """Converged unrestricted SCF: dict(energy, gradient, e_el, e_rep, iterations, converged, nao, n_alpha,
+    n_beta, eps_alpha, eps_beta)."""
+    Z, x = _arr(Z, xyz_bohr)
+    e = ctypes.c_double()
+    g = np.zeros(x.size)
+    info = np.zeros(8)
+    n_max = 4 * len(Z)
+    ea, eb = np.zeros(n_max), np.zeros(n_max)
+    L = lib()
+    L.oracle_scf_uhf.argtypes = [ctypes.c_char_p, ctypes.c_int, _I, _D, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                 ctypes.c_double, ctypes.c_int, ctypes.c_int, _D, _D, _D, _D, _D]
+    rc = L.oracle_scf_uhf(method.encode(), len(Z), Z.ctypes.data_as(_I), x.ctypes.data_as(_D), int(charge),
+                          int(multiplicity), scc, rmsd, max_iter, 1 if gradient else 0, ctypes.byref(e),
+                          g.ctypes.data_as(_D), info.ctypes.data_as(_D), ea.ctypes.data_as(_D), eb.ctypes.data_as(_D))
+    if rc != 0:
+        raise RuntimeError("oracle_scf_uhf failed (%d): %s" % (rc, L.oracle_last_error().decode()))
+    n = int(info[4])
+    return dict(energy=e.value, gradient=g.reshape(-1, 3), e_el=info[0], e_rep=info[1], iterations=int(info[2]),
+                converged=bool(info[3]), nao=n, n_alpha=int(info[5]), n_beta=int(info[6]), eps_alpha=ea[:n],
+                eps_beta=eb[:n])
+
+
 def one_electron(method, Z, xyz_bohr, charge=0):
     Z, x = _arr(Z, xyz_bohr)
     n_max = 4 * len(Z)
