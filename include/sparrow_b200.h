@@ -113,6 +113,11 @@ int32_t sg_get_orbital_energies(const sg_calculator* h, double* eps);
  * triplets; dipoles may be NULL).  SG_ERR_NOT_CONVERGED when the Davidson
  * solver did not reach its residual tolerance (1e-8). */
 int32_t sg_calculate_excitations(sg_calculator* h, int32_t nroots, int32_t triplet, double* omega, double* dipoles);
+/* Unrestricted calculations ("spin_mode" = "unrestricted", or "any" with
+ * "spin_multiplicity" != 1, as NDDOMethodWrapper.cpp:68-92): the beta orbital
+ * energies (N values; sg_get_orbital_energies gives the alpha ones).
+ * SG_ERR_NO_RESULTS after a restricted calculation. */
+int32_t sg_get_beta_orbital_energies(const sg_calculator* h, double* eps);
 int32_t sg_get_density(const sg_calculator* h, double* P);
 int32_t sg_set_density(sg_calculator* h, const double* P);
 
@@ -145,6 +150,11 @@ int32_t sg_diatomic_parameters(const char* method, int32_t Z1, int32_t Z2, doubl
 int32_t sg_batch_create(const char* method, int32_t n_molecules, const int32_t* n_atoms,
                         const int32_t* atomic_numbers, const double* xyz_bohr, const int32_t* charges,
                         sg_batch** out);
+/* Unrestricted (UHF) batch: molecule i has spin multiplicity multiplicities[i]
+ * (NULL: all 1); MNDO / AM1 / PM6 on the batched path (at most 1024 AOs). */
+int32_t sg_batch_create_unrestricted(const char* method, int32_t n_molecules, const int32_t* n_atoms,
+                                     const int32_t* atomic_numbers, const double* xyz_bohr, const int32_t* charges,
+                                     const int32_t* multiplicities, sg_batch** out);
 void sg_batch_destroy(sg_batch* b);
 const char* sg_batch_last_error(const sg_batch* b);
 int32_t sg_batch_set_scf(sg_batch* b, double self_consistence_criterion, double density_rmsd_criterion,

@@ -83,6 +83,9 @@ def lib():
         "sg_batch_excitations": (ctypes.c_int32, [_VP, ctypes.c_int32, ctypes.c_int32, _D, _VP, _VP]),
         "sg_batch_excitation_cycles": (ctypes.c_int32, [_VP, _VP]),
         "sg_set_density": (ctypes.c_int32, [_VP, _D]),
+        "sg_get_beta_orbital_energies": (ctypes.c_int32, [_VP, _D]),
+        "sg_batch_create_unrestricted": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _I32, _D, _I32,
+                                                          _I32, ctypes.POINTER(_VP)]),
         "sg_batch_create": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _I32, _D, _I32,
                                              ctypes.POINTER(_VP)]),
         "sg_batch_destroy": (None, [_VP]),
@@ -291,8 +294,15 @@ class Calculator:
         return P.reshape(n, n)
 
     def orbital_energies(self):
+        """Orbital energies (the alpha ones after an unrestricted calculation)."""
         e = np.zeros(self._nao)
         self._check(lib().sg_get_orbital_energies(self._h, _dptr(e)))
+        return e
+
+    def beta_orbital_energies(self):
+        """Beta orbital energies of an unrestricted calculation."""
+        e = np.zeros(self._nao)
+        self._check(lib().sg_get_beta_orbital_energies(self._h, _dptr(e)))
         return e
 
     def set_density(self, P):
@@ -332,13 +342,28 @@ class Batch:
 
     SCF_PATHS = {"auto": 0, "batched": 1, "large": 2, "large_mixed": 3}
 
-    def __init__(self, method, molecules, charges=None, scc=1e-7, rmsd=1e-5, max_iter=100, scf_path="auto"):
+    def __init__(self, method, molecules, charges=None, scc=1e-7, rmsd=1e-5, max_iter=100, scf_path="auto",
+                 multiplicities=None, unrestricted=None):
+        """multiplicities / unrestricted: an unrestricted (UHF) batch when unrestricted is
+        True, or when it is None and some multiplicity differs from 1 (the reference's
+        spin_mode "any")."""
         L = lib()
         self.n_atoms, Z, X = _flatten(molecules)
         ch = None if charges is None else np.ascontiguousarray(charges, dtype=np.int32)
+        mult = None if multiplicities is None else np.ascontiguousarray(multiplicities, dtype=np.int32)
+        if unrestricted is None:
+            unrestricted = mult is not None and bool(np.any(mult != 1))
+        self.unrestricted = bool(unrestricted)
         h = _VP()
-        rc = L.sg_batch_create(method.encode(), len(molecules), _iptr(self.n_atoms), _iptr(Z), _dptr(X),
-                               _iptr(ch) if ch is not None else None, ctypes.byref(h))
+        if self.unrestricted:
+            rc = L.sg_batch_create_unrestricted(method.encode(), len(molecules), _iptr(self.n_atoms), _iptr(Z),
+                                                _dptr(X), _iptr(ch) if ch is not None else None,
+                                                _iptr(mult) if mult is not None else None, ctypes.byref(h))
+        elif mult is not None and np.any(mult != 1):
+            raise ValueError("a restricted batch needs multiplicity 1 for every molecule")
+        else:
+            rc = L.sg_batch_create(method.encode(), len(molecules), _iptr(self.n_atoms), _iptr(Z), _dptr(X),
+                                   _iptr(ch) if ch is not None else None, ctypes.byref(h))
         if rc != 0:
             raise SparrowError(rc, L.sg_batch_last_error(None).decode())
         self._h = h

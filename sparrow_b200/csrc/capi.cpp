@@ -84,10 +84,20 @@ class Calculator {
     // DFTB: an embedded set name or a Slater-Koster directory; NDDO: a
     // parameters.json path; empty = the method's embedded default
     batch_->set_parameters(settings_.parameters);
-    if (settings_.multiplicity != 1 || settings_.spin_mode == "unrestricted") {
-      error = "only restricted closed-shell singlets are supported";
+    // spin mode as the reference's NDDOMethodWrapper::applySettings
+    // (Implementations/Nddo/NDDOMethodWrapper.cpp:68-92): "any" is unrestricted
+    // for multiplicities other than 1
+    if (settings_.spin_mode == "restricted_open_shell") {
+      error = "restricted open-shell SCF is not supported (use unrestricted)";
       return kErrInvalidArgument;
     }
+    const bool uhf = settings_.spin_mode == "unrestricted" ||
+                     (settings_.spin_mode == "any" && settings_.multiplicity != 1);
+    if (!uhf && settings_.multiplicity != 1) {
+      error = "a restricted calculation needs spin multiplicity 1";
+      return kErrInvalidArgument;
+    }
+    batch_->set_unrestricted(uhf);
     ScfParams sp;
     sp.scc = settings_.scc;
     sp.rmsd = settings_.rmsd;
@@ -97,6 +107,7 @@ class Calculator {
     in[0].Z = Z_;
     in[0].xyz = xyz_;
     in[0].charge = settings_.charge;
+    in[0].multiplicity = settings_.multiplicity;
     int rc = batch_->setup(in, error);
     if (rc) return rc;
     const std::string& sp_name = settings_.scf_path;
@@ -118,6 +129,8 @@ class Calculator {
     have_gradient_ = grad;
     batch_->fetch_density(0, density_, error);
     batch_->fetch_orbital_energies(0, eps_, error);
+    eps_b_.clear();
+    if (uhf) batch_->fetch_orbital_energies(0, eps_b_, error, true);
     if (result_.status != kDevOk) {
       error = "device SCF failure code " + std::to_string(result_.status);
       return kErrDevice;
@@ -160,6 +173,7 @@ class Calculator {
   const MoleculeOutput& result() const { return result_; }
   const std::vector<double>& density() const { return density_; }
   const std::vector<double>& orbital_energies() const { return eps_; }
+  const std::vector<double>& beta_orbital_energies() const { return eps_b_; }
   int set_density(const double* P) {
     if (Z_.empty()) {
       error = "no structure set";
@@ -212,7 +226,7 @@ class Calculator {
   uint32_t required_ = SG_PROP_ENERGY;
   MoleculeOutput result_;
   bool have_result_ = false, have_gradient_ = false;
-  std::vector<double> density_, eps_, state_;
+  std::vector<double> density_, eps_, eps_b_, state_;
 };
 
 }  // namespace sgb
@@ -429,6 +443,15 @@ int32_t sg_get_orbital_energies(const sg_calculator* h, double* eps) {
   return SG_OK;
 }
 
+int32_t sg_get_beta_orbital_energies(const sg_calculator* h, double* eps) {
+  if (!h || !eps) return SG_ERR_INVALID_ARGUMENT;
+  if (!h->impl->have_result()) return SG_ERR_NO_RESULTS;
+  const auto& v = h->impl->beta_orbital_energies();
+  if (v.empty()) return SG_ERR_NO_RESULTS;  // restricted calculation
+  std::memcpy(eps, v.data(), sizeof(double) * v.size());
+  return SG_OK;
+}
+
 int32_t sg_calculate_excitations(sg_calculator* h, int32_t nroots, int32_t triplet, double* omega, double* dipoles) {
   if (!h || !omega) return SG_ERR_INVALID_ARGUMENT;
   return h->impl->excitations(nroots, triplet != 0, omega, dipoles);
@@ -447,8 +470,10 @@ int32_t sg_set_density(sg_calculator* h, const double* P) {
   return h->impl->set_density(P);
 }
 
-int32_t sg_batch_create(const char* method, int32_t n_mol, const int32_t* n_atoms, const int32_t* Z,
-                        const double* xyz, const int32_t* charges, sg_batch** out) {
+namespace {
+
+int32_t batch_create(const char* method, int32_t n_mol, const int32_t* n_atoms, const int32_t* Z, const double* xyz,
+                     const int32_t* charges, const int32_t* multiplicities, bool uhf, sg_batch** out) {
   if (!out) return SG_ERR_INVALID_ARGUMENT;
   *out = nullptr;
   Method m;
@@ -463,9 +488,12 @@ int32_t sg_batch_create(const char* method, int32_t n_mol, const int32_t* n_atom
     g_create_error = err;
     return SG_ERR_EMPTY_STRUCTURE;
   }
+  if (multiplicities)
+    for (int i = 0; i < n_mol; ++i) mols[i].multiplicity = multiplicities[i];
   std::unique_ptr<sg_batch> b(new sg_batch);
   b->impl.reset(new Batch(m));
   b->impl->set_parameters(set);
+  b->impl->set_unrestricted(uhf);
   int rc = b->impl->setup(mols, err);
   if (rc) {
     g_create_error = err;
@@ -473,6 +501,19 @@ int32_t sg_batch_create(const char* method, int32_t n_mol, const int32_t* n_atom
   }
   *out = b.release();
   return SG_OK;
+}
+
+}  // namespace
+
+int32_t sg_batch_create(const char* method, int32_t n_mol, const int32_t* n_atoms, const int32_t* Z,
+                        const double* xyz, const int32_t* charges, sg_batch** out) {
+  return batch_create(method, n_mol, n_atoms, Z, xyz, charges, nullptr, false, out);
+}
+
+int32_t sg_batch_create_unrestricted(const char* method, int32_t n_mol, const int32_t* n_atoms, const int32_t* Z,
+                                     const double* xyz, const int32_t* charges, const int32_t* multiplicities,
+                                     sg_batch** out) {
+  return batch_create(method, n_mol, n_atoms, Z, xyz, charges, multiplicities, true, out);
 }
 
 void sg_batch_destroy(sg_batch* b) { delete b; }

@@ -159,6 +159,10 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
     err = "empty batch";
     return kErrEmptyStructure;
   }
+  if (uhf_ && is_dftb(method_)) {
+    err = "unrestricted (spin-polarised) DFTB is not supported; the unrestricted SCF covers MNDO, AM1 and PM6";
+    return kErrInvalidArgument;
+  }
   nddo_set_.reset();
   if (!is_dftb(method_) && !param_source_.empty()) {
     nddo_set_ = nddo_parameter_set(method_, param_source_, err);
@@ -268,12 +272,26 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
     }
     md.nao = nao;
     md.nel = (int)std::lround(ncore) - mol.charge;
-    if (md.nel < 0 || (md.nel & 1)) {
-      err = "molecule " + std::to_string(mi) + " has " + std::to_string(md.nel) +
-            " electrons: the restricted closed-shell SCF needs an even, non-negative count";
-      return kErrOddElectrons;
+    if (uhf_) {
+      // n_alpha - n_beta = multiplicity - 1
+      const int na2 = md.nel + mol.multiplicity - 1;
+      if (md.nel < 0 || mol.multiplicity < 1 || (na2 & 1) || md.nel - (mol.multiplicity - 1) < 0 || na2 / 2 > nao) {
+        err = "molecule " + std::to_string(mi) + ": " + std::to_string(md.nel) +
+              " electrons do not fit spin multiplicity " + std::to_string(mol.multiplicity);
+        return kErrOddElectrons;
+      }
+      md.nocc = na2 / 2;
+      md.nocc_b = md.nel - md.nocc;
+    } else {
+      if (md.nel < 0 || (md.nel & 1) || mol.multiplicity != 1) {
+        err = "molecule " + std::to_string(mi) + " has " + std::to_string(md.nel) + " electrons and multiplicity " +
+              std::to_string(mol.multiplicity) + ": the restricted closed-shell SCF needs an even, non-negative "
+              "count and a singlet (use the unrestricted SCF)";
+        return kErrOddElectrons;
+      }
+      md.nocc = md.nel / 2;
+      md.nocc_b = md.nocc;
     }
-    md.nocc = md.nel / 2;
     if (nao > 1024 && (in.size() > 1 || is_dftb(method_))) {
       err = "molecule " + std::to_string(mi) + " has more than 1024 AOs: the batched SCF limit (a single NDDO "
             "molecule of that size runs the large-molecule path)";
@@ -373,6 +391,11 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
   const size_t o_Gam = take(method_ == kDFTB3 ? gam_bytes : sizeof(double));
   const size_t o_qat = take(sizeof(double) * (dftb_batch ? atoms_.size() : 1));
   const size_t o_shift = take(sizeof(double) * 4 * (dftb_batch ? atoms_.size() : 1));
+  // unrestricted: spin densities, beta Fock matrix, orbitals, energies and DIIS ring
+  const size_t mat_uhf = uhf_ ? mat_bytes : sizeof(double);
+  const size_t o_Pa = take(mat_uhf), o_Pb = take(mat_uhf), o_Fb = take(mat_uhf), o_Cb = take(mat_uhf);
+  const size_t o_epsb = take(uhf_ ? sizeof(double) * (size_t)ao_base : sizeof(double));
+  const size_t o_diisb = take(uhf_ ? sizeof(double) * (size_t)diis_off : sizeof(double));
   int rc = ensure_arena(off, err);
   if (rc) return rc;
   rc = ensure_terms(stream_, err);
@@ -412,6 +435,15 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
   d.Gam = reinterpret_cast<double*>(base + o_Gam);
   d.qat = reinterpret_cast<double*>(base + o_qat);
   d.ashift = reinterpret_cast<double*>(base + o_shift);
+  d.uhf = uhf_ ? 1 : 0;
+  if (uhf_) {
+    d.Pa = reinterpret_cast<double*>(base + o_Pa);
+    d.Pb = reinterpret_cast<double*>(base + o_Pb);
+    d.Fb = reinterpret_cast<double*>(base + o_Fb);
+    d.Cb = reinterpret_cast<double*>(base + o_Cb);
+    d.epsb = reinterpret_cast<double*>(base + o_epsb);
+    d.diisb = reinterpret_cast<double*>(base + o_diisb);
+  }
   if (dftb_batch) {
     d.dftb_order = method_ == kDFTB3 ? 3 : 2;
     d.gam_total = gam_off;
@@ -595,6 +627,10 @@ int Batch::run(const ScfParams& sp_in, bool gradient, std::string& err) {
       err = "the large-molecule SCF path takes one NDDO molecule";
       return kErrInvalidArgument;
     }
+    if (large && uhf_) {
+      err = "the unrestricted SCF runs on the batched path (at most 1024 AOs)";
+      return kErrInvalidArgument;
+    }
     if (!large && mols_[0].nao > 1024) {
       err = "more than 1024 AOs needs the large-molecule SCF path";
       return kErrInvalidArgument;
@@ -631,7 +667,8 @@ int Batch::run(const ScfParams& sp_in, bool gradient, std::string& err) {
       const int rc = run_large_scf(dev_, mols_[0], sp, scf_path_ == 3 ? 1 : 0, stream_, &launches_, err);
       if (rc != kOk) return rc;
     } else {
-      launch_scf(dev_, sp, dev_.scf_grid, stream_);
+      if (uhf_) launch_uhf_scf(dev_, sp, dev_.scf_grid, stream_);
+      else launch_scf(dev_, sp, dev_.scf_grid, stream_);
       launches_ += 1;
     }
     cudaEventRecord(stage_ev_[3], stream_);
@@ -676,6 +713,7 @@ int Batch::fetch(std::vector<MoleculeOutput>& out, bool gradient, std::string& e
     o.status = r[i].status;
     o.nao = mols_[i].nao;
     o.nocc = mols_[i].nocc;
+    o.nocc_b = mols_[i].nocc_b;
     o.nel = mols_[i].nel;
     if (gradient)
       o.gradient.assign(g.begin() + 3 * mols_[i].atom0, g.begin() + 3 * (mols_[i].atom0 + mols_[i].nat));
@@ -836,15 +874,19 @@ int Batch::fetch_density(int mol, std::vector<double>& P, std::string& err) {
   return kOk;
 }
 
-int Batch::fetch_orbital_energies(int mol, std::vector<double>& eps, std::string& err) {
+int Batch::fetch_orbital_energies(int mol, std::vector<double>& eps, std::string& err, bool beta) {
   if (mol < 0 || mol >= (int)mols_.size()) {
     err = "molecule index out of range";
     return kErrInvalidArgument;
   }
+  if (beta && !dev_.uhf) {
+    err = "beta orbital energies exist for unrestricted calculations only";
+    return kErrNoResults;
+  }
   const MolDev& m = mols_[mol];
   eps.resize(m.nao);
-  cudaError_t e = cudaMemcpyAsync(eps.data(), dev_.eps + m.ao_base, sizeof(double) * m.nao, cudaMemcpyDeviceToHost,
-                                  stream_);
+  const double* src = (beta ? dev_.epsb : dev_.eps) + m.ao_base;
+  cudaError_t e = cudaMemcpyAsync(eps.data(), src, sizeof(double) * m.nao, cudaMemcpyDeviceToHost, stream_);
   if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
   if (e != cudaSuccess) {
     err = cuda_message(e);

@@ -16,12 +16,14 @@ struct MoleculeInput {
   std::vector<int> Z;
   std::vector<double> xyz;  // bohr, 3 per atom
   int charge = 0;
+  int multiplicity = 1;     // 2S + 1 (unrestricted batches)
 };
 
 struct MoleculeOutput {
   double energy = 0, e_el = 0, e_rep = 0;
   int iterations = 0, converged = 0, status = 0;
   int nao = 0, nocc = 0, nel = 0;
+  int nocc_b = 0;  // unrestricted: beta electrons (nocc: alpha electrons)
   std::vector<double> gradient;  // 3 per atom (Hartree/bohr)
 };
 
@@ -67,7 +69,8 @@ class Batch {
   int fetch(std::vector<MoleculeOutput>& out, bool gradient, std::string& err);
   int fetch_density(int mol, std::vector<double>& P, std::string& err);
   int fetch_raw_results(std::vector<MolResult>& r, std::string& err);
-  int fetch_orbital_energies(int mol, std::vector<double>& eps, std::string& err);
+  // alpha orbital energies (restricted: the orbital energies); beta = true: the beta ones
+  int fetch_orbital_energies(int mol, std::vector<double>& eps, std::string& err, bool beta = false);
   // Linear-response TD-DFTB (DFTB2 / DFTB3 batches, after run()): the nroots
   // (<= 16) lowest singlet (or triplet) excitations of every molecule.
   // Asynchronous on stream(); overwrites the orbital scratch (the gradient of
@@ -88,6 +91,11 @@ class Batch {
   // 3ob-3-1, 3ob-2-1) or a directory of Slater-Koster files; NDDO: the path of
   // a parameters.json file.  Takes effect at the next setup().
   void set_parameters(const std::string& source) { param_source_ = source; }
+  // Unrestricted (UHF) SCF for every molecule of the batch, each with its
+  // MoleculeInput::multiplicity (NDDO, batched SCF path).  Takes effect at
+  // the next setup().
+  void set_unrestricted(bool u) { uhf_ = u; }
+  bool unrestricted() const { return uhf_; }
   const std::string& parameters() const { return param_source_; }
   // SCF path: 0 automatic (one NDDO molecule of more than 1024 AOs runs the
   // large-molecule path, anything else the batched kernel), 1 batched
@@ -129,6 +137,7 @@ class Batch {
   std::vector<int> ao_atom_, order_;
   long long npairs_ = 0, nhh_ = 0;  // pair and heavy-pair tables are built on the device
   std::string param_source_;
+  bool uhf_ = false;
   std::shared_ptr<const NddoParamSet> nddo_set_;  // resolved NDDO source (nullptr: embedded)
   int scf_path_ = 0;
   void* td_scratch_ = nullptr;

@@ -71,6 +71,8 @@ struct MolDev {
   int ao_base;    // first AO (global index) in the ao_atom map
   int hh0;        // first entry of this molecule in the list of s/p-s/p pairs
   int nhh;        // number of pairs where both atoms carry an s/p shell
+  int nocc_b;     // unrestricted: beta electrons (nocc holds the alpha count)
+  int pad_;
   long long mat_off;   // N*N matrices (H, P, F, C, scratch) at this offset
   long long diis_off;  // DIIS history
   long long int_off;   // first integral of the molecule

@@ -51,6 +51,15 @@ struct DeviceBatch {
   double* gpair = nullptr;          // [npairs * 3]
   double* grad = nullptr;           // [natoms * 3]
   MolResult* res = nullptr;         // [nmol]
+  // unrestricted (UHF) batches: P holds P_alpha + P_beta, F the alpha Fock
+  // matrix, C / eps the alpha orbitals; the beta ones and both spin densities here
+  int uhf = 0;
+  double* Pa = nullptr;             // [mat_total] alpha density
+  double* Pb = nullptr;             // [mat_total] beta density
+  double* Fb = nullptr;             // [mat_total] beta Fock matrix
+  double* Cb = nullptr;             // [mat_total] beta orbitals (orbital-major)
+  double* epsb = nullptr;           // [nao_total] beta orbital energies
+  double* diisb = nullptr;          // [diis_total] beta DIIS ring
   int use_guess = 1;                // 0: P already holds a start density
   int large = 0;                    // 1: one molecule over the whole GPU (large-molecule path)
   void* large_scratch = nullptr;    // [large_scf_scratch_bytes(nao)] when large
@@ -77,6 +86,8 @@ void launch_build_pairs(const DeviceBatch& b, int max_nat, int* flag, cudaStream
 void launch_pair_values(const DeviceBatch& b, cudaStream_t s);
 void launch_one_electron(const DeviceBatch& b, cudaStream_t s);
 void launch_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s);
+// Unrestricted batches (DeviceBatch::uhf): the same launch shape as launch_scf.
+void launch_uhf_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s);
 void launch_gradient(const DeviceBatch& b, cudaStream_t s);
 void launch_gather_gradient(const DeviceBatch& b, cudaStream_t s);
 // Fock matrix F = H + G(P) of the batch's single (large) molecule over the

@@ -100,6 +100,8 @@ __global__ void __launch_bounds__(128) k_pair_gradient_light(const PairDev* __re
                                                              const DiatomicDev* __restrict__ diat,
                                                              const MolDev* __restrict__ mols, int method,
                                                              const double* __restrict__ Pall,
+                                                             const double* __restrict__ Paall,
+                                                             const double* __restrict__ Pball,
                                                              double* __restrict__ gpair) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npairs) return;
@@ -121,6 +123,15 @@ __global__ void __launch_bounds__(128) k_pair_gradient_light(const PairDev* __re
     for (int j = 0; j < nB; ++j) PB[i][j] = P[(size_t)(b.ao0 + i) * N + b.ao0 + j];
   for (int i = 0; i < nA; ++i)
     for (int j = 0; j < nB; ++j) PAB[i][j] = P[(size_t)(a.ao0 + i) * N + b.ao0 + j];
+  // unrestricted: spin density of the off-diagonal block
+  const bool uhf = Paall != nullptr;
+  double SAB[4][4] = {};
+  if (uhf)
+    for (int i = 0; i < nA; ++i)
+      for (int j = 0; j < nB; ++j) {
+        const size_t ij = m.mat_off + (size_t)(a.ao0 + i) * N + b.ao0 + j;
+        SAB[i][j] = Paall[ij] - Pball[ij];
+      }
   double g[3] = {0, 0, 0};
   double adjA[4][4] = {}, adjB[4][4] = {};
   double dR = 0;
@@ -134,13 +145,14 @@ __global__ void __launch_bounds__(128) k_pair_gradient_light(const PairDev* __re
   if (!rotate) {
     double L, dL;
     local_ss(c_local_terms, R, A, B, false, 0.0, L, dL);
-    dR += density_factor(PA, PB, PAB, 0, 0) * dL;
+    dR += (uhf ? density_factor_uhf(PA, PB, PAB, SAB, 0, 0) : density_factor(PA, PB, PAB, 0, 0)) * dL;
   } else {
     double L[10], dL[10];
     if (nB == 1) local_column(c_local_terms, R, A, B, false, 0.0, L, dL);
     else local_row(c_local_terms, R, A, B, L, dL);
     for (int g2 = 0; g2 < 10; ++g2) {
-      const double Fg = nB == 1 ? density_factor(PA, PB, PAB, g2, 0) : density_factor(PA, PB, PAB, 0, g2);
+      const int fp = nB == 1 ? g2 : 0, fq = nB == 1 ? 0 : g2;
+      const double Fg = uhf ? density_factor_uhf(PA, PB, PAB, SAB, fp, fq) : density_factor(PA, PB, PAB, fp, fq);
       if (Fg == 0.0) continue;
       for (int k = 0; k < 5; ++k) {
         const int q = axis_index(k);
@@ -215,14 +227,15 @@ constexpr int kGradWarps = 4;
 struct HeavyGradShared {
   double L[100], dL[100], W[100], F[100], T1[100], T2[100];
   double Lc[10], dLc[10], Lcb[10], dLcb[10];
-  double PA[4][4], PB[4][4], PAB[4][4];
+  double PA[4][4], PB[4][4], PAB[4][4], SAB[4][4];
   RotGrad ra, rb;
 };
 
 __global__ void __launch_bounds__(kGradWarps * 32) k_pair_gradient_heavy(
     const int* __restrict__ hh, int nhh, const PairDev* __restrict__ pairs, const AtomDev* __restrict__ atoms,
     const ElemDev* __restrict__ elems, const DiatomicDev* __restrict__ diat, const MolDev* __restrict__ mols, int method,
-    const double* __restrict__ Pall, double* __restrict__ gpair) {
+    const double* __restrict__ Pall, const double* __restrict__ Paall, const double* __restrict__ Pball,
+    double* __restrict__ gpair) {
   __shared__ HeavyGradShared shm[kGradWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int w = blockIdx.x * kGradWarps + warp;
@@ -244,6 +257,8 @@ __global__ void __launch_bounds__(kGradWarps * 32) k_pair_gradient_heavy(
     s.PA[i][j] = P[(size_t)(a.ao0 + i) * N + a.ao0 + j];
     s.PB[i][j] = P[(size_t)(b.ao0 + i) * N + b.ao0 + j];
     s.PAB[i][j] = P[(size_t)(a.ao0 + i) * N + b.ao0 + j];
+    const size_t ij = m.mat_off + (size_t)(a.ao0 + i) * N + b.ao0 + j;
+    s.SAB[i][j] = Paall ? Paall[ij] - Pball[ij] : 0.0;
   }
   if (lane == 30) rotation_grad(Dual3(X, 1, 0, 0), Dual3(Y, 0, 1, 0), Dual3(Z, 0, 0, 1), s.ra);
   if (lane == 31) rotation_grad(Dual3(-X, -1, 0, 0), Dual3(-Y, 0, -1, 0), Dual3(-Z, 0, 0, -1), s.rb);
@@ -275,7 +290,8 @@ __global__ void __launch_bounds__(kGradWarps * 32) k_pair_gradient_heavy(
   }
   for (int k = lane; k < 100; k += 32) {
     s.W[k] = w_entry(s.ra.r, k / 10, k % 10);
-    s.F[k] = density_factor(s.PA, s.PB, s.PAB, k / 10, k % 10);
+    s.F[k] = Paall ? density_factor_uhf(s.PA, s.PB, s.PAB, s.SAB, k / 10, k % 10)
+                   : density_factor(s.PA, s.PB, s.PAB, k / 10, k % 10);
   }
   __syncwarp();
   // T1 = F W, T2 = F^T W
@@ -454,11 +470,13 @@ void launch_gradient(const DeviceBatch& b, cudaStream_t s) {
   if (b.npairs > 0) {
     const int th = 128;
     k_pair_gradient_light<<<(b.npairs + th - 1) / th, th, 0, s>>>(b.pairs, b.npairs, b.atoms, b.elems, b.diat, b.mols,
-                                                                   b.method, b.P, b.gpair);
+                                                                   b.method, b.P, b.uhf ? b.Pa : nullptr,
+                                                                   b.uhf ? b.Pb : nullptr, b.gpair);
   }
   if (b.nhh_total > 0) {
     k_pair_gradient_heavy<<<(b.nhh_total + kGradWarps - 1) / kGradWarps, kGradWarps * 32, 0, s>>>(
-        b.hh_pairs, b.nhh_total, b.pairs, b.atoms, b.elems, b.diat, b.mols, b.method, b.P, b.gpair);
+        b.hh_pairs, b.nhh_total, b.pairs, b.atoms, b.elems, b.diat, b.mols, b.method, b.P, b.uhf ? b.Pa : nullptr,
+        b.uhf ? b.Pb : nullptr, b.gpair);
   }
   launch_gather_gradient(b, s);
 }

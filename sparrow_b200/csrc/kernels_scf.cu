@@ -500,6 +500,243 @@ void launch_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_
                                          b.rotbuf, b.res, sp, in_smem);
 }
 
+// ---------------------------------------------------------------------------
+// Unrestricted (UHF) SCF
+// ---------------------------------------------------------------------------
+// With P_T = P_a + P_b and the spin density P_s = P_a - P_b, the unrestricted
+// Fock matrices (TwoElectronMatrix.cpp:98-103, 142-161: G_s = sum P_T (mn|ls)
+// - P_s' (ml|ns) for spin s') are the restricted build on the total density
+// plus a spin-exchange term,
+//   F_a = F_R(P_T) - 1/2 K(P_s),   F_b = F_R(P_T) + 1/2 K(P_s),
+//   K(P)_mn = sum_ls P_ls (ml|ns),
+// and the electronic energy 1/2 sum [P_T H + P_a F_a + P_b F_b]
+// (NDDOElectronicEnergyCalculator.cpp:68-90) is E_R(P_T) - 1/4 sum P_s K(P_s).
+// spin_exchange applies the term: F holds F_R on entry and F_a on return, Fb
+// receives F_b.  Two-centre blocks (exchange only couples the atoms of a pair)
+// take a thread per pair; one-centre blocks a thread per (atom, orbital pair),
+// with K_ss = S_ss g_ss + sum_p S_pp h_sp, K_pp = S_ss h_sp + S_pp g_pp +
+// sum_q!=p S_qq h_pp, K_sp = S_sp (g_sp + h_sp), K_pq = S_pq (g_p2 + h_pp).
+// Returns sum P_s K(P_s) over the CTA.
+__device__ double spin_exchange(const MolDev& m, const AtomDev* __restrict__ atoms, const ElemDev* __restrict__ elems,
+                                const PairDev* __restrict__ pairs, const double* __restrict__ ints,
+                                const double* __restrict__ Pa, const double* __restrict__ Pb, double* F, double* Fb,
+                                double* red) {
+  const int N = m.nao, tid = threadIdx.x;
+  double e = 0;
+  for (int k = tid; k < m.npairs; k += blockDim.x) {
+    const PairDev pr = pairs[m.pair0 + k];
+    const AtomDev aA = atoms[pr.a], aB = atoms[pr.b];
+    const int nA = elems[aA.slot].nao, nB = elems[aB.slot].nao;
+    const int oa = aA.ao0, ob = aB.ao0, dB = nB == 4 ? 10 : 1;
+    const double* W = ints + pr.int_off;
+    double S[4][4];
+    for (int i = 0; i < nA; ++i)
+      for (int j = 0; j < nB; ++j) {
+        const size_t ij = (size_t)(oa + i) * N + ob + j;
+        S[i][j] = Pa[ij] - Pb[ij];
+      }
+    for (int mu = 0; mu < nA; ++mu)
+      for (int la = 0; la < nB; ++la) {
+        double kx = 0;
+        for (int nu = 0; nu < nA; ++nu)
+          for (int si = 0; si < nB; ++si)
+            kx += S[nu][si] * W[(nA == 4 ? pair_index(mu, nu) : 0) * dB + (nB == 4 ? pair_index(la, si) : 0)];
+        const size_t iab = (size_t)(oa + mu) * N + ob + la, iba = (size_t)(ob + la) * N + oa + mu;
+        const double fr = F[iab];
+        F[iab] = F[iba] = fr - 0.5 * kx;
+        Fb[iab] = Fb[iba] = fr + 0.5 * kx;
+        e += 2.0 * S[mu][la] * kx;
+      }
+  }
+  for (int idx = tid; idx < m.nat * 10; idx += blockDim.x) {
+    const int a = idx / 10, p = idx % 10;
+    const AtomDev aA = atoms[m.atom0 + a];
+    const ElemDev& eA = elems[aA.slot];
+    if (p >= (eA.nao == 1 ? 1 : 10)) continue;
+    const int mu = c_pair_mu[p], nu = c_pair_nu[p], o = aA.ao0;
+    auto Sm = [&](int i, int j) {
+      const size_t ij = (size_t)(o + i) * N + o + j;
+      return Pa[ij] - Pb[ij];
+    };
+    double kx;
+    if (eA.nao == 1) {
+      kx = Sm(0, 0) * eA.gss;
+    } else if (mu == nu) {
+      if (mu == 0) {
+        kx = Sm(0, 0) * eA.gss + (Sm(1, 1) + Sm(2, 2) + Sm(3, 3)) * eA.hsp;
+      } else {
+        kx = Sm(0, 0) * eA.hsp + Sm(mu, mu) * eA.gpp;
+        for (int q = 1; q < 4; ++q)
+          if (q != mu) kx += Sm(q, q) * eA.hpp;
+      }
+    } else {
+      kx = Sm(mu, nu) * (mu == 0 ? eA.gsp + eA.hsp : eA.gp2 + eA.hpp);
+    }
+    const size_t i1 = (size_t)(o + mu) * N + o + nu, i2 = (size_t)(o + nu) * N + o + mu;
+    const double fr = F[i1];
+    F[i1] = F[i2] = fr - 0.5 * kx;
+    Fb[i1] = Fb[i2] = fr + 0.5 * kx;
+    e += (mu == nu ? 1.0 : 2.0) * Sm(mu, nu) * kx;
+  }
+  __syncthreads();
+  return cta_sum(e, red);
+}
+
+// New orbitals of one spin from its (extrapolated) Fock matrix Fs: the
+// occupied-virtual rotation of the previous orbitals, or a full
+// diagonalisation at the start, when the rotation asks for one, and when
+// the spin has no occupied or no virtual orbitals.  Returns the Jacobi
+// sweeps of a full diagonalisation (0 when none ran, < 0 when it did not
+// converge).
+__device__ int uhf_orbitals(int N, int ns, double* Fs, double* Cs, double* W1, double* W2, double* epss,
+                            double* Apk, size_t packed_bytes, bool& have, double& drift, double* rot, int cap_rounds,
+                            const ScfParams& sp, int cold_sweeps, int& nfull, ScfShared& sh) {
+  int need_full = !have || ns == 0 || ns == N;
+  if (!need_full) need_full = ov_rotation(N, ns, Fs, Cs, W1, W2, epss, drift, sh);
+  if (!need_full) return 0;
+  const int sw = full_diagonalise(N, Fs, Cs, W1, W2, epss, Apk ? Apk : Fs, Apk ? packed_bytes : 0, have, rot,
+                                  cap_rounds, have ? sp.jacobi_max_sweeps : cold_sweeps, have ? 1e-10 : 1e-3, sh);
+  ++nfull;
+  const bool warm = have;
+  have = true;
+  drift = 0;
+  return sw < 0 ? (warm ? -sp.jacobi_max_sweeps : cold_sweeps) : sw;
+}
+
+// P_s = C_occ C_occ^T of one spin into Ps; returns sum (P_s,new - P_s,old)^2.
+__device__ double uhf_density(int N, int ns, const double* Cs, double* Ps, double* W1, ScfShared& sh) {
+  const size_t NN = (size_t)N * N;
+  if (ns > 0) {
+    cta_gemm(N, N, ns, 1.0, Cs, N, true, Cs, N, false, 0.0, W1, N, sh.gemm, true);
+  } else {
+    for (size_t k = threadIdx.x; k < NN; k += blockDim.x) W1[k] = 0.0;
+    __syncthreads();
+  }
+  double d2 = 0;
+  for (size_t k = threadIdx.x; k < NN; k += blockDim.x) {
+    const double d = W1[k] - Ps[k];
+    d2 += d * d;
+    Ps[k] = W1[k];
+  }
+  return cta_sum(d2, sh.red);
+}
+
+// The persistent kernel of k_scf for unrestricted molecules (MolDev.nocc
+// alpha and MolDev.nocc_b beta electrons): start P_a = P_b = P / 2 from the
+// restricted guess (or a given total density), then per iteration the Fock
+// pair, one DIIS over both spins, new orbitals and densities per spin;
+// convergence on |dE| and the larger rms change of the two spin densities.
+__global__ void __launch_bounds__(kScfThreads, 1) k_uhf_scf(
+    const MolDev* __restrict__ mols, int nmol, const int* __restrict__ order, int* counter,
+    const AtomDev* __restrict__ atoms, const ElemDev* __restrict__ elems, const PairDev* __restrict__ pairs,
+    const double* __restrict__ ints, const int* __restrict__ hh_pairs, double* jbuf, const double* __restrict__ Hall,
+    double* Pall, double* Fall, double* Call, double* W1all, double* W2all, double* epsall, double* diisall,
+    double* Paall, double* Pball, double* Fball, double* Cball, double* epsball, double* diisball, double* rotbuf,
+    MolResult* res, ScfParams sp, int packed_in_smem) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ScfShared& sh = *reinterpret_cast<ScfShared*>(smem_raw);
+  double* smemA = reinterpret_cast<double*>(smem_raw + ((sizeof(ScfShared) + 15) / 16) * 16);
+  const int tid = threadIdx.x;
+  for (;;) {
+    if (tid == 0) {
+      int k = atomicAdd(counter, 1);
+      sh.mol = k < nmol ? order[k] : -1;
+    }
+    __syncthreads();
+    const int mi = sh.mol;
+    __syncthreads();
+    if (mi < 0) return;
+    const MolDev m = mols[mi];
+    const int N = m.nao, na = m.nocc, nb = m.nocc_b;
+    const size_t NN = (size_t)N * N;
+    const double* H = Hall + m.mat_off;
+    double* P = Pall + m.mat_off;
+    double* Pa = Paall + m.mat_off;
+    double* Pb = Pball + m.mat_off;
+    double* Fa = Fall + m.mat_off;
+    double* Fb = Fball + m.mat_off;
+    double* Ca = Call + m.mat_off;
+    double* Cb = Cball + m.mat_off;
+    double* W1 = W1all + m.mat_off;
+    double* W2 = W2all + m.mat_off;
+    double* epsa = epsall + m.ao_base;
+    double* epsb = epsball + m.ao_base;
+    double* histFa = diisall + m.diis_off;
+    double* histEa = histFa + (size_t)kDiisMax * NN;
+    double* histFb = diisball + m.diis_off;
+    double* histEb = histFb + (size_t)kDiisMax * NN;
+    double* Apk = packed_in_smem ? smemA : nullptr;
+    const size_t packed_bytes = sizeof(double) * (size_t)N * (N + 1) / 2;
+    double* rot = rotbuf + (size_t)blockIdx.x * (kRotBudgetBytes / sizeof(double));
+    const int cap_rounds = (int)((kRotBudgetBytes / sizeof(double)) / (2 * ((N + 1) / 2)));
+    const int msize = sp.diis_size < 1 ? 1 : (sp.diis_size > kDiisMax ? kDiisMax : sp.diis_size);
+    const int cold_sweeps = sp.cold_sweeps > 0 ? sp.cold_sweeps : 3;
+    for (size_t k = tid; k < NN; k += blockDim.x) Pa[k] = Pb[k] = 0.5 * P[k];
+    __syncthreads();
+    int nhist = 0, head = 0;
+    bool have_a = false, have_b = false;
+    double drift_a = 0, drift_b = 0, Eold = 0, last_dE = 0, last_rms = 0;
+    int it = 0, converged = 0, status = kDevOk, nfull = 0, nsweeps = 0;
+    for (it = 1; it <= sp.max_iter; ++it) {
+      const double ER = build_fock(m, atoms, elems, pairs, ints, hh_pairs, jbuf, H, P, Fa, sh.red, sh.fockw);
+      __syncthreads();
+      const double E = ER - 0.25 * spin_exchange(m, atoms, elems, pairs, ints, Pa, Pb, Fa, Fb, sh.red);
+      diis_step_uhf(N, Fa, Pa, Fb, Pb, W1, histFa, histEa, histFb, histEb, msize, nhist, head, sh);
+      const bool warm_a = have_a, warm_b = have_b;
+      int sw = uhf_orbitals(N, na, Fa, Ca, W1, W2, epsa, Apk, packed_bytes, have_a, drift_a, rot, cap_rounds, sp,
+                            cold_sweeps, nfull, sh);
+      if (sw < 0 && warm_a) status = kDevJacobiNotConverged;
+      nsweeps += sw < 0 ? -sw : sw;
+      sw = uhf_orbitals(N, nb, Fb, Cb, W1, W2, epsb, Apk, packed_bytes, have_b, drift_b, rot, cap_rounds, sp,
+                        cold_sweeps, nfull, sh);
+      if (sw < 0 && warm_b) status = kDevJacobiNotConverged;
+      nsweeps += sw < 0 ? -sw : sw;
+      const double da = uhf_density(N, na, Ca, Pa, W1, sh);
+      const double db = uhf_density(N, nb, Cb, Pb, W1, sh);
+      for (size_t k = tid; k < NN; k += blockDim.x) P[k] = Pa[k] + Pb[k];
+      __syncthreads();
+      const double rms = sqrt(fmax(da, db) / (double)NN);
+      last_rms = rms;
+      last_dE = it > 1 ? fabs(E - Eold) : 0.0;
+      const bool dE_ok = it > 1 && fabs(E - Eold) < sp.scc;
+      Eold = E;
+      if (!isfinite(E) || !isfinite(rms)) { status = kDevNonFinite; break; }
+      if (dE_ok && rms < sp.rmsd) { converged = 1; break; }
+    }
+    if (it > sp.max_iter) it = sp.max_iter;
+    __syncthreads();
+    const double ER = build_fock(m, atoms, elems, pairs, ints, hh_pairs, jbuf, H, P, Fa, sh.red, sh.fockw);
+    __syncthreads();
+    const double Efin = ER - 0.25 * spin_exchange(m, atoms, elems, pairs, ints, Pa, Pb, Fa, Fb, sh.red);
+    if (tid == 0) {
+      MolResult& r = res[mi];
+      r.e_el = Efin;
+      r.energy = Efin + r.e_rep;
+      r.iterations = it;
+      r.converged = converged;
+      r.status = status;
+      r.last_dE = last_dE;
+      r.last_rmsd = last_rms;
+      r.full_diag = nfull;
+      r.jacobi_sweeps = nsweeps;
+      for (int k = 0; k < 5; ++k) r.cycles[k] = 0;
+    }
+    __syncthreads();
+  }
+}
+
+void launch_uhf_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s) {
+  if (b.nmol == 0) return;
+  int in_smem = 0;
+  const size_t bytes = scf_smem_bytes(b.max_nao, &in_smem);
+  cudaFuncSetAttribute(k_uhf_scf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaMemsetAsync(b.counter, 0, sizeof(int), s);
+  if (grid > b.nmol) grid = b.nmol;
+  k_uhf_scf<<<grid, kScfThreads, bytes, s>>>(b.mols, b.nmol, b.order, b.counter, b.atoms, b.elems, b.pairs, b.ints,
+                                             b.hh_pairs, b.jbuf, b.H, b.P, b.F, b.C, b.W1, b.W2, b.eps, b.diis, b.Pa,
+                                             b.Pb, b.Fb, b.Cb, b.epsb, b.diisb, b.rotbuf, b.res, sp, in_smem);
+}
+
 }  // namespace sgb
 
 // ---------------------------------------------------------------------------

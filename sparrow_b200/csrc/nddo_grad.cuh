@@ -89,6 +89,25 @@ SGB_HD double density_factor(const double PA[4][4], const double PB[4][4], const
   return s;
 }
 
+// Unrestricted: the exchange products of the two spins,
+// P_a P_a + P_b P_b = 1/2 (P P + S S) with S = P_a - P_b the spin density
+// (TwoElectronMatrix.cpp:182-241 with the spin densities).
+SGB_HD double density_factor_uhf(const double PA[4][4], const double PB[4][4], const double PAB[4][4],
+                                 const double SAB[4][4], int p, int q) {
+  int mu, nu, la, si;
+  pair_orbitals(p, mu, nu);
+  pair_orbitals(q, la, si);
+  double s = 0;
+  for (int o1 = 0; o1 < (mu == nu ? 1 : 2); ++o1) {
+    const int m1 = o1 ? nu : mu, n1 = o1 ? mu : nu;
+    for (int o2 = 0; o2 < (la == si ? 1 : 2); ++o2) {
+      const int l1 = o2 ? si : la, s1 = o2 ? la : si;
+      s += PA[m1][n1] * PB[l1][s1] - 0.5 * (PAB[m1][l1] * PAB[n1][s1] + SAB[m1][l1] * SAB[n1][s1]);
+    }
+  }
+  return s;
+}
+
 // fA[p] = sum over the orderings of p of P_mu,nu (one-atom block)
 SGB_HD double atom_factor(const double PA[4][4], int p) {
   int mu, nu;

@@ -488,25 +488,18 @@ struct ScfShared {
 __device__ __forceinline__ int diis_row_e(int N, int i) { return i * (N - 1) - i * (i - 1) / 2; }
 __device__ __forceinline__ int diis_row_f(int N, int i) { return i * N - i * (i - 1) / 2; }
 
-__device__ const double* diis_step(int N, const double* F, const double* P, double* W, double* dst, double* histF,
-                                   double* histE, int msize, int& nhist, int& head, ScfShared& sh) {
+// One spin's store pass: F and E = W - W^T (W = FP) into ring slot `slot`,
+// with <E, E_j> for every stored error vector j accumulated into d (the new
+// one is E itself).  The error vectors only enter the B matrix: they are kept
+// in FP32 (half the ring traffic; relative precision 6e-8 at any magnitude),
+// the Fock matrices that are combined stay FP64.
+__device__ __forceinline__ void diis_store(int N, const double* F, const double* W, double* histF, double* histE,
+                                           int slot, int nhist, double (&d)[kDiisMax]) {
   const int TE = N * (N - 1) / 2, TF = N * (N + 1) / 2;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-  cta_gemm(N, N, N, 1.0, F, N, false, P, N, false, 0.0, W, N, sh.gemm);  // W = FP
-  const int slot = head;
-  head = (head + 1) % msize;
-  if (nhist < msize) ++nhist;
-  // the error vectors only enter the B matrix: they are kept in FP32 (half
-  // the ring traffic; relative precision 6e-8 at any magnitude), the Fock
-  // matrices that are combined stay FP64
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   float* hE = reinterpret_cast<float*>(histE);
   float* eS = hE + (size_t)slot * TE;
   double* fS = histF + (size_t)slot * TF;
-  // one pass over the upper triangle: store E = W - W^T and F, and accumulate
-  // <E, E_j> for every stored error vector j (the new one is E itself)
-  double d[kDiisMax];
-#pragma unroll
-  for (int j = 0; j < kDiisMax; ++j) d[j] = 0.0;
   for (int i = warp; i < N; i += nwarps) {
     const int re = diis_row_e(N, i) - i - 1, rf = diis_row_f(N, i) - i;
     for (int c = i + lane; c < N; c += 32) {
@@ -520,8 +513,14 @@ __device__ const double* diis_step(int N, const double* F, const double* P, doub
         if (j < nhist) d[j] += e * (j == slot ? e : (double)hE[(size_t)j * TE + re + c]);
     }
   }
-  // CTA reduction of the nhist dot products through the (idle) GEMM scratch
-  double* part = sh.gemm;
+}
+
+// CTA reduction of the dot products into row and column `slot` of the B
+// matrix, then the solve for the coefficients (sh.coef).  False when there is
+// nothing to extrapolate (fewer than two entries, or a singular system).
+__device__ __forceinline__ bool diis_solve(int slot, int nhist, double (&d)[kDiisMax], ScfShared& sh) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  double* part = sh.gemm;  // idle GEMM scratch
 #pragma unroll
   for (int j = 0; j < kDiisMax; ++j) d[j] = warp_sum(d[j]);
   if (lane == 0)
@@ -535,7 +534,7 @@ __device__ const double* diis_step(int N, const double* F, const double* P, doub
     sh.bmat[tid * kDiisMax + slot] = b;
   }
   __syncthreads();
-  if (nhist < 2) return F;
+  if (nhist < 2) return false;
   if (tid == 0) {
     const int n = nhist, ld = n + 2;
     double scale = 0;
@@ -579,8 +578,14 @@ __device__ const double* diis_step(int N, const double* F, const double* P, doub
     sh.diis_ok = ok;
   }
   __syncthreads();
-  if (!sh.diis_ok) return F;
-  // F' = sum_i c_i F_i from the packed upper triangles, written to both halves
+  return sh.diis_ok != 0;
+}
+
+// dst = sum_i c_i F_i from the packed upper triangles, written to both halves.
+__device__ __forceinline__ void diis_extrapolate(int N, const double* histF, int nhist, double* dst,
+                                                 ScfShared& sh) {
+  const int TF = N * (N + 1) / 2;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   for (int i = warp; i < N; i += nwarps) {
     const int rf = diis_row_f(N, i) - i;
     for (int c = i + lane; c < N; c += 32) {
@@ -591,7 +596,44 @@ __device__ const double* diis_step(int N, const double* F, const double* P, doub
     }
   }
   __syncthreads();
+}
+
+__device__ const double* diis_step(int N, const double* F, const double* P, double* W, double* dst, double* histF,
+                                   double* histE, int msize, int& nhist, int& head, ScfShared& sh) {
+  cta_gemm(N, N, N, 1.0, F, N, false, P, N, false, 0.0, W, N, sh.gemm);  // W = FP
+  const int slot = head;
+  head = (head + 1) % msize;
+  if (nhist < msize) ++nhist;
+  double d[kDiisMax];
+#pragma unroll
+  for (int j = 0; j < kDiisMax; ++j) d[j] = 0.0;
+  diis_store(N, F, W, histF, histE, slot, nhist, d);
+  if (!diis_solve(slot, nhist, d, sh)) return F;
+  diis_extrapolate(N, histF, nhist, dst, sh);
   return dst;
+}
+
+// Unrestricted DIIS: one B matrix over the stacked error vectors of both
+// spins, <E_i, E_j> = <Ea_i, Ea_j> + <Eb_i, Eb_j>, and one set of coefficients
+// for both Fock matrices, which are replaced in place by the extrapolations
+// (left unchanged when there is nothing to extrapolate).  W scratch.
+__device__ void diis_step_uhf(int N, double* Fa, const double* Pa, double* Fb, const double* Pb, double* W,
+                              double* histFa, double* histEa, double* histFb, double* histEb, int msize, int& nhist,
+                              int& head, ScfShared& sh) {
+  const int slot = head;
+  head = (head + 1) % msize;
+  if (nhist < msize) ++nhist;
+  double d[kDiisMax];
+#pragma unroll
+  for (int j = 0; j < kDiisMax; ++j) d[j] = 0.0;
+  cta_gemm(N, N, N, 1.0, Fa, N, false, Pa, N, false, 0.0, W, N, sh.gemm);
+  diis_store(N, Fa, W, histFa, histEa, slot, nhist, d);
+  __syncthreads();
+  cta_gemm(N, N, N, 1.0, Fb, N, false, Pb, N, false, 0.0, W, N, sh.gemm);
+  diis_store(N, Fb, W, histFb, histEb, slot, nhist, d);
+  if (!diis_solve(slot, nhist, d, sh)) return;
+  diis_extrapolate(N, histFa, nhist, Fa, sh);
+  diis_extrapolate(N, histFb, nhist, Fb, sh);
 }
 
 // Full diagonalisation of Fx (held in F) into orbital-major Ct, sorted by energy.
