@@ -55,6 +55,7 @@ extern "C" {
 /* required-property mask */
 #define SG_PROP_ENERGY 1u
 #define SG_PROP_GRADIENTS 2u
+#define SG_PROP_HESSIAN 4u /* semi-numerical: central differences of analytic gradients */
 
 typedef struct sg_calculator sg_calculator;
 typedef struct sg_batch sg_batch;
@@ -118,6 +119,21 @@ int32_t sg_calculate_excitations(sg_calculator* h, int32_t nroots, int32_t tripl
  * energies (N values; sg_get_orbital_energies gives the alpha ones).
  * SG_ERR_NO_RESULTS after a restricted calculation. */
 int32_t sg_get_beta_orbital_energies(const sg_calculator* h, double* eps);
+/* Hessian (3 n_atoms x 3 n_atoms row-major, Hartree/bohr^2) of the last
+ * calculate() with SG_PROP_HESSIAN required.  Like the reference, which has no
+ * analytic Hessian (GenericMethodWrapper.cpp:58-88, 339-341), it is the
+ * symmetrised central difference of analytic gradients with a 0.01 bohr
+ * step; the 6 n_atoms displaced geometries run as one batch. */
+int32_t sg_get_hessian(const sg_calculator* h, double* hessian);
+/* One call: the same Hessian for one molecule (method spec as for
+ * sg_batch_create; unrestricted != 0 or multiplicity != 1 runs the
+ * unrestricted SCF; step <= 0 takes 0.01 bohr).  not_converged (may be NULL)
+ * receives the number of displaced geometries whose SCF did not converge. */
+int32_t sg_calculate_hessian(const char* method, int32_t n_atoms, const int32_t* atomic_numbers,
+                             const double* xyz_bohr, int32_t charge, int32_t multiplicity, int32_t unrestricted,
+                             double self_consistence_criterion, double density_rmsd_criterion,
+                             int32_t max_iterations, double step, double* hessian, int32_t* not_converged,
+                             char* error_message, int32_t error_capacity);
 int32_t sg_get_density(const sg_calculator* h, double* P);
 int32_t sg_set_density(sg_calculator* h, const double* P);
 

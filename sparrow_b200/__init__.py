@@ -17,7 +17,7 @@ import os
 import numpy as np
 
 __all__ = ["Calculator", "Batch", "Results", "get_calculator", "batch_calculate", "library_path", "SparrowError",
-           "element_parameters", "diatomic_parameters"]
+           "element_parameters", "diatomic_parameters", "hessian"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libsparrow_b200.so")
@@ -25,6 +25,7 @@ _lib = None
 
 SG_PROP_ENERGY = 1
 SG_PROP_GRADIENTS = 2
+SG_PROP_HESSIAN = 4
 SG_ERR_NOT_CONVERGED = 6
 SG_ERR_TIMEOUT = 12
 SG_PENDING = 13
@@ -84,6 +85,11 @@ def lib():
         "sg_batch_excitation_cycles": (ctypes.c_int32, [_VP, _VP]),
         "sg_set_density": (ctypes.c_int32, [_VP, _D]),
         "sg_get_beta_orbital_energies": (ctypes.c_int32, [_VP, _D]),
+        "sg_get_hessian": (ctypes.c_int32, [_VP, _D]),
+        "sg_calculate_hessian": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _D, ctypes.c_int32,
+                                                  ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
+                                                  ctypes.c_int32, ctypes.c_double, _D, _I32, ctypes.c_char_p,
+                                                  ctypes.c_int32]),
         "sg_batch_create_unrestricted": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _I32, _D, _I32,
                                                           _I32, ctypes.POINTER(_VP)]),
         "sg_batch_create": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _I32, _D, _I32,
@@ -152,6 +158,7 @@ class Results:
         self.iterations = iterations
         self.n_aos = n_aos
         self.n_occupied = n_occupied
+        self.hessian = None  # (3 n_atoms, 3 n_atoms) when "hessian" was required
 
 
 class _Settings:
@@ -257,6 +264,8 @@ class Calculator:
                 mask |= SG_PROP_ENERGY
             elif p in ("gradients", "gradient"):
                 mask |= SG_PROP_GRADIENTS | SG_PROP_ENERGY
+            elif p == "hessian":
+                mask |= SG_PROP_HESSIAN | SG_PROP_ENERGY
             else:
                 raise ValueError("unsupported property %r" % p)
         self._check(lib().sg_set_required_properties(self._h, mask))
@@ -276,7 +285,13 @@ class Calculator:
             self._check(L.sg_get_gradients(self._h, _dptr(g)))
             grad = g.reshape(-1, 3)
         self._nao = nao.value
-        return Results(e.value, grad, rc == 0 and bool(conv.value), it.value, nao.value, nocc.value)
+        res = Results(e.value, grad, rc == 0 and bool(conv.value), it.value, nao.value, nocc.value)
+        if getattr(self, "_mask", SG_PROP_ENERGY) & SG_PROP_HESSIAN:
+            n3 = 3 * self._n_atoms
+            H = np.zeros(n3 * n3)
+            self._check(L.sg_get_hessian(self._h, _dptr(H)))
+            res.hessian = H.reshape(n3, n3)
+        return res
 
     def excitations(self, nroots=8, triplet=False):
         """TD-DFTB on the last DFTB2/DFTB3 calculation: (omega [nroots] Hartree,
@@ -511,6 +526,26 @@ def diatomic_parameters(method, Z1, Z2):
     if rc != 0:
         raise SparrowError(rc, err.value.decode())
     return float(out[0]), float(out[1])
+
+
+def hessian(method, atomic_numbers, xyz_bohr, charge=0, multiplicity=1, unrestricted=False, scc=1e-7, rmsd=1e-5,
+            max_iter=100, step=0.01):
+    """Semi-numerical Hessian (Hartree/bohr^2): symmetrised central differences of
+    analytic gradients, the 6 n_atoms displaced geometries in one batch.  Returns
+    (H of shape (3n, 3n), number of displaced SCFs that did not converge)."""
+    L = lib()
+    Z = np.ascontiguousarray(atomic_numbers, dtype=np.int32)
+    X = np.ascontiguousarray(xyz_bohr, dtype=np.float64).reshape(-1)
+    n3 = 3 * Z.size
+    H = np.zeros(n3 * n3)
+    nc = ctypes.c_int32()
+    err = ctypes.create_string_buffer(512)
+    rc = L.sg_calculate_hessian(method.encode(), Z.size, _iptr(Z), _dptr(X), int(charge), int(multiplicity),
+                                1 if unrestricted else 0, scc, rmsd, max_iter, step, _dptr(H), ctypes.byref(nc), err,
+                                512)
+    if rc != 0:
+        raise SparrowError(rc, err.value.decode())
+    return H.reshape(n3, n3), nc.value
 
 
 def batch_calculate(method, molecules, charges=None, scc=1e-7, rmsd=1e-5, max_iter=100, gradients=False):

@@ -14,6 +14,7 @@
 #include "../../include/sparrow_b200.h"
 #include "dftb_params.h"
 #include "engine.h"
+#include "hessian.h"
 #include "params.h"
 #include "server.h"
 
@@ -135,12 +136,26 @@ class Calculator {
       error = "device SCF failure code " + std::to_string(result_.status);
       return kErrDevice;
     }
+    hessian_.clear();
+    if (required_ & SG_PROP_HESSIAN) {
+      // semi-numerical, as the reference (GenericMethodWrapper.cpp:76-88)
+      HessianRequest hr;
+      hr.method = method_;
+      hr.parameters = settings_.parameters;
+      hr.unrestricted = uhf;
+      hr.molecule = in[0];
+      hr.scf = sp;
+      int unconverged = 0;
+      rc = numerical_hessian(hr, hessian_, unconverged, error);
+      if (rc) return rc;
+    }
     if (!result_.converged) {
       error = "SCF did not converge in " + std::to_string(result_.iterations) + " iterations";
       return kErrNotConverged;
     }
     return kOk;
   }
+  const std::vector<double>& hessian() const { return hessian_; }
 
   // TD-DFTB on the converged DFTB reference of the last calculate()
   int excitations(int nroots, bool triplet, double* omega, double* dip) {
@@ -216,6 +231,7 @@ class Calculator {
  private:
   void invalidate(bool new_structure) {
     have_result_ = have_gradient_ = false;
+    hessian_.clear();
     if (new_structure) state_.clear();
   }
   Method method_;
@@ -226,7 +242,7 @@ class Calculator {
   uint32_t required_ = SG_PROP_ENERGY;
   MoleculeOutput result_;
   bool have_result_ = false, have_gradient_ = false;
-  std::vector<double> density_, eps_, eps_b_, state_;
+  std::vector<double> density_, eps_, eps_b_, state_, hessian_;
 };
 
 }  // namespace sgb
@@ -399,7 +415,8 @@ int32_t sg_get_setting_int(const sg_calculator* h, const char* key, int64_t* v) 
 
 int32_t sg_set_required_properties(sg_calculator* h, uint32_t mask) {
   if (!h) return SG_ERR_INVALID_ARGUMENT;
-  if (mask & ~(SG_PROP_ENERGY | SG_PROP_GRADIENTS)) return fail(h, SG_ERR_INVALID_ARGUMENT, "unknown property bit");
+  if (mask & ~(SG_PROP_ENERGY | SG_PROP_GRADIENTS | SG_PROP_HESSIAN))
+    return fail(h, SG_ERR_INVALID_ARGUMENT, "unknown property bit");
   h->impl->set_required(mask);
   return SG_OK;
 }
@@ -421,6 +438,14 @@ int32_t sg_get_gradients(const sg_calculator* h, double* g) {
   if (!h->impl->have_result() || !h->impl->have_gradient()) return SG_ERR_NO_RESULTS;
   const auto& v = h->impl->result().gradient;
   std::memcpy(g, v.data(), sizeof(double) * v.size());
+  return SG_OK;
+}
+
+int32_t sg_get_hessian(const sg_calculator* h, double* hessian) {
+  if (!h || !hessian) return SG_ERR_INVALID_ARGUMENT;
+  const auto& v = h->impl->hessian();
+  if (!h->impl->have_result() || v.empty()) return SG_ERR_NO_RESULTS;
+  std::memcpy(hessian, v.data(), sizeof(double) * v.size());
   return SG_OK;
 }
 
@@ -889,3 +914,41 @@ int32_t sg_diatomic_parameters(const char* method, int32_t Z1, int32_t Z2, doubl
   alpha_x[1] = d.x;
   return SG_OK;
 }
+
+int32_t sg_calculate_hessian(const char* method, int32_t n_atoms, const int32_t* Z, const double* xyz, int32_t charge,
+                             int32_t multiplicity, int32_t unrestricted, double scc, double rmsd, int32_t max_iter,
+                             double step, double* hessian, int32_t* not_converged, char* errmsg, int32_t errcap) {
+  using namespace sgb;
+  HessianRequest hr;
+  std::string src;
+  if (!method || !parse_method_spec(method, hr.method, src)) {
+    copy_message("unknown method", errmsg, errcap);
+    return SG_ERR_UNKNOWN_METHOD;
+  }
+  if (n_atoms <= 0 || !Z || !xyz || !hessian) {
+    copy_message("empty molecular structure or no output buffer", errmsg, errcap);
+    return n_atoms <= 0 ? SG_ERR_EMPTY_STRUCTURE : SG_ERR_INVALID_ARGUMENT;
+  }
+  hr.parameters = src;
+  hr.unrestricted = unrestricted != 0 || multiplicity != 1;
+  hr.molecule.Z.assign(Z, Z + n_atoms);
+  hr.molecule.xyz.assign(xyz, xyz + 3 * (size_t)n_atoms);
+  hr.molecule.charge = charge;
+  hr.molecule.multiplicity = multiplicity;
+  hr.scf.scc = scc;
+  hr.scf.rmsd = rmsd;
+  hr.scf.max_iter = max_iter;
+  if (step > 0) hr.step = step;
+  std::vector<double> H;
+  int unconverged = 0;
+  std::string err;
+  const int rc = numerical_hessian(hr, H, unconverged, err);
+  if (not_converged) *not_converged = unconverged;
+  if (rc) {
+    copy_message(err, errmsg, errcap);
+    return rc;
+  }
+  std::memcpy(hessian, H.data(), sizeof(double) * H.size());
+  return SG_OK;
+}
+
