@@ -99,6 +99,7 @@ struct Elem {
   double es = 0, ep = 0, U = 0, occ = 0, hd = 0;
   double w = 0;  // atomically resolved spin constant (W_pp for p elements, W_ss for s)
   bool has_hd = false, has_w = false;
+  double W[2][2] = {};  // shell spin constants W(l, l'), l = s, p (SKAtom.h:52-66)
 };
 
 struct Pair {
@@ -238,6 +239,10 @@ bool load(const char* set_name, const std::vector<int>& Zs, int order, Params& P
     e.has_hd = r.has_hubbard_derivative != 0;
     e.w = e.nao == 1 ? r.wss : r.wpp;  // SKAtom.h:94-102
     e.has_w = r.has_spin != 0;
+    e.W[0][0] = r.wss;
+    e.W[0][1] = r.wsp;
+    e.W[1][0] = r.wps;
+    e.W[1][1] = r.wpp;
     P.have[r.Z] = true;
   }
   for (int z : Zs) {
@@ -276,6 +281,7 @@ bool load(const char* set_name, const std::vector<int>& Zs, int order, Params& P
 
 struct Mol {
   int nat = 0, nao = 0, nel = 0, nocc = 0, order = 2;
+  int nalpha = 0, nbeta = 0;  // spin-polarised runs
   std::vector<int> Z, ao0, nao_of;
   std::vector<double> pos, core;
   Params P;
@@ -672,17 +678,11 @@ bool scf(const Mol& M, State& st, double scc, double rmsd, int max_iter) {
   return true;
 }
 
-void gradient(const Mol& M, const State& st, std::vector<double>& g) {
+// Nuclear gradient with the overlap multiplier Wm (energy-weighted density
+// minus the density-dependent parts of the Fock matrix that multiply S).
+void gradient_with(const Mol& M, const State& st, const std::vector<double>& Wm, std::vector<double>& g) {
   const int N = M.nao, n = M.nat;
   g.assign(3 * (size_t)n, 0);
-  // W = 2 sum_occ eps_i C_i C_i^T and the overlap multiplier W - HXoverS o P
-  std::vector<double> Wm((size_t)N * N, 0);
-  for (int i = 0; i < N; ++i)
-    for (int j = 0; j < N; ++j) {
-      double s = 0;
-      for (int k = 0; k < M.nocc; ++k) s += st.eps[k] * st.C[(size_t)i * N + k] * st.C[(size_t)j * N + k];
-      Wm[(size_t)i * N + j] = 2 * s - st.shift[(size_t)i * N + j] * st.P[(size_t)i * N + j];
-    }
   for (int a = 0; a < n; ++a)
     for (int b = a + 1; b < n; ++b) {
       double d[3] = {0, 0, 0};
@@ -724,7 +724,21 @@ void gradient(const Mol& M, const State& st, std::vector<double>& g) {
     }
 }
 
-bool setup(const char* set, int order, int nat, const int* Z, const double* xyz, int charge, Mol& M) {
+void gradient(const Mol& M, const State& st, std::vector<double>& g) {
+  const int N = M.nao;
+  // W = 2 sum_occ eps_i C_i C_i^T and the overlap multiplier W - HXoverS o P
+  std::vector<double> Wm((size_t)N * N, 0);
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j) {
+      double s = 0;
+      for (int k = 0; k < M.nocc; ++k) s += st.eps[k] * st.C[(size_t)i * N + k] * st.C[(size_t)j * N + k];
+      Wm[(size_t)i * N + j] = 2 * s - st.shift[(size_t)i * N + j] * st.P[(size_t)i * N + j];
+    }
+  gradient_with(M, st, Wm, g);
+}
+
+bool setup(const char* set, int order, int nat, const int* Z, const double* xyz, int charge, Mol& M,
+           int multiplicity = 0) {
   M = Mol();
   M.order = order;
   M.nat = nat;
@@ -745,12 +759,217 @@ bool setup(const char* set, int order, int nat, const int* Z, const double* xyz,
     occ += e.occ;
   }
   M.nel = (int)std::lround(occ) - charge;
+  if (multiplicity > 0) {
+    const int na2 = M.nel + multiplicity - 1;
+    if (M.nel < 0 || (na2 & 1) || M.nel - (multiplicity - 1) < 0 || na2 / 2 > M.nao) {
+      g_error = "electron count and spin multiplicity do not match";
+      return false;
+    }
+    M.nalpha = na2 / 2;
+    M.nbeta = M.nel - M.nalpha;
+    M.nocc = M.nalpha;
+    return true;
+  }
   if (M.nel < 0 || (M.nel & 1)) {
     g_error = "restricted DFTB needs an even electron count";
     return false;
   }
   M.nocc = M.nel / 2;
   return true;
+}
+
+// ---------------------------------------------------------------------------
+// Spin-polarised DFTB (Utils/SDFTB.cpp:64-293, Utils/ScfFock.cpp:50-103)
+// ---------------------------------------------------------------------------
+// Shell spin populations pdif_{a,l} = sum_{mu in (a, l)} sum_nu (Pa - Pb)_mu,nu S_mu,nu,
+// shell shifts eps_{a,l} = sum_l' W_a(l, l') pdif_{a,l'}, the spin contribution
+// spinC_mu,nu = 1/2 (eps_{a(mu),l(mu)} + eps_{b(nu),l(nu)}) that enters
+// F_alpha = F + spinC o S and F_beta = F - spinC o S, and the energy
+// 1/2 sum_a sum_{l,l'} pdif_{a,l} W_a(l, l') pdif_{a,l'}.
+double spin_terms(const Mol& M, const std::vector<double>& Pa, const std::vector<double>& Pb,
+                  const std::vector<double>& S, std::vector<double>& spinC) {
+  const int N = M.nao, n = M.nat;
+  std::vector<double> pdif(2 * (size_t)n, 0.0), eps(2 * (size_t)n, 0.0);
+  std::vector<int> atom_of(N), shell_of(N);
+  for (int a = 0; a < n; ++a)
+    for (int i = 0; i < M.nao_of[a]; ++i) {
+      atom_of[M.ao0[a] + i] = a;
+      shell_of[M.ao0[a] + i] = i == 0 ? 0 : 1;
+    }
+  for (int u = 0; u < N; ++u) {
+    double s = 0;
+    for (int v = 0; v < N; ++v) s += (Pa[(size_t)u * N + v] - Pb[(size_t)u * N + v]) * S[(size_t)u * N + v];
+    pdif[2 * atom_of[u] + shell_of[u]] += s;
+  }
+  double e = 0;
+  for (int a = 0; a < n; ++a) {
+    const Elem& el = M.P.elem[M.Z[a]];
+    for (int l = 0; l < 2; ++l)
+      for (int k = 0; k < 2; ++k) {
+        eps[2 * a + l] += el.W[l][k] * pdif[2 * a + k];
+        e += 0.5 * pdif[2 * a + l] * el.W[l][k] * pdif[2 * a + k];
+      }
+  }
+  spinC.assign((size_t)N * N, 0.0);
+  for (int u = 0; u < N; ++u)
+    for (int v = 0; v < N; ++v)
+      spinC[(size_t)u * N + v] = 0.5 * (eps[2 * atom_of[u] + shell_of[u]] + eps[2 * atom_of[v] + shell_of[v]]);
+  return e;
+}
+
+struct SpinState {
+  std::vector<double> Pa, Pb, Ca, Cb, epsa, epsb, spinC;
+  double e_spin = 0;
+};
+
+// Unrestricted SCC: both spins from the restricted Fock matrix of the total
+// density plus / minus the spin term; Pulay DIIS on the stacked commutators
+// (F_s P_s S - S P_s F_s) with one set of coefficients; start P_a = P_b = P0 / 2.
+bool scf_uhf(const Mol& M, State& st, SpinState& ss, double scc, double rmsd, int max_iter) {
+  const int N = M.nao;
+  const size_t NN = (size_t)N * N;
+  build_static(M, st);
+  std::vector<double> sw, sv;
+  if (!oracle_la::eigh(N, st.S, sw, sv)) {
+    g_error = "overlap diagonalisation failed";
+    return false;
+  }
+  std::vector<double> X(NN, 0);
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j) {
+      double s = 0;
+      for (int k = 0; k < N; ++k) s += sv[(size_t)i * N + k] * sv[(size_t)j * N + k] / std::sqrt(sw[k]);
+      X[(size_t)i * N + j] = s;
+    }
+  st.P.assign(NN, 0);
+  for (int a = 0; a < M.nat; ++a)
+    for (int i = 0; i < M.nao_of[a]; ++i)
+      st.P[(size_t)(M.ao0[a] + i) * N + M.ao0[a] + i] = M.core[a] / M.nao_of[a];
+  ss.Pa.assign(NN, 0);
+  ss.Pb.assign(NN, 0);
+  for (size_t k = 0; k < NN; ++k) ss.Pa[k] = ss.Pb[k] = 0.5 * st.P[k];
+  std::vector<std::vector<double>> hFa, hFb, hE;
+  std::vector<double> Fa(NN), Fb(NN);
+  auto commutator = [&](const std::vector<double>& F, const std::vector<double>& P, double* out) {
+    const auto FPS = matmul(N, matmul(N, F, P), st.S);
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j) out[(size_t)i * N + j] = FPS[(size_t)i * N + j] - FPS[(size_t)j * N + i];
+  };
+  auto solve_spin = [&](const std::vector<double>& Fx, int nocc, std::vector<double>& C, std::vector<double>& eps,
+                        std::vector<double>& Pn) -> bool {
+    const auto Fp = matmul(N, X, matmul(N, Fx, X));
+    std::vector<double> v;
+    if (!oracle_la::eigh(N, Fp, eps, v)) return false;
+    C = matmul(N, X, v);
+    Pn.assign(NN, 0);
+    for (int i = 0; i < N; ++i)
+      for (int j = 0; j < N; ++j) {
+        double s = 0;
+        for (int k = 0; k < nocc; ++k) s += C[(size_t)i * N + k] * C[(size_t)j * N + k];
+        Pn[(size_t)i * N + j] = s;
+      }
+    return true;
+  };
+  double Eold = 0;
+  st.converged = false;
+  for (int it = 1; it <= max_iter; ++it) {
+    st.iterations = it;
+    fock(M, st);
+    const double E = electronic_energy(M, st) + spin_terms(M, ss.Pa, ss.Pb, st.S, ss.spinC);
+    for (size_t k = 0; k < NN; ++k) {
+      Fa[k] = st.F[k] + ss.spinC[k] * st.S[k];
+      Fb[k] = st.F[k] - ss.spinC[k] * st.S[k];
+    }
+    std::vector<double> err(2 * NN);
+    commutator(Fa, ss.Pa, err.data());
+    commutator(Fb, ss.Pb, err.data() + NN);
+    hFa.push_back(Fa);
+    hFb.push_back(Fb);
+    hE.push_back(err);
+    if (hE.size() > 8) {
+      hFa.erase(hFa.begin());
+      hFb.erase(hFb.begin());
+      hE.erase(hE.begin());
+    }
+    std::vector<double> Fxa = Fa, Fxb = Fb;
+    const int m = (int)hE.size();
+    if (m >= 2) {
+      std::vector<double> B((size_t)(m + 1) * (m + 1), 0), rhs(m + 1, 0);
+      for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) {
+          double s = 0;
+          for (size_t k = 0; k < err.size(); ++k) s += hE[i][k] * hE[j][k];
+          B[i * (m + 1) + j] = s;
+        }
+      for (int i = 0; i < m; ++i) B[i * (m + 1) + m] = B[m * (m + 1) + i] = -1;
+      rhs[m] = -1;
+      if (oracle_la::solve_dense(m + 1, B, rhs)) {
+        std::fill(Fxa.begin(), Fxa.end(), 0.0);
+        std::fill(Fxb.begin(), Fxb.end(), 0.0);
+        for (int i = 0; i < m; ++i)
+          for (size_t k = 0; k < NN; ++k) {
+            Fxa[k] += rhs[i] * hFa[i][k];
+            Fxb[k] += rhs[i] * hFb[i][k];
+          }
+      }
+    }
+    std::vector<double> Pna, Pnb;
+    if (!solve_spin(Fxa, M.nalpha, ss.Ca, ss.epsa, Pna) || !solve_spin(Fxb, M.nbeta, ss.Cb, ss.epsb, Pnb)) {
+      g_error = "Fock diagonalisation failed";
+      return false;
+    }
+    double da = 0, db = 0;
+    for (size_t k = 0; k < NN; ++k) {
+      da += (Pna[k] - ss.Pa[k]) * (Pna[k] - ss.Pa[k]);
+      db += (Pnb[k] - ss.Pb[k]) * (Pnb[k] - ss.Pb[k]);
+    }
+    const double rms = std::sqrt(std::max(da, db) / (double)NN);
+    ss.Pa.swap(Pna);
+    ss.Pb.swap(Pnb);
+    for (size_t k = 0; k < NN; ++k) st.P[k] = ss.Pa[k] + ss.Pb[k];
+    const bool dE_ok = it > 1 && std::fabs(E - Eold) < scc;
+    Eold = E;
+    if (dE_ok && rms < rmsd) {
+      st.converged = true;
+      break;
+    }
+  }
+  fock(M, st);
+  ss.e_spin = spin_terms(M, ss.Pa, ss.Pb, st.S, ss.spinC);
+  st.e_el = electronic_energy(M, st) + ss.e_spin;
+  // orbital energies of the final spin Fock matrices
+  for (size_t k = 0; k < NN; ++k) {
+    Fa[k] = st.F[k] + ss.spinC[k] * st.S[k];
+    Fb[k] = st.F[k] - ss.spinC[k] * st.S[k];
+  }
+  std::vector<double> tmp;
+  solve_spin(Fa, M.nalpha, ss.Ca, ss.epsa, tmp);
+  solve_spin(Fb, M.nbeta, ss.Cb, ss.epsb, tmp);
+  st.e_rep = 0;
+  for (int a = 0; a < M.nat; ++a)
+    for (int b = a + 1; b < M.nat; ++b) {
+      double E, dE;
+      repulsion(M.pair(M.Z[a], M.Z[b]), dist_ab(M, a, b), E, dE);
+      st.e_rep += E;
+    }
+  return true;
+}
+
+// Unrestricted gradient: W = sum_s sum_{occ s} eps C C^T, and the overlap
+// multiplier W - HXoverS o P - spinC o (Pa - Pb) (SDFTB.cpp:60-83 adds
+// 2 (Pa - Pb) spinC dS per atom pair).
+void gradient_uhf(const Mol& M, const State& st, const SpinState& ss, std::vector<double>& g) {
+  const int N = M.nao;
+  std::vector<double> Wm((size_t)N * N, 0);
+  for (int i = 0; i < N; ++i)
+    for (int j = 0; j < N; ++j) {
+      double s = 0;
+      for (int k = 0; k < M.nalpha; ++k) s += ss.epsa[k] * ss.Ca[(size_t)i * N + k] * ss.Ca[(size_t)j * N + k];
+      for (int k = 0; k < M.nbeta; ++k) s += ss.epsb[k] * ss.Cb[(size_t)i * N + k] * ss.Cb[(size_t)j * N + k];
+      const size_t ij = (size_t)i * N + j;
+      Wm[ij] = s - st.shift[ij] * st.P[ij] - ss.spinC[ij] * (ss.Pa[ij] - ss.Pb[ij]);
+    }
+  gradient_with(M, st, Wm, g);
 }
 
 // Linear-response TD-DFTB (restricted reference, singlets or triplets, the
@@ -902,6 +1121,38 @@ int dftb_oracle_scf(const char* set, int order, int nat, const int* Z, const dou
   if (want_grad && grad) {
     std::vector<double> g;
     gradient(M, st, g);
+    std::memcpy(grad, g.data(), sizeof(double) * g.size());
+  }
+  return st.converged ? 0 : 3;
+}
+
+// Spin-polarised (unrestricted) DFTB2/3 single point with spin multiplicity
+// mult.  info[8] = {E_el, E_rep, iterations, converged, nao, n_alpha, n_beta,
+// E_spin}; q_out (Mulliken charges), eps_a / eps_b (nao) optional.
+int dftb_oracle_scf_uhf(const char* set, int order, int nat, const int* Z, const double* xyz, int charge, int mult,
+                        double scc, double rmsd, int max_iter, int want_grad, double* energy, double* grad,
+                        double* info, double* q_out, double* eps_a, double* eps_b) {
+  using namespace dftb_oracle;
+  Mol M;
+  if (mult < 1 || !setup(set, order, nat, Z, xyz, charge, M, mult)) {
+    if (mult < 1) g_error = "spin multiplicity must be positive";
+    return 1;
+  }
+  State st;
+  SpinState ss;
+  if (!scf_uhf(M, st, ss, scc, rmsd, max_iter)) return 2;
+  if (energy) *energy = st.e_el + st.e_rep;
+  if (info) {
+    double v[8] = {st.e_el, st.e_rep, (double)st.iterations, st.converged ? 1.0 : 0.0, (double)M.nao,
+                   (double)M.nalpha, (double)M.nbeta, ss.e_spin};
+    std::memcpy(info, v, sizeof(v));
+  }
+  if (q_out) std::memcpy(q_out, st.q.data(), sizeof(double) * M.nat);
+  if (eps_a) std::memcpy(eps_a, ss.epsa.data(), sizeof(double) * M.nao);
+  if (eps_b) std::memcpy(eps_b, ss.epsb.data(), sizeof(double) * M.nao);
+  if (want_grad && grad) {
+    std::vector<double> g;
+    gradient_uhf(M, st, ss, g);
     std::memcpy(grad, g.data(), sizeof(double) * g.size());
   }
   return st.converged ? 0 : 3;

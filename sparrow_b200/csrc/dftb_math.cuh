@@ -29,8 +29,9 @@ struct DftbElemDev {
   int Z, nao;
   double es, ep, U, occ, hd;
   double w;    // atomically resolved spin constant (W_pp, or W_ss for s-only atoms)
-  int has_w;   // spin constant available (triplet excitations)
+  int has_w;   // spin constants available (triplet excitations, spin-polarised SCC)
   int pad;
+  double wss, wsp, wps, wpp;  // shell-resolved spin constants W(l, l') (SDFTB.cpp, SKAtom.h:52-66)
 };
 
 // Parameters of an ordered element pair (file Z1-Z2): its completed integral

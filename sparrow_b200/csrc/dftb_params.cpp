@@ -98,6 +98,10 @@ bool dftb_prepare(const std::string& set, int order, const std::vector<int>& Zs,
     d.w = nao == 1 ? e->wss : e->wpp;  // SKAtom.h:94-102
     d.has_w = e->has_spin;
     d.pad = 0;
+    d.wss = e->wss;
+    d.wsp = e->wsp;
+    d.wps = e->wps;
+    d.wpp = e->wpp;
   }
   out.pairs.assign(kMaxElementSlots * kMaxElementSlots, DftbPairDev());
   out.table.clear();

@@ -12,8 +12,9 @@ struct DftbElemRaw {
   double fs, fp, fd;     // occupations of the neutral atom
   double hubbard_derivative;
   int has_hubbard_derivative;
-  double wss, wpp;       // spin constants (spin.dat) for triplet excitations
+  double wss, wpp;       // spin constants (spin.dat): triplet excitations, spin-polarised SCC
   int has_spin;
+  double wsp, wps;       // the s-p spin constants (spin-polarised SCC)
 };
 
 struct DftbPairRaw {

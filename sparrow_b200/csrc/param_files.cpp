@@ -663,7 +663,7 @@ bool load_skf_directory(const std::string& dir, DftbSetData& set, std::string& e
   set.name = dir;
   // Hubbard derivatives and spin constants (SkfParser.cpp:255-330)
   std::map<int, double> hubbard;
-  std::map<int, std::pair<double, double>> spin;
+  std::map<int, std::array<double, 4>> spin;  // W_ss, W_sp, W_ps, W_pp
   std::string text;
   if (read_file(dir + "/hubbard.dat", text)) {
     std::istringstream ss(text);
@@ -693,7 +693,7 @@ bool load_skf_directory(const std::string& dir, DftbSetData& set, std::string& e
         return false;
       }
       // order W00 W01 W10 W11 W02 W12 W22 W20 W21: s-s and p-p are the first and fourth
-      if (int z = symbol_to_z(sym)) spin[z] = {w[0], w[3]};
+      if (int z = symbol_to_z(sym)) spin[z] = {w[0], w[1], w[2], w[3]};
     }
   }
   // elements: those with a homonuclear file carrying atomic parameters
@@ -724,8 +724,10 @@ bool load_skf_directory(const std::string& dir, DftbSetData& set, std::string& e
     e.hubbard_derivative = e.has_hubbard_derivative ? h->second : 0.0;
     auto s = spin.find(z);
     e.has_spin = s != spin.end();
-    e.wss = e.has_spin ? s->second.first : 0.0;
-    e.wpp = e.has_spin ? s->second.second : 0.0;
+    e.wss = e.has_spin ? s->second[0] : 0.0;
+    e.wsp = e.has_spin ? s->second[1] : 0.0;
+    e.wps = e.has_spin ? s->second[2] : 0.0;
+    e.wpp = e.has_spin ? s->second[3] : 0.0;
     set.elems.push_back(e);
     zs.push_back(z);
   }

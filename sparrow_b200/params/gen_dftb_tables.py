@@ -125,17 +125,18 @@ def main():
             for line in open(sp_path):
                 t = line.split()
                 if len(t) >= 5 and not t[0].startswith("#"):
-                    spin[t[0]] = (t[1], t[4])
+                    spin[t[0]] = (t[1], t[4], t[2], t[3])  # W_ss, W_pp, W_sp, W_ps
         e0, p0 = len(elems), len(pairs)
         for a in ELEMENTS:
             for b in ELEMENTS:
                 r = parse_skf(os.path.join(d, "%s-%s.skf" % (a, b)), a == b)
                 if a == b:
                     Ed, Ep, Es, SPE, Ud, Up, Us, fd, fp, fs = r["atomic"]
-                    wss, wpp = spin.get(a, ("0.0", "0.0"))
-                    elems.append("{%d, %s, %s, %s, %s, %s, %s, %s, %s, %s, %s, %d, %s, %s, %d}" % (
+                    wss, wpp, wsp, wps = spin.get(a, ("0.0", "0.0", "0.0", "0.0"))
+                    elems.append("{%d, %s, %s, %s, %s, %s, %s, %s, %s, %s, %s, %d, %s, %s, %d, %s, %s}" % (
                         Z[a], lit(Es), lit(Ep), lit(Ed), lit(Us), lit(Up), lit(Ud), lit(fs), lit(fp), lit(fd),
-                        lit(hub.get(a, "0.0")), 1 if a in hub else 0, lit(wss), lit(wpp), 1 if a in spin else 0))
+                        lit(hub.get(a, "0.0")), 1 if a in hub else 0, lit(wss), lit(wpp), 1 if a in spin else 0,
+                        lit(wsp), lit(wps)))
                 t0, s0 = len(table), len(spl)
                 for row in r["table"]:
                     table.append(", ".join(lit(row[c]) for c in KEEP))
@@ -150,7 +151,7 @@ def main():
         f.write("// Generated by sparrow_b200/params/gen_dftb_tables.py from the reference's DFTB\n")
         f.write("// parameter sets (Resources/Dftb/{%s}); do not edit.\n" % ",".join(SETS))
         f.write("// Elements: Z, Es, Ep, Ed, Us, Up, Ud, fs, fp, fd, Hubbard derivative, has it,\n")
-        f.write("// spin constants W_ss, W_pp, has them.\n")
+        f.write("// spin constants W_ss, W_pp, has them, W_sp, W_ps.\n")
         f.write("static const DftbElemRaw kDftbElemRaw[] = {\n  %s};\n" % ",\n  ".join(elems))
         f.write("// Pairs (file Z1-Z2): Z1, Z2, grid distance, rows, first row, spline count, cutoff,\n")
         f.write("// a1, a2, a3, c4, c5, first spline.\n")

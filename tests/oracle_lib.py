@@ -241,6 +241,34 @@ def dftb_scf(order, Z, xyz_bohr, charge=0, parameters=None, scc=1e-7, rmsd=1e-8,
     return out
 
 
+def dftb_scf_uhf(order, Z, xyz_bohr, multiplicity, charge=0, parameters=None, scc=1e-9, rmsd=1e-9, max_iter=1000,
+                 gradient=True):
+    """Converged spin-polarised DFTB2/DFTB3: dict(energy, gradient, e_el, e_rep, e_spin, iterations, converged,
+    nao, n_alpha, n_beta, charges, eps_alpha, eps_beta)."""
+    Z, x = _arr(Z, xyz_bohr)
+    n = len(Z)
+    params = parameters or DFTB_DEFAULT_SET[order]
+    e = ctypes.c_double()
+    g = np.zeros(x.size)
+    info = np.zeros(8)
+    q = np.zeros(n)
+    ea, eb = np.zeros(4 * n), np.zeros(4 * n)
+    L = dftb_lib()
+    L.dftb_oracle_scf_uhf.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _I, _D, ctypes.c_int,
+                                      ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, _D,
+                                      _D, _D, _D, _D, _D]
+    rc = L.dftb_oracle_scf_uhf(params.encode(), order, n, Z.ctypes.data_as(_I), x.ctypes.data_as(_D), int(charge),
+                               int(multiplicity), scc, rmsd, max_iter, 1 if gradient else 0, ctypes.byref(e),
+                               g.ctypes.data_as(_D), info.ctypes.data_as(_D), q.ctypes.data_as(_D),
+                               ea.ctypes.data_as(_D), eb.ctypes.data_as(_D))
+    if rc not in (0, 3):
+        raise RuntimeError(L.dftb_oracle_last_error().decode())
+    nao = int(info[4])
+    return dict(energy=e.value, gradient=g.reshape(-1, 3), e_el=info[0], e_rep=info[1], e_spin=info[7],
+                iterations=int(info[2]), converged=bool(info[3]), nao=nao, n_alpha=int(info[5]), n_beta=int(info[6]),
+                charges=q, eps_alpha=ea[:nao], eps_beta=eb[:nao])
+
+
 def dftb_matrices(order, Z, xyz_bohr, parameters=None):
     """H0, S (N x N), gamma (nat x nat) and Gamma (nat x nat, DFTB3) at a geometry."""
     Z, x = _arr(Z, xyz_bohr)

@@ -165,7 +165,7 @@ def dftb_embedded(set_name):
         out["elems"][z] = {"Es": float(f[1]), "Ep": float(f[2]), "Ed": float(f[3]), "Us": float(f[4]),
                            "Up": float(f[5]), "Ud": float(f[6]), "fs": float(f[7]), "fp": float(f[8]),
                            "fd": float(f[9]), "hub": float(f[10]), "has_hub": int(f[11]), "wss": float(f[12]),
-                           "wpp": float(f[13]), "has_spin": int(f[14])}
+                           "wpp": float(f[13]), "has_spin": int(f[14]), "wsp": float(f[15]), "wps": float(f[16])}
     for p in pairs[p0:p0 + npair]:
         f = [t.strip() for t in p]
         z1, z2, rows, row0, nspl, sp0 = int(f[0]), int(f[1]), int(f[3]), int(f[4]), int(f[5]), int(f[12])
@@ -255,5 +255,6 @@ def write_skf_directory(path, set_name, elements=None, hubbard=True, spin=True, 
             for z in zs:
                 e = d["elems"][z]
                 if e["has_spin"]:
-                    f.write("%s %s 0.0 0.0 %s 0.0 0.0 0.0 0.0 0.0\n" % (SYMBOL[z], _num(e["wss"]), _num(e["wpp"])))
+                    f.write("%s %s %s %s %s 0.0 0.0 0.0 0.0 0.0\n" % (SYMBOL[z], _num(e["wss"]), _num(e["wsp"]),
+                                                                      _num(e["wps"]), _num(e["wpp"])))
     return d
