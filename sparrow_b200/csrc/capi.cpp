@@ -104,6 +104,7 @@ class Calculator {
     sp.rmsd = settings_.rmsd;
     sp.max_iter = settings_.max_iter;
     sp.diis_size = settings_.mixer == "diis" ? kDiisMax : 1;
+    sp.canonical = 1;  // results report orbital energies
     std::vector<MoleculeInput> in(1);
     in[0].Z = Z_;
     in[0].xyz = xyz_;

@@ -159,10 +159,6 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
     err = "empty batch";
     return kErrEmptyStructure;
   }
-  if (uhf_ && is_dftb(method_)) {
-    err = "unrestricted (spin-polarised) DFTB is not supported; the unrestricted SCF covers MNDO, AM1 and PM6";
-    return kErrInvalidArgument;
-  }
   nddo_set_.reset();
   if (!is_dftb(method_) && !param_source_.empty()) {
     nddo_set_ = nddo_parameter_set(method_, param_source_, err);
@@ -220,6 +216,12 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
     for (const auto& e : elems_) zs.push_back(e.Z);
     const std::string set = param_source_.empty() ? dftb_default_set(method_) : param_source_;
     if (!dftb_prepare(set, method_ == kDFTB3 ? 3 : 2, zs, dftb, err)) return kErrUnsupportedElement;
+    if (uhf_)
+      for (const auto& e : dftb.elems)
+        if (!e.has_w) {
+          err = "spin-polarised DFTB needs spin constants (spin.dat) for element Z=" + std::to_string(e.Z);
+          return kErrUnsupportedElement;
+        }
   }
   for (size_t i = 0; i < elems_.size() && !is_dftb(method_); ++i)
     for (size_t j = 0; j < elems_.size(); ++j) {
@@ -385,7 +387,7 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
   const size_t o_rot = take(scf_rotation_bytes_per_cta() * (size_t)grid_eff);
   const size_t o_res = take(sizeof(MolResult) * mols_.size());
   const size_t mat_dftb = dftb_batch ? mat_bytes : sizeof(double);
-  const size_t o_S = take(mat_dftb), o_X = take(mat_dftb), o_Pp = take(mat_dftb);
+  const size_t o_S = take(mat_dftb), o_X = take(mat_dftb), o_Pp = take(mat_dftb), o_W3 = take(mat_dftb);
   const size_t gam_bytes = sizeof(double) * (dftb_batch ? std::max<long long>(gam_off, 1) : 1);
   const size_t o_gam = take(gam_bytes);
   const size_t o_Gam = take(method_ == kDFTB3 ? gam_bytes : sizeof(double));
@@ -396,6 +398,9 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
   const size_t o_Pa = take(mat_uhf), o_Pb = take(mat_uhf), o_Fb = take(mat_uhf), o_Cb = take(mat_uhf);
   const size_t o_epsb = take(uhf_ ? sizeof(double) * (size_t)ao_base : sizeof(double));
   const size_t o_diisb = take(uhf_ ? sizeof(double) * (size_t)diis_off : sizeof(double));
+  const bool uhf_dftb = uhf_ && dftb_batch;  // spin-polarised DFTB: beta orthogonal-basis density, shell shifts
+  const size_t o_Ppb = take(uhf_dftb ? mat_bytes : sizeof(double));
+  const size_t o_sshift = take(sizeof(double) * 2 * (uhf_dftb ? atoms_.size() : 1));
   int rc = ensure_arena(off, err);
   if (rc) return rc;
   rc = ensure_terms(stream_, err);
@@ -431,6 +436,7 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
   d.S = reinterpret_cast<double*>(base + o_S);
   d.X = reinterpret_cast<double*>(base + o_X);
   d.Pp = reinterpret_cast<double*>(base + o_Pp);
+  d.W3 = reinterpret_cast<double*>(base + o_W3);
   d.gam = reinterpret_cast<double*>(base + o_gam);
   d.Gam = reinterpret_cast<double*>(base + o_Gam);
   d.qat = reinterpret_cast<double*>(base + o_qat);
@@ -443,6 +449,10 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
     d.Cb = reinterpret_cast<double*>(base + o_Cb);
     d.epsb = reinterpret_cast<double*>(base + o_epsb);
     d.diisb = reinterpret_cast<double*>(base + o_diisb);
+    if (uhf_dftb) {
+      d.Ppb = reinterpret_cast<double*>(base + o_Ppb);
+      d.sshift = reinterpret_cast<double*>(base + o_sshift);
+    }
   }
   if (dftb_batch) {
     d.dftb_order = method_ == kDFTB3 ? 3 : 2;
@@ -615,6 +625,10 @@ int Batch::run(const ScfParams& sp_in, bool gradient, std::string& err) {
     cudaEventRecord(stage_ev_[2], stream_);
     launch_dftb_scf(dev_, sp, dev_.scf_grid, stream_);
     launches_ += 1;
+    if (sp.canonical) {
+      launch_dftb_canonical(dev_, sp, dev_.scf_grid, stream_);
+      launches_ += 1;
+    }
     cudaEventRecord(stage_ev_[3], stream_);
     if (gradient) {
       launch_dftb_gradient(dev_, stream_);
@@ -670,6 +684,10 @@ int Batch::run(const ScfParams& sp_in, bool gradient, std::string& err) {
       if (uhf_) launch_uhf_scf(dev_, sp, dev_.scf_grid, stream_);
       else launch_scf(dev_, sp, dev_.scf_grid, stream_);
       launches_ += 1;
+      if (sp.canonical) {
+        launch_canonical(dev_, sp, dev_.scf_grid, stream_);
+        launches_ += 1;
+      }
     }
     cudaEventRecord(stage_ev_[3], stream_);
     if (gradient) {
@@ -728,8 +746,8 @@ int Batch::run_tddftb(int nroots, bool triplet, double tol, int max_iter, std::s
     err = "no structure";
     return kErrEmptyStructure;
   }
-  if (!is_dftb(method_)) {
-    err = "TD-DFTB needs a DFTB2 or DFTB3 reference";
+  if (!is_dftb(method_) || uhf_) {
+    err = "TD-DFTB needs a restricted DFTB2 or DFTB3 reference";
     return kErrInvalidArgument;
   }
   if (!stages_recorded_) {

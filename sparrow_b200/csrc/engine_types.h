@@ -108,6 +108,12 @@ struct ScfParams {
   // 3: the rotations converge the rest cheaper than more sweeps; DFTB 6: the
   // small gaps of conjugated chains need the better start)
   int cold_sweeps = 0;
+  // 1: after convergence, diagonalise the final Fock matrix from the current
+  // orbitals (a warm Jacobi), so the orbital energies are its eigenvalues.
+  // The occupied-virtual rotation leaves the occupied-occupied and
+  // virtual-virtual blocks unrotated, which changes no density or energy but
+  // leaves the individual orbital energies as diagonal elements.
+  int canonical = 0;
   // large-molecule mixed-precision path: purification switches from split-BF16
   // to FP64 once rms(Delta P) falls below this (or stops halving below 1e-4)
   double mixed_switch_rmsd = 1e-5;

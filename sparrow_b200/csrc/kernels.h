@@ -60,6 +60,8 @@ struct DeviceBatch {
   double* Cb = nullptr;             // [mat_total] beta orbitals (orbital-major)
   double* epsb = nullptr;           // [nao_total] beta orbital energies
   double* diisb = nullptr;          // [diis_total] beta DIIS ring
+  double* Ppb = nullptr;            // [mat_total] DFTB: beta density in the orthogonal basis
+  double* sshift = nullptr;         // [natoms * 2] DFTB: shell spin shifts eps_{a,s}, eps_{a,p}
   int use_guess = 1;                // 0: P already holds a start density
   int large = 0;                    // 1: one molecule over the whole GPU (large-molecule path)
   void* large_scratch = nullptr;    // [large_scf_scratch_bytes(nao)] when large
@@ -69,6 +71,7 @@ struct DeviceBatch {
   double* S = nullptr;              // [mat_total] overlap
   double* X = nullptr;              // [mat_total] S^-1/2
   double* Pp = nullptr;             // [mat_total] density in the orthogonal basis
+  double* W3 = nullptr;             // [mat_total] scratch of the canonical-orbital pass (F, W1 stay intact)
   double* gam = nullptr;            // [gam_total] gamma (nat x nat per molecule)
   double* Gam = nullptr;            // [gam_total] Gamma (DFTB3)
   double* qat = nullptr;            // [natoms] Mulliken charges
@@ -96,6 +99,10 @@ void launch_fock_grid(const DeviceBatch& b, const double* P, double* F, double* 
 // DFTB: pair and on-site terms (+ start density), SCC loop, gradient
 void launch_dftb_setup(const DeviceBatch& b, cudaStream_t s);
 void launch_dftb_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s);
+// Canonical orbitals after convergence (ScfParams::canonical): warm
+// diagonalisations of the final Fock matrices left by the SCF kernels.
+void launch_canonical(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s);
+void launch_dftb_canonical(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s);
 void launch_dftb_gradient(const DeviceBatch& b, cudaStream_t s);
 // Large-molecule SCF of the batch's single molecule m (host-driven grid
 // kernels, SP2 density): precision 0 FP64, 1 mixed (split-BF16 SP2 products

@@ -439,6 +439,266 @@ __global__ void __launch_bounds__(64) k_dftb_gradient(const PairDev* __restrict_
   for (int k = 0; k < 3; ++k) gpair[(size_t)p * 3 + k] = d[k] + coef * R[k] / dist;
 }
 
+// ---------------------------------------------------------------------------
+// Spin-polarised (unrestricted) DFTB, Utils/SDFTB.cpp:64-293 and
+// Utils/ScfFock.cpp:50-103: the spin Fock matrices are the restricted SCC
+// Fock matrix of the total density plus / minus spinC o S,
+//   spinC_mu,nu = 1/2 (eps_{a(mu),l(mu)} + eps_{b(nu),l(nu)}),
+//   eps_{a,l} = sum_l' W_a(l, l') pdif_{a,l'},
+//   pdif_{a,l} = sum_{mu in (a, l)} sum_nu (P_a - P_b)_mu,nu S_mu,nu,
+// with the energy 1/2 sum_a sum_{l,l'} pdif_{a,l} W_a(l, l') pdif_{a,l'}.
+// ---------------------------------------------------------------------------
+// Shell shifts eps_{a,s}, eps_{a,p} of the molecule's atoms into sps (2 per
+// atom); pop: N doubles of scratch.  Returns the spin energy.
+__device__ double dftb_spin_shifts(const MolDev& m, const AtomDev* __restrict__ atoms,
+                                   const DftbElemDev* __restrict__ el, const double* Pa, const double* Pb,
+                                   const double* S, double* pop, double* sps, double* red) {
+  const int N = m.nao;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  for (int i = warp; i < N; i += nwarps) {
+    double s = 0;
+    for (int j = lane; j < N; j += 32) {
+      const size_t ij = (size_t)i * N + j;
+      s += (Pa[ij] - Pb[ij]) * S[ij];
+    }
+    s = warp_sum(s);
+    if (lane == 0) pop[i] = s;
+  }
+  __syncthreads();
+  double e = 0;
+  for (int a = tid; a < m.nat; a += blockDim.x) {
+    const AtomDev A = atoms[m.atom0 + a];
+    const DftbElemDev& E = el[A.slot];
+    const double ps = pop[A.ao0];
+    const double pp = E.nao == 4 ? pop[A.ao0 + 1] + pop[A.ao0 + 2] + pop[A.ao0 + 3] : 0.0;
+    const double es = E.wss * ps + E.wsp * pp, ep = E.wps * ps + E.wpp * pp;
+    sps[2 * a] = es;
+    sps[2 * a + 1] = ep;
+    e += 0.5 * (ps * es + pp * ep);
+  }
+  __syncthreads();
+  return cta_sum(e, red);
+}
+
+// spinC of AO pair (u, v) from the shell shifts
+__device__ __forceinline__ double dftb_spin_c(const MolDev& m, const AtomDev* __restrict__ atoms,
+                                              const int* __restrict__ ao_atom, const double* sps, int u, int v) {
+  const int A = ao_atom[m.ao_base + u], B = ao_atom[m.ao_base + v];
+  const double eu = sps[2 * (A - m.atom0) + (u == atoms[A].ao0 ? 0 : 1)];
+  const double ev = sps[2 * (B - m.atom0) + (v == atoms[B].ao0 ? 0 : 1)];
+  return 0.5 * (eu + ev);
+}
+
+__global__ void __launch_bounds__(kScfThreads, 1) k_dftb_uhf_scf(
+    const MolDev* __restrict__ mols, int nmol, const int* __restrict__ order_list, int* counter,
+    const AtomDev* __restrict__ atoms, const DftbElemDev* __restrict__ el, const int* __restrict__ ao_atom,
+    const double* __restrict__ H0all, const double* __restrict__ Sall, double* Xall, double* Pall, double* Ppall,
+    double* Fall, double* Call, double* W1all, double* W2all, double* epsall, double* diisall, double* Paall,
+    double* Pball, double* Ppball, double* Fball, double* Cball, double* epsball, double* diisball, double* sshall,
+    double* rotbuf, const double* __restrict__ gamall, const double* __restrict__ Gamall, double* qall, double* shall,
+    MolResult* res, ScfParams sp, int packed_in_smem, int order) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ScfShared& sh = *reinterpret_cast<ScfShared*>(smem_raw);
+  double* smemA = reinterpret_cast<double*>(smem_raw + ((sizeof(ScfShared) + 15) / 16) * 16);
+  const int tid = threadIdx.x;
+  while (true) {
+    if (tid == 0) sh.mol = atomicAdd(counter, 1);
+    __syncthreads();
+    const int slot = sh.mol;
+    __syncthreads();
+    if (slot >= nmol) break;
+    const int mi = order_list[slot];
+    const MolDev m = mols[mi];
+    const int N = m.nao, na = m.nocc, nb = m.nocc_b;
+    const size_t NN = (size_t)N * N;
+    const double* H0 = H0all + m.mat_off;
+    const double* S = Sall + m.mat_off;
+    double* X = Xall + m.mat_off;
+    double* P = Pall + m.mat_off;
+    double* Pa = Paall + m.mat_off;
+    double* Pb = Pball + m.mat_off;
+    double* Ppa = Ppall + m.mat_off;
+    double* Ppb = Ppball + m.mat_off;
+    double* Fa = Fall + m.mat_off;
+    double* Fb = Fball + m.mat_off;
+    double* Ca = Call + m.mat_off;
+    double* Cb = Cball + m.mat_off;
+    double* W1 = W1all + m.mat_off;
+    double* W2 = W2all + m.mat_off;
+    double* epsa = epsall + m.ao_base;
+    double* epsb = epsball + m.ao_base;
+    double* histFa = diisall + m.diis_off;
+    double* histEa = histFa + (size_t)kDiisMax * NN;
+    double* histFb = diisball + m.diis_off;
+    double* histEb = histFb + (size_t)kDiisMax * NN;
+    const double* gm = gamall + m.gam_off;
+    const double* Gm = Gamall + (order == 3 ? m.gam_off : 0);
+    double* q = qall + m.atom0;
+    double* sh4 = shall + 4 * (size_t)m.atom0;
+    double* sps = sshall + 2 * (size_t)m.atom0;
+    double* Apk = packed_in_smem ? smemA : nullptr;
+    const size_t packed_bytes = sizeof(double) * (size_t)N * (N + 1) / 2;
+    double* rot = rotbuf + (size_t)blockIdx.x * (kRotBudgetBytes / sizeof(double));
+    const int cap_rounds = (int)((kRotBudgetBytes / sizeof(double)) / (2 * ((N + 1) / 2)));
+    const int msize = sp.diis_size < 1 ? 1 : (sp.diis_size > kDiisMax ? kDiisMax : sp.diis_size);
+    const int cold_sweeps = sp.cold_sweeps > 0 ? sp.cold_sweeps : 6;
+    int status = kDevOk;
+    const int ns_it = inverse_sqrt(N, S, X, W1, Fa, Ca, W2, sh);
+    if (ns_it < 0) status = kDevNonFinite;
+    for (size_t k = tid; k < NN; k += blockDim.x) Pa[k] = Pb[k] = 0.5 * P[k];
+    __syncthreads();
+    int nhist = 0, head = 0, it = 0, converged = 0, nfull = 0, nsweeps = 0;
+    bool have_a = false, have_b = false;
+    double drift_a = 0, drift_b = 0, Eold = 0, last_dE = 0, last_rms = 0;
+    for (it = 1; it <= sp.max_iter && status == kDevOk; ++it) {
+      const double e23 = charges_and_shifts(m, order, atoms, el, P, S, gm, Gm, W2, q, sh4, sh.red);
+      const double eb = dftb_fock(m, ao_atom, H0, S, P, sh4, Fa, sh.red);
+      const double es = dftb_spin_shifts(m, atoms, el, Pa, Pb, S, W2, sps, sh.red);
+      for (size_t k = tid; k < NN; k += blockDim.x) {
+        const int u = (int)(k / N), v = (int)(k % N);
+        const double c = dftb_spin_c(m, atoms, ao_atom, sps, u, v) * S[k];
+        const double fr = Fa[k];
+        Fa[k] = fr + c;
+        Fb[k] = fr - c;
+      }
+      __syncthreads();
+      const double E = eb + e23 + es;
+      // F'_s = X F_s X
+      cta_gemm(N, N, N, 1.0, Fa, N, false, X, N, false, 0.0, W1, N, sh.gemm);
+      cta_gemm(N, N, N, 1.0, X, N, false, W1, N, false, 0.0, Fa, N, sh.gemm);
+      cta_gemm(N, N, N, 1.0, Fb, N, false, X, N, false, 0.0, W1, N, sh.gemm);
+      cta_gemm(N, N, N, 1.0, X, N, false, W1, N, false, 0.0, Fb, N, sh.gemm);
+      if (have_a && have_b)
+        diis_step_uhf(N, Fa, Ppa, Fb, Ppb, W1, histFa, histEa, histFb, histEb, msize, nhist, head, sh);
+      const bool warm_a = have_a, warm_b = have_b;
+      int sw = uhf_orbitals(N, na, Fa, Ca, W1, W2, epsa, Apk, packed_bytes, have_a, drift_a, rot, cap_rounds, sp,
+                            cold_sweeps, nfull, sh);
+      if (sw < 0 && warm_a) status = kDevJacobiNotConverged;
+      nsweeps += sw < 0 ? -sw : sw;
+      sw = uhf_orbitals(N, nb, Fb, Cb, W1, W2, epsb, Apk, packed_bytes, have_b, drift_b, rot, cap_rounds, sp,
+                        cold_sweeps, nfull, sh);
+      if (sw < 0 && warm_b) status = kDevJacobiNotConverged;
+      nsweeps += sw < 0 ? -sw : sw;
+      // P'_s = C'_occ C'_occ^T, P_s = X P'_s X; rms of the AO spin densities
+      double d2max = 0;
+      for (int spin = 0; spin < 2; ++spin) {
+        double* Pps = spin ? Ppb : Ppa;
+        double* Ps = spin ? Pb : Pa;
+        uhf_density(N, spin ? nb : na, spin ? Cb : Ca, Pps, W1, sh);
+        cta_gemm(N, N, N, 1.0, X, N, false, Pps, N, false, 0.0, W1, N, sh.gemm);
+        cta_gemm(N, N, N, 1.0, W1, N, false, X, N, false, 0.0, W2, N, sh.gemm, true);
+        double d2 = 0;
+        for (size_t k = tid; k < NN; k += blockDim.x) {
+          const double d = W2[k] - Ps[k];
+          d2 += d * d;
+          Ps[k] = W2[k];
+        }
+        d2max = fmax(d2max, cta_sum(d2, sh.red));
+      }
+      for (size_t k = tid; k < NN; k += blockDim.x) P[k] = Pa[k] + Pb[k];
+      __syncthreads();
+      const double rms = sqrt(d2max / (double)NN);
+      last_rms = rms;
+      last_dE = it > 1 ? fabs(E - Eold) : 0.0;
+      const bool dE_ok = it > 1 && fabs(E - Eold) < sp.scc;
+      Eold = E;
+      if (!isfinite(E) || !isfinite(rms)) {
+        status = kDevNonFinite;
+        break;
+      }
+      if (dE_ok && rms < sp.rmsd) {
+        converged = 1;
+        break;
+      }
+    }
+    if (it > sp.max_iter) it = sp.max_iter;
+    __syncthreads();
+    // final charges, spin Fock matrices and energy of the converged densities;
+    // the gradient's overlap multiplier into W1:
+    //   P_a F_a P_a + P_b F_b P_b - spinC o (P_a - P_b)
+    // (energy-weighted densities; SDFTB.cpp:60-83 adds 2 (P_a - P_b) spinC dS)
+    const double e23 = charges_and_shifts(m, order, atoms, el, P, S, gm, Gm, W2, q, sh4, sh.red);
+    const double eb = dftb_fock(m, ao_atom, H0, S, P, sh4, Fa, sh.red);
+    const double es = dftb_spin_shifts(m, atoms, el, Pa, Pb, S, W2, sps, sh.red);
+    for (size_t k = tid; k < NN; k += blockDim.x) {
+      const int u = (int)(k / N), v = (int)(k % N);
+      const double c = dftb_spin_c(m, atoms, ao_atom, sps, u, v) * S[k];
+      const double fr = Fa[k];
+      Fa[k] = fr + c;
+      Fb[k] = fr - c;
+    }
+    __syncthreads();
+    cta_gemm(N, N, N, 1.0, Fa, N, false, Pa, N, false, 0.0, W2, N, sh.gemm);
+    cta_gemm(N, N, N, 1.0, Pa, N, false, W2, N, false, 0.0, W1, N, sh.gemm, true);
+    cta_gemm(N, N, N, 1.0, Fb, N, false, Pb, N, false, 0.0, W2, N, sh.gemm);
+    cta_gemm(N, N, N, 1.0, Pb, N, false, W2, N, false, 1.0, W1, N, sh.gemm, true);
+    for (size_t k = tid; k < NN; k += blockDim.x) {
+      const int u = (int)(k / N), v = (int)(k % N);
+      W1[k] -= dftb_spin_c(m, atoms, ao_atom, sps, u, v) * (Pa[k] - Pb[k]);
+    }
+    __syncthreads();
+    if (tid == 0) {
+      MolResult& r = res[mi];
+      r.e_el = eb + e23 + es;
+      r.energy = r.e_el + r.e_rep;
+      r.iterations = it;
+      r.converged = converged;
+      r.status = status;
+      r.last_dE = last_dE;
+      r.last_rmsd = last_rms;
+      r.full_diag = nfull;
+      r.jacobi_sweeps = nsweeps;
+      r.cycles[0] = ns_it;
+    }
+    __syncthreads();
+  }
+}
+
+// Canonical orbitals after a DFTB convergence (ScfParams::canonical): F' =
+// X F X of each spin's final Fock matrix (left in F / Fb by the SCC kernels)
+// into the orthogonal-basis density buffer (free after convergence), then a
+// warm diagonalisation with W2 and W3 as scratch.  F / Fb (read by TD-DFTB)
+// and W1 (the gradient's energy-weighted density) stay intact.
+__global__ void __launch_bounds__(kScfThreads, 1) k_dftb_canonical(
+    const MolDev* __restrict__ mols, int nmol, const int* __restrict__ order_list, int* counter,
+    const double* __restrict__ Xall, const double* __restrict__ Fall, double* Call, double* Ppall, double* W2all,
+    double* W3all, double* epsall, const double* __restrict__ Fball, double* Cball, double* Ppball, double* epsball,
+    double* rotbuf, ScfParams sp, int packed_in_smem) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ScfShared& sh = *reinterpret_cast<ScfShared*>(smem_raw);
+  double* smemA = reinterpret_cast<double*>(smem_raw + ((sizeof(ScfShared) + 15) / 16) * 16);
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int k = atomicAdd(counter, 1);
+      sh.mol = k < nmol ? order_list[k] : -1;
+    }
+    __syncthreads();
+    const int mi = sh.mol;
+    __syncthreads();
+    if (mi < 0) return;
+    const MolDev m = mols[mi];
+    const int N = m.nao;
+    const double* X = Xall + m.mat_off;
+    double* W2 = W2all + m.mat_off;
+    double* W3 = W3all + m.mat_off;
+    double* Apk = packed_in_smem ? smemA : nullptr;
+    const size_t packed_bytes = sizeof(double) * (size_t)N * (N + 1) / 2;
+    double* rot = rotbuf + (size_t)blockIdx.x * (kRotBudgetBytes / sizeof(double));
+    const int cap_rounds = (int)((kRotBudgetBytes / sizeof(double)) / (2 * ((N + 1) / 2)));
+    for (int spin = 0; spin < (Fball ? 2 : 1); ++spin) {
+      const double* F = (spin ? Fball : Fall) + m.mat_off;
+      double* Fp = (spin ? Ppball : Ppall) + m.mat_off;
+      cta_gemm(N, N, N, 1.0, F, N, false, X, N, false, 0.0, W2, N, sh.gemm);
+      cta_gemm(N, N, N, 1.0, X, N, false, W2, N, false, 0.0, Fp, N, sh.gemm);
+      full_diagonalise(N, Fp, (spin ? Cball : Call) + m.mat_off, W3, W2, (spin ? epsball : epsall) + m.ao_base,
+                       Apk ? Apk : Fp, Apk ? packed_bytes : 0, true, rot, cap_rounds, sp.jacobi_max_sweeps, 1e-10,
+                       sh);
+    }
+    __syncthreads();
+  }
+}
+
+
 size_t dftb_smem_bytes(int max_nao, int* packed_in_smem) {
   const size_t base = ((sizeof(ScfShared) + 15) / 16) * 16;
   const size_t pk = sizeof(double) * (size_t)max_nao * (max_nao + 1) / 2;
@@ -466,6 +726,18 @@ void launch_dftb_setup(const DeviceBatch& b, cudaStream_t s) {
                                        b.Gam, b.P, b.res, b.use_guess);
 }
 
+void launch_dftb_canonical(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s) {
+  if (b.nmol == 0) return;
+  int in_smem = 0;
+  const size_t bytes = dftb_smem_bytes(b.max_nao, &in_smem);
+  cudaFuncSetAttribute(k_dftb_canonical, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaMemsetAsync(b.counter, 0, sizeof(int), s);
+  if (grid > b.nmol) grid = b.nmol;
+  k_dftb_canonical<<<grid, kScfThreads, bytes, s>>>(b.mols, b.nmol, b.order, b.counter, b.X, b.F, b.C, b.Pp, b.W2,
+                                                    b.W3, b.eps, b.uhf ? b.Fb : nullptr, b.Cb, b.Ppb, b.epsb,
+                                                    b.rotbuf, sp, in_smem);
+}
+
 void launch_dftb_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s) {
   if (b.nmol == 0) return;
   int in_smem = 0;
@@ -473,6 +745,14 @@ void launch_dftb_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaSt
   cudaFuncSetAttribute(k_dftb_scf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
   cudaMemsetAsync(b.counter, 0, sizeof(int), s);
   if (grid > b.nmol) grid = b.nmol;
+  if (b.uhf) {
+    cudaFuncSetAttribute(k_dftb_uhf_scf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    k_dftb_uhf_scf<<<grid, kScfThreads, bytes, s>>>(
+        b.mols, b.nmol, b.order, b.counter, b.atoms, b.delems, b.ao_atom, b.H, b.S, b.X, b.P, b.Pp, b.F, b.C, b.W1,
+        b.W2, b.eps, b.diis, b.Pa, b.Pb, b.Ppb, b.Fb, b.Cb, b.epsb, b.diisb, b.sshift, b.rotbuf, b.gam, b.Gam, b.qat,
+        b.ashift, b.res, sp, in_smem, b.dftb_order);
+    return;
+  }
   k_dftb_scf<<<grid, kScfThreads, bytes, s>>>(b.mols, b.nmol, b.order, b.counter, b.atoms, b.delems, b.ao_atom, b.H,
                                               b.S, b.X, b.P, b.Pp, b.F, b.C, b.W1, b.W2, b.eps, b.diis, b.rotbuf,
                                               b.gam, b.Gam, b.qat, b.ashift, b.res, sp, in_smem, b.dftb_order);

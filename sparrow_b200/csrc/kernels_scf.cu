@@ -582,45 +582,6 @@ __device__ double spin_exchange(const MolDev& m, const AtomDev* __restrict__ ato
   return cta_sum(e, red);
 }
 
-// New orbitals of one spin from its (extrapolated) Fock matrix Fs: the
-// occupied-virtual rotation of the previous orbitals, or a full
-// diagonalisation at the start, when the rotation asks for one, and when
-// the spin has no occupied or no virtual orbitals.  Returns the Jacobi
-// sweeps of a full diagonalisation (0 when none ran, < 0 when it did not
-// converge).
-__device__ int uhf_orbitals(int N, int ns, double* Fs, double* Cs, double* W1, double* W2, double* epss,
-                            double* Apk, size_t packed_bytes, bool& have, double& drift, double* rot, int cap_rounds,
-                            const ScfParams& sp, int cold_sweeps, int& nfull, ScfShared& sh) {
-  int need_full = !have || ns == 0 || ns == N;
-  if (!need_full) need_full = ov_rotation(N, ns, Fs, Cs, W1, W2, epss, drift, sh);
-  if (!need_full) return 0;
-  const int sw = full_diagonalise(N, Fs, Cs, W1, W2, epss, Apk ? Apk : Fs, Apk ? packed_bytes : 0, have, rot,
-                                  cap_rounds, have ? sp.jacobi_max_sweeps : cold_sweeps, have ? 1e-10 : 1e-3, sh);
-  ++nfull;
-  const bool warm = have;
-  have = true;
-  drift = 0;
-  return sw < 0 ? (warm ? -sp.jacobi_max_sweeps : cold_sweeps) : sw;
-}
-
-// P_s = C_occ C_occ^T of one spin into Ps; returns sum (P_s,new - P_s,old)^2.
-__device__ double uhf_density(int N, int ns, const double* Cs, double* Ps, double* W1, ScfShared& sh) {
-  const size_t NN = (size_t)N * N;
-  if (ns > 0) {
-    cta_gemm(N, N, ns, 1.0, Cs, N, true, Cs, N, false, 0.0, W1, N, sh.gemm, true);
-  } else {
-    for (size_t k = threadIdx.x; k < NN; k += blockDim.x) W1[k] = 0.0;
-    __syncthreads();
-  }
-  double d2 = 0;
-  for (size_t k = threadIdx.x; k < NN; k += blockDim.x) {
-    const double d = W1[k] - Ps[k];
-    d2 += d * d;
-    Ps[k] = W1[k];
-  }
-  return cta_sum(d2, sh.red);
-}
-
 // The persistent kernel of k_scf for unrestricted molecules (MolDev.nocc
 // alpha and MolDev.nocc_b beta electrons): start P_a = P_b = P / 2 from the
 // restricted guess (or a given total density), then per iteration the Fock
@@ -723,6 +684,55 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_uhf_scf(
     }
     __syncthreads();
   }
+}
+
+// Canonical orbitals after convergence (ScfParams::canonical): a warm
+// diagonalisation of the final Fock matrix of each spin from the current
+// orbitals, so the orbital energies are its eigenvalues.  The SCF kernels
+// leave the final Fock matrices in F (and Fb).
+__global__ void __launch_bounds__(kScfThreads, 1) k_canonical(const MolDev* __restrict__ mols, int nmol,
+                                                            const int* __restrict__ order, int* counter, double* Fall,
+                                                            double* Call, double* W1all, double* W2all,
+                                                            double* epsall, double* Fball, double* Cball,
+                                                            double* epsball, double* rotbuf, ScfParams sp,
+                                                            int packed_in_smem) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  ScfShared& sh = *reinterpret_cast<ScfShared*>(smem_raw);
+  double* smemA = reinterpret_cast<double*>(smem_raw + ((sizeof(ScfShared) + 15) / 16) * 16);
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int k = atomicAdd(counter, 1);
+      sh.mol = k < nmol ? order[k] : -1;
+    }
+    __syncthreads();
+    const int mi = sh.mol;
+    __syncthreads();
+    if (mi < 0) return;
+    const MolDev m = mols[mi];
+    const int N = m.nao;
+    double* Apk = packed_in_smem ? smemA : nullptr;
+    const size_t packed_bytes = sizeof(double) * (size_t)N * (N + 1) / 2;
+    double* rot = rotbuf + (size_t)blockIdx.x * (kRotBudgetBytes / sizeof(double));
+    const int cap_rounds = (int)((kRotBudgetBytes / sizeof(double)) / (2 * ((N + 1) / 2)));
+    for (int spin = 0; spin < (Fball ? 2 : 1); ++spin) {
+      double* F = (spin ? Fball : Fall) + m.mat_off;
+      full_diagonalise(N, F, (spin ? Cball : Call) + m.mat_off, W1all + m.mat_off, W2all + m.mat_off,
+                       (spin ? epsball : epsall) + m.ao_base, Apk ? Apk : F, Apk ? packed_bytes : 0, true, rot,
+                       cap_rounds, sp.jacobi_max_sweeps, 1e-10, sh);
+    }
+    __syncthreads();
+  }
+}
+
+void launch_canonical(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s) {
+  if (b.nmol == 0) return;
+  int in_smem = 0;
+  const size_t bytes = scf_smem_bytes(b.max_nao, &in_smem);
+  cudaFuncSetAttribute(k_canonical, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaMemsetAsync(b.counter, 0, sizeof(int), s);
+  if (grid > b.nmol) grid = b.nmol;
+  k_canonical<<<grid, kScfThreads, bytes, s>>>(b.mols, b.nmol, b.order, b.counter, b.F, b.C, b.W1, b.W2, b.eps,
+                                               b.uhf ? b.Fb : nullptr, b.Cb, b.epsb, b.rotbuf, sp, in_smem);
 }
 
 void launch_uhf_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStream_t s) {

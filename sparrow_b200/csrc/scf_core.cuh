@@ -438,13 +438,19 @@ __device__ int jacobi_diagonalise(int N, double* A, double* Ct, bool cold, doubl
       break;
     }
   }
-  // eigenvalues and ranks (A still alive), then the final replay with sorting
+  // eigenvalues and ranks (A still alive), then the final replay with sorting.
+  // The order compares eigenvalues on a 1e-9 Hartree grid and breaks ties by
+  // the current index: orbitals that are degenerate to rounding keep their
+  // order from one diagonalisation to the next (a half-filled degenerate
+  // shell then keeps the same occupied member, as a stable eigensolver
+  // would), and the ranks still form a permutation.
   for (int k = tid; k < N; k += blockDim.x) {
     const double ek = A[packed(k, k)];
+    const long long qk = __double2ll_rd(ek * 1e9);
     int rk = 0;
     for (int j = 0; j < N; ++j) {
-      const double ej = A[packed(j, j)];
-      rk += (ej < ek || (ej == ek && j < k)) ? 1 : 0;
+      const long long qj = __double2ll_rd(A[packed(j, j)] * 1e9);
+      rk += (qj < qk || (qj == qk && j < k)) ? 1 : 0;
     }
     eps[rk] = ek;
     rank[k] = rk;
@@ -749,4 +755,43 @@ __device__ int ov_rotation(int N, int no, double* F, double* Ct, double* W1, dou
 }
 
 }  // namespace
+// New orbitals of one spin from its (extrapolated) Fock matrix Fs: the
+// occupied-virtual rotation of the previous orbitals, or a full
+// diagonalisation at the start, when the rotation asks for one, and when
+// the spin has no occupied or no virtual orbitals.  Returns the Jacobi
+// sweeps of a full diagonalisation (0 when none ran, < 0 when it did not
+// converge).
+__device__ int uhf_orbitals(int N, int ns, double* Fs, double* Cs, double* W1, double* W2, double* epss,
+                            double* Apk, size_t packed_bytes, bool& have, double& drift, double* rot, int cap_rounds,
+                            const ScfParams& sp, int cold_sweeps, int& nfull, ScfShared& sh) {
+  int need_full = !have || ns == 0 || ns == N;
+  if (!need_full) need_full = ov_rotation(N, ns, Fs, Cs, W1, W2, epss, drift, sh);
+  if (!need_full) return 0;
+  const int sw = full_diagonalise(N, Fs, Cs, W1, W2, epss, Apk ? Apk : Fs, Apk ? packed_bytes : 0, have, rot,
+                                  cap_rounds, have ? sp.jacobi_max_sweeps : cold_sweeps, have ? 1e-10 : 1e-3, sh);
+  ++nfull;
+  const bool warm = have;
+  have = true;
+  drift = 0;
+  return sw < 0 ? (warm ? -sp.jacobi_max_sweeps : cold_sweeps) : sw;
+}
+
+// P_s = C_occ C_occ^T of one spin into Ps; returns sum (P_s,new - P_s,old)^2.
+__device__ double uhf_density(int N, int ns, const double* Cs, double* Ps, double* W1, ScfShared& sh) {
+  const size_t NN = (size_t)N * N;
+  if (ns > 0) {
+    cta_gemm(N, N, ns, 1.0, Cs, N, true, Cs, N, false, 0.0, W1, N, sh.gemm, true);
+  } else {
+    for (size_t k = threadIdx.x; k < NN; k += blockDim.x) W1[k] = 0.0;
+    __syncthreads();
+  }
+  double d2 = 0;
+  for (size_t k = threadIdx.x; k < NN; k += blockDim.x) {
+    const double d = W1[k] - Ps[k];
+    d2 += d * d;
+    Ps[k] = W1[k];
+  }
+  return cta_sum(d2, sh.red);
+}
+
 }  // namespace sgb

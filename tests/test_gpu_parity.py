@@ -212,3 +212,22 @@ def test_single_atom_and_positions_update():
     r2 = c.calculate()
     ref2 = O.scf("AM1", Z, x2, rmsd=1e-8)
     assert abs(r2.energy - ref2["energy"]) < E_TOL
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", ["PM6", "DFTB2"])
+def test_calculator_orbital_energies_are_fock_eigenvalues(method):
+    # the Calculator asks for canonical orbitals: its orbital energies are the
+    # eigenvalues of the final Fock matrix, as the reference's results report
+    Z, xa = geometry.water_cluster(4, seed=2)
+    x = geometry.to_bohr(xa)
+    c = sparrow_b200.get_calculator(method)
+    c.set_structure(Z, x)
+    c.settings["density_rmsd_criterion"] = 1e-10
+    c.settings["self_consistence_criterion"] = 1e-11
+    assert c.calculate().successful_calculation
+    if method == "PM6":
+        ref = O.scf("PM6", Z, x, scc=1e-11, rmsd=1e-10, want_density=True)["eps"]
+    else:
+        ref = O.dftb_scf(2, Z, x, scc=1e-11, rmsd=1e-10)["eps"]
+    assert np.max(np.abs(np.sort(c.orbital_energies()) - np.sort(ref))) < 1e-6

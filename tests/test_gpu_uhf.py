@@ -11,6 +11,7 @@ import pytest
 import sparrow_b200
 from sparrow_b200 import geometry
 from tests import oracle_lib as O
+from tests import param_sets as PS
 
 E_TOL = 1e-6
 G_TOL = 1e-5
@@ -115,7 +116,7 @@ def test_calculator_spin_modes():
         c.beta_orbital_energies()
 
 
-def test_unrestricted_batches_are_checked_on_the_host():
+def test_unrestricted_batches_are_checked_on_the_host(tmp_path):
     oh = [(np.array([8, 1]), np.array([[0, 0, 0], [0, 0, 1.84]]))]
     with pytest.raises(sparrow_b200.SparrowError) as ei:   # 7 electrons cannot be a triplet
         sparrow_b200.Batch("PM6", oh, multiplicities=[3])
@@ -125,6 +126,8 @@ def test_unrestricted_batches_are_checked_on_the_host():
     assert ei.value.code == 5
     with pytest.raises(ValueError):
         sparrow_b200.Batch("PM6", oh, multiplicities=[2], unrestricted=False)
-    with pytest.raises(sparrow_b200.SparrowError) as ei:
-        sparrow_b200.Batch("DFTB2", oh, multiplicities=[2])
-    assert ei.value.code == 1
+    with pytest.raises(sparrow_b200.SparrowError) as ei:   # spin-polarised DFTB needs spin constants
+        d = tmp_path / "no-spin"
+        PS.write_skf_directory(str(d), "mio-1-1", spin=False)
+        sparrow_b200.Batch("DFTB2:" + str(d), oh, multiplicities=[2])
+    assert ei.value.code == 3 and "spin constants" in str(ei.value)
