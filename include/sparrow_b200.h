@@ -251,6 +251,11 @@ void sg_server_destroy(sg_server* s);
 const char* sg_server_last_error(void);
 int32_t sg_server_submit(sg_server* s, const char* method, int32_t n_atoms, const int32_t* atomic_numbers,
                          const double* xyz_bohr, int32_t charge, uint32_t properties, int64_t* request_id);
+/* As sg_server_submit with a spin multiplicity: != 1 runs the unrestricted
+ * SCF (the reference's spin mode "any"); batches never mix spin treatments. */
+int32_t sg_server_submit_spin(sg_server* s, const char* method, int32_t n_atoms, const int32_t* atomic_numbers,
+                              const double* xyz_bohr, int32_t charge, int32_t multiplicity, uint32_t properties,
+                              int64_t* request_id);
 /* Wait up to timeout_s (< 0: forever) for a request.  Returns SG_OK when the
  * request is finished (its own status in *status: SG_OK, SG_ERR_NOT_CONVERGED
  * with results, or an error), SG_ERR_TIMEOUT, or SG_ERR_INVALID_ARGUMENT for

@@ -118,6 +118,8 @@ def lib():
                                               ctypes.c_double, ctypes.c_int32, ctypes.POINTER(_VP)]),
         "sg_server_destroy": (None, [_VP]),
         "sg_server_last_error": (ctypes.c_char_p, []),
+        "sg_server_submit_spin": (ctypes.c_int32, [_VP, ctypes.c_char_p, ctypes.c_int32, _I32, _D, ctypes.c_int32,
+                                                   ctypes.c_int32, ctypes.c_uint32, ctypes.POINTER(ctypes.c_int64)]),
         "sg_server_submit": (ctypes.c_int32, [_VP, ctypes.c_char_p, ctypes.c_int32, _I32, _D, ctypes.c_int32,
                                               ctypes.c_uint32, ctypes.POINTER(ctypes.c_int64)]),
         "sg_server_wait": (ctypes.c_int32, [_VP, ctypes.c_int64, ctypes.c_double, _D, _D, _I32, _I32, _D]),
@@ -629,13 +631,14 @@ class Server:
         self._h = h
         self._req = {}
 
-    def submit(self, method, atomic_numbers, xyz_bohr, charge=0, gradients=True):
+    def submit(self, method, atomic_numbers, xyz_bohr, charge=0, gradients=True, multiplicity=1):
+        """Queue one molecule; multiplicity != 1 runs the unrestricted SCF."""
         Z = np.ascontiguousarray(atomic_numbers, dtype=np.int32)
         X = np.ascontiguousarray(xyz_bohr, dtype=np.float64).reshape(-1)
         rid = ctypes.c_int64()
         props = SG_PROP_ENERGY | (SG_PROP_GRADIENTS if gradients else 0)
-        rc = lib().sg_server_submit(self._h, method.encode(), int(Z.size), _iptr(Z), _dptr(X), int(charge), props,
-                                    ctypes.byref(rid))
+        rc = lib().sg_server_submit_spin(self._h, method.encode(), int(Z.size), _iptr(Z), _dptr(X), int(charge),
+                                         int(multiplicity), props, ctypes.byref(rid))
         if rc != 0:
             raise SparrowError(rc, lib().sg_server_last_error().decode())
         self._req[rid.value] = (int(Z.size), gradients)

@@ -749,6 +749,11 @@ const char* sg_server_last_error(void) { return g_server_error.c_str(); }
 
 int32_t sg_server_submit(sg_server* s, const char* method, int32_t n, const int32_t* Z, const double* xyz,
                          int32_t charge, uint32_t props, int64_t* id) {
+  return sg_server_submit_spin(s, method, n, Z, xyz, charge, 1, props, id);
+}
+
+int32_t sg_server_submit_spin(sg_server* s, const char* method, int32_t n, const int32_t* Z, const double* xyz,
+                              int32_t charge, int32_t multiplicity, uint32_t props, int64_t* id) {
   if (!s || !id) return SG_ERR_INVALID_ARGUMENT;
   sgb::Method m;
   std::string set;
@@ -764,6 +769,7 @@ int32_t sg_server_submit(sg_server* s, const char* method, int32_t n, const int3
   mol.Z.assign(Z, Z + n);
   mol.xyz.assign(xyz, xyz + 3 * (size_t)n);
   mol.charge = charge;
+  mol.multiplicity = multiplicity;
   std::string err;
   const long long r = s->impl->submit(m, std::move(mol), (props & SG_PROP_GRADIENTS) != 0, err);
   if (r < 0) {

@@ -39,7 +39,7 @@ double Server::now() {
   return duration<double>(steady_clock::now().time_since_epoch()).count();
 }
 
-size_t Server::estimate_bytes(Method m, const MoleculeInput& mol) {
+size_t Server::estimate_bytes(Method m, const MoleculeInput& mol, bool uhf) {
   long long nao = 0, s_sum = 0, s_sq = 0;
   for (int z : mol.Z) {
     const int n = engine_n_aos(m, z);
@@ -52,7 +52,9 @@ size_t Server::estimate_bytes(Method m, const MoleculeInput& mol) {
   const long long pairs = nat * (nat - 1) / 2;
   const long long nint = (s_sum * s_sum - s_sq) / 2;
   // matrices H P F C W1 W2 + DIIS ring + eps, integrals, per-pair buffers and tables, atoms, AO map
-  long long b = 8 * (6 * nao * nao + 2LL * kDiisMax * nao * nao + nao) + 8 * nint +
+  // (unrestricted: four more matrices, a second DIIS ring and orbital energies)
+  const long long spin = uhf ? 8 * (5 * nao * nao + 2LL * kDiisMax * nao * nao + nao + 2 * nat) : 0;
+  long long b = spin + 8 * (6 * nao * nao + 2LL * kDiisMax * nao * nao + nao) + 8 * nint +
                 pairs * (8 * (20 + 20 + 16 + 1 + 3) + (long long)sizeof(PairDev) + 4) +
                 nat * ((long long)sizeof(AtomDev) + 24) + 4 * nao + (long long)sizeof(MolDev) + sizeof(MolResult) + 4096;
   return (size_t)b;
@@ -104,8 +106,15 @@ long long Server::submit(Method m, MoleculeInput&& mol, bool gradient, std::stri
     return -kErrInvalidArgument;
   }
   const long long nel = std::lround(ncore) - mol.charge;
-  if (nel < 0 || (nel & 1)) {
-    err = std::to_string(nel) + " electrons: the restricted closed-shell SCF needs an even, non-negative count";
+  const bool uhf = mol.multiplicity != 1;
+  if (uhf) {
+    const long long na2 = nel + mol.multiplicity - 1;
+    if (mol.multiplicity < 1 || nel < 0 || (na2 & 1) || nel - (mol.multiplicity - 1) < 0 || na2 / 2 > nao) {
+      err = std::to_string(nel) + " electrons do not fit spin multiplicity " + std::to_string(mol.multiplicity);
+      return -kErrOddElectrons;
+    }
+  } else if (nel < 0 || (nel & 1)) {
+    err = std::to_string(nel) + " electrons: a singlet needs an even, non-negative count";
     return -kErrOddElectrons;
   }
   for (int a = 0; a < n; ++a) {
@@ -126,7 +135,8 @@ long long Server::submit(Method m, MoleculeInput&& mol, bool gradient, std::stri
   ServerRequest r;
   r.method = m;
   r.gradient = gradient;
-  r.bytes = estimate_bytes(m, mol);
+  r.uhf = uhf;
+  r.bytes = estimate_bytes(m, mol, uhf);
   r.size_class = (int)std::min<long long>((nao - 1) / 64, 7);
   r.mol = std::move(mol);
   r.t_submit = now();
@@ -181,6 +191,7 @@ ServerStats Server::stats() {
 
 bool Server::launch(Slot& s, std::vector<ServerRequest>&& reqs) {
   const Method m = reqs.front().method;
+  const bool uhf = reqs.front().uhf;
   std::vector<MoleculeInput> mols(reqs.size());
   s.gradient = false;
   for (size_t i = 0; i < reqs.size(); ++i) {
@@ -189,6 +200,7 @@ bool Server::launch(Slot& s, std::vector<ServerRequest>&& reqs) {
   }
   s.reqs = std::move(reqs);
   if (!s.batch || s.batch->method() != m) s.batch.reset(new Batch(m));
+  s.batch->set_unrestricted(uhf);
   std::string err;
   int rc = s.batch->setup(mols, err, false);
   if (rc == kOk) rc = s.batch->run(sp_, s.gradient, err);
@@ -278,17 +290,18 @@ void Server::worker() {
       progress = true;
     }
     // admit pending requests into free slots: the oldest request fixes the
-    // method and size class; later requests of both follow in arrival order while
+    // method, spin treatment and size class; later matching requests follow in arrival order while
     // the device budget allows (one batch is always admitted when the device
     // is otherwise idle, so progress never depends on the budget)
     for (auto& s : slots_) {
       if (s.busy || pending_.empty()) continue;
       const Method m = pending_.front().method;
       const int cls = pending_.front().size_class;
+      const bool uhf = pending_.front().uhf;
       std::vector<ServerRequest> take;
       size_t bytes = 0;
       for (auto it = pending_.begin(); it != pending_.end() && (int)take.size() < max_batch_;) {
-        if (it->method != m || it->size_class != cls) {
+        if (it->method != m || it->size_class != cls || it->uhf != uhf) {
           ++it;
           continue;
         }

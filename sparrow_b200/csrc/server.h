@@ -36,6 +36,7 @@ struct ServerRequest {
   double t_submit = 0;  // seconds, steady clock
   size_t bytes = 0;     // estimated device bytes
   int size_class = 0;   // AO-count class: batches never mix classes
+  bool uhf = false;     // unrestricted (multiplicity != 1): batches never mix spin treatments
 };
 
 struct ServerResult {
@@ -62,6 +63,7 @@ class Server {
   Server& operator=(const Server&) = delete;
 
   // Queue a request; returns its id (> 0) or a negative Status on invalid input.
+  // mol.multiplicity != 1 runs the unrestricted SCF (the reference's spin mode "any")
   long long submit(Method m, MoleculeInput&& mol, bool gradient, std::string& err);
   // Block until request id is done (timeout_s < 0: forever).  Returns 0 and
   // moves the result out, or 1 on timeout, or kErrInvalidArgument for an
@@ -74,7 +76,7 @@ class Server {
   ServerStats stats();
   static double now();
   // Estimated device bytes a molecule occupies inside a batch.
-  static size_t estimate_bytes(Method m, const MoleculeInput& mol);
+  static size_t estimate_bytes(Method m, const MoleculeInput& mol, bool uhf = false);
 
  private:
   struct Slot {

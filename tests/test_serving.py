@@ -45,6 +45,9 @@ def test_submit_validation_without_gpu_work():
         with pytest.raises(sparrow_b200.SparrowError) as e:
             srv.submit("PM6", [17, 17], np.array([0, 0, 0, 3.8, 0, 0.0]))
         assert e.value.code == 3
+        with pytest.raises(sparrow_b200.SparrowError) as e:  # 7 electrons: no triplet
+            srv.submit("PM6", [8, 1], np.array([0, 0, 0, 0, 0, 1.8]), multiplicity=3)
+        assert e.value.code == 5
 
 
 @pytest.mark.gpu
@@ -99,3 +102,33 @@ def test_tiny_budget_still_makes_progress():
         st = srv.stats()
     assert all(r is not None and r.successful_calculation for r in res)
     assert st["max_batch"] == 1  # admitted one at a time
+
+
+@pytest.mark.gpu
+def test_open_shells_are_served_beside_closed_shells():
+    # radicals (unrestricted) and closed shells (restricted) interleaved; batches
+    # never mix the two spin treatments, and each result matches the oracle
+    from tests.test_gpu_sdftb import _radicals as dftb_radicals
+    from tests.test_gpu_uhf import _radicals as nddo_radicals
+    reqs = [("PM6", z, x, c, m) for z, x, c, m in nddo_radicals()]
+    reqs += [("DFTB2", z, x, c, m) for z, x, c, m in dftb_radicals()]
+    reqs += [(m, z, x, 0, 1) for z, x, m in _mix(12, seed=9)]
+    order = np.random.default_rng(2).permutation(len(reqs))
+    with sparrow_b200.Server(device_budget_gb=4.0, slots=3, scc=1e-10, rmsd=1e-9, max_iter=500) as srv:
+        ids = {int(i): srv.submit(reqs[i][0], reqs[i][1], reqs[i][2], charge=reqs[i][3], multiplicity=reqs[i][4])
+               for i in order}
+        res = {i: srv.wait(r) for i, r in ids.items()}
+    for i, (method, Z, x, ch, mult) in enumerate(reqs):
+        r = res[i]
+        assert r.successful_calculation, (method, i)
+        if mult == 1 and method != "DFTB2":
+            ref = O.scf(method, Z, x, charge=ch, scc=1e-10, rmsd=1e-9)
+        elif mult == 1:
+            ref = O.dftb_scf(2, Z, x, charge=ch, scc=1e-10, rmsd=1e-9)
+        elif method == "DFTB2":
+            ref = O.dftb_scf_uhf(2, Z, x, mult, charge=ch, scc=1e-10, rmsd=1e-9)
+        else:
+            ref = O.scf_uhf(method, Z, x, mult, charge=ch, scc=1e-10, rmsd=1e-9)
+        assert abs(r.energy - ref["energy"]) < E_TOL, (method, i)
+        assert np.max(np.abs(r.gradients - ref["gradient"])) < G_TOL, (method, i)
+
