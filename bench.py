@@ -55,6 +55,8 @@ def parse():
     p.add_argument("--no-large", action="store_true", help="skip the large-molecule (water cluster) leg")
     p.add_argument("--no-tddftb", action="store_true", help="skip the DFTB3 + TD-DFTB polyene leg")
     p.add_argument("--no-plain", action="store_true", help="skip the plain one-molecule-per-launch GPU leg")
+    p.add_argument("--no-open-shell", action="store_true", help="skip the unrestricted (radical) leg")
+    p.add_argument("--no-hessian", action="store_true", help="skip the semi-numerical Hessian leg")
     p.add_argument("--serving-loads", default="250,500,1000,2000", help="offered loads (req/s) of the serving leg")
     return p.parse_args()
 
@@ -301,6 +303,99 @@ def tddftb_leg(count=1024, seed=6, nroots=8, cpu_seconds=10.0):
                                      "Casida diagonalisation, %.1f s wall" % (
                                          done, len(mols[order[0]][0]), len(mols[order[max(done - 1, 0)]][0]), wall),
                            "max_abs_domega_gpu_vs_oracle_hartree": dmax}
+    return out
+
+
+def open_shell_leg(count=1024, seed=8, cpu_seconds=5.0):
+    """Unrestricted SCF throughput: a batch of alkyl radicals (alkanes C_nH_2n+2,
+    n ~ U[2,30], without their last hydrogen; doublets), energy+gradient, PM6
+    (UHF) and DFTB2 mio-1-1 (spin-polarised): device ms and solves/s, with the
+    CPU oracle on a bounded sample of the same radicals (PM6)."""
+    import numpy as np
+    import sparrow_b200
+    from sparrow_b200 import geometry
+    rad = [(np.asarray(z)[:-1], geometry.to_bohr(x)[:-1]) for z, x in geometry.alkane_batch(count, seed=seed)]
+    out = {"workload": "%d alkyl radicals C_nH_2n+1 (n~U[2,30], seed %d), doublets, energy+gradient, rms dP 1e-8" % (
+        count, seed)}
+    energies = {}
+    for method in ("PM6", "DFTB2"):
+        for rep in range(2):  # the first pass pays module loading
+            b = sparrow_b200.Batch(method, rad, multiplicities=[2] * count, scc=1e-7, rmsd=1e-8, max_iter=300)
+            b.record_event(0)
+            b.run(gradients=True)
+            b.record_event(1)
+            e, _, it, conv = b.results()
+            ms = b.elapsed_ms(0, 1)
+        energies[method] = e
+        out[method] = {"device_ms": ms, "solves_per_s": count / (ms / 1e3), "converged": int(conv.sum()),
+                       "mean_iterations": float(it.mean())}
+    from tests import oracle_lib as O
+    rng = np.random.default_rng(3)
+    t0, done, dmax = time.perf_counter(), 0, 0.0
+    for i in rng.permutation(count):
+        if time.perf_counter() - t0 > cpu_seconds:
+            break
+        r = O.scf_uhf("PM6", rad[i][0], rad[i][1], 2, scc=1e-7, rmsd=1e-8)
+        dmax = max(dmax, abs(r["energy"] - energies["PM6"][i]))
+        done += 1
+    wall = time.perf_counter() - t0
+    out["cpu_baseline"] = {"value": done / wall, "unit": "solves/s", "cores": 1, "kind": "port",
+                           "sample": "%d random radicals of the batch, oracle PM6 UHF energy+gradient, %.1f s wall" % (
+                               done, wall),
+                           "max_abs_dE_gpu_vs_oracle_hartree": dmax}
+    return out
+
+
+def hessian_leg(cpu_step_seconds=30.0):
+    """Semi-numerical Hessian (central differences of analytic gradients, 0.01
+    bohr; the reference's only Hessian): the 28-atom structure of the
+    reference's frequency tests and a C30H62 alkane, PM6.  GPU wall ms (all 6n
+    displaced geometries as batches) against the CPU oracle doing the same
+    displacements one after another (sft_1 only), and the lowest harmonic
+    frequency of sft_1 against the reference's -125.561 cm^-1."""
+    import json as _json
+    import numpy as np
+    import sparrow_b200
+    from sparrow_b200 import geometry
+    from tests import harmonic
+    from tests import oracle_lib as O
+    gold = _json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden",
+                                        "hessian_known_answers.json")))
+    st = gold["structures"]["sft_1"]
+    sym = {"H": 1, "C": 6, "N": 7, "O": 8}
+    Z = [sym[e] for e in st["elements"]]
+    x = np.array(st["xyz_angstrom"]) * O.bohr_per_angstrom()
+    out = {"workload": "PM6 Hessians: sft_1 (C10H14O4, 28 atoms, 168 displaced geometries) and C30H62 "
+                       "(92 atoms, 552 displaced geometries)"}
+    sparrow_b200.hessian("PM6", Z, x)  # module loading
+    t0 = time.perf_counter()
+    H, nc = sparrow_b200.hessian("PM6", Z, x, scc=1e-9, rmsd=1e-9)
+    gpu_ms = (time.perf_counter() - t0) * 1e3
+    f = harmonic.frequencies(Z, x, H)
+    rng = np.random.default_rng(1)
+    za, xa = geometry.alkane(30, rng)
+    t0 = time.perf_counter()
+    Hb, ncb = sparrow_b200.hessian("PM6", za, geometry.to_bohr(xa))
+    big_ms = (time.perf_counter() - t0) * 1e3
+    # the oracle: the same central differences, displacement after displacement, on a bounded share
+    t0, done = time.perf_counter(), 0
+    for k in range(3 * len(Z)):
+        if time.perf_counter() - t0 > cpu_step_seconds:
+            break
+        for sgn in (1, -1):
+            xs = x.copy().reshape(-1)
+            xs[k] += 0.01 * sgn
+            O.scf("PM6", Z, xs.reshape(-1, 3), scc=1e-9, rmsd=1e-9)
+        done += 1
+    wall = time.perf_counter() - t0
+    cpu_full_s = wall / max(done, 1) * 3 * len(Z)
+    out["sft_1"] = {"gpu_wall_ms": gpu_ms, "not_converged": nc, "lowest_frequency_cm": float(f[0]),
+                    "reference_lowest_frequency_cm": -125.561,
+                    "cpu_baseline": {"value": cpu_full_s, "unit": "s per Hessian", "cores": 1, "kind": "port",
+                                     "sample": "%d of %d coordinates (both displacements) in %.1f s, scaled" % (
+                                         done, 3 * len(Z), wall)},
+                    "gpu_over_cpu": cpu_full_s / (gpu_ms / 1e3)}
+    out["C30H62"] = {"gpu_wall_ms": big_ms, "not_converged": ncb}
     return out
 
 
@@ -559,6 +654,12 @@ def run_engine(args, rank, world):
     tddftb = None
     if rank == 0 and not args.no_tddftb:
         tddftb = tddftb_leg()
+    open_shell = None
+    if rank == 0 and not args.no_open_shell:
+        open_shell = open_shell_leg()
+    hessian = None
+    if rank == 0 and not args.no_hessian:
+        hessian = hessian_leg()
 
     # roofline of the SCF kernel (average launch)
     scf_ms = stage_sum[2] / args.steps
@@ -592,6 +693,8 @@ def run_engine(args, rank, world):
         "serving": serving,
         "large_molecules": large,
         "tddftb": tddftb,
+        "open_shell": open_shell,
+        "hessian": hessian,
         "clocks": clk,
     }
     if rank == 0:
