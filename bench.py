@@ -75,7 +75,7 @@ def _oracle_solve(args):
     from tests import oracle_lib
     t0 = time.perf_counter()
     r = oracle_lib.scf(method, Z, x, scc=SCC, rmsd=RMSD, max_iter=MAX_ITER, gradient=True)
-    return time.perf_counter() - t0, r["energy"], r["iterations"]
+    return time.perf_counter() - t0, r["energy"], r["iterations"], r["gradient"]
 
 
 def cpu_rate(method, mols, target_seconds, procs, rng_seed=12345):
@@ -90,11 +90,13 @@ def cpu_rate(method, mols, target_seconds, procs, rng_seed=12345):
         res = pool.map(_oracle_solve, [(method, z, x) for z, x in calib])
         per_mol = sum(r[0] for r in res) / len(res)
         count = int(max(procs, min(len(mols), target_seconds * procs / max(per_mol, 1e-3))))
-        sample = [mols[i] for i in rng.choice(len(mols), size=count, replace=False)]
+        idx = rng.choice(len(mols), size=count, replace=False)
+        sample = [mols[i] for i in idx]
         t0 = time.perf_counter()
         res = pool.map(_oracle_solve, [(method, z, x) for z, x in sample], chunksize=1)
         wall = time.perf_counter() - t0
-    return count / wall, count, wall, [r[1] for r in res]
+    # (molecule index, oracle energy, oracle gradient) of the timed sample
+    return count / wall, count, wall, [(int(i), r[1], r[3]) for i, r in zip(idx, res)]
 
 
 def plain_gpu_rate(method, mols, target_seconds=8.0, max_count=512, rng_seed=777):
@@ -570,7 +572,7 @@ def run_engine(args, rank, world):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         procs = host_cores()
-        rate, count, wall, _ = cpu_rate(args.method, mols, args.cpu_seconds, procs)
+        rate, count, wall, cpu_results = cpu_rate(args.method, mols, args.cpu_seconds, procs)
         cpu = {"value": rate, "unit": "solves/s", "cores": procs, "kind": "port",
                "sample": "%d random molecules of the batch, oracle (C++ FP64 restatement of the reference path), "
                          "molecule-parallel over %d processes, %.1f s wall" % (count, procs, wall)}
@@ -613,6 +615,11 @@ def run_engine(args, rank, world):
     n_total = args.molecules * world
     value = n_total * args.steps / (dev_ms / 1e3)
     not_conv = int((~conv).sum())
+    if cpu is not None:
+        # accuracy of the timed run against the oracle on the CPU sample
+        cpu["max_abs_dE_gpu_vs_oracle_hartree"] = float(max(abs(e[i] - eo) for i, eo, _ in cpu_results))
+        cpu["max_abs_dgrad_gpu_vs_oracle_hartree_per_bohr"] = float(
+            max(np.max(np.abs(g[i] - go)) for i, _, go in cpu_results))
 
     # end to end from host buffers through the public batch call
     t_e2e = []
