@@ -131,3 +131,32 @@ def test_unrestricted_batches_are_checked_on_the_host(tmp_path):
         PS.write_skf_directory(str(d), "mio-1-1", spin=False)
         sparrow_b200.Batch("DFTB2:" + str(d), oh, multiplicities=[2])
     assert ei.value.code == 3 and "spin constants" in str(ei.value)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", ["PM6", "AM1", "MNDO"])
+def test_edge_occupations(method):
+    # H atom (no beta electron), N atom quartet (alpha shell full), NH3+ doublet
+    # (ionised from the non-degenerate lone pair; a Jahn-Teller radical such as
+    # tetrahedral CH4+ has several broken-symmetry UHF solutions, so two
+    # solvers may rightly land on different ones)
+    b = O.bohr_per_angstrom()
+    cases = [([1], ATOM * b, 0, 2), ([7], ATOM * b, 0, 4),
+             ([7, 1, 1, 1], np.array([[0, 0, 0], [0.94, 0, 0.38], [-0.47, 0.814, 0.38], [-0.47, -0.814, 0.38]]) * b,
+              1, 2)]
+    for Z, x, ch, mult in cases:
+        c = sparrow_b200.get_calculator(method)
+        c.set_structure(Z, x)
+        c.settings["molecular_charge"] = ch
+        c.settings["spin_multiplicity"] = mult
+        c.settings["density_rmsd_criterion"] = 1e-9
+        c.settings["self_consistence_criterion"] = 1e-10
+        c.settings["max_scf_iterations"] = 500
+        c.set_required_properties(["energy", "gradients"])
+        r = c.calculate()
+        ref = O.scf_uhf(method, Z, x, mult, charge=ch, scc=1e-10, rmsd=1e-9)
+        assert r.successful_calculation and ref["converged"], (method, Z)
+        assert abs(r.energy - ref["energy"]) < E_TOL, (method, Z)
+        assert np.max(np.abs(r.gradients - ref["gradient"])) < G_TOL, (method, Z)
+        assert np.max(np.abs(np.sort(c.orbital_energies()) - ref["eps_alpha"])) < 1e-6
+        assert np.max(np.abs(np.sort(c.beta_orbital_energies()) - ref["eps_beta"])) < 1e-6
