@@ -56,6 +56,7 @@ extern "C" {
 #define SG_PROP_ENERGY 1u
 #define SG_PROP_GRADIENTS 2u
 #define SG_PROP_HESSIAN 4u /* semi-numerical: central differences of analytic gradients */
+#define SG_PROP_ATOMIC_CHARGES 8u
 
 typedef struct sg_calculator sg_calculator;
 typedef struct sg_batch sg_batch;
@@ -125,6 +126,11 @@ int32_t sg_get_beta_orbital_energies(const sg_calculator* h, double* eps);
  * symmetrised central difference of analytic gradients with a 0.01 bohr
  * step; the 6 n_atoms displaced geometries run as one batch. */
 int32_t sg_get_hessian(const sg_calculator* h, double* hessian);
+/* Atomic charges (n_atoms) of the last calculate() with SG_PROP_ATOMIC_CHARGES
+ * required (results().AtomicCharges, GenericMethodWrapper.cpp:212-214): DFTB
+ * the SCC's Mulliken charges, NDDO the core charge minus the atom's diagonal
+ * density (Mulliken charges in the orthogonal NDDO basis). */
+int32_t sg_get_atomic_charges(const sg_calculator* h, double* charges);
 /* One call: the same Hessian for one molecule (method spec as for
  * sg_batch_create; unrestricted != 0 or multiplicity != 1 runs the
  * unrestricted SCF; step <= 0 takes 0.01 bohr).  not_converged (may be NULL)

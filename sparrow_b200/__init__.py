@@ -26,6 +26,7 @@ _lib = None
 SG_PROP_ENERGY = 1
 SG_PROP_GRADIENTS = 2
 SG_PROP_HESSIAN = 4
+SG_PROP_ATOMIC_CHARGES = 8
 SG_ERR_NOT_CONVERGED = 6
 SG_ERR_TIMEOUT = 12
 SG_PENDING = 13
@@ -86,6 +87,7 @@ def lib():
         "sg_set_density": (ctypes.c_int32, [_VP, _D]),
         "sg_get_beta_orbital_energies": (ctypes.c_int32, [_VP, _D]),
         "sg_get_hessian": (ctypes.c_int32, [_VP, _D]),
+        "sg_get_atomic_charges": (ctypes.c_int32, [_VP, _D]),
         "sg_calculate_hessian": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _D, ctypes.c_int32,
                                                   ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                                                   ctypes.c_int32, ctypes.c_double, _D, _I32, ctypes.c_char_p,
@@ -161,6 +163,7 @@ class Results:
         self.n_aos = n_aos
         self.n_occupied = n_occupied
         self.hessian = None  # (3 n_atoms, 3 n_atoms) when "hessian" was required
+        self.atomic_charges = None  # (n_atoms,) when "atomic_charges" was required
 
 
 class _Settings:
@@ -268,6 +271,8 @@ class Calculator:
                 mask |= SG_PROP_GRADIENTS | SG_PROP_ENERGY
             elif p == "hessian":
                 mask |= SG_PROP_HESSIAN | SG_PROP_ENERGY
+            elif p in ("atomic_charges", "charges"):
+                mask |= SG_PROP_ATOMIC_CHARGES | SG_PROP_ENERGY
             else:
                 raise ValueError("unsupported property %r" % p)
         self._check(lib().sg_set_required_properties(self._h, mask))
@@ -288,6 +293,10 @@ class Calculator:
             grad = g.reshape(-1, 3)
         self._nao = nao.value
         res = Results(e.value, grad, rc == 0 and bool(conv.value), it.value, nao.value, nocc.value)
+        if getattr(self, "_mask", SG_PROP_ENERGY) & SG_PROP_ATOMIC_CHARGES:
+            q = np.zeros(self._n_atoms)
+            self._check(L.sg_get_atomic_charges(self._h, _dptr(q)))
+            res.atomic_charges = q
         if getattr(self, "_mask", SG_PROP_ENERGY) & SG_PROP_HESSIAN:
             n3 = 3 * self._n_atoms
             H = np.zeros(n3 * n3)

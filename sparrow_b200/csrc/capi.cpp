@@ -131,6 +131,8 @@ class Calculator {
     have_gradient_ = grad;
     batch_->fetch_density(0, density_, error);
     batch_->fetch_orbital_energies(0, eps_, error);
+    charges_.clear();
+    if (required_ & SG_PROP_ATOMIC_CHARGES) batch_->fetch_charges(0, charges_, error);
     eps_b_.clear();
     if (uhf) batch_->fetch_orbital_energies(0, eps_b_, error, true);
     if (result_.status != kDevOk) {
@@ -157,6 +159,7 @@ class Calculator {
     return kOk;
   }
   const std::vector<double>& hessian() const { return hessian_; }
+  const std::vector<double>& atomic_charges() const { return charges_; }
 
   // TD-DFTB on the converged DFTB reference of the last calculate()
   int excitations(int nroots, bool triplet, double* omega, double* dip) {
@@ -243,7 +246,7 @@ class Calculator {
   uint32_t required_ = SG_PROP_ENERGY;
   MoleculeOutput result_;
   bool have_result_ = false, have_gradient_ = false;
-  std::vector<double> density_, eps_, eps_b_, state_, hessian_;
+  std::vector<double> density_, eps_, eps_b_, state_, hessian_, charges_;
 };
 
 }  // namespace sgb
@@ -416,7 +419,7 @@ int32_t sg_get_setting_int(const sg_calculator* h, const char* key, int64_t* v) 
 
 int32_t sg_set_required_properties(sg_calculator* h, uint32_t mask) {
   if (!h) return SG_ERR_INVALID_ARGUMENT;
-  if (mask & ~(SG_PROP_ENERGY | SG_PROP_GRADIENTS | SG_PROP_HESSIAN))
+  if (mask & ~(SG_PROP_ENERGY | SG_PROP_GRADIENTS | SG_PROP_HESSIAN | SG_PROP_ATOMIC_CHARGES))
     return fail(h, SG_ERR_INVALID_ARGUMENT, "unknown property bit");
   h->impl->set_required(mask);
   return SG_OK;
@@ -439,6 +442,14 @@ int32_t sg_get_gradients(const sg_calculator* h, double* g) {
   if (!h->impl->have_result() || !h->impl->have_gradient()) return SG_ERR_NO_RESULTS;
   const auto& v = h->impl->result().gradient;
   std::memcpy(g, v.data(), sizeof(double) * v.size());
+  return SG_OK;
+}
+
+int32_t sg_get_atomic_charges(const sg_calculator* h, double* charges) {
+  if (!h || !charges) return SG_ERR_INVALID_ARGUMENT;
+  const auto& v = h->impl->atomic_charges();
+  if (!h->impl->have_result() || v.empty()) return SG_ERR_NO_RESULTS;
+  std::memcpy(charges, v.data(), sizeof(double) * v.size());
   return SG_OK;
 }
 

@@ -892,6 +892,36 @@ int Batch::fetch_density(int mol, std::vector<double>& P, std::string& err) {
   return kOk;
 }
 
+int Batch::fetch_charges(int mol, std::vector<double>& q, std::string& err) {
+  if (mol < 0 || mol >= (int)mols_.size()) {
+    err = "molecule index out of range";
+    return kErrInvalidArgument;
+  }
+  const MolDev& m = mols_[mol];
+  q.resize(m.nat);
+  if (is_dftb(method_)) {
+    cudaError_t e = cudaMemcpyAsync(q.data(), dev_.qat + m.atom0, sizeof(double) * m.nat, cudaMemcpyDeviceToHost,
+                                    stream_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+    if (e != cudaSuccess) {
+      err = cuda_message(e);
+      return kErrCuda;
+    }
+    return kOk;
+  }
+  std::vector<double> P;
+  const int rc = fetch_density(mol, P, err);
+  if (rc) return rc;
+  for (int a = 0; a < m.nat; ++a) {
+    const AtomDev& A = atoms_[m.atom0 + a];
+    const ElemDev& E = elems_[A.slot];
+    double pop = 0;
+    for (int k = 0; k < E.nao; ++k) pop += P[(size_t)(A.ao0 + k) * m.nao + A.ao0 + k];
+    q[a] = E.core - pop;
+  }
+  return kOk;
+}
+
 int Batch::fetch_orbital_energies(int mol, std::vector<double>& eps, std::string& err, bool beta) {
   if (mol < 0 || mol >= (int)mols_.size()) {
     err = "molecule index out of range";

@@ -69,6 +69,10 @@ class Batch {
   int fetch(std::vector<MoleculeOutput>& out, bool gradient, std::string& err);
   int fetch_density(int mol, std::vector<double>& P, std::string& err);
   int fetch_raw_results(std::vector<MolResult>& r, std::string& err);
+  // Atomic charges of molecule mol after run(): DFTB the Mulliken charges of
+  // the SCC (computed on the device with the final density), NDDO core charge
+  // minus the atom's diagonal density (Mulliken in the orthogonal NDDO basis).
+  int fetch_charges(int mol, std::vector<double>& q, std::string& err);
   // alpha orbital energies (restricted: the orbital energies); beta = true: the beta ones
   int fetch_orbital_energies(int mol, std::vector<double>& eps, std::string& err, bool beta = false);
   // Linear-response TD-DFTB (DFTB2 / DFTB3 batches, after run()): the nroots
