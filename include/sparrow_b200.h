@@ -120,6 +120,12 @@ int32_t sg_calculate_excitations(sg_calculator* h, int32_t nroots, int32_t tripl
  * energies (N values; sg_get_orbital_energies gives the alpha ones).
  * SG_ERR_NO_RESULTS after a restricted calculation. */
 int32_t sg_get_beta_orbital_energies(const sg_calculator* h, double* eps);
+/* Unrestricted state (getState / loadState with spin-resolved densities,
+ * GenericMethodWrapper.cpp:268-282): the alpha and beta densities (N x N
+ * each) of the last calculate(), and start spin densities for the next one
+ * (their sum also replaces the sg_set_density state). */
+int32_t sg_get_spin_densities(const sg_calculator* h, double* alpha, double* beta);
+int32_t sg_set_spin_densities(sg_calculator* h, const double* alpha, const double* beta);
 /* Hessian (3 n_atoms x 3 n_atoms row-major, Hartree/bohr^2) of the last
  * calculate() with SG_PROP_HESSIAN required.  Like the reference, which has no
  * analytic Hessian (GenericMethodWrapper.cpp:58-88, 339-341), it is the

@@ -88,6 +88,8 @@ def lib():
         "sg_get_beta_orbital_energies": (ctypes.c_int32, [_VP, _D]),
         "sg_get_hessian": (ctypes.c_int32, [_VP, _D]),
         "sg_get_atomic_charges": (ctypes.c_int32, [_VP, _D]),
+        "sg_get_spin_densities": (ctypes.c_int32, [_VP, _D, _D]),
+        "sg_set_spin_densities": (ctypes.c_int32, [_VP, _D, _D]),
         "sg_calculate_hessian": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _D, ctypes.c_int32,
                                                   ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                                                   ctypes.c_int32, ctypes.c_double, _D, _I32, ctypes.c_char_p,
@@ -324,6 +326,19 @@ class Calculator:
         e = np.zeros(self._nao)
         self._check(lib().sg_get_orbital_energies(self._h, _dptr(e)))
         return e
+
+    def spin_densities(self):
+        """(P_alpha, P_beta) of an unrestricted calculation."""
+        n = self._nao
+        Pa, Pb = np.zeros(n * n), np.zeros(n * n)
+        self._check(lib().sg_get_spin_densities(self._h, _dptr(Pa), _dptr(Pb)))
+        return Pa.reshape(n, n), Pb.reshape(n, n)
+
+    def set_spin_densities(self, Pa, Pb):
+        """Start spin densities of the next unrestricted calculate()."""
+        Pa = np.ascontiguousarray(Pa, dtype=np.float64)
+        Pb = np.ascontiguousarray(Pb, dtype=np.float64)
+        self._check(lib().sg_set_spin_densities(self._h, _dptr(Pa), _dptr(Pb)))
 
     def beta_orbital_energies(self):
         """Beta orbital energies of an unrestricted calculation."""

@@ -116,7 +116,10 @@ class Calculator {
     rc = batch_->set_scf_path(sp_name == "batched" ? 1 : sp_name == "large" ? 2 : sp_name == "large_mixed" ? 3 : 0,
                               error);
     if (rc) return rc;
-    if (!state_.empty()) {
+    if (uhf && !state_a_.empty()) {
+      rc = batch_->set_start_spin_densities(state_a_.data(), state_b_.data(), error);
+      if (rc) return rc;
+    } else if (!state_.empty()) {
       rc = batch_->set_start_density(state_.data(), error);
       if (rc) return rc;
     }
@@ -134,7 +137,12 @@ class Calculator {
     charges_.clear();
     if (required_ & SG_PROP_ATOMIC_CHARGES) batch_->fetch_charges(0, charges_, error);
     eps_b_.clear();
-    if (uhf) batch_->fetch_orbital_energies(0, eps_b_, error, true);
+    dens_a_.clear();
+    dens_b_.clear();
+    if (uhf) {
+      batch_->fetch_orbital_energies(0, eps_b_, error, true);
+      batch_->fetch_spin_densities(0, dens_a_, dens_b_, error);
+    }
     if (result_.status != kDevOk) {
       error = "device SCF failure code " + std::to_string(result_.status);
       return kErrDevice;
@@ -160,6 +168,20 @@ class Calculator {
   }
   const std::vector<double>& hessian() const { return hessian_; }
   const std::vector<double>& atomic_charges() const { return charges_; }
+  const std::vector<double>& alpha_density() const { return dens_a_; }
+  const std::vector<double>& beta_density() const { return dens_b_; }
+  int set_spin_densities(const double* Pa, const double* Pb) {
+    const int n = n_aos();
+    if (n == 0) {
+      error = "no structure set";
+      return kErrEmptyStructure;
+    }
+    state_a_.assign(Pa, Pa + (size_t)n * n);
+    state_b_.assign(Pb, Pb + (size_t)n * n);
+    state_.resize((size_t)n * n);
+    for (size_t k = 0; k < state_.size(); ++k) state_[k] = state_a_[k] + state_b_[k];
+    return kOk;
+  }
 
   // TD-DFTB on the converged DFTB reference of the last calculate()
   int excitations(int nroots, bool triplet, double* omega, double* dip) {
@@ -236,6 +258,7 @@ class Calculator {
   void invalidate(bool new_structure) {
     have_result_ = have_gradient_ = false;
     hessian_.clear();
+    if (new_structure) state_a_.clear(), state_b_.clear();
     if (new_structure) state_.clear();
   }
   Method method_;
@@ -247,6 +270,7 @@ class Calculator {
   MoleculeOutput result_;
   bool have_result_ = false, have_gradient_ = false;
   std::vector<double> density_, eps_, eps_b_, state_, hessian_, charges_;
+  std::vector<double> dens_a_, dens_b_, state_a_, state_b_;  // unrestricted: spin densities and their start
 };
 
 }  // namespace sgb
@@ -443,6 +467,21 @@ int32_t sg_get_gradients(const sg_calculator* h, double* g) {
   const auto& v = h->impl->result().gradient;
   std::memcpy(g, v.data(), sizeof(double) * v.size());
   return SG_OK;
+}
+
+int32_t sg_get_spin_densities(const sg_calculator* h, double* Pa, double* Pb) {
+  if (!h || !Pa || !Pb) return SG_ERR_INVALID_ARGUMENT;
+  const auto& a = h->impl->alpha_density();
+  const auto& b = h->impl->beta_density();
+  if (!h->impl->have_result() || a.empty()) return SG_ERR_NO_RESULTS;
+  std::memcpy(Pa, a.data(), sizeof(double) * a.size());
+  std::memcpy(Pb, b.data(), sizeof(double) * b.size());
+  return SG_OK;
+}
+
+int32_t sg_set_spin_densities(sg_calculator* h, const double* Pa, const double* Pb) {
+  if (!h || !Pa || !Pb) return SG_ERR_INVALID_ARGUMENT;
+  return h->impl->set_spin_densities(Pa, Pb);
 }
 
 int32_t sg_get_atomic_charges(const sg_calculator* h, double* charges) {

@@ -153,6 +153,7 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
   ao_atom_.clear();
   order_.clear();
   density_given_ = false;
+  spin_given_ = false;
   stages_recorded_ = false;
   td_roots_ = 0;
   if (in.empty()) {
@@ -603,6 +604,55 @@ int Batch::set_start_density(const double* P, std::string& err) {
   return cudaStreamSynchronize(stream_) == cudaSuccess ? kOk : kErrCuda;
 }
 
+int Batch::set_start_spin_densities(const double* Pa, const double* Pb, std::string& err) {
+  if (mols_.empty()) {
+    err = "no structure";
+    return kErrEmptyStructure;
+  }
+  if (!uhf_) {
+    err = "spin densities apply to unrestricted calculations";
+    return kErrInvalidArgument;
+  }
+  const size_t n = (size_t)dev_.mat_total;
+  std::vector<double> P(n);
+  for (size_t k = 0; k < n; ++k) P[k] = Pa[k] + Pb[k];
+  cudaError_t e = cudaMemcpyAsync(dev_.Pa, Pa, sizeof(double) * n, cudaMemcpyHostToDevice, stream_);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dev_.Pb, Pb, sizeof(double) * n, cudaMemcpyHostToDevice, stream_);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dev_.P, P.data(), sizeof(double) * n, cudaMemcpyHostToDevice, stream_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  density_given_ = true;
+  spin_given_ = true;
+  return kOk;
+}
+
+int Batch::fetch_spin_densities(int mol, std::vector<double>& Pa, std::vector<double>& Pb, std::string& err) {
+  if (mol < 0 || mol >= (int)mols_.size()) {
+    err = "molecule index out of range";
+    return kErrInvalidArgument;
+  }
+  if (!dev_.uhf) {
+    err = "spin densities exist for unrestricted calculations only";
+    return kErrNoResults;
+  }
+  const MolDev& m = mols_[mol];
+  Pa.resize((size_t)m.nao * m.nao);
+  Pb.resize(Pa.size());
+  cudaError_t e = cudaMemcpyAsync(Pa.data(), dev_.Pa + m.mat_off, sizeof(double) * Pa.size(), cudaMemcpyDeviceToHost,
+                                  stream_);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(Pb.data(), dev_.Pb + m.mat_off, sizeof(double) * Pb.size(), cudaMemcpyDeviceToHost, stream_);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(stream_);
+  if (e != cudaSuccess) {
+    err = cuda_message(e);
+    return kErrCuda;
+  }
+  return kOk;
+}
+
 int Batch::run(const ScfParams& sp_in, bool gradient, std::string& err) {
   if (mols_.empty()) {
     err = "no structure";
@@ -613,6 +663,7 @@ int Batch::run(const ScfParams& sp_in, bool gradient, std::string& err) {
   ScfParams sp = sp_in;
   if (density_given_) sp.cold_sweeps = std::max(sp.cold_sweeps, 6);
   dev_.use_guess = density_given_ ? 0 : 1;
+  dev_.spin_given = spin_given_ ? 1 : 0;
   for (auto& ev : stage_ev_)
     if (!ev) cudaEventCreate(&ev);
   launches_ = 0;
@@ -698,6 +749,7 @@ int Batch::run(const ScfParams& sp_in, bool gradient, std::string& err) {
   cudaEventRecord(stage_ev_[4], stream_);
   stages_recorded_ = true;
   density_given_ = false;
+  spin_given_ = false;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     err = cuda_message(e);

@@ -73,6 +73,11 @@ class Batch {
   // the SCC (computed on the device with the final density), NDDO core charge
   // minus the atom's diagonal density (Mulliken in the orthogonal NDDO basis).
   int fetch_charges(int mol, std::vector<double>& q, std::string& err);
+  // Unrestricted batches: the spin densities of molecule mol, and start spin
+  // densities for the next run() (mat_total doubles each, the molecules' N x N
+  // blocks in order; the warm start of an open-shell geometry step).
+  int fetch_spin_densities(int mol, std::vector<double>& Pa, std::vector<double>& Pb, std::string& err);
+  int set_start_spin_densities(const double* Pa, const double* Pb, std::string& err);
   // alpha orbital energies (restricted: the orbital energies); beta = true: the beta ones
   int fetch_orbital_energies(int mol, std::vector<double>& eps, std::string& err, bool beta = false);
   // Linear-response TD-DFTB (DFTB2 / DFTB3 batches, after run()): the nroots
@@ -142,6 +147,7 @@ class Batch {
   long long npairs_ = 0, nhh_ = 0;  // pair and heavy-pair tables are built on the device
   std::string param_source_;
   bool uhf_ = false;
+  bool spin_given_ = false;
   std::shared_ptr<const NddoParamSet> nddo_set_;  // resolved NDDO source (nullptr: embedded)
   int scf_path_ = 0;
   void* td_scratch_ = nullptr;

@@ -63,6 +63,7 @@ struct DeviceBatch {
   double* Ppb = nullptr;            // [mat_total] DFTB: beta density in the orthogonal basis
   double* sshift = nullptr;         // [natoms * 2] DFTB: shell spin shifts eps_{a,s}, eps_{a,p}
   int use_guess = 1;                // 0: P already holds a start density
+  int spin_given = 0;               // unrestricted: Pa / Pb hold given start spin densities (P = Pa + Pb)
   int large = 0;                    // 1: one molecule over the whole GPU (large-molecule path)
   void* large_scratch = nullptr;    // [large_scf_scratch_bytes(nao)] when large
   // DFTB (H holds H0)

@@ -496,7 +496,7 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_dftb_uhf_scf(
     double* Fall, double* Call, double* W1all, double* W2all, double* epsall, double* diisall, double* Paall,
     double* Pball, double* Ppball, double* Fball, double* Cball, double* epsball, double* diisball, double* sshall,
     double* rotbuf, const double* __restrict__ gamall, const double* __restrict__ Gamall, double* qall, double* shall,
-    MolResult* res, ScfParams sp, int packed_in_smem, int order) {
+    MolResult* res, ScfParams sp, int packed_in_smem, int order, int spin_given) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ScfShared& sh = *reinterpret_cast<ScfShared*>(smem_raw);
   double* smemA = reinterpret_cast<double*>(smem_raw + ((sizeof(ScfShared) + 15) / 16) * 16);
@@ -545,7 +545,8 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_dftb_uhf_scf(
     int status = kDevOk;
     const int ns_it = inverse_sqrt(N, S, X, W1, Fa, Ca, W2, sh);
     if (ns_it < 0) status = kDevNonFinite;
-    for (size_t k = tid; k < NN; k += blockDim.x) Pa[k] = Pb[k] = 0.5 * P[k];
+    if (!spin_given)  // given spin densities (warm start) keep their polarisation
+      for (size_t k = tid; k < NN; k += blockDim.x) Pa[k] = Pb[k] = 0.5 * P[k];
     __syncthreads();
     int nhist = 0, head = 0, it = 0, converged = 0, nfull = 0, nsweeps = 0;
     bool have_a = false, have_b = false;
@@ -750,7 +751,7 @@ void launch_dftb_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaSt
     k_dftb_uhf_scf<<<grid, kScfThreads, bytes, s>>>(
         b.mols, b.nmol, b.order, b.counter, b.atoms, b.delems, b.ao_atom, b.H, b.S, b.X, b.P, b.Pp, b.F, b.C, b.W1,
         b.W2, b.eps, b.diis, b.Pa, b.Pb, b.Ppb, b.Fb, b.Cb, b.epsb, b.diisb, b.sshift, b.rotbuf, b.gam, b.Gam, b.qat,
-        b.ashift, b.res, sp, in_smem, b.dftb_order);
+        b.ashift, b.res, sp, in_smem, b.dftb_order, b.spin_given);
     return;
   }
   k_dftb_scf<<<grid, kScfThreads, bytes, s>>>(b.mols, b.nmol, b.order, b.counter, b.atoms, b.delems, b.ao_atom, b.H,

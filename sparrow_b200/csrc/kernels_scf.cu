@@ -584,7 +584,8 @@ __device__ double spin_exchange(const MolDev& m, const AtomDev* __restrict__ ato
 
 // The persistent kernel of k_scf for unrestricted molecules (MolDev.nocc
 // alpha and MolDev.nocc_b beta electrons): start P_a = P_b = P / 2 from the
-// restricted guess (or a given total density), then per iteration the Fock
+// restricted guess or a given total density (or from given spin densities,
+// spin_given, with P = P_a + P_b), then per iteration the Fock
 // pair, one DIIS over both spins, new orbitals and densities per spin;
 // convergence on |dE| and the larger rms change of the two spin densities.
 __global__ void __launch_bounds__(kScfThreads, 1) k_uhf_scf(
@@ -593,7 +594,7 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_uhf_scf(
     const double* __restrict__ ints, const int* __restrict__ hh_pairs, double* jbuf, const double* __restrict__ Hall,
     double* Pall, double* Fall, double* Call, double* W1all, double* W2all, double* epsall, double* diisall,
     double* Paall, double* Pball, double* Fball, double* Cball, double* epsball, double* diisball, double* rotbuf,
-    MolResult* res, ScfParams sp, int packed_in_smem) {
+    MolResult* res, ScfParams sp, int packed_in_smem, int spin_given) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   ScfShared& sh = *reinterpret_cast<ScfShared*>(smem_raw);
   double* smemA = reinterpret_cast<double*>(smem_raw + ((sizeof(ScfShared) + 15) / 16) * 16);
@@ -632,7 +633,8 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_uhf_scf(
     const int cap_rounds = (int)((kRotBudgetBytes / sizeof(double)) / (2 * ((N + 1) / 2)));
     const int msize = sp.diis_size < 1 ? 1 : (sp.diis_size > kDiisMax ? kDiisMax : sp.diis_size);
     const int cold_sweeps = sp.cold_sweeps > 0 ? sp.cold_sweeps : 3;
-    for (size_t k = tid; k < NN; k += blockDim.x) Pa[k] = Pb[k] = 0.5 * P[k];
+    if (!spin_given)
+      for (size_t k = tid; k < NN; k += blockDim.x) Pa[k] = Pb[k] = 0.5 * P[k];
     __syncthreads();
     int nhist = 0, head = 0;
     bool have_a = false, have_b = false;
@@ -744,7 +746,8 @@ void launch_uhf_scf(const DeviceBatch& b, const ScfParams& sp, int grid, cudaStr
   if (grid > b.nmol) grid = b.nmol;
   k_uhf_scf<<<grid, kScfThreads, bytes, s>>>(b.mols, b.nmol, b.order, b.counter, b.atoms, b.elems, b.pairs, b.ints,
                                              b.hh_pairs, b.jbuf, b.H, b.P, b.F, b.C, b.W1, b.W2, b.eps, b.diis, b.Pa,
-                                             b.Pb, b.Fb, b.Cb, b.epsb, b.diisb, b.rotbuf, b.res, sp, in_smem);
+                                             b.Pb, b.Fb, b.Cb, b.epsb, b.diisb, b.rotbuf, b.res, sp, in_smem,
+                                             b.spin_given);
 }
 
 }  // namespace sgb

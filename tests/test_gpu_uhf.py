@@ -160,3 +160,26 @@ def test_edge_occupations(method):
         assert np.max(np.abs(r.gradients - ref["gradient"])) < G_TOL, (method, Z)
         assert np.max(np.abs(np.sort(c.orbital_energies()) - ref["eps_alpha"])) < 1e-6
         assert np.max(np.abs(np.sort(c.beta_orbital_energies()) - ref["eps_beta"])) < 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("method", ["PM6", "DFTB2"])
+def test_spin_density_warm_start(method):
+    # getState / loadState of an open shell: a restart from the converged spin
+    # densities is converged at once, with the same energy
+    Z, x, _, _ = _radicals()[1]  # CH3
+    c = sparrow_b200.get_calculator(method)
+    c.set_structure(Z, x)
+    c.settings["spin_multiplicity"] = 2
+    c.settings["density_rmsd_criterion"] = 1e-9
+    c.settings["self_consistence_criterion"] = 1e-10
+    r1 = c.calculate()
+    Pa, Pb = c.spin_densities()
+    if method == "PM6":  # orthonormal basis: the traces count the electrons of each spin
+        assert abs(np.trace(Pa) - 4) < 1e-9 and abs(np.trace(Pb) - 3) < 1e-9
+    assert np.max(np.abs(Pa + Pb - c.density())) < 1e-12
+    c.set_spin_densities(Pa, Pb)
+    r2 = c.calculate()
+    assert r1.successful_calculation and r2.successful_calculation
+    assert r2.iterations <= 3 < r1.iterations
+    assert abs(r1.energy - r2.energy) < 1e-9
