@@ -57,6 +57,7 @@ extern "C" {
 #define SG_PROP_GRADIENTS 2u
 #define SG_PROP_HESSIAN 4u /* semi-numerical: central differences of analytic gradients */
 #define SG_PROP_ATOMIC_CHARGES 8u
+#define SG_PROP_DIPOLE 16u
 
 typedef struct sg_calculator sg_calculator;
 typedef struct sg_batch sg_batch;
@@ -137,6 +138,12 @@ int32_t sg_get_hessian(const sg_calculator* h, double* hessian);
  * the SCC's Mulliken charges, NDDO the core charge minus the atom's diagonal
  * density (Mulliken charges in the orthogonal NDDO basis). */
 int32_t sg_get_atomic_charges(const sg_calculator* h, double* charges);
+/* Dipole moment (x, y, z in e bohr) of the last calculate() with
+ * SG_PROP_DIPOLE required: DFTB sum_a q_a R_a with the Mulliken charges
+ * (Dftb/Utils/DipoleUtils/DFTBDipoleMomentCalculator.cpp:23-35); NDDO in the
+ * NDDO approximation about the centre of mass, sum_a q_a (R_a - R_cm) -
+ * 2 D_sp1 P_{s,p} per s/p atom (Nddo/Utils/DipoleUtils/NDDODipoleMomentCalculator.cpp:76-110). */
+int32_t sg_get_dipole(const sg_calculator* h, double* dipole3);
 /* One call: the same Hessian for one molecule (method spec as for
  * sg_batch_create; unrestricted != 0 or multiplicity != 1 runs the
  * unrestricted SCF; step <= 0 takes 0.01 bohr).  not_converged (may be NULL)

@@ -27,6 +27,7 @@ SG_PROP_ENERGY = 1
 SG_PROP_GRADIENTS = 2
 SG_PROP_HESSIAN = 4
 SG_PROP_ATOMIC_CHARGES = 8
+SG_PROP_DIPOLE = 16
 SG_ERR_NOT_CONVERGED = 6
 SG_ERR_TIMEOUT = 12
 SG_PENDING = 13
@@ -88,6 +89,7 @@ def lib():
         "sg_get_beta_orbital_energies": (ctypes.c_int32, [_VP, _D]),
         "sg_get_hessian": (ctypes.c_int32, [_VP, _D]),
         "sg_get_atomic_charges": (ctypes.c_int32, [_VP, _D]),
+        "sg_get_dipole": (ctypes.c_int32, [_VP, _D]),
         "sg_get_spin_densities": (ctypes.c_int32, [_VP, _D, _D]),
         "sg_set_spin_densities": (ctypes.c_int32, [_VP, _D, _D]),
         "sg_calculate_hessian": (ctypes.c_int32, [ctypes.c_char_p, ctypes.c_int32, _I32, _D, ctypes.c_int32,
@@ -166,6 +168,7 @@ class Results:
         self.n_occupied = n_occupied
         self.hessian = None  # (3 n_atoms, 3 n_atoms) when "hessian" was required
         self.atomic_charges = None  # (n_atoms,) when "atomic_charges" was required
+        self.dipole = None  # (3,) e bohr when "dipole" was required
 
 
 class _Settings:
@@ -275,6 +278,8 @@ class Calculator:
                 mask |= SG_PROP_HESSIAN | SG_PROP_ENERGY
             elif p in ("atomic_charges", "charges"):
                 mask |= SG_PROP_ATOMIC_CHARGES | SG_PROP_ENERGY
+            elif p == "dipole":
+                mask |= SG_PROP_DIPOLE | SG_PROP_ENERGY
             else:
                 raise ValueError("unsupported property %r" % p)
         self._check(lib().sg_set_required_properties(self._h, mask))
@@ -299,6 +304,10 @@ class Calculator:
             q = np.zeros(self._n_atoms)
             self._check(L.sg_get_atomic_charges(self._h, _dptr(q)))
             res.atomic_charges = q
+        if getattr(self, "_mask", SG_PROP_ENERGY) & SG_PROP_DIPOLE:
+            d = np.zeros(3)
+            self._check(L.sg_get_dipole(self._h, _dptr(d)))
+            res.dipole = d
         if getattr(self, "_mask", SG_PROP_ENERGY) & SG_PROP_HESSIAN:
             n3 = 3 * self._n_atoms
             H = np.zeros(n3 * n3)

@@ -136,6 +136,11 @@ class Calculator {
     batch_->fetch_orbital_energies(0, eps_, error);
     charges_.clear();
     if (required_ & SG_PROP_ATOMIC_CHARGES) batch_->fetch_charges(0, charges_, error);
+    dipole_.clear();
+    if (required_ & SG_PROP_DIPOLE) {
+      dipole_.resize(3);
+      batch_->dipole(0, dipole_.data(), error);
+    }
     eps_b_.clear();
     dens_a_.clear();
     dens_b_.clear();
@@ -168,6 +173,7 @@ class Calculator {
   }
   const std::vector<double>& hessian() const { return hessian_; }
   const std::vector<double>& atomic_charges() const { return charges_; }
+  const std::vector<double>& dipole() const { return dipole_; }
   const std::vector<double>& alpha_density() const { return dens_a_; }
   const std::vector<double>& beta_density() const { return dens_b_; }
   int set_spin_densities(const double* Pa, const double* Pb) {
@@ -269,7 +275,7 @@ class Calculator {
   uint32_t required_ = SG_PROP_ENERGY;
   MoleculeOutput result_;
   bool have_result_ = false, have_gradient_ = false;
-  std::vector<double> density_, eps_, eps_b_, state_, hessian_, charges_;
+  std::vector<double> density_, eps_, eps_b_, state_, hessian_, charges_, dipole_;
   std::vector<double> dens_a_, dens_b_, state_a_, state_b_;  // unrestricted: spin densities and their start
 };
 
@@ -443,7 +449,7 @@ int32_t sg_get_setting_int(const sg_calculator* h, const char* key, int64_t* v) 
 
 int32_t sg_set_required_properties(sg_calculator* h, uint32_t mask) {
   if (!h) return SG_ERR_INVALID_ARGUMENT;
-  if (mask & ~(SG_PROP_ENERGY | SG_PROP_GRADIENTS | SG_PROP_HESSIAN | SG_PROP_ATOMIC_CHARGES))
+  if (mask & ~(SG_PROP_ENERGY | SG_PROP_GRADIENTS | SG_PROP_HESSIAN | SG_PROP_ATOMIC_CHARGES | SG_PROP_DIPOLE))
     return fail(h, SG_ERR_INVALID_ARGUMENT, "unknown property bit");
   h->impl->set_required(mask);
   return SG_OK;
@@ -482,6 +488,14 @@ int32_t sg_get_spin_densities(const sg_calculator* h, double* Pa, double* Pb) {
 int32_t sg_set_spin_densities(sg_calculator* h, const double* Pa, const double* Pb) {
   if (!h || !Pa || !Pb) return SG_ERR_INVALID_ARGUMENT;
   return h->impl->set_spin_densities(Pa, Pb);
+}
+
+int32_t sg_get_dipole(const sg_calculator* h, double* dipole3) {
+  if (!h || !dipole3) return SG_ERR_INVALID_ARGUMENT;
+  const auto& v = h->impl->dipole();
+  if (!h->impl->have_result() || v.size() != 3) return SG_ERR_NO_RESULTS;
+  std::memcpy(dipole3, v.data(), 3 * sizeof(double));
+  return SG_OK;
 }
 
 int32_t sg_get_atomic_charges(const sg_calculator* h, double* charges) {

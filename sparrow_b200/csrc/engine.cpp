@@ -974,6 +974,46 @@ int Batch::fetch_charges(int mol, std::vector<double>& q, std::string& err) {
   return kOk;
 }
 
+int Batch::dipole(int mol, double out[3], std::string& err) {
+  std::vector<double> q;
+  int rc = fetch_charges(mol, q, err);
+  if (rc) return rc;
+  const MolDev& m = mols_[mol];
+  out[0] = out[1] = out[2] = 0.0;
+  if (is_dftb(method_)) {
+    for (int a = 0; a < m.nat; ++a) {
+      const AtomDev& A = atoms_[m.atom0 + a];
+      out[0] += q[a] * A.x;
+      out[1] += q[a] * A.y;
+      out[2] += q[a] * A.z;
+    }
+    return kOk;
+  }
+  std::vector<double> P;
+  rc = fetch_density(mol, P, err);
+  if (rc) return rc;
+  double com[3] = {0, 0, 0}, mass = 0;
+  for (int a = 0; a < m.nat; ++a) {
+    const AtomDev& A = atoms_[m.atom0 + a];
+    const double w = standard_atomic_mass(elems_[A.slot].Z);
+    com[0] += w * A.x;
+    com[1] += w * A.y;
+    com[2] += w * A.z;
+    mass += w;
+  }
+  for (double& c : com) c = mass > 0 ? c / mass : 0.0;
+  for (int a = 0; a < m.nat; ++a) {
+    const AtomDev& A = atoms_[m.atom0 + a];
+    const ElemDev& E = elems_[A.slot];
+    out[0] += q[a] * (A.x - com[0]);
+    out[1] += q[a] * (A.y - com[1]);
+    out[2] += q[a] * (A.z - com[2]);
+    if (E.nao == 4)
+      for (int k = 0; k < 3; ++k) out[k] -= 2.0 * E.D[1] * P[(size_t)A.ao0 * m.nao + A.ao0 + 1 + k];
+  }
+  return kOk;
+}
+
 int Batch::fetch_orbital_energies(int mol, std::vector<double>& eps, std::string& err, bool beta) {
   if (mol < 0 || mol >= (int)mols_.size()) {
     err = "molecule index out of range";

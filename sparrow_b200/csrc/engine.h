@@ -73,6 +73,11 @@ class Batch {
   // the SCC (computed on the device with the final density), NDDO core charge
   // minus the atom's diagonal density (Mulliken in the orthogonal NDDO basis).
   int fetch_charges(int mol, std::vector<double>& q, std::string& err);
+  // Dipole moment (e bohr) of molecule mol after run(): DFTB sum_a q_a R_a
+  // (Dftb/Utils/DipoleUtils/DFTBDipoleMomentCalculator.cpp:23-35); NDDO the
+  // NDDO approximation about the centre of mass, sum_a q_a (R_a - R_cm) minus
+  // 2 D_sp1 P_{s,p} per s/p atom (Nddo/Utils/DipoleUtils/NDDODipoleMomentCalculator.cpp:76-110).
+  int dipole(int mol, double out[3], std::string& err);
   // Unrestricted batches: the spin densities of molecule mol, and start spin
   // densities for the next run() (mat_total doubles each, the molecules' N x N
   // blocks in order; the warm start of an open-shell geometry step).

@@ -140,6 +140,20 @@ const NddoRawDiatomic* nddo_embedded_diatomic(Method m, size_t& count) {
 
 int nddo_shell_n(int Z, int l) { return l == 0 ? shell_n_s(Z) : shell_n_p(Z); }
 
+double standard_atomic_mass(int Z) {
+  // IUPAC standard atomic weights (conventional values), Z = 1..56
+  static const double m[] = {0.0,       1.00794,    4.002602,  6.941,       9.012182,  10.811,     12.0107,
+                             14.0067,   15.9994,    18.9984032, 20.1797,    22.98976928, 24.3050,  26.9815386,
+                             28.0855,   30.973762,  32.065,    35.453,      39.948,    39.0983,    40.078,
+                             44.955912, 47.867,     50.9415,   51.9961,     54.938045, 55.845,     58.933195,
+                             58.6934,   63.546,     65.38,     69.723,      72.64,     74.92160,   78.96,
+                             79.904,    83.798,     85.4678,   87.62,       88.90585,  91.224,     92.90638,
+                             95.96,     98.0,       101.07,    102.90550,   106.42,    107.8682,   112.411,
+                             114.818,   118.710,    121.760,   127.60,      126.90447, 131.293,    132.9054519,
+                             137.327};
+  return (Z >= 1 && Z < (int)(sizeof(m) / sizeof(m[0]))) ? m[Z] : 0.0;
+}
+
 int engine_n_aos(Method m, int Z, const NddoParamSet* set) {
   if (is_dftb(m)) return dftb_n_aos(dftb_default_set(m), Z);
   const NddoRawAtomic* r = raw_for(m, Z, set);

@@ -41,6 +41,10 @@ DiatomicDev make_diatomic(Method m, int Z1, int Z2, const NddoParamSet* set = nu
 const NddoRawAtomic* nddo_embedded_atomic(Method m, size_t& count);
 const NddoRawDiatomic* nddo_embedded_diatomic(Method m, size_t& count);
 
+// Standard atomic weight of element Z (u), 0 for elements outside the table
+// (centre of mass of the NDDO dipole moment).
+double standard_atomic_mass(int Z);
+
 // Principal quantum number of the valence s (l = 0) or p (l = 1) shell of
 // element Z (PrincipalQuantumNumbers.cpp:20-57).
 int nddo_shell_n(int Z, int l);
