@@ -104,6 +104,9 @@ int32_t sg_get_energy(const sg_calculator* h, double* energy);
 int32_t sg_get_gradients(const sg_calculator* h, double* gradients);
 int32_t sg_get_scf_info(const sg_calculator* h, int32_t* iterations, int32_t* converged, int32_t* n_aos,
                         int32_t* n_occupied);
+/* Orbital energies (n_aos); SG_ERR_NO_RESULTS after a calculation on the
+ * large-molecule path ("scf_path" large / large_mixed, or automatic above 1024
+ * AOs), which purifies the density and computes no orbitals. */
 int32_t sg_get_orbital_energies(const sg_calculator* h, double* eps);
 /* density matrix (n_aos x n_aos, row-major) of the last calculation, and a
  * start density for the next one (warm start) */

@@ -133,6 +133,7 @@ class Calculator {
     have_result_ = true;
     have_gradient_ = grad;
     batch_->fetch_density(0, density_, error);
+    eps_.clear();  // stays empty on the large-molecule path, which has no orbitals
     batch_->fetch_orbital_energies(0, eps_, error);
     charges_.clear();
     if (required_ & SG_PROP_ATOMIC_CHARGES) batch_->fetch_charges(0, charges_, error);
@@ -527,8 +528,8 @@ int32_t sg_get_scf_info(const sg_calculator* h, int32_t* it, int32_t* conv, int3
 
 int32_t sg_get_orbital_energies(const sg_calculator* h, double* eps) {
   if (!h || !eps) return SG_ERR_INVALID_ARGUMENT;
-  if (!h->impl->have_result()) return SG_ERR_NO_RESULTS;
   const auto& v = h->impl->orbital_energies();
+  if (!h->impl->have_result() || v.empty()) return SG_ERR_NO_RESULTS;  // none on the large-molecule path
   std::memcpy(eps, v.data(), sizeof(double) * v.size());
   return SG_OK;
 }

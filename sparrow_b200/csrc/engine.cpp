@@ -1023,6 +1023,10 @@ int Batch::fetch_orbital_energies(int mol, std::vector<double>& eps, std::string
     err = "beta orbital energies exist for unrestricted calculations only";
     return kErrNoResults;
   }
+  if (dev_.large) {
+    err = "the large-molecule path (density purification) computes no orbitals";
+    return kErrNoResults;
+  }
   const MolDev& m = mols_[mol];
   eps.resize(m.nao);
   const double* src = (beta ? dev_.epsb : dev_.eps) + m.ao_base;

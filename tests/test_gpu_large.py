@@ -84,6 +84,10 @@ def test_calculator_takes_large_path_above_1024_aos():
     assert res.successful_calculation and res.n_aos == 1056
     _, e, _, _, conv = run_one("PM6", Z, x, "large", gradients=False)
     assert conv and abs(res.energy - e) < 1e-9
+    # density purification: no orbitals, so no orbital energies
+    with pytest.raises(sparrow_b200.SparrowError) as ei:
+        c.orbital_energies()
+    assert ei.value.code == 9
 
 
 def test_large_path_rejects_batches_and_dftb():
