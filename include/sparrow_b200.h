@@ -22,6 +22,12 @@
  *   sg_get_density / sg_set_density
  *                             Implementations/GenericMethodWrapper.cpp:268-282 (getState/loadState)
  *   sg_get_orbital_energies   results() OrbitalEnergies
+ *   sg_get_beta_orbital_energies  results() OrbitalEnergies (beta, unrestricted)
+ *   sg_get_hessian            results() Hessian (GenericMethodWrapper.cpp:58-88: semi-numerical)
+ *   sg_get_atomic_charges     results() AtomicCharges (GenericMethodWrapper.cpp:212-214)
+ *   sg_get_dipole             results() Dipole (GenericMethodWrapper.cpp:89-92)
+ *   sg_get_spin_densities / sg_set_spin_densities
+ *                             getState / loadState of an unrestricted calculation
  *   sg_clone                  Implementations/Nddo/Pm6/Wrapper/PM6MethodWrapper.cpp:38-45 (clone)
  * The batch entry points (sg_batch_*) have no counterpart in the reference:
  * they run many independent molecules through one device launch sequence.
