@@ -84,3 +84,22 @@ def test_excitation_entry_points_check_their_arguments():
     assert L.sg_batch_excitations(None, 4, 0, om_p, None, None) == 1
     assert L.sg_batch_set_scf_path(None, 2) == 1
     assert L.sg_batch_set_mixed_switch(None, 1e-5) == 1
+
+
+def test_property_getters_check_their_arguments():
+    # charges, dipole, Hessian and the open-shell getters: null arguments are
+    # SG_ERR_INVALID_ARGUMENT, a handle without a calculation SG_ERR_NO_RESULTS
+    L = sparrow_b200.lib()
+    c = sparrow_b200.get_calculator("PM6")
+    buf = np.zeros(64)
+    p = buf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    for name in ("sg_get_hessian", "sg_get_atomic_charges", "sg_get_dipole", "sg_get_beta_orbital_energies"):
+        fn = getattr(L, name)
+        assert fn(None, p) == 1, name
+        assert fn(c._h, None) == 1, name
+        assert fn(c._h, p) == 9, name
+    assert L.sg_get_spin_densities(None, p, p) == 1
+    assert L.sg_get_spin_densities(c._h, p, None) == 1
+    assert L.sg_get_spin_densities(c._h, p, p) == 9
+    assert L.sg_set_spin_densities(None, p, p) == 1
+    assert L.sg_set_spin_densities(c._h, None, p) == 1
