@@ -455,12 +455,13 @@ class ClockSampler:
 
     def __init__(self):
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "bench_clocks.csv")
+        self.path = None
 
     def start(self):
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
-            self.f = open(self.path, "w")
+            import tempfile
+            fd, self.path = tempfile.mkstemp(prefix="sparrow_b200_clocks_", suffix=".csv")
+            self.f = os.fdopen(fd, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
                                           "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
@@ -491,6 +492,10 @@ class ClockSampler:
             for n, v in zip(names, parts[5:9]):
                 if v.lower() == "active":
                     reasons.add(n)
+        try:
+            os.unlink(self.path)
+        except OSError:
+            pass
         if not sm:
             return None
         sm.sort()

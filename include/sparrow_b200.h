@@ -307,12 +307,15 @@ int32_t sg_server_stats(sg_server* s, int64_t* submitted, int64_t* completed, in
  * fixed host array: the call performs no device or pinned allocation.
  * Limits: SG_STATIC_MAX_ATOMS atoms and SG_STATIC_MAX_AOS AOs; larger
  * molecules return SG_ERR_INVALID_ARGUMENT with a message.
- * The first call on a device (with that device current) does a one-time
- * set-up: it looks the scratch array up with cudaGetSymbolAddress, uploads
- * the constant multipole tables and synchronises the stream; make that first
- * call before any stream capture.  Calls that overlap in time share the
- * scratch and race: serialise them.  stream is a cudaStream_t (NULL = the
- * default stream); the call returns after the stream has been synchronised.
+ * The first call on a device (with that device current) does the set-up: it
+ * looks the scratch array up with cudaGetSymbolAddress; make that first call
+ * before any stream capture begins.  Every call repeats that lookup, copies
+ * the constant multipole table and the molecule's descriptors from pageable
+ * host memory, and synchronises the stream before it returns, so a
+ * cudaDeviceReset between calls is safe.  Calls that overlap in time share
+ * the scratch and race: serialise them.  stream is a cudaStream_t (NULL = the
+ * default stream).  The electron count must be even and fit the orbitals
+ * (SG_ERR_ODD_ELECTRONS otherwise, before any device work).
  * Status codes as for sg_batch_results (SG_ERR_NOT_CONVERGED still fills the
  * outputs). */
 #define SG_STATIC_MAX_ATOMS 64

@@ -274,24 +274,31 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
       heavy += e.nao == 4 ? 1 : 0;
     }
     md.nao = nao;
-    md.nel = (int)std::lround(ncore) - mol.charge;
+    // electron count in 64 bits: any int charge or multiplicity is range-checked
+    // before it can size an orbital block (n_occ <= n_AO for every spin)
+    const long long nel = std::llround(ncore) - (long long)mol.charge;
     if (uhf_) {
       // n_alpha - n_beta = multiplicity - 1
-      const int na2 = md.nel + mol.multiplicity - 1;
-      if (md.nel < 0 || mol.multiplicity < 1 || (na2 & 1) || md.nel - (mol.multiplicity - 1) < 0 || na2 / 2 > nao) {
-        err = "molecule " + std::to_string(mi) + ": " + std::to_string(md.nel) +
-              " electrons do not fit spin multiplicity " + std::to_string(mol.multiplicity);
+      const long long na2 = nel + (long long)mol.multiplicity - 1;
+      if (nel < 0 || mol.multiplicity < 1 || (na2 & 1) || nel - ((long long)mol.multiplicity - 1) < 0 ||
+          na2 / 2 > nao) {
+        err = "molecule " + std::to_string(mi) + ": " + std::to_string(nel) +
+              " electrons do not fit spin multiplicity " + std::to_string(mol.multiplicity) + " in " +
+              std::to_string(nao) + " orbitals";
         return kErrOddElectrons;
       }
-      md.nocc = na2 / 2;
+      md.nel = (int)nel;
+      md.nocc = (int)(na2 / 2);
       md.nocc_b = md.nel - md.nocc;
     } else {
-      if (md.nel < 0 || (md.nel & 1) || mol.multiplicity != 1) {
-        err = "molecule " + std::to_string(mi) + " has " + std::to_string(md.nel) + " electrons and multiplicity " +
-              std::to_string(mol.multiplicity) + ": the restricted closed-shell SCF needs an even, non-negative "
-              "count and a singlet (use the unrestricted SCF)";
+      if (nel < 0 || (nel & 1) || mol.multiplicity != 1 || nel / 2 > nao) {
+        err = "molecule " + std::to_string(mi) + " has " + std::to_string(nel) + " electrons, " +
+              std::to_string(nao) + " orbitals and multiplicity " + std::to_string(mol.multiplicity) +
+              ": the restricted closed-shell SCF needs an even, non-negative count of at most two per "
+              "orbital and a singlet (use the unrestricted SCF)";
         return kErrOddElectrons;
       }
+      md.nel = (int)nel;
       md.nocc = md.nel / 2;
       md.nocc_b = md.nocc;
     }

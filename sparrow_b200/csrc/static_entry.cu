@@ -8,11 +8,14 @@
 // use on the per-call path.
 //
 // Set-up: the first call on a device (with that device current) looks up the
-// scratch array's address with cudaGetSymbolAddress, uploads the local
-// multipole term table to constant memory and records that the device is
-// ready.  The first call should therefore come before any stream capture.
-// Calls that overlap in time (from two host threads, or on two streams of one
-// device) share the scratch and race; callers serialise them.
+// scratch array's address with cudaGetSymbolAddress and builds the local
+// multipole term table on the host; make that first call before any stream
+// capture begins.  Every call (the first included) repeats the address lookup,
+// uploads the term table to constant memory from pageable host memory and
+// synchronises the stream before it returns, so the entry point stays valid
+// after a cudaDeviceReset.  Calls that overlap in time (from two host threads,
+// or on two streams of one device) share the scratch and race; callers
+// serialise them.
 #include <cctype>
 #include <cmath>
 #include <cstdarg>
@@ -186,12 +189,15 @@ extern "C" int32_t sg_calculate_static(const char* method, int32_t n_atoms, cons
     set_error(error_message, error_capacity, "%d AOs exceed the allocation-free limit of %d AOs", nao, kStaticMaxAos);
     return SG_ERR_INVALID_ARGUMENT;
   }
-  const int nel = (int)std::lround(ncore) - charge;
-  if (nel < 0 || (nel & 1)) {
+  // 64-bit count: any int charge is range-checked before it sizes the occupied block
+  const long long nel_ll = std::llround(ncore) - (long long)charge;
+  if (nel_ll < 0 || (nel_ll & 1) || nel_ll / 2 > nao) {
     set_error(error_message, error_capacity,
-              "%d electrons: the restricted closed-shell SCF needs an even, non-negative count", nel);
+              "%lld electrons in %d orbitals: the restricted closed-shell SCF needs an even, non-negative count of "
+              "at most two per orbital", nel_ll, nao);
     return SG_ERR_ODD_ELECTRONS;
   }
+  const int nel = (int)nel_ll;
   DiatomicDev diat[kMaxElementSlots * kMaxElementSlots];
   for (int i = 0; i < kMaxElementSlots * kMaxElementSlots; ++i) diat[i] = DiatomicDev();
   for (int i = 0; i < n_slots; ++i)
@@ -266,7 +272,12 @@ extern "C" int32_t sg_calculate_static(const char* method, int32_t n_atoms, cons
     return SG_ERR_CUDA;
   }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (!g_scratch_ptr[dev]) {
+  // The scratch address is looked up on every call (a host-side table lookup
+  // after the first) and compared with the cached one, and the constant
+  // multipole table (a few KB) is uploaded on every call: after a
+  // cudaDeviceReset the next call sees the new context's address and refills
+  // its constant memory instead of using a stale pointer or an empty table.
+  {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_static_scratch);
     if (e != cudaSuccess || !p) {
@@ -278,14 +289,9 @@ extern "C" int32_t sg_calculate_static(const char* method, int32_t n_atoms, cons
       build_local_term_table(g_static_terms);
       g_static_terms_built = true;
     }
-    upload_local_terms(g_static_terms, s);
-    e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
-      set_error(error_message, error_capacity, "constant table upload failed: %s", cudaGetErrorString(e));
-      return SG_ERR_CUDA;
-    }
     g_scratch_ptr[dev] = static_cast<unsigned char*>(p);
   }
+  upload_local_terms(g_static_terms, s);
   unsigned char* base = g_scratch_ptr[dev];
 
   DeviceBatch d;

@@ -26,6 +26,13 @@ import os
 import re
 import sys
 
+
+def _reference_root():
+    """The reference checkout, a required first command-line argument."""
+    if len(sys.argv) < 2:
+        sys.exit("usage: %s <path of the reference checkout>" % os.path.basename(sys.argv[0]))
+    return sys.argv[1]
+
 ELEMENTS = ["H", "C", "N", "O"]
 Z = {"H": 1, "C": 6, "N": 7, "O": 8}
 SETS = ["mio-1-1", "3ob-3-1", "3ob-2-1"]
@@ -105,7 +112,7 @@ def lit(s):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = _reference_root()
     base = os.path.join(ref, "src/Sparrow/Sparrow/Resources/Dftb")
     here = os.path.dirname(os.path.abspath(__file__))
     out = os.path.join(here, "..", "csrc", "dftb_tables.inc")

@@ -24,6 +24,13 @@ import os
 import re
 import sys
 
+
+def _reference_root():
+    """The reference checkout, a required first command-line argument."""
+    if len(sys.argv) < 2:
+        sys.exit("usage: %s <path of the reference checkout>" % os.path.basename(sys.argv[0]))
+    return sys.argv[1]
+
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "..", "csrc", "nddo_tables.inc")
 
@@ -53,7 +60,7 @@ def read_sto6g(path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = _reference_root()
     res = os.path.join(ref, "src", "Sparrow", "Sparrow", "Resources")
     out = []
     out.append("// Generated by sparrow_b200/params/gen_tables.py from the reference's published\n")

@@ -8,7 +8,7 @@ commented-out) restricted test: the geometry (Angstrom), the parameter set,
 the expected energy (Hartree) with its tolerance, Mulliken charges,
 orbital energies and forces with their tolerances, and the source file:line.
 
-It runs only where the reference checkout exists (/root/reference by default);
+It runs only where the reference checkout exists (its path is the first argument);
 the JSON it writes is committed and is what the tests read.
 
 Usage: python tests/golden/extract_dftb_vectors.py [reference_root]
@@ -21,6 +21,13 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 from extract_reference_vectors import NUM, XYZ_LINE, test_blocks  # noqa: E402
+
+
+def _reference_root():
+    """The reference checkout, a required first command-line argument."""
+    if len(sys.argv) < 2:
+        sys.exit("usage: %s <path of the reference checkout>" % os.path.basename(sys.argv[0]))
+    return sys.argv[1]
 
 OUT = os.path.join(HERE, "dftb_known_answers.json")
 
@@ -66,7 +73,7 @@ def parse(name, body, line, rel, order):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = _reference_root()
     out = {"tests": []}
     for fname, order in (("DFTB2Test.cpp", 2), ("DFTB3Test.cpp", 3)):
         rel = "src/Sparrow/Tests/MethodsTests/Dftb/" + fname

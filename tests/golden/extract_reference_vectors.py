@@ -7,7 +7,7 @@ the geometry (Angstrom, or bohr for the Python test), the expected one-electron
 matrix (eV), energies (eV or Hartree) and gradients, with the tolerance the
 reference asserts and the source file:line it came from.
 
-It runs only where the reference checkout exists (/root/reference by default);
+It runs only where the reference checkout exists (its path is the first argument);
 the JSON it writes is committed and is what the tests read.
 
 Usage: python tests/golden/extract_reference_vectors.py [reference_root]
@@ -16,6 +16,13 @@ import json
 import os
 import re
 import sys
+
+
+def _reference_root():
+    """The reference checkout, a required first command-line argument."""
+    if len(sys.argv) < 2:
+        sys.exit("usage: %s <path of the reference checkout>" % os.path.basename(sys.argv[0]))
+    return sys.argv[1]
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "nddo_known_answers.json")
@@ -79,7 +86,7 @@ def parse_block(name, body, line, rel):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = _reference_root()
     tests = os.path.join(ref, "src", "Sparrow", "Tests", "MethodsTests")
     out = {"note": "transcribed from the reference's test sources by extract_reference_vectors.py",
            "methods": {}}

@@ -8,7 +8,7 @@ same molecule.  This script reads that source as text and records, per
 test, the geometry (Angstrom), the parameter set, the expected values with
 their tolerances and the source file:line.
 
-It runs only where the reference checkout exists (/root/reference by default);
+It runs only where the reference checkout exists (its path is the first argument);
 the JSON it writes is committed and is what the tests read.
 
 Usage: python tests/golden/extract_tddftb_vectors.py [reference_root]
@@ -22,12 +22,19 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 from extract_reference_vectors import NUM, XYZ_LINE, test_blocks  # noqa: E402
 
+
+def _reference_root():
+    """The reference checkout, a required first command-line argument."""
+    if len(sys.argv) < 2:
+        sys.exit("usage: %s <path of the reference checkout>" % os.path.basename(sys.argv[0]))
+    return sys.argv[1]
+
 OUT = os.path.join(HERE, "tddftb_known_answers.json")
 REL = "src/Sparrow/Tests/TimeDependent/TDDFTBTest.cpp"
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = _reference_root()
     text = open(os.path.join(ref, REL)).read()
     out = {"source": REL, "tests": []}
     for name, body, line in test_blocks(text):

@@ -9,12 +9,19 @@ and with DFTB2 on ethanol the DFTB+ vector (-0.36023764, -0.21653604,
 -0.38972594) e bohr at 1e-6 (:220-230).  This script copies the structures
 out of the test file and writes tests/golden/dipole_known_answers.json.
 Run from the repository root with the reference checkout at the given path
-(default /root/reference).
+(a required argument).
 """
 import json
 import os
 import re
 import sys
+
+
+def _reference_root():
+    """The reference checkout, a required first command-line argument."""
+    if len(sys.argv) < 2:
+        sys.exit("usage: %s <path of the reference checkout>" % os.path.basename(sys.argv[0]))
+    return sys.argv[1]
 
 TEST = "src/Sparrow/Tests/Dipole/MopacDipoleTest.cpp"
 
@@ -49,4 +56,4 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(_reference_root())

@@ -9,11 +9,18 @@ structures of src/Sparrow/Tests/AppTests/:
   MNDO -320.713, AM1 -410.523, PM6 -125.561, DFTB2 -158.922, DFTB3 -69.2154.
 This script copies the two geometries (Angstrom) and those values into
 tests/golden/hessian_known_answers.json.  Run from the repository root with the
-reference checkout at the given path (default /root/reference).
+reference checkout at the given path (a required argument).
 """
 import json
 import os
 import sys
+
+
+def _reference_root():
+    """The reference checkout, a required first command-line argument."""
+    if len(sys.argv) < 2:
+        sys.exit("usage: %s <path of the reference checkout>" % os.path.basename(sys.argv[0]))
+    return sys.argv[1]
 
 REF_TESTS = "src/Sparrow/Tests/AppTests"
 
@@ -48,4 +55,4 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(_reference_root())

@@ -103,3 +103,48 @@ def test_property_getters_check_their_arguments():
     assert L.sg_get_spin_densities(c._h, p, p) == 9
     assert L.sg_set_spin_densities(None, p, p) == 1
     assert L.sg_set_spin_densities(c._h, None, p) == 1
+
+
+def test_electron_count_beyond_the_orbitals_is_rejected_on_host():
+    # a charge that leaves more than two electrons per orbital (or overflows
+    # the electron count) is SG_ERR_ODD_ELECTRONS before any device work, in
+    # the batch entry points and in the allocation-free call
+    L = sparrow_b200.lib()
+    Z = np.array([8, 1, 1], dtype=np.int32)
+    X = np.array([0.0, 0.0, 0.0, 1.8, 0.0, 0.0, -0.4, 1.7, 0.0])
+    nat = np.array([3], dtype=np.int32)
+    buf = ctypes.create_string_buffer(256)
+    for charge in (-8, -(2 ** 31), -(2 ** 31 - 1)):
+        ch = np.array([charge], dtype=np.int32)
+        h = ctypes.c_void_p()
+        rc = L.sg_batch_create(b"PM6", 1, nat.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                               Z.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                               X.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                               ch.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(h))
+        assert rc == 5, (charge, rc)
+        assert not h.value
+        mult = np.array([1], dtype=np.int32)
+        rc = L.sg_batch_create_unrestricted(b"PM6", 1, nat.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                            Z.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                            X.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                            ch.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                            mult.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(h))
+        assert rc == 5, (charge, rc)
+        e = ctypes.c_double()
+        it = ctypes.c_int32()
+        cv = ctypes.c_int32()
+        rc = L.sg_calculate_static(b"PM6", 3, Z.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                   X.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), charge, 1e-7, 1e-5, 50, 1,
+                                   None, ctypes.byref(e), None, ctypes.byref(it), ctypes.byref(cv), buf, 256)
+        assert rc == 5, (charge, rc, buf.value)
+        assert b"orbital" in buf.value
+    # a huge multiplicity overflows n_alpha in 32 bits: rejected the same way
+    mult = np.array([2 ** 31 - 1], dtype=np.int32)
+    ch = np.array([0], dtype=np.int32)
+    h = ctypes.c_void_p()
+    rc = L.sg_batch_create_unrestricted(b"PM6", 1, nat.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                        Z.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                        X.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                        ch.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                        mult.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), ctypes.byref(h))
+    assert rc == 5
