@@ -216,6 +216,19 @@ int32_t sg_batch_set_scf_path(sg_batch* b, int32_t path);
  * to FP64 (default 1e-5; also when the mixed densities stop halving below
  * 1e-4) */
 int32_t sg_batch_set_mixed_switch(sg_batch* b, double density_rmsd);
+/* Orbital update of the restricted NDDO SCF (no counterpart in the
+ * reference, which diagonalises through its SCF library every iteration):
+ * molecules of at least large_min_aos AOs use large_mode, the others
+ * small_mode.  Modes: SG_ORBITALS_EXACT (a full diagonalisation of the
+ * extrapolated Fock matrix every iteration, Householder tridiagonal solver),
+ * SG_ORBITALS_HYBRID (the tridiagonal solver at the start, then
+ * occupied-virtual rotations), SG_ORBITALS_ROTATION (a Jacobi start, then
+ * rotations).  Every mode converges to the same fixed point; the default is
+ * the tuned table built into the library. */
+#define SG_ORBITALS_EXACT 0
+#define SG_ORBITALS_HYBRID 1
+#define SG_ORBITALS_ROTATION 2
+int32_t sg_batch_set_orbital_update(sg_batch* b, int32_t small_mode, int32_t large_mode, int32_t large_min_aos);
 /* TD-DFTB of every molecule of a DFTB batch after sg_batch_run: omega
  * [n_molecules * nroots], dipoles [n_molecules * nroots * 3] (may be NULL),
  * status [n_molecules] (0 ok, 1 not converged, 2 orbital diagonalisation,

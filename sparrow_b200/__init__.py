@@ -105,6 +105,7 @@ def lib():
         "sg_batch_set_scf": (ctypes.c_int32, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int32]),
         "sg_batch_set_scf_path": (ctypes.c_int32, [_VP, ctypes.c_int32]),
         "sg_batch_set_mixed_switch": (ctypes.c_int32, [_VP, ctypes.c_double]),
+        "sg_batch_set_orbital_update": (ctypes.c_int32, [_VP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
         "sg_batch_set_positions": (ctypes.c_int32, [_VP, _D]),
         "sg_batch_run": (ctypes.c_int32, [_VP, ctypes.c_uint32]),
         "sg_batch_results": (ctypes.c_int32, [_VP, _D, _D, _I32, _I32]),
@@ -429,6 +430,17 @@ class Batch:
         if path not in self.SCF_PATHS:
             raise ValueError(f"unknown scf_path {path!r}")
         self._check(lib().sg_batch_set_scf_path(self._h, self.SCF_PATHS[path]))
+
+    ORBITAL_UPDATES = {"exact": 0, "hybrid": 1, "rotation": 2}
+
+    def set_orbital_update(self, small="hybrid", large="hybrid", large_min_aos=1 << 30):
+        """Orbital update of the restricted NDDO SCF: molecules of at least
+        large_min_aos AOs use `large`, the others `small`; each one of "exact"
+        (tridiagonal diagonalisation every iteration), "hybrid" (tridiagonal
+        start, then occupied-virtual rotations) or "rotation" (Jacobi start,
+        then rotations)."""
+        self._check(lib().sg_batch_set_orbital_update(self._h, self.ORBITAL_UPDATES[small],
+                                                      self.ORBITAL_UPDATES[large], int(large_min_aos)))
 
     def set_mixed_switch(self, rmsd):
         """rms(dP) below which "large_mixed" purifies in FP64 (default 1e-5)."""

@@ -630,6 +630,15 @@ int32_t sg_batch_set_mixed_switch(sg_batch* b, double rmsd) {
   return SG_OK;
 }
 
+int32_t sg_batch_set_orbital_update(sg_batch* b, int32_t small_mode, int32_t large_mode, int32_t large_min_aos) {
+  auto ok = [](int32_t m) { return m == kEigExact || m == kEigHybrid || m == kEigRotation; };
+  if (!b || !ok(small_mode) || !ok(large_mode) || large_min_aos < 1) return SG_ERR_INVALID_ARGUMENT;
+  b->sp.eig_mode_small = small_mode;
+  b->sp.eig_mode_large = large_mode;
+  b->sp.exact_eig_min_nao = large_min_aos;
+  return SG_OK;
+}
+
 int32_t sg_batch_excitations(sg_batch* b, int32_t nroots, int32_t triplet, double* omega, double* dipoles,
                              int32_t* status) {
   if (!b || !omega) return SG_ERR_INVALID_ARGUMENT;

@@ -97,6 +97,8 @@ struct MolResult {
   long long cycles[5];
 };
 
+constexpr int kEigExact = 0, kEigHybrid = 1, kEigRotation = 2;
+
 struct ScfParams {
   double scc = 1e-7;   // |Delta E| criterion (Hartree)
   double rmsd = 1e-5;  // rms(Delta P) criterion
@@ -114,10 +116,24 @@ struct ScfParams {
   // virtual-virtual blocks unrotated, which changes no density or energy but
   // leaves the individual orbital energies as diagonal elements.
   int canonical = 0;
+  // orbital update of the NDDO restricted SCF, per molecule size: molecules
+  // of at least exact_eig_min_nao AOs use eig_mode_large, the others
+  // eig_mode_small.  Modes (kEig*): exact = a full diagonalisation of the
+  // extrapolated Fock matrix every iteration (Householder tridiagonal solver,
+  // Jacobi on clustered spectra); hybrid = the tridiagonal solver for the
+  // start, then occupied-virtual rotations; rotation = a Jacobi start, then
+  // occupied-virtual rotations.
+  int eig_mode_small = 1;
+  int eig_mode_large = 1;
+  int exact_eig_min_nao = 1 << 30;
   // large-molecule mixed-precision path: purification switches from split-BF16
   // to FP64 once rms(Delta P) falls below this (or stops halving below 1e-4)
   double mixed_switch_rmsd = 1e-5;
 };
+
+__host__ __device__ inline int scf_eig_mode(const ScfParams& sp, int nao) {
+  return nao >= sp.exact_eig_min_nao ? sp.eig_mode_large : sp.eig_mode_small;
+}
 
 // Device failure codes (MolResult::status)
 enum DeviceStatus : int {

@@ -383,10 +383,20 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_scf(const MolDev* __restrict
     bool have_orbitals = false;
     double drift = 0;
     double Eold = 0;
+    const int mode = scf_eig_mode(sp, N);
     int it = 0, converged = 0, status = kDevOk;
     double last_dE = 0, last_rms = 0;
 
     long long cyc[5] = {0, 0, 0, 0, 0};
+#ifdef SGB_EIG_PROFILE
+    // profiling build: the result's cycle counters report the eigensolver's
+    // stages (tridiagonalisation, bisection, vectors, back-transformation,
+    // everything else)
+    long long eprof_buf[4] = {0, 0, 0, 0};
+    long long* eprof = eprof_buf;
+#else
+    long long* eprof = nullptr;
+#endif
     int nfull = 0, nsweeps = 0;
     for (it = 1; it <= sp.max_iter; ++it) {
       long long t0 = clock64();
@@ -403,17 +413,35 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_scf(const MolDev* __restrict
       long long t2 = clock64();
       cyc[1] += t2 - t1;
       int need_full = !have_orbitals;
-      if (have_orbitals) need_full = ov_rotation(N, no, F, Ct, W1, W2, eps, drift, sh);
+      if (mode != kEigExact && have_orbitals) need_full = ov_rotation(N, no, F, Ct, W1, W2, eps, drift, sh);
+      if (mode == kEigExact || (need_full && mode == kEigHybrid)) {
+        // exact: every iteration the lowest eigenvalues and the occupied
+        // eigenvectors of the extrapolated F; hybrid: every eigenpair at the
+        // start (or when the occupied/virtual ordering breaks), the rotations
+        // take over from there.  Jacobi only for clustered spectra.
+        const bool all = mode != kEigExact;
+        need_full = eigh_tridiag(N, F, all ? N : (no < N ? no + 1 : N), all ? N : no, Ct, N, eps, sh.gemm,
+                                 eig_workspace_doubles(sh, smem_raw), W2, W1, Ct, F, sh.red, &sh.flag, eprof);
+        if (!all) {
+          have_orbitals = false;  // a fallback diagonalises from scratch
+        } else if (!need_full) {
+          have_orbitals = true;
+          drift = 0;
+          ++nfull;
+        }
+      }
       long long t3 = clock64();
       cyc[2] += t3 - t2;
       if (need_full) {
-        // the first (cold) diagonalisation only has to separate occupied from virtual
-        // orbitals; the rotations of the later iterations converge them
+        // the first (cold) diagonalisation of the rotation mode only has to
+        // separate occupied from virtual orbitals; a fallback of the
+        // tridiagonal mode converges fully
+        const bool full_acc = have_orbitals || mode == kEigExact;
         const int sw = full_diagonalise(N, F, Ct, W1, W2, eps, Apk ? Apk : F, Apk ? packed_bytes : 0, have_orbitals,
-                                        rot, cap_rounds, have_orbitals ? sp.jacobi_max_sweeps : cold_sweeps,
-                                        have_orbitals ? 1e-10 : 1e-3, sh);
-        if (sw < 0 && have_orbitals) status = kDevJacobiNotConverged;
-        nsweeps += sw < 0 ? (have_orbitals ? sp.jacobi_max_sweeps : cold_sweeps) : sw;
+                                        rot, cap_rounds, full_acc ? sp.jacobi_max_sweeps : cold_sweeps,
+                                        full_acc ? 1e-10 : 1e-3, sh);
+        if (sw < 0 && full_acc) status = kDevJacobiNotConverged;
+        nsweeps += sw < 0 ? (full_acc ? sp.jacobi_max_sweeps : cold_sweeps) : sw;
         ++nfull;
         have_orbitals = true;
         drift = 0;
@@ -453,25 +481,34 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_scf(const MolDev* __restrict
       r.last_rmsd = last_rms;
       r.full_diag = nfull;
       r.jacobi_sweeps = nsweeps;
+#ifdef SGB_EIG_PROFILE
+      long long tot = 0;
+      for (int k = 0; k < 5; ++k) tot += cyc[k];
+      for (int k = 0; k < 4; ++k) {
+        r.cycles[k] = eprof[k];
+        tot -= eprof[k];
+      }
+      r.cycles[4] = tot;
+#else
       for (int k = 0; k < 5; ++k) r.cycles[k] = cyc[k];
+#endif
     }
     __syncthreads();
   }
 }
 
 namespace {
+// The persistent SCF kernels run one CTA per SM, so they take all the shared
+// memory a block may opt in to: the Jacobi solver's packed matrix sits there
+// when it fits, and the tridiagonal solver tiles molecules of up to 192 AOs.
 size_t scf_smem_bytes(int max_nao, int* packed_in_smem) {
   const size_t base = ((sizeof(ScfShared) + 15) / 16) * 16;
   const size_t pk = sizeof(double) * (size_t)max_nao * (max_nao + 1) / 2;
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  if (base + pk <= (size_t)optin) {
-    *packed_in_smem = 1;
-    return base + pk;
-  }
-  *packed_in_smem = 0;
-  return base;
+  *packed_in_smem = base + pk <= (size_t)optin ? 1 : 0;
+  return (size_t)optin > base ? (size_t)optin : base;
 }
 }  // namespace
 
@@ -718,9 +755,15 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_canonical(const MolDev* __re
     const int cap_rounds = (int)((kRotBudgetBytes / sizeof(double)) / (2 * ((N + 1) / 2)));
     for (int spin = 0; spin < (Fball ? 2 : 1); ++spin) {
       double* F = (spin ? Fball : Fall) + m.mat_off;
-      full_diagonalise(N, F, (spin ? Cball : Call) + m.mat_off, W1all + m.mat_off, W2all + m.mat_off,
-                       (spin ? epsball : epsall) + m.ao_base, Apk ? Apk : F, Apk ? packed_bytes : 0, true, rot,
-                       cap_rounds, sp.jacobi_max_sweeps, 1e-10, sh);
+      double* Ct = (spin ? Cball : Call) + m.mat_off;
+      double* eps = (spin ? epsball : epsall) + m.ao_base;
+      // all eigenpairs of the final Fock matrix by the tridiagonal solver;
+      // clustered spectra by a Jacobi diagonalisation from scratch
+      const int st = eigh_tridiag(N, F, N, N, Ct, N, eps, sh.gemm, eig_workspace_doubles(sh, smem_raw),
+                                  W2all + m.mat_off, W1all + m.mat_off, Ct, F, sh.red, &sh.flag);
+      if (st != 0)
+        full_diagonalise(N, F, Ct, W1all + m.mat_off, W2all + m.mat_off, eps, Apk ? Apk : F, Apk ? packed_bytes : 0,
+                         false, rot, cap_rounds, sp.jacobi_max_sweeps, 1e-10, sh);
     }
     __syncthreads();
   }

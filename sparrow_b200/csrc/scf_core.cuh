@@ -754,6 +754,29 @@ __device__ int ov_rotation(int N, int no, double* F, double* Ct, double* W1, dou
   return 0;
 }
 
+// Dynamic shared memory of the launch (bytes).
+__device__ __forceinline__ unsigned dynamic_smem_bytes() {
+  unsigned r;
+  asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(r));
+  return r;
+}
+
+}  // namespace
+}  // namespace sgb
+
+#include "eigh_tridiag.cuh"
+
+namespace sgb {
+namespace {
+
+// Doubles of the eigensolver's shared workspace: the phase-scratch union and
+// everything after it in the dynamic shared memory (the packed-matrix region).
+__device__ __forceinline__ size_t eig_workspace_doubles(const ScfShared& sh, const unsigned char* smem_raw) {
+  const size_t off = (size_t)(reinterpret_cast<const unsigned char*>(sh.gemm) - smem_raw);
+  const size_t total = dynamic_smem_bytes();
+  return total > off ? (total - off) / sizeof(double) : 0;
+}
+
 }  // namespace
 // New orbitals of one spin from its (extrapolated) Fock matrix Fs: the
 // occupied-virtual rotation of the previous orbitals, or a full
