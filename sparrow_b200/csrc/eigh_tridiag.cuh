@@ -155,20 +155,25 @@ __device__ __forceinline__ void tridiagonalise_tiles(int N, double* A, double* v
       const double* __restrict__ T = A + tri_index(I, J) * kTileDoubles;
       const double* __restrict__ vI = v + 32 * I;
       const double* __restrict__ vJ = v + 32 * J;
-      double yr = 0.0, yc = 0.0;
+      double yr0 = 0.0, yr1 = 0.0, yc0 = 0.0, yc1 = 0.0;
       if (I != J) {
 #pragma unroll 8
-        for (int c = 0; c < 32; ++c) {
-          yr = fma(T[lane * kTileLd + c], vJ[c], yr);
-          yc = fma(T[c * kTileLd + lane], vI[c], yc);
+        for (int c = 0; c < 32; c += 2) {
+          yr0 = fma(T[lane * kTileLd + c], vJ[c], yr0);
+          yc0 = fma(T[c * kTileLd + lane], vI[c], yc0);
+          yr1 = fma(T[lane * kTileLd + c + 1], vJ[c + 1], yr1);
+          yc1 = fma(T[(c + 1) * kTileLd + lane], vI[c + 1], yc1);
         }
       } else {
 #pragma unroll 8
-        for (int c = 0; c < 32; ++c) yr = fma(T[lane * kTileLd + c], vJ[c], yr);
+        for (int c = 0; c < 32; c += 2) {
+          yr0 = fma(T[lane * kTileLd + c], vJ[c], yr0);
+          yr1 = fma(T[lane * kTileLd + c + 1], vJ[c + 1], yr1);
+        }
       }
       double* pt = part + tri_index(I, J) * 64;
-      pt[lane] = yr;
-      pt[32 + lane] = yc;
+      pt[lane] = yr0 + yr1;
+      pt[32 + lane] = yc0 + yc1;
     }
     __syncthreads();
     // p = t A v (sum of the partials), w = p - t/2 (p.v) v
@@ -191,14 +196,13 @@ __device__ __forceinline__ void tridiagonalise_tiles(int N, double* A, double* v
       int a, b;
       tri_decode(q, a, b);
       const int I = K0 + a, J = K0 + b;
-      double* __restrict__ T = A + tri_index(I, J) * kTileDoubles + lane * kTileLd;
-      const double vr = v[32 * I + lane], wr = w[32 * I + lane];
-      const double vjl = v[32 * J + lane], wjl = w[32 * J + lane];
+      // lane = tile column: v, w of the column in registers, of the row broadcast
+      double* __restrict__ T = A + tri_index(I, J) * kTileDoubles + lane;
+      const double* __restrict__ vI = v + 32 * I;
+      const double* __restrict__ wI = w + 32 * I;
+      const double vc = v[32 * J + lane], wc = w[32 * J + lane];
 #pragma unroll 8
-      for (int c = 0; c < 32; ++c) {
-        const double vj = __shfl_sync(0xffffffffu, vjl, c), wj = __shfl_sync(0xffffffffu, wjl, c);
-        T[c] -= fma(vr, wj, wr * vj);
-      }
+      for (int r = 0; r < 32; ++r) T[r * kTileLd] -= fma(vI[r], wc, wI[r] * vc);
     }
     __syncthreads();
     // w leaves the trailing block with this step: zero it (the next use is
@@ -581,9 +585,19 @@ __device__ __forceinline__ int eigh_tridiag(int N, const double* __restrict__ F,
   if (failed) return 1;
   group_factors(N, A, tau, Tg, gV);
   __syncthreads();
-  if (N <= 128) back_transform_groups<4>(N, nvec, gV, Tg, Zl, ldz, zscale, Ct, ldc);
-  else if (N <= 256) back_transform_groups<8>(N, nvec, gV, Tg, Zl, ldz, zscale, Ct, ldc);
-  else back_transform_groups_mem(N, nvec, gV, Tg, Zl, ldz, zscale, Ct, ldc);
+  // the tiles are dead now: stage the reflectors' group layout in their
+  // shared-memory place when the tiles lived there
+  const int nref = N - 2, ngroup = nref > 0 ? (nref + 3) >> 2 : 0;
+  const size_t vsize = (size_t)group_off(N, ngroup);
+  const double* V = gV;
+  if (in_smem && vsize <= tiles) {
+    for (size_t q = tid; q < vsize; q += bd) A[q] = gV[q];
+    __syncthreads();
+    V = A;
+  }
+  if (N <= 128) back_transform_groups<4>(N, nvec, V, Tg, Zl, ldz, zscale, Ct, ldc);
+  else if (N <= 256) back_transform_groups<8>(N, nvec, V, Tg, Zl, ldz, zscale, Ct, ldc);
+  else back_transform_groups_mem(N, nvec, V, Tg, Zl, ldz, zscale, Ct, ldc);
   __syncthreads();
   if (prof && tid == 0) prof[3] += clock64() - tp3;
   return 0;

@@ -316,6 +316,18 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_dftb_scf(
       }
       int need_full = !have_orbitals;
       if (have_orbitals) need_full = ov_rotation(N, no, F, Ct, W1, W2, eps, drift, sh);
+      if (need_full && scf_eig_mode(sp, N) != kEigRotation) {
+        // every eigenpair of F' by the tridiagonal solver; the rotations take over
+        need_full = eigh_tridiag(N, F, N, N, Ct, N, eps, sh.gemm, eig_workspace_doubles(sh, smem_raw), W2, W1, Ct, F,
+                                 sh.red, &sh.flag);
+        if (need_full) {
+          have_orbitals = false;  // the solver used Ct as scratch: the fallback starts cold
+        } else {
+          have_orbitals = true;
+          drift = 0;
+          ++nfull;
+        }
+      }
       if (need_full) {
         const int sw = full_diagonalise(N, F, Ct, W1, W2, eps, Apk ? Apk : F, Apk ? packed_bytes : 0, have_orbitals,
                                         rot, cap_rounds, have_orbitals ? sp.jacobi_max_sweeps : cold_sweeps,
@@ -572,12 +584,13 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_dftb_uhf_scf(
       if (have_a && have_b)
         diis_step_uhf(N, Fa, Ppa, Fb, Ppb, W1, histFa, histEa, histFb, histEb, msize, nhist, head, sh);
       const bool warm_a = have_a, warm_b = have_b;
+      const size_t wsd = eig_workspace_doubles(sh, smem_raw);
       int sw = uhf_orbitals(N, na, Fa, Ca, W1, W2, epsa, Apk, packed_bytes, have_a, drift_a, rot, cap_rounds, sp,
-                            cold_sweeps, nfull, sh);
+                            cold_sweeps, nfull, sh, sh.gemm, wsd);
       if (sw < 0 && warm_a) status = kDevJacobiNotConverged;
       nsweeps += sw < 0 ? -sw : sw;
       sw = uhf_orbitals(N, nb, Fb, Cb, W1, W2, epsb, Apk, packed_bytes, have_b, drift_b, rot, cap_rounds, sp,
-                        cold_sweeps, nfull, sh);
+                        cold_sweeps, nfull, sh, sh.gemm, wsd);
       if (sw < 0 && warm_b) status = kDevJacobiNotConverged;
       nsweeps += sw < 0 ? -sw : sw;
       // P'_s = C'_occ C'_occ^T, P_s = X P'_s X; rms of the AO spin densities
@@ -691,27 +704,32 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_dftb_canonical(
       double* Fp = (spin ? Ppball : Ppall) + m.mat_off;
       cta_gemm(N, N, N, 1.0, F, N, false, X, N, false, 0.0, W2, N, sh.gemm);
       cta_gemm(N, N, N, 1.0, X, N, false, W2, N, false, 0.0, Fp, N, sh.gemm);
-      full_diagonalise(N, Fp, (spin ? Cball : Call) + m.mat_off, W3, W2, (spin ? epsball : epsall) + m.ao_base,
-                       Apk ? Apk : Fp, Apk ? packed_bytes : 0, true, rot, cap_rounds, sp.jacobi_max_sweeps, 1e-10,
-                       sh);
+      double* Ct = (spin ? Cball : Call) + m.mat_off;
+      double* eps = (spin ? epsball : epsall) + m.ao_base;
+      // every eigenpair of F' by the tridiagonal solver; clustered spectra by a
+      // Jacobi diagonalisation from scratch (the solver used Ct as scratch)
+      const int st = eigh_tridiag(N, Fp, N, N, Ct, N, eps, sh.gemm, eig_workspace_doubles(sh, smem_raw), W2, W3, Ct,
+                                  Fp, sh.red, &sh.flag);
+      if (st != 0)
+        full_diagonalise(N, Fp, Ct, W3, W2, eps, Apk ? Apk : Fp, Apk ? packed_bytes : 0, false, rot, cap_rounds,
+                         sp.jacobi_max_sweeps, 1e-10, sh);
     }
     __syncthreads();
   }
 }
 
 
+// One CTA per SM: the persistent kernels take all the opt-in shared memory
+// (the Jacobi solver's packed matrix when it fits, the tridiagonal solver's
+// tiles up to 192 AOs).
 size_t dftb_smem_bytes(int max_nao, int* packed_in_smem) {
   const size_t base = ((sizeof(ScfShared) + 15) / 16) * 16;
   const size_t pk = sizeof(double) * (size_t)max_nao * (max_nao + 1) / 2;
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  if (base + pk <= (size_t)optin) {
-    *packed_in_smem = 1;
-    return base + pk;
-  }
-  *packed_in_smem = 0;
-  return base;
+  *packed_in_smem = base + pk <= (size_t)optin ? 1 : 0;
+  return (size_t)optin > base ? (size_t)optin : base;
 }
 
 }  // namespace

@@ -422,9 +422,10 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_scf(const MolDev* __restrict
         const bool all = mode != kEigExact;
         need_full = eigh_tridiag(N, F, all ? N : (no < N ? no + 1 : N), all ? N : no, Ct, N, eps, sh.gemm,
                                  eig_workspace_doubles(sh, smem_raw), W2, W1, Ct, F, sh.red, &sh.flag, eprof);
-        if (!all) {
-          have_orbitals = false;  // a fallback diagonalises from scratch
-        } else if (!need_full) {
+        if (!all || need_full) {
+          // a fallback diagonalises from scratch (the solver used Ct as scratch)
+          have_orbitals = false;
+        } else {
           have_orbitals = true;
           drift = 0;
           ++nfull;
@@ -683,12 +684,13 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_uhf_scf(
       const double E = ER - 0.25 * spin_exchange(m, atoms, elems, pairs, ints, Pa, Pb, Fa, Fb, sh.red);
       diis_step_uhf(N, Fa, Pa, Fb, Pb, W1, histFa, histEa, histFb, histEb, msize, nhist, head, sh);
       const bool warm_a = have_a, warm_b = have_b;
+      const size_t wsd = eig_workspace_doubles(sh, smem_raw);
       int sw = uhf_orbitals(N, na, Fa, Ca, W1, W2, epsa, Apk, packed_bytes, have_a, drift_a, rot, cap_rounds, sp,
-                            cold_sweeps, nfull, sh);
+                            cold_sweeps, nfull, sh, sh.gemm, wsd);
       if (sw < 0 && warm_a) status = kDevJacobiNotConverged;
       nsweeps += sw < 0 ? -sw : sw;
       sw = uhf_orbitals(N, nb, Fb, Cb, W1, W2, epsb, Apk, packed_bytes, have_b, drift_b, rot, cap_rounds, sp,
-                        cold_sweeps, nfull, sh);
+                        cold_sweeps, nfull, sh, sh.gemm, wsd);
       if (sw < 0 && warm_b) status = kDevJacobiNotConverged;
       nsweeps += sw < 0 ? -sw : sw;
       const double da = uhf_density(N, na, Ca, Pa, W1, sh);

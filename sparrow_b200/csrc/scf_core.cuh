@@ -595,8 +595,14 @@ __device__ __forceinline__ void diis_extrapolate(int N, const double* histF, int
   for (int i = warp; i < N; i += nwarps) {
     const int rf = diis_row_f(N, i) - i;
     for (int c = i + lane; c < N; c += 32) {
+      // the ring's entries are independent loads: all in flight at once
+      double f[kDiisMax];
+#pragma unroll
+      for (int k = 0; k < kDiisMax; ++k) f[k] = k < nhist ? histF[(size_t)k * TF + rf + c] : 0.0;
       double v = 0;
-      for (int k = 0; k < nhist; ++k) v += sh.coef[k] * histF[(size_t)k * TF + rf + c];
+#pragma unroll
+      for (int k = 0; k < kDiisMax; ++k)
+        if (k < nhist) v += sh.coef[k] * f[k];
       dst[i * N + c] = v;
       dst[c * N + i] = v;
     }
@@ -784,12 +790,25 @@ __device__ __forceinline__ size_t eig_workspace_doubles(const ScfShared& sh, con
 // the spin has no occupied or no virtual orbitals.  Returns the Jacobi
 // sweeps of a full diagonalisation (0 when none ran, < 0 when it did not
 // converge).
+// Unless sp selects the rotation mode for this size, a full diagonalisation
+// runs the tridiagonal solver first (ws: its shared workspace of ws_doubles)
+// and falls back to a cold Jacobi on clustered spectra.
 __device__ int uhf_orbitals(int N, int ns, double* Fs, double* Cs, double* W1, double* W2, double* epss,
                             double* Apk, size_t packed_bytes, bool& have, double& drift, double* rot, int cap_rounds,
-                            const ScfParams& sp, int cold_sweeps, int& nfull, ScfShared& sh) {
+                            const ScfParams& sp, int cold_sweeps, int& nfull, ScfShared& sh, double* ws,
+                            size_t ws_doubles) {
   int need_full = !have || ns == 0 || ns == N;
   if (!need_full) need_full = ov_rotation(N, ns, Fs, Cs, W1, W2, epss, drift, sh);
   if (!need_full) return 0;
+  if (scf_eig_mode(sp, N) != kEigRotation) {
+    if (eigh_tridiag(N, Fs, N, N, Cs, N, epss, ws, ws_doubles, W2, W1, Cs, Fs, sh.red, &sh.flag) == 0) {
+      ++nfull;
+      have = true;
+      drift = 0;
+      return 0;
+    }
+    have = false;  // the solver used Cs as scratch: the fallback starts cold
+  }
   const int sw = full_diagonalise(N, Fs, Cs, W1, W2, epss, Apk ? Apk : Fs, Apk ? packed_bytes : 0, have, rot,
                                   cap_rounds, have ? sp.jacobi_max_sweeps : cold_sweeps, have ? 1e-10 : 1e-3, sh);
   ++nfull;
