@@ -19,7 +19,9 @@ against the measured FP64 GEMM rate; `cpu_baseline` is the oracle on a
 bounded random sample of the same molecules.  Side legs (rank 0): the plain
 one-molecule-per-launch GPU form, the request server's p50/p99 latency, and
 the large-molecule path on (H2O)_256/512/1024 in FP64 and mixed precision,
-and DFTB3 + TD-DFTB excitations over 1024 polyenes.
+and DFTB3 + TD-DFTB excitations over 1024 polyenes; PM6 on one (H2O)_32
+cluster (the plain single-point form against the oracle on one and on all
+cores) and the batch with AM1.
 """
 import argparse
 import json
@@ -57,6 +59,8 @@ def parse():
     p.add_argument("--no-plain", action="store_true", help="skip the plain one-molecule-per-launch GPU leg")
     p.add_argument("--no-open-shell", action="store_true", help="skip the unrestricted (radical) leg")
     p.add_argument("--no-hessian", action="store_true", help="skip the semi-numerical Hessian leg")
+    p.add_argument("--no-water32", action="store_true", help="skip the (H2O)_32 single-point leg")
+    p.add_argument("--no-am1", action="store_true", help="skip the AM1 batch leg")
     p.add_argument("--serving-loads", default="250,500,1000,2000", help="offered loads (req/s) of the serving leg")
     return p.parse_args()
 
@@ -269,10 +273,10 @@ def tddftb_leg(count=1024, seed=6, nroots=8, cpu_seconds=10.0):
     import sparrow_b200
     from sparrow_b200 import geometry
     mols = [(z, geometry.to_bohr(x)) for z, x in geometry.polyene_batch(count, seed=seed)]
-    out = {"workload": "%d polyenes C_2kH_2k+2, k~U[5,40], seed %d, DFTB3 3ob-3-1, rms dP 1e-8, %d lowest singlets "
-                       "(full TD-DFTB, Davidson residual 1e-8)" % (count, seed, nroots)}
+    out = {"workload": "%d polyenes C_2kH_2k+2, k~U[5,40], seed %d, DFTB3 3ob-3-1, rms dP 1e-10, %d lowest singlets "
+                       "(full TD-DFTB, Davidson residual 1e-10)" % (count, seed, nroots)}
     for rep in range(2):  # the first pass pays module loading
-        b = sparrow_b200.Batch("DFTB3", mols, scc=1e-7, rmsd=1e-8, max_iter=200)
+        b = sparrow_b200.Batch("DFTB3", mols, scc=1e-9, rmsd=1e-10, max_iter=300)
         b.record_event(0)
         b.run()
         b.record_event(1)
@@ -288,24 +292,126 @@ def tddftb_leg(count=1024, seed=6, nroots=8, cpu_seconds=10.0):
                 "tddftb_cycle_share": {"canonical_orbitals": float(cyc[:, 0].sum() / cyc.sum()),
                                        "transition_charges": float(cyc[:, 1].sum() / cyc.sum()),
                                        "davidson": float(cyc[:, 2].sum() / cyc.sum())}})
-    # CPU oracle on the smallest molecules, within the time budget
-    from tests import oracle_lib as O
-    order = sorted(range(count), key=lambda i: len(mols[i][0]))
-    t0 = time.perf_counter()
-    done, dmax = 0, 0.0
-    for i in order:
-        if time.perf_counter() - t0 > cpu_seconds:
-            break
-        r = O.dftb_tddftb(3, mols[i][0], mols[i][1], nroots=nroots)
-        dmax = max(dmax, float(np.max(np.abs(r["omega"] - om[i][:len(r["omega"])]))))
-        done += 1
-    wall = time.perf_counter() - t0
-    out["cpu_baseline"] = {"value": done / wall, "unit": "molecules/s", "cores": 1, "kind": "port",
-                           "sample": "the %d smallest polyenes of the batch (%d-%d atoms), oracle DFTB3 SCF + dense "
-                                     "Casida diagonalisation, %.1f s wall" % (
-                                         done, len(mols[order[0]][0]), len(mols[order[max(done - 1, 0)]][0]), wall),
-                           "max_abs_domega_gpu_vs_oracle_hartree": dmax}
+    # CPU oracle on a random sample across the whole k range, all host cores
+    import multiprocessing as mp
+    procs = host_cores()
+    rng = np.random.default_rng(99)
+    pick = rng.choice(count, size=min(count, procs), replace=False)
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        t0 = time.perf_counter()
+        res = pool.map(_oracle_tddftb, [(3, mols[i][0], mols[i][1], nroots) for i in pick], chunksize=1)
+        wall = time.perf_counter() - t0
+    dmax, mmax = 0.0, 0.0
+    for i, (_, omr, dpr) in zip(pick, res):
+        dmax = max(dmax, float(np.max(np.abs(omr - om[i][:len(omr)]))))
+        for r_ in range(len(omr)):
+            sgn = 1.0 if np.dot(dpr[r_], mu[i][r_]) >= 0 else -1.0
+            mmax = max(mmax, float(np.max(np.abs(dpr[r_] - sgn * mu[i][r_]))))
+    ks = sorted((len(mols[i][0]) - 2) // 4 for i in pick)
+    out["cpu_baseline"] = {"value": len(pick) / wall, "unit": "molecules/s", "cores": procs, "kind": "port",
+                           "cpu": cpu_info(),
+                           "sample": "%d random polyenes of the batch (k = %s), oracle DFTB3 SCF + TD-DFTB (dense "
+                                     "Casida up to 2000 transitions, matrix-free Davidson above), one per process, "
+                                     "%.1f s wall" % (len(pick), ",".join(str(k) for k in ks), wall),
+                           "max_abs_domega_gpu_vs_oracle_hartree": dmax,
+                           "max_abs_dmu_gpu_vs_oracle_ebohr": mmax}
     return out
+
+
+def _oracle_tddftb(args):
+    order, Z, x, nroots = args
+    from tests import oracle_lib as O
+    t0 = time.perf_counter()
+    r = O.dftb_tddftb(order, Z, x, nroots=nroots, scc=1e-9, rmsd=1e-10)
+    return time.perf_counter() - t0, r["omega"], r["dipoles"]
+
+
+def _oracle_plain(args):
+    method, Z, x, reps = args
+    from tests import oracle_lib as O
+    out = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        r = O.scf(method, Z, x, scc=SCC, rmsd=RMSD, max_iter=MAX_ITER, gradient=True)
+        out.append(time.perf_counter() - t0)
+    return out, r["energy"], r["gradient"]
+
+
+def water32_leg(gpu_calls=20):
+    """PM6 energy + gradient of one (H2O)_32 cluster (96 atoms, 192 AOs; the
+    4x4x2 jittered grid, seed 0), rms dP 1e-8: the plain GPU form (one
+    Calculator.calculate per solve, host buffers in and out), the oracle on
+    one core (one solve after another) and on all cores (independent solves,
+    one per process), with the GPU's energy and gradient error."""
+    import multiprocessing as mp
+    import numpy as np
+    import sparrow_b200
+    from sparrow_b200 import geometry
+    Z, xa = geometry.water_cluster(32, seed=0)
+    x = geometry.to_bohr(xa)
+    calc = sparrow_b200.get_calculator("PM6")
+    calc.settings["self_consistence_criterion"] = SCC
+    calc.settings["density_rmsd_criterion"] = RMSD
+    calc.set_required_properties(["energy", "gradients"])
+    calc.set_structure(Z, x)
+    for _ in range(3):
+        res = calc.calculate()
+    lat = []
+    for _ in range(gpu_calls):
+        t0 = time.perf_counter()
+        calc.set_structure(Z, x)
+        res = calc.calculate()
+        lat.append(time.perf_counter() - t0)
+    lat = np.array(lat) * 1e3
+    procs = host_cores()
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        one = pool.map(_oracle_plain, [("PM6", Z, x, 3)])[0]
+        t0 = time.perf_counter()
+        allc = pool.map(_oracle_plain, [("PM6", Z, x, 1)] * procs)
+        wall_all = time.perf_counter() - t0
+    t1 = float(np.median(one[0]))
+    return {"workload": "PM6 (H2O)_32, 96 atoms, 192 AOs, seed 0, energy+gradient, rms dP 1e-8",
+            "gpu_plain": {"p50_ms": float(np.median(lat)), "p99_ms": float(np.percentile(lat, 99)),
+                          "solves_per_s": 1e3 / float(np.median(lat)), "iterations": int(res.iterations)},
+            "cpu_1core": {"seconds_per_solve": t1, "solves_per_s": 1.0 / t1, "kind": "port", "cores": 1,
+                          "cpu": cpu_info()},
+            "cpu_all_cores": {"solves_per_s": procs / wall_all, "cores": procs, "kind": "port",
+                              "sample": "%d independent solves, one per process" % procs},
+            "gpu_over_cpu_1core": t1 / (float(np.median(lat)) / 1e3),
+            "abs_dE_hartree": abs(res.energy - one[1]),
+            "max_abs_dgrad_hartree_per_bohr": float(np.max(np.abs(res.gradients - one[2])))}
+
+
+def am1_leg(mols, steps=3, cpu_seconds=10.0):
+    """The same 4096-alkane batch with AM1: device solves/s of the batched
+    energy + gradient (CUDA events over `steps` runs), and the oracle on a
+    random sample over all host cores with the GPU's largest errors on it."""
+    import numpy as np
+    import sparrow_b200
+    b = sparrow_b200.Batch("AM1", mols, scc=SCC, rmsd=RMSD, max_iter=MAX_ITER)
+    for _ in range(2):
+        b.run(gradients=True)
+        e, g, it, conv = b.results()
+    b.record_event(0)
+    for _ in range(steps):
+        b.run(gradients=True)
+        e, g, it, conv = b.results()
+    b.record_event(1)
+    ms = b.elapsed_ms(0, 1) / steps
+    procs = host_cores()
+    rate, count, wall, cpu_results = cpu_rate("AM1", mols, cpu_seconds, procs, rng_seed=4242)
+    return {"workload": "%d alkanes C_nH_2n+2, n~U[2,30], AM1 energy+gradient, rms dP 1e-8" % len(mols),
+            "value": len(mols) / (ms / 1e3), "unit": "solves/s", "ms_per_step": ms,
+            "mean_scf_iterations": float(np.mean(it)), "not_converged": int((~conv).sum()),
+            "cpu_baseline": {"value": rate, "unit": "solves/s", "cores": procs, "kind": "port", "cpu": cpu_info(),
+                             "sample": "%d random molecules, molecule-parallel over %d processes, %.1f s wall" % (
+                                 count, procs, wall),
+                             "max_abs_dE_gpu_vs_oracle_hartree": float(max(abs(e[i] - eo) for i, eo, _ in cpu_results)),
+                             "max_abs_dgrad_gpu_vs_oracle_hartree_per_bohr": float(
+                                 max(np.max(np.abs(g[i] - go)) for i, _, go in cpu_results))},
+            "device_over_cpu": (len(mols) / (ms / 1e3)) / rate}
 
 
 def open_shell_leg(count=1024, seed=8, cpu_seconds=5.0):
@@ -341,7 +447,7 @@ def open_shell_leg(count=1024, seed=8, cpu_seconds=5.0):
         dmax = max(dmax, abs(r["energy"] - energies["PM6"][i]))
         done += 1
     wall = time.perf_counter() - t0
-    out["cpu_baseline"] = {"value": done / wall, "unit": "solves/s", "cores": 1, "kind": "port",
+    out["cpu_baseline"] = {"value": done / wall, "unit": "solves/s", "cores": 1, "kind": "port", "cpu": cpu_info(),
                            "sample": "%d random radicals of the batch, oracle PM6 UHF energy+gradient, %.1f s wall" % (
                                done, wall),
                            "max_abs_dE_gpu_vs_oracle_hartree": dmax}
@@ -393,10 +499,10 @@ def hessian_leg(cpu_step_seconds=30.0):
     cpu_full_s = wall / max(done, 1) * 3 * len(Z)
     out["sft_1"] = {"gpu_wall_ms": gpu_ms, "not_converged": nc, "lowest_frequency_cm": float(f[0]),
                     "reference_lowest_frequency_cm": -125.561,
-                    "cpu_baseline": {"value": cpu_full_s, "unit": "s per Hessian", "cores": 1, "kind": "port",
+                    "cpu_baseline": {"value": cpu_full_s, "unit": "s per Hessian", "cores": 1, "kind": "port", "cpu": cpu_info(),
                                      "sample": "%d of %d coordinates (both displacements) in %.1f s, scaled" % (
                                          done, 3 * len(Z), wall)},
-                    "gpu_over_cpu": cpu_full_s / (gpu_ms / 1e3)}
+                    "gpu_over_cpu_1core": cpu_full_s / (gpu_ms / 1e3)}
     out["C30H62"] = {"gpu_wall_ms": big_ms, "not_converged": ncb}
     return out
 
@@ -406,6 +512,32 @@ def host_cores():
         return len(os.sched_getaffinity(0))
     except Exception:
         return os.cpu_count() or 1
+
+
+def cpu_info():
+    """The host CPU as the CPU baselines see it: model string, logical CPUs,
+    CPUs this process may run on, physical cores, OMP_NUM_THREADS."""
+    model, phys = None, set()
+    try:
+        pid = cid = None
+        for line in open("/proc/cpuinfo"):
+            k, _, v = line.partition(":")
+            k, v = k.strip(), v.strip()
+            if k == "model name" and model is None:
+                model = v
+            elif k == "physical id":
+                pid = v
+            elif k == "core id":
+                cid = v
+            elif not k and pid is not None:
+                phys.add((pid, cid))
+                pid = cid = None
+        if pid is not None:
+            phys.add((pid, cid))
+    except OSError:
+        pass
+    return {"model": model, "logical_cpus": os.cpu_count(), "usable_cpus": host_cores(),
+            "physical_cores": len(phys) or None, "OMP_NUM_THREADS": os.environ.get("OMP_NUM_THREADS")}
 
 
 # ----------------------------------------------------------------------------
@@ -512,6 +644,13 @@ def load_traffic():
 
 
 # ----------------------------------------------------------------------------
+def workload_config(args, world):
+    """The workload description both arms print: the same keys and values."""
+    return {"workload": "%d alkanes C_nH_2n+2, n~U[2,30] per GPU, %s energy+gradient, rms dP 1e-8" % (
+        args.molecules, args.method), "molecules_per_gpu": args.molecules, "method": args.method,
+        "replicas": world, "l2": "inputs larger than L2: the batch's integrals and matrices occupy ~8 GB"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -532,9 +671,9 @@ def run_reference(args, rank, world):
         "unit": "solves/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * sum(r[2] for r in rates) / len(rates), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, no dataset)",
-        "config": {"workload": "%d alkanes C_nH_2n+2, n~U[2,30], %s, rms dP 1e-8" % (args.molecules, args.method),
-                   "molecules": args.molecules, "method": args.method, "parallelism": "cpu processes"},
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": procs, "kind": "port", "sample": sample},
+        "config": workload_config(args, world),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": procs, "kind": "port", "sample": sample,
+                         "cpu": cpu_info()},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -578,7 +717,7 @@ def run_engine(args, rank, world):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         procs = host_cores()
         rate, count, wall, cpu_results = cpu_rate(args.method, mols, args.cpu_seconds, procs)
-        cpu = {"value": rate, "unit": "solves/s", "cores": procs, "kind": "port",
+        cpu = {"value": rate, "unit": "solves/s", "cores": procs, "kind": "port", "cpu": cpu_info(),
                "sample": "%d random molecules of the batch, oracle (C++ FP64 restatement of the reference path), "
                          "molecule-parallel over %d processes, %.1f s wall" % (count, procs, wall)}
 
@@ -626,6 +765,27 @@ def run_engine(args, rank, world):
         cpu["max_abs_dgrad_gpu_vs_oracle_hartree_per_bohr"] = float(
             max(np.max(np.abs(g[i] - go)) for i, _, go in cpu_results))
 
+    # the tuned table in force, against the previous fixed choices (a Jacobi
+    # start and occupied-virtual rotations, Pulay subspace 6) on the same batch
+    tuning = None
+    if rank == 0:
+        b.set_tuning("rotation", 6)
+        b.run()
+        b.results()
+        b.run()
+        b.results()
+        fixed_ms = float(b.stage_times()[2])
+        b.set_tuning(None, None)
+        b.run()
+        b.results()
+        b.run()
+        b.results()
+        tuned_ms = float(b.stage_times()[2])
+        tuning = {"table": [{"first_ao": t[0], "orbital_update": t[1], "diis_size": t[2]}
+                            for t in sparrow_b200.tuning_table()],
+                  "scf_ms_tuned": tuned_ms, "scf_ms_fixed_rotation_diis6": fixed_ms,
+                  "gain_over_fixed": fixed_ms / tuned_ms}
+
     # end to end from host buffers through the public batch call
     t_e2e = []
     h2d = d2h = 0
@@ -672,6 +832,12 @@ def run_engine(args, rank, world):
     hessian = None
     if rank == 0 and not args.no_hessian:
         hessian = hessian_leg()
+    water32 = None
+    if rank == 0 and not args.no_water32:
+        water32 = water32_leg()
+    am1 = None
+    if rank == 0 and not args.no_am1:
+        am1 = am1_leg(mols)
 
     # roofline of the SCF kernel (average launch)
     scf_ms = stage_sum[2] / args.steps
@@ -691,12 +857,10 @@ def run_engine(args, rank, world):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dev_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator, no dataset)",
-        "config": {"workload": "%d alkanes C_nH_2n+2, n~U[2,30] per GPU, %s energy+gradient, rms dP 1e-8" % (
-            args.molecules, args.method), "molecules_per_gpu": args.molecules, "method": args.method,
-                   "parallelism": "replicas x%d (molecules sharded, no collective)" % world,
-                   "l2": "inputs larger than L2: the batch's integrals and matrices occupy ~%.1f GB" % (
-                       b_bytes / 1e9),
-                   "mean_scf_iterations": float(np.mean(it)), "not_converged": not_conv},
+        "config": workload_config(args, world),
+        "run": {"parallelism": "replicas x%d (molecules sharded, no collective)" % world,
+                "batch_matrix_bytes": int(b_bytes), "mean_scf_iterations": float(np.mean(it)),
+                "not_converged": not_conv},
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(launches),
         "roofline": roof,
@@ -707,6 +871,9 @@ def run_engine(args, rank, world):
         "tddftb": tddftb,
         "open_shell": open_shell,
         "hessian": hessian,
+        "tuning": tuning,
+        "water32_pm6": water32,
+        "am1": am1,
         "clocks": clk,
     }
     if rank == 0:

@@ -123,7 +123,7 @@ int32_t sg_get_orbital_energies(const sg_calculator* h, double* eps);
  * nroots (1..16) lowest excitation energies omega (Hartree, ascending) and,
  * for singlets, the transition dipoles (nroots x 3, e bohr; zero for
  * triplets; dipoles may be NULL).  SG_ERR_NOT_CONVERGED when the Davidson
- * solver did not reach its residual tolerance (1e-8). */
+ * solver did not reach its residual tolerance (1e-10 on the Casida matrix). */
 int32_t sg_calculate_excitations(sg_calculator* h, int32_t nroots, int32_t triplet, double* omega, double* dipoles);
 /* Unrestricted calculations ("spin_mode" = "unrestricted", or "any" with
  * "spin_multiplicity" != 1, as NDDOMethodWrapper.cpp:68-92): the beta orbital
@@ -216,19 +216,23 @@ int32_t sg_batch_set_scf_path(sg_batch* b, int32_t path);
  * to FP64 (default 1e-5; also when the mixed densities stop halving below
  * 1e-4) */
 int32_t sg_batch_set_mixed_switch(sg_batch* b, double density_rmsd);
-/* Orbital update of the restricted NDDO SCF (no counterpart in the
- * reference, which diagonalises through its SCF library every iteration):
- * molecules of at least large_min_aos AOs use large_mode, the others
- * small_mode.  Modes: SG_ORBITALS_EXACT (a full diagonalisation of the
+/* Tuning of the batched SCF (no counterpart in the reference, which
+ * diagonalises through its SCF library every iteration).  The library
+ * carries a table, measured by its autotuner (sparrow_b200/autotune.py), of
+ * the orbital update and the Pulay subspace size per molecule-size bin of 32
+ * AOs.  sg_batch_set_tuning overrides it for every molecule of the batch:
+ * orbital_update one of SG_ORBITALS_EXACT (a full diagonalisation of the
  * extrapolated Fock matrix every iteration, Householder tridiagonal solver),
  * SG_ORBITALS_HYBRID (the tridiagonal solver at the start, then
  * occupied-virtual rotations), SG_ORBITALS_ROTATION (a Jacobi start, then
- * rotations).  Every mode converges to the same fixed point; the default is
- * the tuned table built into the library. */
+ * rotations), diis_size 1..6; -1 keeps the table's choice for that knob.
+ * Every choice converges to the same fixed point.  sg_tuning_table writes
+ * the table (capacity entries at most) and returns its number of bins. */
 #define SG_ORBITALS_EXACT 0
 #define SG_ORBITALS_HYBRID 1
 #define SG_ORBITALS_ROTATION 2
-int32_t sg_batch_set_orbital_update(sg_batch* b, int32_t small_mode, int32_t large_mode, int32_t large_min_aos);
+int32_t sg_batch_set_tuning(sg_batch* b, int32_t orbital_update, int32_t diis_size);
+int32_t sg_tuning_table(int32_t* orbital_update, int32_t* diis_size, int32_t capacity);
 /* TD-DFTB of every molecule of a DFTB batch after sg_batch_run: omega
  * [n_molecules * nroots], dipoles [n_molecules * nroots * 3] (may be NULL),
  * status [n_molecules] (0 ok, 1 not converged, 2 orbital diagonalisation,

@@ -33,6 +33,7 @@
 //     coordinate (SKPair.cpp:99-128, 178-190);
 //   * the DFTB3 gradient builds d Gamma_ba / dR without the sign flip its
 //     gamma term receives (ThirdOrderFock.cpp:73-77, 206-212).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -986,8 +987,124 @@ void gradient_uhf(const Mol& M, const State& st, const SpinState& ss, std::vecto
 //   matrix D_ia = sum_A q_A^{ia} R_A; the restricted singlet factor sqrt(2)
 //   of the spin-adapted transition density, restated for the un-vendored
 //   Utils::TransitionDipoleCalculator): mu_I = sqrt(2) sum_ia c_ia D_ia.
-// The eigenproblem is solved densely (the reference's Davidson lives in the
-// un-vendored scine_utilities; converged eigenpairs do not depend on it).
+// The eigenproblem is solved densely up to 2000 transitions; above that by a
+// matrix-free Davidson iteration on Omega (the reference's Davidson lives in
+// the un-vendored scine_utilities; converged eigenpairs do not depend on it).
+//
+// Lowest nroots eigenpairs of Omega = diag(delta^2) + 4 sqrt(delta) qG q^T
+// sqrt(delta) without forming it: products through the atoms (dim * nat),
+// unit start vectors of the smallest diagonal entries, diagonal
+// preconditioner, Gram-Schmidt twice, restart to the Ritz vectors when the
+// subspace is full, residual norm 1e-10 (Davidson, J. Comput. Phys. 17, 1975).
+static int g_dense_casida_limit = 2000;  // transitions up to which Omega is diagonalised densely
+
+static bool davidson_lowest(int dim, int nat, int nroots, const std::vector<double>& delta,
+                            const std::vector<double>& q, const std::vector<double>& qG, std::vector<double>& w_out,
+                            std::vector<double>& X_out) {
+  auto apply = [&](const double* x, double* y) {
+    std::vector<double> t(nat, 0.0);
+    for (int k = 0; k < dim; ++k) {
+      const double sk = std::sqrt(delta[k]) * x[k];
+      for (int B = 0; B < nat; ++B) t[B] += qG[(size_t)k * nat + B] * sk;
+    }
+    for (int k = 0; k < dim; ++k) {
+      double s = 0;
+      for (int B = 0; B < nat; ++B) s += q[(size_t)k * nat + B] * t[B];
+      y[k] = delta[k] * delta[k] * x[k] + 4.0 * std::sqrt(delta[k]) * s;
+    }
+  };
+  const int maxsub = std::min(dim, std::max(8 * nroots, 32));
+  std::vector<std::vector<double>> V, AV;
+  std::vector<int> idx(dim);
+  for (int k = 0; k < dim; ++k) idx[k] = k;
+  std::sort(idx.begin(), idx.end(), [&](int a, int b) { return delta[a] < delta[b] || (delta[a] == delta[b] && a < b); });
+  auto add_vector = [&](std::vector<double> x) -> bool {
+    double n0 = 0;
+    for (double xk : x) n0 += xk * xk;
+    n0 = std::sqrt(n0);
+    if (!(n0 > 0)) return false;
+    for (double& xk : x) xk /= n0;  // unit length first: the test below is relative
+    for (int pass = 0; pass < 2; ++pass)
+      for (const auto& v : V) {
+        double d = 0;
+        for (int k = 0; k < dim; ++k) d += v[k] * x[k];
+        for (int k = 0; k < dim; ++k) x[k] -= d * v[k];
+      }
+    double nrm = 0;
+    for (double xk : x) nrm += xk * xk;
+    nrm = std::sqrt(nrm);
+    if (nrm < 1e-6) return false;  // (almost) inside the subspace already
+    for (double& xk : x) xk /= nrm;
+    std::vector<double> ax(dim);
+    apply(x.data(), ax.data());
+    V.push_back(std::move(x));
+    AV.push_back(std::move(ax));
+    return true;
+  };
+  for (int j = 0; j < std::min(dim, 2 * nroots); ++j) {
+    std::vector<double> e(dim, 0.0);
+    e[idx[j]] = 1.0;
+    add_vector(e);
+  }
+  for (int iter = 0; iter < 500; ++iter) {
+    const int m = (int)V.size();
+    std::vector<double> Hs((size_t)m * m);
+    for (int a = 0; a < m; ++a)
+      for (int b = 0; b <= a; ++b) {
+        double s = 0;
+        for (int k = 0; k < dim; ++k) s += V[a][k] * AV[b][k];
+        Hs[(size_t)a * m + b] = Hs[(size_t)b * m + a] = s;
+      }
+    std::vector<double> th, U;
+    if (!oracle_la::eigh(m, Hs, th, U)) return false;
+    // Ritz vectors and residuals of the lowest nroots
+    std::vector<std::vector<double>> X(nroots, std::vector<double>(dim, 0.0)), R(nroots, std::vector<double>(dim, 0.0));
+    double rmax = 0;
+    for (int I = 0; I < nroots; ++I) {
+      for (int a = 0; a < m; ++a) {
+        const double u = U[(size_t)a * m + I];
+        for (int k = 0; k < dim; ++k) {
+          X[I][k] += u * V[a][k];
+          R[I][k] += u * AV[a][k];
+        }
+      }
+      double rn = 0;
+      for (int k = 0; k < dim; ++k) {
+        R[I][k] -= th[I] * X[I][k];
+        rn += R[I][k] * R[I][k];
+      }
+      rmax = std::max(rmax, std::sqrt(rn));
+    }
+    if (rmax < 1e-10) {
+      w_out.assign(th.begin(), th.begin() + nroots);
+      X_out.assign((size_t)dim * nroots, 0.0);
+      for (int I = 0; I < nroots; ++I)
+        for (int k = 0; k < dim; ++k) X_out[(size_t)k * nroots + I] = X[I][k];
+      return true;
+    }
+    if (m + nroots > maxsub) {  // restart from the Ritz vectors
+      V.clear();
+      AV.clear();
+      for (int I = 0; I < nroots; ++I) add_vector(X[I]);
+    }
+    int added = 0;
+    for (int I = 0; I < nroots; ++I) {
+      double rn = 0;
+      for (double r : R[I]) rn += r * r;
+      if (std::sqrt(rn) < 1e-10) continue;
+      std::vector<double> t(dim);
+      for (int k = 0; k < dim; ++k) {
+        double den = th[I] - delta[k] * delta[k];
+        if (std::fabs(den) < 1e-8) den = den < 0 ? -1e-8 : 1e-8;
+        t[k] = R[I][k] / den;
+      }
+      if (add_vector(t)) ++added;
+    }
+    if (!added) return false;
+  }
+  return false;
+}
+
 bool tddftb(const Mol& M, const State& st, int triplet, int nroots, std::vector<double>& omega,
             std::vector<double>& dip) {
   const int N = M.nao, no = M.nocc, nv = N - no, nat = M.nat;
@@ -1037,19 +1154,28 @@ bool tddftb(const Mol& M, const State& st, int triplet, int nroots, std::vector<
       for (int A = 0; A < nat; ++A) s += q[(size_t)k * nat + A] * G[(size_t)A * nat + B];
       qG[(size_t)k * nat + B] = s;
     }
-  std::vector<double> Om((size_t)dim * dim);
-  for (int k = 0; k < dim; ++k)
-    for (int l = 0; l <= k; ++l) {
-      double s = 0;
-      for (int B = 0; B < nat; ++B) s += qG[(size_t)k * nat + B] * q[(size_t)l * nat + B];
-      double v = 4.0 * std::sqrt(delta[k]) * s * std::sqrt(delta[l]);
-      if (k == l) v += delta[k] * delta[k];
-      Om[(size_t)k * dim + l] = Om[(size_t)l * dim + k] = v;
-    }
   std::vector<double> w, V;
-  if (!oracle_la::eigh(dim, Om, w, V)) {
-    g_error = "Casida diagonalisation failed";
-    return false;
+  int ldv = dim;  // V[k * ldv + I]: component k of eigenvector I
+  if (dim <= g_dense_casida_limit) {
+    std::vector<double> Om((size_t)dim * dim);
+    for (int k = 0; k < dim; ++k)
+      for (int l = 0; l <= k; ++l) {
+        double s = 0;
+        for (int B = 0; B < nat; ++B) s += qG[(size_t)k * nat + B] * q[(size_t)l * nat + B];
+        double v = 4.0 * std::sqrt(delta[k]) * s * std::sqrt(delta[l]);
+        if (k == l) v += delta[k] * delta[k];
+        Om[(size_t)k * dim + l] = Om[(size_t)l * dim + k] = v;
+      }
+    if (!oracle_la::eigh(dim, Om, w, V)) {
+      g_error = "Casida diagonalisation failed";
+      return false;
+    }
+  } else {
+    if (!davidson_lowest(dim, nat, nroots, delta, q, qG, w, V)) {
+      g_error = "Casida Davidson iteration failed";
+      return false;
+    }
+    ldv = nroots;
   }
   omega.assign(nroots, 0.0);
   dip.assign(3 * (size_t)nroots, 0.0);
@@ -1062,7 +1188,7 @@ bool tddftb(const Mol& M, const State& st, int triplet, int nroots, std::vector<
     omega[I] = om;
     if (triplet) continue;
     for (int k = 0; k < dim; ++k) {
-      const double c = std::sqrt(delta[k] / om) * V[(size_t)k * dim + I];
+      const double c = std::sqrt(delta[k] / om) * V[(size_t)k * ldv + I];
       for (int A = 0; A < nat; ++A)
         for (int x = 0; x < 3; ++x) dip[3 * I + x] += std::sqrt(2.0) * c * q[(size_t)k * nat + A] * M.pos[3 * A + x];
     }
@@ -1075,6 +1201,10 @@ bool tddftb(const Mol& M, const State& st, int triplet, int nroots, std::vector<
 extern "C" {
 
 const char* dftb_oracle_last_error() { return dftb_oracle::g_error.c_str(); }
+
+// Transitions up to which the TD-DFTB eigenproblem is solved densely (the
+// Davidson path above); tests set 0 to check the two paths against each other.
+void dftb_oracle_set_dense_casida_limit(int limit) { dftb_oracle::g_dense_casida_limit = limit; }
 
 // H0 and S (N x N, both triangles), gamma (nat x nat) and, for DFTB3, Gamma
 // (Gamma[a][b] = Gamma_ab).  nao_out receives N.

@@ -105,7 +105,8 @@ def lib():
         "sg_batch_set_scf": (ctypes.c_int32, [_VP, ctypes.c_double, ctypes.c_double, ctypes.c_int32]),
         "sg_batch_set_scf_path": (ctypes.c_int32, [_VP, ctypes.c_int32]),
         "sg_batch_set_mixed_switch": (ctypes.c_int32, [_VP, ctypes.c_double]),
-        "sg_batch_set_orbital_update": (ctypes.c_int32, [_VP, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32]),
+        "sg_batch_set_tuning": (ctypes.c_int32, [_VP, ctypes.c_int32, ctypes.c_int32]),
+        "sg_tuning_table": (ctypes.c_int32, [_I32, _I32, ctypes.c_int32]),
         "sg_batch_set_positions": (ctypes.c_int32, [_VP, _D]),
         "sg_batch_run": (ctypes.c_int32, [_VP, ctypes.c_uint32]),
         "sg_batch_results": (ctypes.c_int32, [_VP, _D, _D, _I32, _I32]),
@@ -433,14 +434,14 @@ class Batch:
 
     ORBITAL_UPDATES = {"exact": 0, "hybrid": 1, "rotation": 2}
 
-    def set_orbital_update(self, small="hybrid", large="hybrid", large_min_aos=1 << 30):
-        """Orbital update of the restricted NDDO SCF: molecules of at least
-        large_min_aos AOs use `large`, the others `small`; each one of "exact"
-        (tridiagonal diagonalisation every iteration), "hybrid" (tridiagonal
-        start, then occupied-virtual rotations) or "rotation" (Jacobi start,
-        then rotations)."""
-        self._check(lib().sg_batch_set_orbital_update(self._h, self.ORBITAL_UPDATES[small],
-                                                      self.ORBITAL_UPDATES[large], int(large_min_aos)))
+    def set_tuning(self, orbital_update=None, diis_size=None):
+        """Override the library's tuned table for every molecule of the batch:
+        orbital_update "exact" (tridiagonal diagonalisation every iteration),
+        "hybrid" (tridiagonal start, then occupied-virtual rotations) or
+        "rotation" (Jacobi start, then rotations); diis_size 1..6.  None keeps
+        the table's choice."""
+        mode = -1 if orbital_update is None else self.ORBITAL_UPDATES[orbital_update]
+        self._check(lib().sg_batch_set_tuning(self._h, mode, -1 if diis_size is None else int(diis_size)))
 
     def set_mixed_switch(self, rmsd):
         """rms(dP) below which "large_mixed" purifies in FP64 (default 1e-5)."""
@@ -534,6 +535,16 @@ class Batch:
     @property
     def stream(self):
         return lib().sg_batch_stream(self._h)
+
+
+def tuning_table():
+    """The library's tuned SCF choices per molecule-size bin of 32 AOs:
+    list of (first AO count of the bin, orbital update, Pulay subspace size)."""
+    names = {v: k for k, v in Batch.ORBITAL_UPDATES.items()}
+    modes = np.zeros(64, dtype=np.int32)
+    diis = np.zeros(64, dtype=np.int32)
+    n = lib().sg_tuning_table(_iptr(modes), _iptr(diis), 64)
+    return [(32 * k, names[int(modes[k])], int(diis[k])) for k in range(n)]
 
 
 def element_parameters(method, Z):

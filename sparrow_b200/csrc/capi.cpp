@@ -196,7 +196,7 @@ class Calculator {
       error = "TD-DFTB needs a converged reference calculation";
       return kErrNoResults;
     }
-    int rc = batch_->run_tddftb(nroots, triplet, 1e-8, 200, error);
+    int rc = batch_->run_tddftb(nroots, triplet, kTddftbResidual, kTddftbMaxIter, error);
     if (rc) return rc;
     std::vector<double> om, dp;
     std::vector<int> info;
@@ -630,19 +630,32 @@ int32_t sg_batch_set_mixed_switch(sg_batch* b, double rmsd) {
   return SG_OK;
 }
 
-int32_t sg_batch_set_orbital_update(sg_batch* b, int32_t small_mode, int32_t large_mode, int32_t large_min_aos) {
-  auto ok = [](int32_t m) { return m == kEigExact || m == kEigHybrid || m == kEigRotation; };
-  if (!b || !ok(small_mode) || !ok(large_mode) || large_min_aos < 1) return SG_ERR_INVALID_ARGUMENT;
-  b->sp.eig_mode_small = small_mode;
-  b->sp.eig_mode_large = large_mode;
-  b->sp.exact_eig_min_nao = large_min_aos;
+int32_t sg_batch_set_tuning(sg_batch* b, int32_t orbital_update, int32_t diis_size) {
+  const bool mode_ok = orbital_update == -1 || orbital_update == kEigExact || orbital_update == kEigHybrid ||
+                       orbital_update == kEigRotation;
+  if (!b || !mode_ok || diis_size == 0 || diis_size < -1 || diis_size > kDiisMax) return SG_ERR_INVALID_ARGUMENT;
+  const ScfParams tuned;
+  for (int k = 0; k < kTuneBins; ++k) {
+    b->sp.eig_mode_bin[k] = (signed char)(orbital_update >= 0 ? orbital_update : tuned.eig_mode_bin[k]);
+    b->sp.diis_bin[k] = (signed char)(diis_size > 0 ? diis_size : tuned.diis_bin[k]);
+  }
   return SG_OK;
+}
+
+int32_t sg_tuning_table(int32_t* orbital_update, int32_t* diis_size, int32_t capacity) {
+  if (capacity < 0 || (capacity > 0 && (!orbital_update || !diis_size))) return -SG_ERR_INVALID_ARGUMENT;
+  const ScfParams tuned;
+  for (int k = 0; k < kTuneBins && k < capacity; ++k) {
+    orbital_update[k] = tuned.eig_mode_bin[k];
+    diis_size[k] = tuned.diis_bin[k];
+  }
+  return kTuneBins;
 }
 
 int32_t sg_batch_excitations(sg_batch* b, int32_t nroots, int32_t triplet, double* omega, double* dipoles,
                              int32_t* status) {
   if (!b || !omega) return SG_ERR_INVALID_ARGUMENT;
-  int rc = b->impl->run_tddftb(nroots, triplet != 0, 1e-8, 200, b->error);
+  int rc = b->impl->run_tddftb(nroots, triplet != 0, kTddftbResidual, kTddftbMaxIter, b->error);
   if (rc) return rc;
   std::vector<double> om, dp;
   std::vector<int> info;

@@ -12,6 +12,14 @@
 
 namespace sgb {
 
+// Residual norm at which the TD-DFTB Davidson iteration stops (on the Casida
+// matrix, whose eigenvalues are omega^2 ~ 1e-3..1e-1 Hartree^2).  An
+// eigenvector error is about the residual over the gap to the next root; the
+// lowest roots of long polyenes lie ~2e-4 Hartree^2 apart, so 1e-10 keeps
+// transition dipoles of several e bohr within 1e-5.
+constexpr double kTddftbResidual = 1e-10;
+constexpr int kTddftbMaxIter = 300;
+
 struct MoleculeInput {
   std::vector<int> Z;
   std::vector<double> xyz;  // bohr, 3 per atom

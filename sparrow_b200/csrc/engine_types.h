@@ -98,6 +98,10 @@ struct MolResult {
 };
 
 constexpr int kEigExact = 0, kEigHybrid = 1, kEigRotation = 2;
+constexpr int kTuneBins = 16;  // molecule-size bins of 32 AOs for the tuned SCF choices
+}  // namespace sgb
+#include "tuned_table.h"
+namespace sgb {
 
 struct ScfParams {
   double scc = 1e-7;   // |Delta E| criterion (Hartree)
@@ -116,23 +120,27 @@ struct ScfParams {
   // virtual-virtual blocks unrotated, which changes no density or energy but
   // leaves the individual orbital energies as diagonal elements.
   int canonical = 0;
-  // orbital update of the NDDO restricted SCF, per molecule size: molecules
-  // of at least exact_eig_min_nao AOs use eig_mode_large, the others
-  // eig_mode_small.  Modes (kEig*): exact = a full diagonalisation of the
-  // extrapolated Fock matrix every iteration (Householder tridiagonal solver,
-  // Jacobi on clustered spectra); hybrid = the tridiagonal solver for the
-  // start, then occupied-virtual rotations; rotation = a Jacobi start, then
-  // occupied-virtual rotations.
-  int eig_mode_small = 1;
-  int eig_mode_large = 1;
-  int exact_eig_min_nao = 1 << 30;
+  // Orbital update and Pulay subspace size per molecule-size bin (32 AOs per
+  // bin, the last one open), defaulting to the autotuner's table
+  // (tuned_table.h).  Orbital-update modes (kEig*): exact = a full
+  // diagonalisation of the extrapolated Fock matrix every iteration
+  // (Householder tridiagonal solver, Jacobi on clustered spectra); hybrid =
+  // the tridiagonal solver for the start, then occupied-virtual rotations;
+  // rotation = a Jacobi start, then occupied-virtual rotations.  diis_size
+  // above caps every bin's subspace.
+  signed char eig_mode_bin[kTuneBins] = SGB_TUNED_ORBITAL_UPDATE;
+  signed char diis_bin[kTuneBins] = SGB_TUNED_DIIS_SIZE;
   // large-molecule mixed-precision path: purification switches from split-BF16
   // to FP64 once rms(Delta P) falls below this (or stops halving below 1e-4)
   double mixed_switch_rmsd = 1e-5;
 };
 
-__host__ __device__ inline int scf_eig_mode(const ScfParams& sp, int nao) {
-  return nao >= sp.exact_eig_min_nao ? sp.eig_mode_large : sp.eig_mode_small;
+__host__ __device__ inline int tune_bin(int nao) { return (nao >> 5) < kTuneBins ? (nao >> 5) : kTuneBins - 1; }
+__host__ __device__ inline int scf_eig_mode(const ScfParams& sp, int nao) { return sp.eig_mode_bin[tune_bin(nao)]; }
+__host__ __device__ inline int scf_diis_size(const ScfParams& sp, int nao) {
+  int m = sp.diis_bin[tune_bin(nao)];
+  if (sp.diis_size < m) m = sp.diis_size;
+  return m < 1 ? 1 : (m > kDiisMax ? kDiisMax : m);
 }
 
 // Device failure codes (MolResult::status)

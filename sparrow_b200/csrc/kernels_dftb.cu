@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_dftb_scf(
     const size_t packed_bytes = sizeof(double) * (size_t)N * (N + 1) / 2;
     double* rot = rotbuf + (size_t)blockIdx.x * (kRotBudgetBytes / sizeof(double));
     const int cap_rounds = (int)((kRotBudgetBytes / sizeof(double)) / (2 * ((N + 1) / 2)));
-    const int msize = sp.diis_size < 1 ? 1 : (sp.diis_size > kDiisMax ? kDiisMax : sp.diis_size);
+    const int msize = scf_diis_size(sp, N);
     const int cold_sweeps = sp.cold_sweeps > 0 ? sp.cold_sweeps : 6;
     int status = kDevOk;
 
@@ -552,7 +552,7 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_dftb_uhf_scf(
     const size_t packed_bytes = sizeof(double) * (size_t)N * (N + 1) / 2;
     double* rot = rotbuf + (size_t)blockIdx.x * (kRotBudgetBytes / sizeof(double));
     const int cap_rounds = (int)((kRotBudgetBytes / sizeof(double)) / (2 * ((N + 1) / 2)));
-    const int msize = sp.diis_size < 1 ? 1 : (sp.diis_size > kDiisMax ? kDiisMax : sp.diis_size);
+    const int msize = scf_diis_size(sp, N);
     const int cold_sweeps = sp.cold_sweeps > 0 ? sp.cold_sweeps : 6;
     int status = kDevOk;
     const int ns_it = inverse_sqrt(N, S, X, W1, Fa, Ca, W2, sh);

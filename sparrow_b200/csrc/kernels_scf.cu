@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_scf(const MolDev* __restrict
     // recorded Jacobi rotations: this CTA's slice of the rotation buffer
     double* rot = rotbuf + (size_t)blockIdx.x * (kRotBudgetBytes / sizeof(double));
     const int cap_rounds = (int)((kRotBudgetBytes / sizeof(double)) / (2 * ((N + 1) / 2)));
-    const int msize = sp.diis_size < 1 ? 1 : (sp.diis_size > kDiisMax ? kDiisMax : sp.diis_size);
+    const int msize = scf_diis_size(sp, N);
     const int cold_sweeps = sp.cold_sweeps > 0 ? sp.cold_sweeps : 3;
     int nhist = 0, head = 0;
     bool have_orbitals = false;
@@ -669,7 +669,7 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_uhf_scf(
     const size_t packed_bytes = sizeof(double) * (size_t)N * (N + 1) / 2;
     double* rot = rotbuf + (size_t)blockIdx.x * (kRotBudgetBytes / sizeof(double));
     const int cap_rounds = (int)((kRotBudgetBytes / sizeof(double)) / (2 * ((N + 1) / 2)));
-    const int msize = sp.diis_size < 1 ? 1 : (sp.diis_size > kDiisMax ? kDiisMax : sp.diis_size);
+    const int msize = scf_diis_size(sp, N);
     const int cold_sweeps = sp.cold_sweeps > 0 ? sp.cold_sweeps : 3;
     if (!spin_given)
       for (size_t k = tid; k < NN; k += blockDim.x) Pa[k] = Pb[k] = 0.5 * P[k];

@@ -207,11 +207,18 @@ def dftb_lib():
         L.dftb_oracle_tddftb.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, _I, _D, ctypes.c_int,
                                          ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          _D, ctypes.c_void_p, _D]
+        L.dftb_oracle_set_dense_casida_limit.argtypes = [ctypes.c_int]
         _dlib = L
     return _dlib
 
 
 DFTB_DEFAULT_SET = {2: "mio-1-1", 3: "3ob-3-1"}
+
+
+def set_dense_casida_limit(limit):
+    """Transitions up to which the oracle's TD-DFTB solves the Casida problem
+    densely (default 2000; the matrix-free Davidson iteration above)."""
+    dftb_lib().dftb_oracle_set_dense_casida_limit(int(limit))
 
 
 def dftb_scf(order, Z, xyz_bohr, charge=0, parameters=None, scc=1e-7, rmsd=1e-8, max_iter=1000, gradient=True,

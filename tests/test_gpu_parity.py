@@ -231,3 +231,21 @@ def test_calculator_orbital_energies_are_fock_eigenvalues(method):
     else:
         ref = O.dftb_scf(2, Z, x, scc=1e-11, rmsd=1e-10)["eps"]
     assert np.max(np.abs(np.sort(c.orbital_energies()) - np.sort(ref))) < 1e-6
+
+
+@pytest.mark.parametrize("method", ["PM6", "AM1"])
+def test_long_alkanes_match_oracle(method):
+    # the upper end of the 4096-alkane workload: C20, C25, C30 (122-182 AOs)
+    rng = np.random.default_rng(17)
+    mols = []
+    for n in (20, 25, 30):
+        Z, xa = geometry.alkane(n, rng)
+        mols.append((Z, geometry.to_bohr(xa)))
+    b = sparrow_b200.Batch(method, mols, rmsd=1e-8)
+    b.run(gradients=True)
+    e, g, it, conv = b.results()
+    assert conv.all()
+    for i, (Z, x) in enumerate(mols):
+        ref = O.scf(method, Z, x)
+        assert abs(e[i] - ref["energy"]) < E_TOL, i
+        assert np.max(np.abs(g[i] - ref["gradient"])) < G_TOL, i

@@ -99,3 +99,29 @@ def test_excitations_need_a_dftb_reference():
     om, mu, st = d.excitations(4)  # H2: one transition
     ref = O.dftb_tddftb(2, [1, 1], mols[0][1], nroots=4)
     assert st[0] == 0 and abs(om[0, 0] - ref["omega"][0]) < W_TOL and np.all(om[0, 1:] == 0)
+
+
+def test_long_polyenes_match_oracle():
+    # the upper end of the 1024-polyene workload (k = 20, 30, 40: 202-402
+    # AOs, up to 40401 transitions): the occupied and virtual Jacobi blocks
+    # of the canonical-orbital step leave shared memory there; the oracle
+    # solves the Casida problem by its matrix-free Davidson iteration.  Both
+    # SCFs converge to rms(dP) 1e-11: the k = 30 chain has two bright roots
+    # 1e-4 Hartree apart, whose individual dipoles follow the ground state's
+    # residual error (1.5e-5 e bohr apart at rms 1e-9)
+    rng = np.random.default_rng(21)
+    mols = []
+    for k in (20, 30, 40):
+        Z, xa = geometry.polyene(k, rng)
+        mols.append((Z, geometry.to_bohr(xa)))
+    b = sparrow_b200.Batch("DFTB3", mols, scc=1e-11, rmsd=1e-11, max_iter=300)
+    b.run()
+    e, _, _, conv = b.results()
+    assert conv.all()
+    om, mu, st = b.excitations(8)
+    assert (st == 0).all()
+    for i, (Z, x) in enumerate(mols):
+        ref = O.dftb_tddftb(3, Z, x, nroots=8, scc=1e-11, rmsd=1e-11)
+        assert abs(e[i] - ref["energy"]) < 1e-6, i
+        assert np.max(np.abs(om[i] - ref["omega"])) < W_TOL, i
+        assert _aligned_dipole_error(mu[i], ref["dipoles"]) < MU_TOL, i

@@ -52,3 +52,26 @@ def test_excitations_invariant_under_translation():
     for i in range(6):
         s = 1.0 if np.dot(a["dipoles"][i], b["dipoles"][i]) >= 0 else -1.0
         assert np.max(np.abs(a["dipoles"][i] - s * b["dipoles"][i])) < 1e-7
+
+
+def test_davidson_path_matches_dense_diagonalisation():
+    # the oracle's matrix-free Davidson iteration (used above 2000
+    # transitions) against its dense diagonalisation on the same polyene and
+    # on the reference's methane: energies and transition dipoles
+    from sparrow_b200 import geometry
+    rng = np.random.default_rng(4)
+    Z, xa = geometry.polyene(6, rng)
+    cases = [(3, Z, geometry.to_bohr(xa), None), (2,) + _case("CanPerformRestrictedSingletTDDFTCalculation")[1:] +
+             ("mio-1-1",)]
+    try:
+        for order, Zc, xc, params in cases:
+            O.set_dense_casida_limit(100000)
+            dense = O.dftb_tddftb(order, Zc, xc, nroots=8, parameters=params)
+            O.set_dense_casida_limit(0)
+            dav = O.dftb_tddftb(order, Zc, xc, nroots=8, parameters=params)
+            assert np.max(np.abs(dense["omega"] - dav["omega"])) < 1e-10
+            for i in range(len(dense["omega"])):
+                s = 1.0 if np.dot(dense["dipoles"][i], dav["dipoles"][i]) >= 0 else -1.0
+                assert np.max(np.abs(dense["dipoles"][i] - s * dav["dipoles"][i])) < 1e-7
+    finally:
+        O.set_dense_casida_limit(2000)

@@ -14,6 +14,22 @@ E_TOL = 1e-6   # Hartree
 G_TOL = 1e-5   # Hartree / bohr
 
 
+def _co2_cluster(n, seed):
+    """(CO2)_n: linear O=C=O (1.16 A) on a 3.4 A cubic grid, random
+    orientations, all-heavy atoms (4 AOs each): 12 AOs per molecule."""
+    rng = np.random.default_rng(seed)
+    side = int(np.ceil(n ** (1.0 / 3.0)))
+    Z, X = [], []
+    for k in range(n):
+        c = 3.4 * np.array([k % side, (k // side) % side, k // (side * side)], float)
+        u = rng.normal(size=3)
+        u /= np.linalg.norm(u)
+        for z, s in ((6, 0.0), (8, 1.16), (8, -1.16)):
+            Z.append(z)
+            X.append(c + s * u)
+    return np.asarray(Z, dtype=np.int32), geometry.to_bohr(np.array(X))
+
+
 def _water(n, seed):
     Z, X = geometry.water_cluster(n, seed)
     return np.asarray(Z, dtype=np.int32), geometry.to_bohr(X)
@@ -78,3 +94,24 @@ def test_static_energy_only_and_errors():
     with pytest.raises(sparrow_b200.SparrowError) as ei:
         sparrow_b200.calculate_static("PM6", Zc, np.arange(3 * 65, dtype=np.float64) * 3.0)
     assert ei.value.code == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n_co2", [17, 21])
+def test_static_at_the_upper_size_limit(n_co2):
+    # 204 and 252 AOs (51 and 63 atoms): the eigensolver's tiled matrix no
+    # longer fits shared memory above 192 AOs and runs from the static
+    # scratch; static, batched and oracle agree
+    from tests import oracle_lib as O
+    Z, X = _co2_cluster(n_co2, 2)
+    assert 200 <= 12 * n_co2 <= sparrow_b200.SG_STATIC_MAX_AOS
+    e_ref, g_ref, _, conv_ref = sparrow_b200.batch_calculate("PM6", [(Z, X)], scc=1e-9, rmsd=1e-8, gradients=True)
+    assert conv_ref[0]
+    ref = O.scf("PM6", Z, X, scc=1e-9, rmsd=1e-8)
+    assert abs(e_ref[0] - ref["energy"]) < E_TOL
+    for _ in range(2):
+        e, g, it, conv = sparrow_b200.calculate_static("PM6", Z, X, scc=1e-9, rmsd=1e-8, gradients=True)
+        assert conv
+        assert abs(e - e_ref[0]) < E_TOL
+        assert np.max(np.abs(g - g_ref[0])) < G_TOL
+        assert np.max(np.abs(g - ref["gradient"])) < G_TOL
