@@ -627,6 +627,40 @@ def batch_calculate(method, molecules, charges=None, scc=1e-7, rmsd=1e-5, max_it
     return e, grads, it, conv.astype(bool)
 
 
+def flatten_molecules(molecules):
+    """(n_atoms, Z, xyz) flat arrays of a list of (atomic_numbers, positions_bohr):
+    the layout batch_calculate_flat and the C-ABI batch entry points take."""
+    return _flatten(molecules)
+
+
+def batch_calculate_flat(method, n_atoms, Z, xyz_bohr, charges=None, scc=1e-7, rmsd=1e-5, max_iter=100,
+                         gradients=False):
+    """batch_calculate on flat host arrays (n_atoms [n], Z [sum n_atoms], xyz
+    [3 sum n_atoms], bohr): no per-molecule Python work on either side.
+    Returns (energies [n], gradients [sum n_atoms, 3] or None, iterations [n],
+    converged [n])."""
+    L = lib()
+    n_atoms = np.ascontiguousarray(n_atoms, dtype=np.int32)
+    Z = np.ascontiguousarray(Z, dtype=np.int32)
+    X = np.ascontiguousarray(xyz_bohr, dtype=np.float64).reshape(-1)
+    if X.size != 3 * Z.size or int(n_atoms.sum()) != Z.size:
+        raise ValueError("n_atoms, Z and xyz sizes disagree")
+    n = n_atoms.size
+    ch = None if charges is None else np.ascontiguousarray(charges, dtype=np.int32)
+    e = np.zeros(n)
+    it = np.zeros(n, dtype=np.int32)
+    conv = np.zeros(n, dtype=np.int32)
+    g = np.zeros(3 * Z.size) if gradients else None
+    msg = ctypes.create_string_buffer(512)
+    props = SG_PROP_ENERGY | (SG_PROP_GRADIENTS if gradients else 0)
+    rc = L.sg_batch_calculate(method.encode(), n, _iptr(n_atoms), _iptr(Z), _dptr(X),
+                              _iptr(ch) if ch is not None else None, scc, rmsd, max_iter, props, _dptr(e),
+                              _dptr(g) if g is not None else None, _iptr(it), _iptr(conv), msg, 512)
+    if rc != 0 and rc != SG_ERR_NOT_CONVERGED:
+        raise SparrowError(rc, msg.value.decode())
+    return e, (g.reshape(-1, 3) if g is not None else None), it, conv.astype(bool)
+
+
 def calculate_static(method, atomic_numbers, xyz_bohr, charge=0, scc=1e-7, rmsd=1e-5, max_iter=100,
                      gradients=False, stream=None):
     """One molecule through the allocation-free entry point (sg_calculate_static).

@@ -54,14 +54,7 @@ __device__ __forceinline__ size_t tiled_doubles(int N) {
   const int nt = (N + 31) >> 5;
   return (size_t)tri_index(nt, 0) * kTileDoubles;
 }
-// tile (I, J) of the q-th lower tile in row-major order over I >= J
-__device__ __forceinline__ void tri_decode(int q, int& a, int& b) {
-  int r = (int)((sqrtf(8.0f * (float)q + 1.0f) - 1.0f) * 0.5f);
-  while (r * (r + 1) / 2 > q) --r;
-  while ((r + 1) * (r + 2) / 2 <= q) ++r;
-  a = r;
-  b = q - r * (r + 1) / 2;
-}
+// (tri_decode, the q-th lower tile in row-major order, comes with the SCF helpers)
 
 // Number of eigenvalues of T (diagonal d, squared off-diagonal e2) below x:
 // sign changes of the leading principal minors of T - x I.  The minors are

@@ -236,6 +236,16 @@ int Batch::setup(const std::vector<MoleculeInput>& in, std::string& err, bool ch
     }
   long long int_off = 0, mat_off = 0, diis_off = 0, gam_off = 0;
   int ao_base = 0, max_nao = 0;
+  {
+    size_t natoms_total = 0, nao_total = 0;
+    for (const auto& m : in) {
+      natoms_total += m.Z.size();
+      for (int z : m.Z) nao_total += (size_t)elems_[slot_of[z]].nao;
+    }
+    mols_.reserve(in.size());
+    atoms_.reserve(natoms_total);
+    ao_atom_.reserve(nao_total);
+  }
   for (size_t mi = 0; mi < in.size(); ++mi) {
     const auto& mol = in[mi];
     MolDev md{};

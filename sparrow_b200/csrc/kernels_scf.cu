@@ -320,19 +320,78 @@ __device__ double fock_diagonal(const MolDev& m, const AtomDev* __restrict__ ato
   return e;
 }
 
+// The same with a warp per atom: lanes walk the partner atoms (the Coulomb
+// vectors of many pairs in flight at once), a warp-private row of 10
+// partials per lane in ws (32 * 10 doubles per warp) is summed by lanes 0-9,
+// which then add the one-centre terms.  Warp w of nw handles atoms w, w + nw, ...
+__device__ double fock_diagonal_warp(const MolDev& m, const AtomDev* __restrict__ atoms,
+                                     const ElemDev* __restrict__ elems, const double* __restrict__ jbuf,
+                                     const double* __restrict__ H, const double* __restrict__ P, double* F, double* ws,
+                                     int warp, int nw) {
+  const int N = m.nao, lane = threadIdx.x & 31;
+  double e = 0;
+  for (int a = warp; a < m.nat; a += nw) {
+    const AtomDev aA = atoms[m.atom0 + a];
+    const ElemDev& eA = elems[aA.slot];
+    const int np = eA.nao == 1 ? 1 : 10;
+    double js[10];
+#pragma unroll
+    for (int q = 0; q < 10; ++q) js[q] = 0.0;
+    for (int c = lane; c < m.nat; c += 32) {
+      if (c == a) continue;
+      const double* jb = jbuf + (size_t)(a < c ? pair_slot(m, a, c) : pair_slot(m, c, a)) * 20 + (a < c ? 0 : 10);
+      if (np == 1) {
+        js[0] += jb[0];
+      } else {
+#pragma unroll
+        for (int q = 0; q < 10; ++q) js[q] += jb[q];
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 10; ++q) ws[lane * 10 + q] = js[q];
+    __syncwarp();
+    if (lane < np) {
+      double j = 0;
+      for (int l = 0; l < 32; ++l) j += ws[l * 10 + lane];
+      const int mu = c_pair_mu[lane], nu = c_pair_nu[lane];
+      const double g = one_centre_g(eA, mu, nu, P, N, aA.ao0) + j;
+      const size_t i1 = (size_t)(aA.ao0 + mu) * N + aA.ao0 + nu;
+      const double h = H[i1];
+      const double f = h + g;
+      F[i1] = f;
+      if (mu != nu) F[(size_t)(aA.ao0 + nu) * N + aA.ao0 + mu] = f;
+      e += (mu == nu ? 0.5 : 1.0) * P[i1] * (h + f);
+    }
+    __syncwarp();
+  }
+  return e;
+}
+
+// prof (optional): cycles of the light pairs, the heavy pairs with the
+// barrier, the diagonal blocks with the barrier and the energy sum added to
+// prof[0..3].
 __device__ double build_fock(const MolDev& m, const AtomDev* __restrict__ atoms, const ElemDev* __restrict__ elems,
                              const PairDev* __restrict__ pairs, const double* __restrict__ ints,
                              const int* __restrict__ hh_pairs, double* __restrict__ jbuf,
                              const double* __restrict__ H, const double* __restrict__ P, double* F, double* red,
-                             double* wscratch) {
+                             double* wscratch, long long* prof = nullptr) {
   const int tid = threadIdx.x, warp = tid >> 5, nwarps = blockDim.x >> 5;
+  long long t = clock64();
   double e = fock_light_pairs(m, atoms, elems, pairs, ints, hh_pairs, jbuf, H, P, F, tid, blockDim.x);
+  prof_mark(prof, 0, t);
   e += fock_heavy_pairs(m, atoms, elems, pairs, ints, hh_pairs, jbuf, H, P, F, wscratch + (size_t)warp * kFockWarpScratch,
                         warp, nwarps);
   __syncthreads();
-  e += fock_diagonal(m, atoms, elems, pairs, ints, hh_pairs, jbuf, H, P, F, tid, blockDim.x);
+  prof_mark(prof, 1, t);
+  // wscratch holds kFockWarpScratch doubles per warp for the heavy pairs; the
+  // diagonal phase needs 320 per warp: the phase-scratch union has room for
+  // that (a barrier separates the two uses)
+  e += fock_diagonal_warp(m, atoms, elems, jbuf, H, P, F, wscratch + (size_t)warp * 320, warp, nwarps);
   __syncthreads();
-  return cta_sum(e, red);
+  prof_mark(prof, 2, t);
+  const double s = cta_sum(e, red);
+  prof_mark(prof, 3, t);
+  return s;
 }
 
 __global__ void __launch_bounds__(kScfThreads, 1) k_scf(const MolDev* __restrict__ mols, int nmol,
@@ -388,23 +447,29 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_scf(const MolDev* __restrict
     double last_dE = 0, last_rms = 0;
 
     long long cyc[5] = {0, 0, 0, 0, 0};
-#ifdef SGB_EIG_PROFILE
-    // profiling build: the result's cycle counters report the eigensolver's
-    // stages (tridiagonalisation, bisection, vectors, back-transformation,
-    // everything else)
-    long long eprof_buf[4] = {0, 0, 0, 0};
-    long long* eprof = eprof_buf;
+#ifdef SGB_PROFILE_GROUP
+    // profiling build: the result's cycle counters report four stages of one
+    // phase (SGB_PROFILE_GROUP 1: the eigensolver, 2: DIIS, 3: the
+    // occupied-virtual rotation, 4: the Fock build) and everything else
+    long long gprof[4] = {0, 0, 0, 0};
+    long long* eprof = SGB_PROFILE_GROUP == 1 ? gprof : nullptr;
+    long long* dprof = SGB_PROFILE_GROUP == 2 ? gprof : nullptr;
+    long long* oprof = SGB_PROFILE_GROUP == 3 ? gprof : nullptr;
+    long long* fprof = SGB_PROFILE_GROUP == 4 ? gprof : nullptr;
 #else
     long long* eprof = nullptr;
+    long long* dprof = nullptr;
+    long long* oprof = nullptr;
+    long long* fprof = nullptr;
 #endif
     int nfull = 0, nsweeps = 0;
     for (it = 1; it <= sp.max_iter; ++it) {
       long long t0 = clock64();
-      const double E = build_fock(m, atoms, elems, pairs, ints, hh_pairs, jbuf, H, P, F, sh.red, sh.fockw);
+      const double E = build_fock(m, atoms, elems, pairs, ints, hh_pairs, jbuf, H, P, F, sh.red, sh.fockw, fprof);
       __syncthreads();
       long long t1 = clock64();
       cyc[0] += t1 - t0;
-      const double* Fx = diis_step(N, F, P, W1, W2, histF, histE, msize, nhist, head, sh);
+      const double* Fx = diis_step(N, F, P, W1, W2, histF, histE, msize, nhist, head, sh, dprof);
       // Fx lives in F or W2; move it to F so W1/W2 are free as scratch
       if (Fx != F) {
         for (size_t k = tid; k < NN; k += blockDim.x) F[k] = W2[k];
@@ -413,7 +478,7 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_scf(const MolDev* __restrict
       long long t2 = clock64();
       cyc[1] += t2 - t1;
       int need_full = !have_orbitals;
-      if (mode != kEigExact && have_orbitals) need_full = ov_rotation(N, no, F, Ct, W1, W2, eps, drift, sh);
+      if (mode != kEigExact && have_orbitals) need_full = ov_rotation(N, no, F, Ct, W1, W2, eps, drift, sh, oprof);
       if (mode == kEigExact || (need_full && mode == kEigHybrid)) {
         // exact: every iteration the lowest eigenvalues and the occupied
         // eigenvectors of the extrapolated F; hybrid: every eigenpair at the
@@ -482,12 +547,12 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_scf(const MolDev* __restrict
       r.last_rmsd = last_rms;
       r.full_diag = nfull;
       r.jacobi_sweeps = nsweeps;
-#ifdef SGB_EIG_PROFILE
+#ifdef SGB_PROFILE_GROUP
       long long tot = 0;
       for (int k = 0; k < 5; ++k) tot += cyc[k];
       for (int k = 0; k < 4; ++k) {
-        r.cycles[k] = eprof[k];
-        tot -= eprof[k];
+        r.cycles[k] = gprof[k];
+        tot -= gprof[k];
       }
       r.cycles[4] = tot;
 #else

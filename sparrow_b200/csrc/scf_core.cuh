@@ -480,10 +480,19 @@ struct ScfShared {
   // are never live at the same time
   union __align__(16) {
     double gemm[2 * kGemmStages * kGemmStage];
-    double fockw[(kScfThreads / 32) * kFockWarpScratch];
+    double fockw[(kScfThreads / 32) * (kFockWarpScratch > 320 ? kFockWarpScratch : 320)];
     JacobiShared js;
   };
 };
+
+// q-th tile (a, b), a >= b, of the lower triangle of tiles in row-major order.
+__device__ __forceinline__ void tri_decode(int q, int& a, int& b) {
+  int r = (int)((sqrtf(8.0f * (float)q + 1.0f) - 1.0f) * 0.5f);
+  while (r * (r + 1) / 2 > q) --r;
+  while ((r + 1) * (r + 2) / 2 <= q) ++r;
+  a = r;
+  b = q - r * (r + 1) / 2;
+}
 
 // Pulay DIIS: store (F, FP - PF) in the ring, extend the B matrix, solve.
 // Returns the extrapolated Fock matrix (F itself or dst).  The ring keeps the
@@ -610,9 +619,23 @@ __device__ __forceinline__ void diis_extrapolate(int N, const double* histF, int
   __syncthreads();
 }
 
+// Profiling builds: thread 0 adds the cycles since *t to prof[k] and moves *t on.
+__device__ __forceinline__ void prof_mark(long long* prof, int k, long long& t) {
+  if (prof && threadIdx.x == 0) {
+    const long long now = clock64();
+    prof[k] += now - t;
+    t = now;
+  }
+}
+
+// prof (optional): cycles of the FP product, the store pass, the solve and
+// the extrapolation added to prof[0..3].
 __device__ const double* diis_step(int N, const double* F, const double* P, double* W, double* dst, double* histF,
-                                   double* histE, int msize, int& nhist, int& head, ScfShared& sh) {
+                                   double* histE, int msize, int& nhist, int& head, ScfShared& sh,
+                                   long long* prof = nullptr) {
+  long long t = clock64();
   cta_gemm(N, N, N, 1.0, F, N, false, P, N, false, 0.0, W, N, sh.gemm);  // W = FP
+  prof_mark(prof, 0, t);
   const int slot = head;
   head = (head + 1) % msize;
   if (nhist < msize) ++nhist;
@@ -620,8 +643,12 @@ __device__ const double* diis_step(int N, const double* F, const double* P, doub
 #pragma unroll
   for (int j = 0; j < kDiisMax; ++j) d[j] = 0.0;
   diis_store(N, F, W, histF, histE, slot, nhist, d);
-  if (!diis_solve(slot, nhist, d, sh)) return F;
+  prof_mark(prof, 1, t);
+  const bool ok = diis_solve(slot, nhist, d, sh);
+  prof_mark(prof, 2, t);
+  if (!ok) return F;
   diis_extrapolate(N, histF, nhist, dst, sh);
+  prof_mark(prof, 3, t);
   return dst;
 }
 
@@ -690,12 +717,16 @@ __device__ int full_diagonalise(int N, double* F, double* Ct, double* W1, double
 // large (a full diagonalisation is needed instead); Ct is unchanged then.
 // F holds the (extrapolated) Fock matrix on entry and is used as scratch.
 // Scratch: W1 (N x N), W2 (N x N).  eps receives diag(C^T F C).
+// prof (optional): cycles of C^T F with the diagonal, the X step and its
+// quadratic terms, the rotation product, the re-orthonormalisation added to
+// prof[0..3].
 __device__ int ov_rotation(int N, int no, double* F, double* Ct, double* W1, double* W2, double* eps, double& drift,
-                           ScfShared& sh) {
+                           ScfShared& sh, long long* prof = nullptr) {
   const int nv = N - no;
   const size_t NN = (size_t)N * N;
   const int tid = threadIdx.x;
   if (no == 0 || nv == 0) return 0;
+  long long tprof = clock64();
   cta_gemm(N, N, N, 1.0, Ct, N, false, F, N, false, 0.0, W1, N, sh.gemm);  // W1 = C^T F (row k = c_k^T F)
   {
     const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
@@ -714,6 +745,7 @@ __device__ int ov_rotation(int N, int no, double* F, double* Ct, double* W1, dou
   }
   homo = cta_max(homo, sh.red);
   lumo = -cta_max(-lumo, sh.red);
+  prof_mark(prof, 0, tprof);
   if (!(homo < lumo - 1e-4)) return 1;
   // X (nv x no) = F_vo / (e_i - e_a), F_vo[a][i] = c_a^T F c_i = sum_nu Ct[a][nu] W1[i][nu]
   double* X = W2;
@@ -740,9 +772,11 @@ __device__ int ov_rotation(int N, int no, double* F, double* Ct, double* W1, dou
   }
   for (int k = tid; k < N; k += blockDim.x) W1[(size_t)k * N + k] += 1.0;
   __syncthreads();
+  prof_mark(prof, 1, tprof);
   cta_gemm(N, N, N, 1.0, W1, N, false, Ct, N, false, 0.0, F, N, sh.gemm);
   for (size_t e = tid; e < NN; e += blockDim.x) Ct[e] = F[e];
   __syncthreads();
+  prof_mark(prof, 2, tprof);
   // the second-order rotation is orthogonal up to |K|^4 / 4: re-orthonormalise when needed
   drift += 0.25 * xmax * xmax * xmax * xmax;
   if (drift > 1e-12) {
@@ -756,6 +790,7 @@ __device__ int ov_rotation(int N, int no, double* F, double* Ct, double* W1, dou
     for (size_t e = tid; e < NN; e += blockDim.x) Ct[e] = W2[e];
     __syncthreads();
     drift = 0;
+    prof_mark(prof, 3, tprof);
   }
   return 0;
 }

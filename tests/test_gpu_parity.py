@@ -131,6 +131,11 @@ def test_batch_calculate_from_host_buffers():
     e2, g2, _, _ = b.results()
     assert np.allclose(e, e2, atol=1e-10, rtol=0)
     assert conv.all()
+    # the same through flat host arrays
+    n_atoms, Z, X = sparrow_b200.flatten_molecules(mols)
+    e3, g3, it3, conv3 = sparrow_b200.batch_calculate_flat("AM1", n_atoms, Z, X, rmsd=1e-8, gradients=True)
+    assert np.allclose(e, e3, atol=1e-10, rtol=0) and conv3.all() and (it3 == it).all()
+    assert np.allclose(np.concatenate(g), g3, atol=1e-9, rtol=0)
 
 
 def test_non_convergence_is_a_flag_not_an_error():
