@@ -738,7 +738,7 @@ static void build_one_electron(Molecule& M) {
     const Element& e = M.el[a];
     for (int k = 0; k < e.nao; ++k) H(M.ao0[a] + k, M.ao0[a] + k) = k == 0 ? e.Uss : e.Upp;
   }
-  M.Erep = 0;
+  oracle_la::CompensatedSum erep;
   for (const auto& P : M.pairs) {
     const Element &A = M.el[P.a], &B = M.el[P.b];
     int oa = M.ao0[P.a], ob = M.ao0[P.b];
@@ -766,8 +766,9 @@ static void build_one_electron(Molecule& M) {
     double Rabs = std::sqrt(R[0] * R[0] + R[1] * R[1] + R[2] * R[2]);
     double E, dE;
     repulsion(M.method, A, B, Rabs, E, dE);
-    M.Erep += E;
+    erep.add(E);
   }
+  M.Erep = erep.value();
 }
 
 // Full two-electron matrix (TwoElectronMatrix.cpp:82-166, written for the
@@ -827,9 +828,9 @@ static void build_G(const Molecule& M, const std::vector<double>& P, std::vector
 }
 
 static double electronic_energy(const std::vector<double>& P, const std::vector<double>& H, const std::vector<double>& G) {
-  double e = 0;
-  for (size_t k = 0; k < P.size(); ++k) e += 0.5 * P[k] * (2 * H[k] + G[k]);
-  return e;
+  oracle_la::CompensatedSum e;
+  for (size_t k = 0; k < P.size(); ++k) e.add(0.5 * P[k] * (2 * H[k] + G[k]));
+  return e.value();
 }
 
 struct ScfSettings {
@@ -954,9 +955,9 @@ struct ScfResultU {
 
 static double uhf_energy(const Molecule& M, const std::vector<double>& Pa, const std::vector<double>& Pb,
                          const std::vector<double>& Ga, const std::vector<double>& Gb) {
-  double e = 0;
-  for (size_t k = 0; k < Pa.size(); ++k) e += (Pa[k] + Pb[k]) * M.H[k] + 0.5 * (Pa[k] * Ga[k] + Pb[k] * Gb[k]);
-  return e;
+  oracle_la::CompensatedSum e;
+  for (size_t k = 0; k < Pa.size(); ++k) e.add((Pa[k] + Pb[k]) * M.H[k] + 0.5 * (Pa[k] * Ga[k] + Pb[k] * Gb[k]));
+  return e.value();
 }
 
 static bool run_uhf(Molecule& M, int na, int nb, const ScfSettings& st, ScfResultU& r) {

@@ -7,6 +7,20 @@
 
 namespace oracle_la {
 
+// Neumaier-compensated running sum.  The NDDO energies are differences of
+// sums over millions of terms that reach 1e5 Hartree for a few thousand AOs
+// (E_el and E_rep cancel to 1e3); a plain running sum there loses 1e-8 to
+// 1e-6 Hartree, above the precision the checks ask for.
+struct CompensatedSum {
+  double s = 0, c = 0;
+  void add(double x) {
+    const double t = s + x;
+    c += std::fabs(s) >= std::fabs(x) ? (s - t) + x : (x - t) + s;
+    s = t;
+  }
+  double value() const { return s + c; }
+};
+
 // Householder reduction of symmetric A to tridiagonal form; A is overwritten
 // with the accumulated orthogonal transform Q (A_in = Q T Q^T); d = diagonal,
 // e[i] = sub-diagonal T(i, i-1) for i >= 1.

@@ -22,6 +22,11 @@ namespace sgb {
 
 constexpr int kMaxAtomsPerMolecule = 4096;
 constexpr int kDiisMax = 6;          // Pulay subspace size
+// Largest stored <E, E> below which every Pulay error vector is rounding
+// noise: F and P commute to working precision (a converged system, or one
+// pinned by symmetry such as H2, where FP - PF vanishes identically).  The B
+// matrix is then noise and its solution arbitrary, so the step keeps F.
+constexpr double kDiisNoiseNorm = 1e-24;
 constexpr int kMaxElementSlots = 16; // distinct elements in one batch
 
 enum Method : int { kMNDO = 0, kAM1 = 1, kPM6 = 2, kDFTB2 = 3, kDFTB3 = 4 };

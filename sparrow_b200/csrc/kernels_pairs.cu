@@ -1,11 +1,12 @@
 // Pair kernels: two-centre integrals (values) and the nuclear gradient.
 //
-// One thread per atom pair.  The value kernel writes, per pair, the global
-// two-electron block, both core-attraction vectors, the overlap block and
-// the core-core repulsion (the density-independent part that the reference
-// builds in TwoCenterIntegralContainer::update, OneElectronMatrix::calculate
-// and PM6RepulsionEnergy::calculateRepulsion).  The gradient kernel repeats
-// the pair math in dual numbers and contracts it with the converged density
+// The value kernels (a thread per pair with hydrogen, a warp per s/p-s/p
+// pair) write, per pair, the global two-electron block, both core-attraction
+// vectors, the overlap block and the core-core repulsion (the
+// density-independent part that the reference builds in
+// TwoCenterIntegralContainer::update, OneElectronMatrix::calculate and
+// PM6RepulsionEnergy::calculateRepulsion).  The gradient kernels contract the
+// pair math's derivatives with the converged density in reverse mode
 // (OneElectronMatrix.cpp:136-229, TwoElectronMatrix.cpp:168-241).
 #include <cuda_runtime.h>
 
@@ -16,49 +17,123 @@
 namespace sgb {
 
 __constant__ LocalTermTable c_local_terms;
+// Global-memory copy of the term table, for reads at lane-dependent indices
+// (the constant bank serialises a warp's distinct addresses).
+__device__ LocalTermTable g_local_terms;
 
 void upload_local_terms(const LocalTermTable& tab, cudaStream_t stream) {
   cudaMemcpyToSymbolAsync(c_local_terms, &tab, sizeof(LocalTermTable), 0, cudaMemcpyHostToDevice, stream);
+  cudaMemcpyToSymbolAsync(g_local_terms, &tab, sizeof(LocalTermTable), 0, cudaMemcpyHostToDevice, stream);
 }
 
-// Values of pair p (see the file comment).
-__device__ __forceinline__ void pair_values_one(int p, const PairDev& pr, const AtomDev& a, const AtomDev& b,
-                                                const ElemDev& A, const ElemDev& B,
-                                                const DiatomicDev* __restrict__ diat, int method,
-                                                double* __restrict__ ints, double* __restrict__ vcore,
-                                                double* __restrict__ ovl, double* __restrict__ erep) {
-  const double X = b.x - a.x, Y = b.y - a.y, Z = b.z - a.z;
-  const int dA = A.nao == 1 ? 1 : 10, dB = B.nao == 1 ? 1 : 10;
+// Evaluated local entries (table entries of local_terms.cpp, whose order
+// follows Local2c2eMatrix.cpp:91-149) of the sigma column (p | ss) and row
+// (ss | p) for the local orbital pairs ss, xx (= yy), sz and zz: the only
+// local entries that are nonzero when one side is an s function or a bare
+// core.
+constexpr int kColSS = 0, kColXX = 4, kColSZ = 5, kColZZ = 6;
+constexpr int kRowSS = 0, kRowXX = 1, kRowSZ = 2, kRowZZ = 3;
 
-  double G[10][10];
-  global_block<double>(c_local_terms, A, B, X, Y, Z, G);
-  double* out = ints + pr.int_off;
-  for (int i = 0; i < dA; ++i)
-    for (int j = 0; j < dB; ++j) out[i * dB + j] = G[i][j];
-
-  double V[10];
-  core_vector<double>(c_local_terms, A, B, X, Y, Z, V);
-  double* vc = vcore + (size_t)p * 20;
-  for (int i = 0; i < 10; ++i) vc[i] = i < dA ? V[i] : 0.0;
-  core_vector<double>(c_local_terms, B, A, -X, -Y, -Z, V);
-  for (int i = 0; i < 10; ++i) vc[10 + i] = i < dB ? V[i] : 0.0;
-
-  double R[3] = {X, Y, Z};
-  double S[4][4];
-  overlap_block<double>(A, B, R, S);
-  double* so = ovl + (size_t)p * 16;
-  for (int i = 0; i < 4; ++i)
-    for (int j = 0; j < 4; ++j) so[i * 4 + j] = S[i][j];
-
-  double E, dE;
-  core_repulsion(method, A, B, diat[a.slot * kMaxElementSlots + b.slot], sqrt(X * X + Y * Y + Z * Z), E, dE);
-  erep[p] = E;
+// Value of evaluated local entry e (no derivative; rsqrt of the squared
+// charge distance, within an ulp of 1/sqrt).
+__device__ __forceinline__ double local_value(const LocalTermTable& tab, int e, double R, const ElemDev& A,
+                                              const ElemDev& B, bool coreB, double rhoCoreB) {
+  double val = 0.0;
+  const int s = tab.start[e], n = tab.count[e];
+  for (int t = s; t < s + n; ++t) {
+    const LocalTerm& T = tab.term[t];
+    const double rA = A.rho[T.c1];
+    const double rB = coreB ? rhoCoreB : B.rho[T.c2];
+    const double D1 = A.D[T.c1];
+    const double d2 = coreB ? 0.0 : B.D[T.c2];
+    const double dx = d2 * T.x2 - D1 * T.x1;
+    const double dy = d2 * T.y2 - D1 * T.y1;
+    const double dz = R + d2 * T.z2 - D1 * T.z1;
+    const double rr = rA + rB;
+    val = fma(T.q, rsqrt(dx * dx + dy * dy + dz * dz + rr * rr), val);
+  }
+  return val;
 }
 
-// Pairs with at least one s-only atom, one thread each.  s/p-s/p pairs cost
-// two orders of magnitude more and sit in the same rows of the pair table
-// (heavy atoms first): they go to k_pair_values_heavy, so that no warp waits
-// on one of them while its other lanes idle.
+// Orbital pair (mu, nu), mu <= nu, of packed index p = nu (nu + 1) / 2 + mu.
+__device__ __forceinline__ void pair_of(int p, int& mu, int& nu) {
+  nu = p < 1 ? 0 : (p < 3 ? 1 : (p < 6 ? 2 : 3));
+  mu = p - nu * (nu + 1) / 2;
+}
+
+// Global value of orbital pair g of an s/p atom from a local block whose
+// other side is an s function or a bare core.  Only the sigma entries ss,
+// sz, xx = yy and zz are nonzero in the local frame, and global_block's
+// pair rotation reduces to G[ss] = L_ss, G[s nu] = rot[nu][z] L_sz,
+// G[mu nu] = sum_m rot[mu][m] rot[nu][m] L_mm for p orbitals mu, nu.
+__device__ __forceinline__ double sigma_entry(const double rot[4][4], int g, double Lss, double Lsz, double Lxx,
+                                              double Lzz) {
+  int mu, nu;
+  pair_of(g, mu, nu);
+  if (nu == 0) return Lss;
+  if (mu == 0) return rot[nu][3] * Lsz;
+  return rot[mu][1] * rot[nu][1] * Lxx + rot[mu][2] * rot[nu][2] * Lxx + rot[mu][3] * rot[nu][3] * Lzz;
+}
+
+// Entry (p, q) of global_block's pair rotation W (both atoms s/p, same frame).
+__device__ __forceinline__ double pair_rotation_entry(const double rot[4][4], int p, int q) {
+  int mu, nu, m, n;
+  pair_of(p, mu, nu);
+  pair_of(q, m, n);
+  double w = rot[mu][m] * rot[nu][n];
+  if (m != n) w += rot[mu][n] * rot[nu][m];
+  return w;
+}
+
+// Overlap block of an atom pair from five primitive sums.  With p = a + b and
+// K = c_a c_b (pi/p)^(3/2) exp(-a b R^2 / p) over the 6 x 6 STO-6G primitive
+// products of a shell pair (R = B - A; Gaussian product centre A + (b/p) R),
+// the entries of overlap_block (orbital i of A, j of B; 0 = s, 1..3 = x, y, z)
+// are
+//   S[s][s] = sum_ss K                S[u][s] = R_u sum_ps K b/p
+//   S[s][w] = -R_w sum_sp K a/p       S[u][w] = -R_u R_w sum_pp K a b/p^2 + [u = w] sum_pp K / (2p)
+// so that every primitive product costs one exponential, shared by the
+// entries of its shell pair.
+struct OverlapSums {
+  double ss, sp, ps, pp, pp0;
+};
+
+// Adds primitive product (ii, jj) of shell pair `shell` (0 ss, 1 s on A / p on
+// B, 2 p on A / s on B, 3 pp) to o; R2 = |R|^2.
+__device__ __forceinline__ void overlap_accumulate(const ElemDev& A, const ElemDev& B, int shell, int ii, int jj,
+                                                   double R2, OverlapSums& o) {
+  const double pi = 3.14159265358979323846;
+  const bool la = shell >= 2, lb = (shell & 1) != 0;
+  const double a = la ? A.p_exp[ii] : A.s_exp[ii], ca = la ? A.p_coef[ii] : A.s_coef[ii];
+  const double b = lb ? B.p_exp[jj] : B.s_exp[jj], cb = lb ? B.p_coef[jj] : B.s_coef[jj];
+  const double ip = 1.0 / (a + b);
+  const double s00 = sqrt(pi * ip);
+  const double K = (s00 * s00 * s00) * ((ca * cb) * exp((-a * b * ip) * R2));
+  switch (shell) {
+    case 0: o.ss += K; break;
+    case 1: o.sp += K * (a * ip); break;
+    case 2: o.ps += K * (b * ip); break;
+    default:
+      o.pp += K * (a * b * ip * ip);
+      o.pp0 += K * (0.5 * ip);
+      break;
+  }
+}
+
+__device__ __forceinline__ double overlap_from_sums(const OverlapSums& o, const double R[3], int i, int j) {
+  if (i == 0 && j == 0) return o.ss;
+  if (j == 0) return R[i - 1] * o.ps;
+  if (i == 0) return -R[j - 1] * o.sp;
+  return -R[i - 1] * R[j - 1] * o.pp + (i == j ? o.pp0 : 0.0);
+}
+
+// Pairs with at least one s-only atom, one thread each.  Their local blocks
+// are sigma columns or rows (or the single (ss|ss)), so the global values
+// follow from a few local entries and the frame rotation in closed form
+// (sigma_entry), with no 10 x 10 intermediates.  s/p-s/p pairs cost two
+// orders of magnitude more and sit in the same rows of the pair table (heavy
+// atoms first): they go to k_pair_values_heavy, so that no warp waits on one
+// of them while its other lanes idle.
 __global__ void __launch_bounds__(128) k_pair_values(const PairDev* __restrict__ pairs, int npairs,
                                                       const AtomDev* __restrict__ atoms,
                                                       const ElemDev* __restrict__ elems,
@@ -72,23 +147,238 @@ __global__ void __launch_bounds__(128) k_pair_values(const PairDev* __restrict__
   const ElemDev& A = elems[a.slot];
   const ElemDev& B = elems[b.slot];
   if (A.nao == 4 && B.nao == 4) return;
-  pair_values_one(p, pr, a, b, A, B, diat, method, ints, vcore, ovl, erep);
+  const LocalTermTable& tab = c_local_terms;
+  const double X = b.x - a.x, Y = b.y - a.y, Z = b.z - a.z;
+  double rot[4][4], R;
+  frame_rotation<double>(X, Y, Z, rot, R);
+  // two-centre block (dA x dB with dA, dB in {1, 10})
+  double* out = ints + pr.int_off;
+  if (A.nao == 1 && B.nao == 1) {
+    out[0] = local_value(tab, kColSS, R, A, B, false, 0.0);
+  } else if (A.nao == 4) {
+    const double ss = local_value(tab, kColSS, R, A, B, false, 0.0), sz = local_value(tab, kColSZ, R, A, B, false, 0.0);
+    const double xx = local_value(tab, kColXX, R, A, B, false, 0.0), zz = local_value(tab, kColZZ, R, A, B, false, 0.0);
+    for (int g = 0; g < 10; ++g) out[g] = sigma_entry(rot, g, ss, sz, xx, zz);
+  } else {
+    const double ss = local_value(tab, kRowSS, R, A, B, false, 0.0), sz = local_value(tab, kRowSZ, R, A, B, false, 0.0);
+    const double xx = local_value(tab, kRowXX, R, A, B, false, 0.0), zz = local_value(tab, kRowZZ, R, A, B, false, 0.0);
+    for (int g = 0; g < 10; ++g) out[g] = sigma_entry(rot, g, ss, sz, xx, zz);
+  }
+  // core attraction: A's orbitals against B's core, B's against A's, both in
+  // the frame of A -> B (reversing the axis negates the frame's z column,
+  // which enters the sigma entries through L_sz alone)
+  double* vc = vcore + (size_t)p * 20;
+  if (A.nao == 4) {
+    const double ss = local_value(tab, kColSS, R, A, B, true, B.pcore), sz = local_value(tab, kColSZ, R, A, B, true, B.pcore);
+    const double xx = local_value(tab, kColXX, R, A, B, true, B.pcore), zz = local_value(tab, kColZZ, R, A, B, true, B.pcore);
+    for (int g = 0; g < 10; ++g) vc[g] = (-B.core) * sigma_entry(rot, g, ss, sz, xx, zz);
+  } else {
+    vc[0] = (-B.core) * local_value(tab, kColSS, R, A, B, true, B.pcore);
+    for (int g = 1; g < 10; ++g) vc[g] = 0.0;
+  }
+  if (B.nao == 4) {
+    const double ss = local_value(tab, kColSS, R, B, A, true, A.pcore), sz = local_value(tab, kColSZ, R, B, A, true, A.pcore);
+    const double xx = local_value(tab, kColXX, R, B, A, true, A.pcore), zz = local_value(tab, kColZZ, R, B, A, true, A.pcore);
+    for (int g = 0; g < 10; ++g) vc[10 + g] = (-A.core) * sigma_entry(rot, g, ss, -sz, xx, zz);
+  } else {
+    vc[10] = (-A.core) * local_value(tab, kColSS, R, B, A, true, A.pcore);
+    for (int g = 1; g < 10; ++g) vc[10 + g] = 0.0;
+  }
+  // overlap block (the entries outside the atoms' orbitals are zero); the
+  // shell pairs present: ss, and sp or ps when one atom has p functions
+  const double Rv[3] = {X, Y, Z};
+  OverlapSums o = {0.0, 0.0, 0.0, 0.0, 0.0};
+  const double R2v = X * X + Y * Y + Z * Z;
+  const int shell2 = B.nao == 4 ? 1 : (A.nao == 4 ? 2 : -1);
+  for (int k = 0; k < 36; ++k) overlap_accumulate(A, B, 0, k / 6, k % 6, R2v, o);
+  if (shell2 > 0)
+    for (int k = 0; k < 36; ++k) overlap_accumulate(A, B, shell2, k / 6, k % 6, R2v, o);
+  double* so = ovl + (size_t)p * 16;
+  for (int i = 0; i < 4; ++i)
+    for (int j = 0; j < 4; ++j) so[i * 4 + j] = (i < A.nao && j < B.nao) ? overlap_from_sums(o, Rv, i, j) : 0.0;
+  double E, dE;
+  core_repulsion(method, A, B, diat[a.slot * kMaxElementSlots + b.slot], R, E, dE);
+  erep[p] = E;
 }
 
-// The s/p-s/p pairs (the heavy-pair list), one thread each.
-__global__ void __launch_bounds__(128) k_pair_values_heavy(const int* __restrict__ hh, int nhh,
-                                                            const PairDev* __restrict__ pairs,
-                                                            const AtomDev* __restrict__ atoms,
-                                                            const ElemDev* __restrict__ elems,
-                                                            const DiatomicDev* __restrict__ diat, int method,
-                                                            double* __restrict__ ints, double* __restrict__ vcore,
-                                                            double* __restrict__ ovl, double* __restrict__ erep) {
-  const int h = blockIdx.x * blockDim.x + threadIdx.x;
-  if (h >= nhh) return;
-  const int p = hh[h];
-  const PairDev pr = pairs[p];
-  const AtomDev a = atoms[pr.a], b = atoms[pr.b];
-  pair_values_one(p, pr, a, b, elems[a.slot], elems[b.slot], diat, method, ints, vcore, ovl, erep);
+// One point-charge term of a local entry (local_value's summand).
+__device__ __forceinline__ double term_value(const LocalTerm& T, double R, const ElemDev& A, const ElemDev& B,
+                                             bool coreB, double rhoCoreB) {
+  const double rA = A.rho[T.c1];
+  const double rB = coreB ? rhoCoreB : B.rho[T.c2];
+  const double D1 = A.D[T.c1];
+  const double d2 = coreB ? 0.0 : B.D[T.c2];
+  const double dx = d2 * T.x2 - D1 * T.x1;
+  const double dy = d2 * T.y2 - D1 * T.y1;
+  const double dz = R + d2 * T.z2 - D1 * T.z1;
+  const double rr = rA + rB;
+  return T.q * rsqrt(dx * dx + dy * dy + dz * dz + rr * rr);
+}
+
+__device__ __forceinline__ double warp_total(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Symmetry copies of the local 10 x 10 block (Local2c2eMatrix.cpp:91-149) as
+// flat (destination, source) indices; every source is an evaluated entry.
+__device__ const unsigned char kLocalCopies[12][2] = {{5, 2},  {50, 20}, {33, 11}, {38, 17}, {52, 25}, {55, 22},
+                                                      {56, 26}, {59, 29}, {65, 62}, {83, 71}, {88, 77}, {95, 92}};
+
+// The s/p-s/p pairs (the heavy-pair list), a warp per group of 32 pairs.
+// First thread per pair: the frame rotation, distance and core repulsion of
+// the lane's pair, staged in shared memory.  Then pair by pair the warp
+// shares the work:
+//   - the point-charge terms of the 21 evaluated local integrals and of the
+//     two core-attraction sigma columns, one term per lane (coalesced reads
+//     of g_local_terms), summed per entry from shared memory;
+//   - the 4 x 36 primitive products of the overlap block, one exponential
+//     each, reduced over the warp into the five OverlapSums;
+//   - the symmetry copies of the local block and its rotation G = W L W^T
+//     with the pair rotation W of the common frame (global_block), one
+//     output entry per lane step.
+// The core attraction of B's orbitals is taken in A's frame: reversing the
+// pair axis negates only the frame's z column, which enters the sigma
+// entries through L_sz alone.
+constexpr int kValWarps = 4;
+constexpr int kValGroup = 32;
+struct HeavyValShared {
+  double frame[kValGroup][13];  // 3 x 3 p block of the frame rotation (row-major), R, and B - A
+  int pair[kValGroup], sa[kValGroup], sb[kValGroup], ioff[kValGroup];
+  double v[kPairTermSlots];  // term values, then the product L W^T
+  double L[100], W[100];
+};
+
+__global__ void __launch_bounds__(kValWarps * 32) k_pair_values_heavy(
+    const int* __restrict__ hh, int nhh, const PairDev* __restrict__ pairs, const AtomDev* __restrict__ atoms,
+    const ElemDev* __restrict__ elems, const DiatomicDev* __restrict__ diat, int method, double* __restrict__ ints,
+    double* __restrict__ vcore, double* __restrict__ ovl, double* __restrict__ erep) {
+  __shared__ HeavyValShared shm[kValWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g0 = (blockIdx.x * kValWarps + warp) * kValGroup;
+  if (g0 >= nhh) return;  // uniform per warp
+  HeavyValShared& s = shm[warp];
+  const int ng = min(kValGroup, nhh - g0);
+  if (lane < ng) {
+    const int p = hh[g0 + lane];
+    const PairDev pr = pairs[p];
+    const AtomDev a = atoms[pr.a], b = atoms[pr.b];
+    const double X = b.x - a.x, Y = b.y - a.y, Z = b.z - a.z;
+    double rot[4][4], R;
+    frame_rotation<double>(X, Y, Z, rot, R);
+    double* f = s.frame[lane];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) f[i * 3 + j] = rot[1 + i][1 + j];
+    f[9] = R;
+    f[10] = X;
+    f[11] = Y;
+    f[12] = Z;
+    s.pair[lane] = p;
+    s.sa[lane] = a.slot;
+    s.sb[lane] = b.slot;
+    s.ioff[lane] = pr.int_off;
+    double E, dE;
+    core_repulsion(method, elems[a.slot], elems[b.slot], diat[a.slot * kMaxElementSlots + b.slot], R, E, dE);
+    erep[p] = E;
+  }
+  __syncwarp();
+  const LocalTermTable& tab = g_local_terms;
+  const int nT = tab.n_terms;
+  // core-attraction terms per side: the sigma column's ss, sz, xx, zz entries in turn
+  const int c0 = tab.count[kColSS], c1 = c0 + tab.count[kColSZ], c2 = c1 + tab.count[kColXX];
+  const int nc = c2 + tab.count[kColZZ];
+  const int njobs = nT + 2 * nc;
+  for (int i = 0; i < ng; ++i) {
+    const ElemDev& A = elems[s.sa[i]];
+    const ElemDev& B = elems[s.sb[i]];
+    const double* f = s.frame[i];
+    double rot[4][4];
+    rot[0][0] = 1.0;
+    for (int k = 1; k < 4; ++k) rot[0][k] = rot[k][0] = 0.0;
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 3; ++c) rot[1 + r][1 + c] = f[r * 3 + c];
+    const double R = f[9];
+    const double Rv[3] = {f[10], f[11], f[12]};
+    for (int k = lane; k < 100; k += 32) {
+      s.L[k] = 0.0;
+      s.W[k] = pair_rotation_entry(rot, k / 10, k % 10);
+    }
+    for (int j = lane; j < njobs; j += 32) {
+      double v;
+      if (j < nT) {
+        v = term_value(tab.term[j], R, A, B, false, 0.0);
+      } else {
+        const int side = j - nT >= nc, k = j - nT - side * nc;
+        const int t = k < c0   ? tab.start[kColSS] + k
+                      : k < c1 ? tab.start[kColSZ] + (k - c0)
+                      : k < c2 ? tab.start[kColXX] + (k - c1)
+                               : tab.start[kColZZ] + (k - c2);
+        v = side ? term_value(tab.term[t], R, B, A, true, A.pcore) : term_value(tab.term[t], R, A, B, true, B.pcore);
+      }
+      s.v[j] = v;
+    }
+    OverlapSums o = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const double R2 = Rv[0] * Rv[0] + Rv[1] * Rv[1] + Rv[2] * Rv[2];
+    for (int k = lane; k < 144; k += 32) overlap_accumulate(A, B, k / 36, (k % 36) / 6, k % 6, R2, o);
+    o.ss = warp_total(o.ss);
+    o.sp = warp_total(o.sp);
+    o.ps = warp_total(o.ps);
+    o.pp = warp_total(o.pp);
+    o.pp0 = warp_total(o.pp0);
+    __syncwarp();
+    // entry sums: lanes 0-20 the evaluated local integrals, lanes 21-28 the
+    // core sigma entries (ss, sz, xx, zz of side 0, then of side 1)
+    double lcv = 0.0;
+    if (lane < kLocalUnique) {
+      const int t0 = tab.start[lane], t1 = t0 + tab.count[lane];
+      double acc = 0.0;
+      for (int t = t0; t < t1; ++t) acc += s.v[t];
+      s.L[tab.row[lane] * 10 + tab.col[lane]] = acc;
+    } else if (lane < kLocalUnique + 8) {
+      const int q = lane - kLocalUnique, e = q & 3;
+      const int lo = e == 0 ? 0 : (e == 1 ? c0 : (e == 2 ? c1 : c2));
+      const int hi = e == 0 ? c0 : (e == 1 ? c1 : (e == 2 ? c2 : nc));
+      const double* vs = s.v + nT + (q >> 2) * nc;
+      for (int k = lo; k < hi; ++k) lcv += vs[k];
+    }
+    double lc[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) lc[q] = __shfl_sync(0xffffffffu, lcv, kLocalUnique + q);
+    __syncwarp();
+    if (lane < 12) {
+      s.L[kLocalCopies[lane][0]] = s.L[kLocalCopies[lane][1]];
+    } else if (lane == 12) {
+      s.L[44] = 0.5 * (s.L[22] - s.L[25]);
+    }
+    __syncwarp();
+    // T = L W^T (in the term slots), then G = W T
+    double* T = s.v;
+    for (int k = lane; k < 100; k += 32) {
+      const int r = k / 10, c = k % 10;
+      double t = 0.0;
+#pragma unroll
+      for (int q = 0; q < 10; ++q) t = fma(s.L[r * 10 + q], s.W[c * 10 + q], t);
+      T[k] = t;
+    }
+    __syncwarp();
+    double* out = ints + s.ioff[i];
+    for (int k = lane; k < 100; k += 32) {
+      const int r = k / 10, c = k % 10;
+      double g = 0.0;
+#pragma unroll
+      for (int q = 0; q < 10; ++q) g = fma(s.W[r * 10 + q], T[q * 10 + c], g);
+      out[k] = g;
+    }
+    const int p = s.pair[i];
+    if (lane < 10) {
+      vcore[(size_t)p * 20 + lane] = (-B.core) * sigma_entry(rot, lane, lc[0], lc[1], lc[2], lc[3]);
+    } else if (lane < 20) {
+      vcore[(size_t)p * 20 + lane] = (-A.core) * sigma_entry(rot, lane - 10, lc[4], -lc[5], lc[6], lc[7]);
+    }
+    if (lane < 16) ovl[(size_t)p * 16 + lane] = overlap_from_sums(o, Rv, lane >> 2, lane & 3);
+    __syncwarp();
+  }
 }
 
 // Pair gradient, reverse mode (see nddo_grad.cuh), for pairs with at least
@@ -461,9 +751,8 @@ void launch_pair_values(const DeviceBatch& b, cudaStream_t s) {
   k_pair_values<<<(b.npairs + th - 1) / th, th, 0, s>>>(b.pairs, b.npairs, b.atoms, b.elems, b.diat, b.method,
                                                          b.ints, b.vcore, b.ovl, b.erep);
   if (b.nhh_total > 0)
-    k_pair_values_heavy<<<(b.nhh_total + th - 1) / th, th, 0, s>>>(b.hh_pairs, b.nhh_total, b.pairs, b.atoms,
-                                                                   b.elems, b.diat, b.method, b.ints, b.vcore,
-                                                                   b.ovl, b.erep);
+    k_pair_values_heavy<<<(b.nhh_total + kValWarps * kValGroup - 1) / (kValWarps * kValGroup), kValWarps * 32, 0, s>>>(
+        b.hh_pairs, b.nhh_total, b.pairs, b.atoms, b.elems, b.diat, b.method, b.ints, b.vcore, b.ovl, b.erep);
 }
 
 void launch_gradient(const DeviceBatch& b, cudaStream_t s) {

@@ -305,12 +305,14 @@ cublasHandle_t blas_handle(std::string& err) {
 
 // Pulay DIIS coefficients from the B matrix (row-major kDiisMax stride) of n
 // vectors: the same scaled, pivoted elimination as the batched kernel.
-// Returns false when the system is singular.
+// Returns false when the system is singular or the error vectors are rounding
+// noise.
 bool diis_solve(const double* bm, int n, double* coef) {
   const int ld = n + 2;
   std::vector<double> sys((size_t)(n + 1) * ld);
   double scale = 0;
   for (int i = 0; i < n; ++i) scale = std::max(scale, std::fabs(bm[i * kDiisMax + i]));
+  if (!(scale > kDiisNoiseNorm)) return false;
   scale = scale > 0 ? 1.0 / scale : 1.0;
   for (int i = 0; i <= n; ++i) {
     for (int j = 0; j <= n; ++j)

@@ -109,6 +109,17 @@ void build_local_term_table(LocalTermTable& tab) {
     tab.count[e] = nt - tab.start[e];
   }
   tab.n_terms = nt;
+  // sigma column (p | ss) entries 0, 4, 5, 6 and row (ss | p) entries 0, 1, 2, 3
+  // for p = ss, xx, sz, zz
+  static const int kCol[4] = {0, 4, 5, 6}, kRow[4] = {0, 1, 2, 3}, kSig[4] = {0, 2, 6, 9};
+  for (int k = 0; k < 4; ++k)
+    if (tab.row[kCol[k]] != kSig[k] || tab.col[kCol[k]] != 0 || tab.row[kRow[k]] != 0 || tab.col[kRow[k]] != kSig[k])
+      throw std::runtime_error("local term table: unexpected sigma entry order");
+  // the heavy-pair value kernel stages every two-electron term and both
+  // core-attraction sigma columns' terms of one pair in kPairTermSlots slots
+  int ncore = 0;
+  for (int k = 0; k < 4; ++k) ncore += tab.count[kCol[k]];
+  if (nt + 2 * ncore > kPairTermSlots) throw std::runtime_error("local term table: more terms than pair slots");
 }
 
 }  // namespace sgb

@@ -79,6 +79,10 @@ struct LocalTerm {
 
 constexpr int kLocalUnique = 21;
 constexpr int kLocalMaxTerms = 512;
+// Term slots of one pair in the heavy-pair value kernel: every two-electron
+// term plus the terms of both core-attraction sigma columns (checked when the
+// table is built).
+constexpr int kPairTermSlots = 256;
 
 struct LocalTermTable {
   int row[kLocalUnique], col[kLocalUnique];  // orbital-pair indices of the evaluated entries

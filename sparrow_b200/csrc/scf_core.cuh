@@ -532,7 +532,8 @@ __device__ __forceinline__ void diis_store(int N, const double* F, const double*
 
 // CTA reduction of the dot products into row and column `slot` of the B
 // matrix, then the solve for the coefficients (sh.coef).  False when there is
-// nothing to extrapolate (fewer than two entries, or a singular system).
+// nothing to extrapolate (fewer than two entries, error vectors at rounding
+// level, or a singular system).
 __device__ __forceinline__ bool diis_solve(int slot, int nhist, double (&d)[kDiisMax], ScfShared& sh) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
   double* part = sh.gemm;  // idle GEMM scratch
@@ -554,6 +555,7 @@ __device__ __forceinline__ bool diis_solve(int slot, int nhist, double (&d)[kDii
     const int n = nhist, ld = n + 2;
     double scale = 0;
     for (int i = 0; i < n; ++i) scale = fmax(scale, fabs(sh.bmat[i * kDiisMax + i]));
+    int ok = scale > kDiisNoiseNorm ? 1 : 0;
     scale = scale > 0 ? 1.0 / scale : 1.0;
     for (int i = 0; i <= n; ++i)
       for (int j = 0; j <= n; ++j) {
@@ -564,7 +566,6 @@ __device__ __forceinline__ bool diis_solve(int slot, int nhist, double (&d)[kDii
         sh.sys[i * ld + j] = v;
       }
     for (int i = 0; i <= n; ++i) sh.sys[i * ld + n + 1] = (i == n) ? -1.0 : 0.0;
-    int ok = 1;
     for (int c = 0; c <= n && ok; ++c) {
       int piv = c;
       for (int r = c + 1; r <= n; ++r)
