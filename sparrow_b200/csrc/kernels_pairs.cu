@@ -99,25 +99,66 @@ struct OverlapSums {
 };
 
 // Adds primitive product (ii, jj) of shell pair `shell` (0 ss, 1 s on A / p on
-// B, 2 p on A / s on B, 3 pp) to o; R2 = |R|^2.
+// B, 2 p on A / s on B, 3 pp) to o; R2 = |R|^2.  kMu: also to m, weighted by
+// mu = a b / p (for the gradient, see overlap_gradient).
+template <bool kMu>
 __device__ __forceinline__ void overlap_accumulate(const ElemDev& A, const ElemDev& B, int shell, int ii, int jj,
-                                                   double R2, OverlapSums& o) {
+                                                   double R2, OverlapSums& o, OverlapSums* m = nullptr) {
   const double pi = 3.14159265358979323846;
   const bool la = shell >= 2, lb = (shell & 1) != 0;
   const double a = la ? A.p_exp[ii] : A.s_exp[ii], ca = la ? A.p_coef[ii] : A.s_coef[ii];
   const double b = lb ? B.p_exp[jj] : B.s_exp[jj], cb = lb ? B.p_coef[jj] : B.s_coef[jj];
   const double ip = 1.0 / (a + b);
+  const double mu = a * b * ip;
   const double s00 = sqrt(pi * ip);
-  const double K = (s00 * s00 * s00) * ((ca * cb) * exp((-a * b * ip) * R2));
+  const double K = (s00 * s00 * s00) * ((ca * cb) * exp(-mu * R2));
   switch (shell) {
-    case 0: o.ss += K; break;
-    case 1: o.sp += K * (a * ip); break;
-    case 2: o.ps += K * (b * ip); break;
-    default:
-      o.pp += K * (a * b * ip * ip);
-      o.pp0 += K * (0.5 * ip);
+    case 0:
+      o.ss += K;
+      if (kMu) m->ss += mu * K;
       break;
+    case 1: {
+      const double w = K * (a * ip);
+      o.sp += w;
+      if (kMu) m->sp += mu * w;
+      break;
+    }
+    case 2: {
+      const double w = K * (b * ip);
+      o.ps += w;
+      if (kMu) m->ps += mu * w;
+      break;
+    }
+    default: {
+      const double w = K * (mu * ip), w0 = K * (0.5 * ip);
+      o.pp += w;
+      o.pp0 += w0;
+      if (kMu) {
+        m->pp += mu * w;
+        m->pp0 += mu * w0;
+      }
+      break;
+    }
   }
+}
+
+// Gradient with respect to R = B - A of the overlap energy sum_ij f[i][j]
+// S[i][j] (f zero outside the atoms' orbitals) from the sums o and their
+// mu-weighted copies m: every sum X = sum K w has dX/dR = -2 R sum mu K w.
+__device__ __forceinline__ void overlap_gradient(const OverlapSums& o, const OverlapSums& m, const double f[4][4],
+                                                 const double R[3], double g[3]) {
+  double a = 0.0, b = 0.0, c = 0.0, t = 0.0, fR[3], Rf[3];
+  for (int u = 0; u < 3; ++u) {
+    a += f[1 + u][0] * R[u];
+    b += f[0][1 + u] * R[u];
+    t += f[1 + u][1 + u];
+    fR[u] = f[1 + u][1] * R[0] + f[1 + u][2] * R[1] + f[1 + u][3] * R[2];
+    Rf[u] = f[1][1 + u] * R[0] + f[2][1 + u] * R[1] + f[3][1 + u] * R[2];
+  }
+  for (int u = 0; u < 3; ++u) c += R[u] * fR[u];
+  const double radial = -2.0 * (f[0][0] * m.ss + a * m.ps - b * m.sp - c * m.pp + t * m.pp0);
+  for (int d = 0; d < 3; ++d)
+    g[d] += radial * R[d] + f[1 + d][0] * o.ps - f[0][1 + d] * o.sp - (fR[d] + Rf[d]) * o.pp;
 }
 
 __device__ __forceinline__ double overlap_from_sums(const OverlapSums& o, const double R[3], int i, int j) {
@@ -190,9 +231,9 @@ __global__ void __launch_bounds__(128) k_pair_values(const PairDev* __restrict__
   OverlapSums o = {0.0, 0.0, 0.0, 0.0, 0.0};
   const double R2v = X * X + Y * Y + Z * Z;
   const int shell2 = B.nao == 4 ? 1 : (A.nao == 4 ? 2 : -1);
-  for (int k = 0; k < 36; ++k) overlap_accumulate(A, B, 0, k / 6, k % 6, R2v, o);
+  for (int k = 0; k < 36; ++k) overlap_accumulate<false>(A, B, 0, k / 6, k % 6, R2v, o);
   if (shell2 > 0)
-    for (int k = 0; k < 36; ++k) overlap_accumulate(A, B, shell2, k / 6, k % 6, R2v, o);
+    for (int k = 0; k < 36; ++k) overlap_accumulate<false>(A, B, shell2, k / 6, k % 6, R2v, o);
   double* so = ovl + (size_t)p * 16;
   for (int i = 0; i < 4; ++i)
     for (int j = 0; j < 4; ++j) so[i * 4 + j] = (i < A.nao && j < B.nao) ? overlap_from_sums(o, Rv, i, j) : 0.0;
@@ -320,7 +361,7 @@ __global__ void __launch_bounds__(kValWarps * 32) k_pair_values_heavy(
     }
     OverlapSums o = {0.0, 0.0, 0.0, 0.0, 0.0};
     const double R2 = Rv[0] * Rv[0] + Rv[1] * Rv[1] + Rv[2] * Rv[2];
-    for (int k = lane; k < 144; k += 32) overlap_accumulate(A, B, k / 36, (k % 36) / 6, k % 6, R2, o);
+    for (int k = lane; k < 144; k += 32) overlap_accumulate<false>(A, B, k / 36, (k % 36) / 6, k % 6, R2, o);
     o.ss = warp_total(o.ss);
     o.sp = warp_total(o.sp);
     o.ps = warp_total(o.ps);
@@ -484,11 +525,15 @@ __global__ void __launch_bounds__(128) k_pair_gradient_light(const PairDev* __re
     for (int i = 0; i < nA; ++i)
       for (int j = 0; j < nB; ++j)
         f[i][j] = ((i == 0 ? A.betaS : A.betaP) + (j == 0 ? B.betaS : B.betaP)) * PAB[i][j];
+    // shell pairs ss, and sp or ps when one atom has p functions
     const double Rv[3] = {X, Y, Z};
-    for (int la = 0; la < (nA == 4 ? 2 : 1); ++la)
-      for (int lb = 0; lb < (nB == 4 ? 2 : 1); ++lb)
-        for (int i = 0; i < 6; ++i)
-          for (int j = 0; j < 6; ++j) overlap_primitive_grad(A, B, Rv, la, lb, i, j, f, g);
+    const double R2v = X * X + Y * Y + Z * Z;
+    OverlapSums o = {0.0, 0.0, 0.0, 0.0, 0.0}, mo = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const int shell2 = nB == 4 ? 1 : (nA == 4 ? 2 : -1);
+    for (int k = 0; k < 36; ++k) overlap_accumulate<true>(A, B, 0, k / 6, k % 6, R2v, o, &mo);
+    if (shell2 > 0)
+      for (int k = 0; k < 36; ++k) overlap_accumulate<true>(A, B, shell2, k / 6, k % 6, R2v, o, &mo);
+    overlap_gradient(o, mo, f, Rv, g);
   }
   // core repulsion
   {
@@ -508,14 +553,40 @@ __global__ void __launch_bounds__(128) k_pair_gradient_light(const PairDev* __re
   gpair[(size_t)p * 3 + 2] = g[2];
 }
 
-// Pair gradient, reverse mode, for pairs of two s/p atoms: one warp per pair
-// with the 10 x 10 blocks in shared memory.  Lanes split the 21 unique local
-// integrals, the 100-entry matrices and products, the rotation adjoints and
-// the 144 primitive pairs of the overlap; each lane's partial gradient is
-// summed across the warp at the end.
+// Value and d/dR of one point-charge term (local_entry's summand).
+__device__ __forceinline__ void term_value_grad(const LocalTerm& T, double R, const ElemDev& A, const ElemDev& B,
+                                                bool coreB, double rhoCoreB, double& v, double& dv) {
+  const double rA = A.rho[T.c1];
+  const double rB = coreB ? rhoCoreB : B.rho[T.c2];
+  const double D1 = A.D[T.c1];
+  const double d2 = coreB ? 0.0 : B.D[T.c2];
+  const double dx = d2 * T.x2 - D1 * T.x1;
+  const double dy = d2 * T.y2 - D1 * T.y1;
+  const double dz = R + d2 * T.z2 - D1 * T.z1;
+  const double rr = rA + rB;
+  const double inv = 1.0 / sqrt(dx * dx + dy * dy + dz * dz + rr * rr);
+  v = T.q * inv;
+  dv = -dz * T.q * inv * inv * inv;
+}
+
+// Pair gradient, reverse mode, for pairs of two s/p atoms: a warp per group
+// of 32 pairs.  First thread per pair: the core-repulsion derivative of the
+// lane's pair, staged in shared memory.  Then pair by pair the warp shares
+// the work with the 10 x 10 blocks in shared memory:
+//   - the point-charge terms (value and d/dR) of the 21 evaluated local
+//     integrals and of the two core-attraction sigma columns, one term per
+//     lane (coalesced reads of g_local_terms), summed per entry;
+//   - the 4 x 36 primitive products of the overlap block, one exponential
+//     each, reduced over the warp into the sums of overlap_gradient;
+//   - both frame rotations with their derivatives (lanes 30 and 31 in one
+//     pass), the 100-entry matrices and products and the rotation adjoints;
+// each lane's partial gradient is summed across the warp at the end.
 constexpr int kGradWarps = 4;
+constexpr int kGradGroup = 32;
 struct HeavyGradShared {
-  double L[100], dL[100], W[100], F[100], T1[100], T2[100];
+  double dErep[kGradGroup];
+  double v[kPairTermSlots], dv[kPairTermSlots];  // term values and derivatives, then T1 = F W, T2 = F^T W
+  double L[100], dL[100], W[100], F[100];
   double Lc[10], dLc[10], Lcb[10], dLcb[10];
   double PA[4][4], PB[4][4], PAB[4][4], SAB[4][4];
   RotGrad ra, rb;
@@ -528,127 +599,191 @@ __global__ void __launch_bounds__(kGradWarps * 32) k_pair_gradient_heavy(
     double* __restrict__ gpair) {
   __shared__ HeavyGradShared shm[kGradWarps];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int w = blockIdx.x * kGradWarps + warp;
-  if (w >= nhh) return;  // uniform per warp
+  const int g0 = (blockIdx.x * kGradWarps + warp) * kGradGroup;
+  if (g0 >= nhh) return;  // uniform per warp
   HeavyGradShared& s = shm[warp];
-  const int p = hh[w];
-  const PairDev pr = pairs[p];
-  const AtomDev a = atoms[pr.a], b = atoms[pr.b];
-  const ElemDev& A = elems[a.slot];
-  const ElemDev& B = elems[b.slot];
-  const MolDev m = mols[pr.mol];
-  const int N = m.nao;
-  const double* P = Pall + m.mat_off;
-  const double X = b.x - a.x, Y = b.y - a.y, Z = b.z - a.z;
-  const double R = sqrt(X * X + Y * Y + Z * Z);
-  const LocalTermTable& tab = c_local_terms;
-  if (lane < 16) {
-    const int i = lane >> 2, j = lane & 3;
-    s.PA[i][j] = P[(size_t)(a.ao0 + i) * N + a.ao0 + j];
-    s.PB[i][j] = P[(size_t)(b.ao0 + i) * N + b.ao0 + j];
-    s.PAB[i][j] = P[(size_t)(a.ao0 + i) * N + b.ao0 + j];
-    const size_t ij = m.mat_off + (size_t)(a.ao0 + i) * N + b.ao0 + j;
-    s.SAB[i][j] = Paall ? Paall[ij] - Pball[ij] : 0.0;
-  }
-  if (lane == 30) rotation_grad(Dual3(X, 1, 0, 0), Dual3(Y, 0, 1, 0), Dual3(Z, 0, 0, 1), s.ra);
-  if (lane == 31) rotation_grad(Dual3(-X, -1, 0, 0), Dual3(-Y, 0, -1, 0), Dual3(-Z, 0, 0, -1), s.rb);
-  for (int k = lane; k < 100; k += 32) s.L[k] = s.dL[k] = 0.0;
-  if (lane < 10) s.Lc[lane] = s.dLc[lane] = s.Lcb[lane] = s.dLcb[lane] = 0.0;
-  __syncwarp();
-  if (lane < kLocalUnique) {
-    const int r = tab.row[lane], c = tab.col[lane];
-    double v, d;
-    local_entry(tab, lane, R, A, B, false, 0.0, v, d);
-    s.L[r * 10 + c] = v;
-    s.dL[r * 10 + c] = d;
-    if (c == 0) {
-      local_entry(tab, lane, R, A, B, true, B.pcore, v, d);
-      s.Lc[r] = v;
-      s.dLc[r] = d;
-      local_entry(tab, lane, R, B, A, true, A.pcore, v, d);
-      s.Lcb[r] = v;
-      s.dLcb[r] = d;
-    }
-  }
-  __syncwarp();
-  if (lane == 0) {
-    local_copies(10, 10, reinterpret_cast<double(*)[10]>(s.L), reinterpret_cast<double(*)[10]>(s.dL));
-    s.Lc[5] = s.Lc[2];
-    s.dLc[5] = s.dLc[2];
-    s.Lcb[5] = s.Lcb[2];
-    s.dLcb[5] = s.dLcb[2];
-  }
-  for (int k = lane; k < 100; k += 32) {
-    s.W[k] = w_entry(s.ra.r, k / 10, k % 10);
-    s.F[k] = Paall ? density_factor_uhf(s.PA, s.PB, s.PAB, s.SAB, k / 10, k % 10)
-                   : density_factor(s.PA, s.PB, s.PAB, k / 10, k % 10);
-  }
-  __syncwarp();
-  // T1 = F W, T2 = F^T W
-  for (int k = lane; k < 100; k += 32) {
-    const int r = k / 10, c = k % 10;
-    double t1 = 0, t2 = 0;
-    for (int l = 0; l < 10; ++l) {
-      t1 += s.F[r * 10 + l] * s.W[l * 10 + c];
-      t2 += s.F[l * 10 + r] * s.W[l * 10 + c];
-    }
-    s.T1[k] = t1;
-    s.T2[k] = t2;
-  }
-  __syncwarp();
-  double adjA[4][4] = {}, adjB[4][4] = {};
-  double dR = 0, g[3] = {0, 0, 0};
-  // two-centre: dE/dW[p][q] = sum_j T1[p][j] L[q][j] + sum_a T2[p][a] L[a][q];
-  // dE/dL[x][y] = sum_g W[g][x] T1[g][y]
-  for (int k = lane; k < 100; k += 32) {
-    const int pp = k / 10, qq = k % 10;
-    double adw = 0;
-    for (int j = 0; j < 10; ++j) adw += s.T1[pp * 10 + j] * s.L[qq * 10 + j] + s.T2[pp * 10 + j] * s.L[j * 10 + qq];
-    if (adw != 0.0) w_adjoint(s.ra.r, pp, qq, adw, adjA);
-    if (s.dL[k] != 0.0) {
-      double mm = 0;
-      for (int g2 = 0; g2 < 10; ++g2) mm += s.W[g2 * 10 + pp] * s.T1[g2 * 10 + qq];
-      dR += s.dL[k] * mm;
-    }
-  }
-  // core attraction (both sides), 10 orbital pairs x 5 axis entries each
-  for (int k = lane; k < 100; k += 32) {
-    const int side = k / 50, g2 = (k % 50) / 5, q = axis_index(k % 5);
-    const double* Lv = side ? s.Lcb : s.Lc;
-    const double* dLv = side ? s.dLcb : s.dLc;
-    if (Lv[q] == 0.0 && dLv[q] == 0.0) continue;
-    const double f = -(side ? A.core : B.core) * atom_factor(side ? s.PB : s.PA, g2);
-    if (f == 0.0) continue;
-    const RotGrad& rg = side ? s.rb : s.ra;
-    w_adjoint(rg.r, g2, q, f * Lv[q], side ? adjB : adjA);
-    dR += f * w_entry(rg.r, g2, q) * dLv[q];
-  }
-  // overlap: 2 x 2 shells x 6 x 6 primitives
-  {
-    double f[4][4];
-    for (int i = 0; i < 4; ++i)
-      for (int j = 0; j < 4; ++j)
-        f[i][j] = ((i == 0 ? A.betaS : A.betaP) + (j == 0 ? B.betaS : B.betaP)) * s.PAB[i][j];
-    const double Rv[3] = {X, Y, Z};
-    for (int k = lane; k < 144; k += 32)
-      overlap_primitive_grad(A, B, Rv, k / 72, (k / 36) % 2, (k / 6) % 6, k % 6, f, g);
-  }
-  if (lane == 0) {
+  const int ng = min(kGradGroup, nhh - g0);
+  if (lane < ng) {
+    const PairDev pr = pairs[hh[g0 + lane]];
+    const AtomDev a = atoms[pr.a], b = atoms[pr.b];
+    const double X = b.x - a.x, Y = b.y - a.y, Z = b.z - a.z;
     double E, dE;
-    core_repulsion(method, A, B, diat[a.slot * kMaxElementSlots + b.slot], R, E, dE);
-    dR += dE;
+    core_repulsion(method, elems[a.slot], elems[b.slot], diat[a.slot * kMaxElementSlots + b.slot],
+                   sqrt(X * X + Y * Y + Z * Z), E, dE);
+    s.dErep[lane] = dE;
   }
-  g[0] += dR * X / R;
-  g[1] += dR * Y / R;
-  g[2] += dR * Z / R;
-  add_rotation_gradient(s.ra, adjA, g);
-  add_rotation_gradient(s.rb, adjB, g);
-  for (int k = 0; k < 3; ++k)
-    for (int o = 16; o > 0; o >>= 1) g[k] += __shfl_xor_sync(0xffffffffu, g[k], o);
-  if (lane == 0) {
-    gpair[(size_t)p * 3 + 0] = g[0];
-    gpair[(size_t)p * 3 + 1] = g[1];
-    gpair[(size_t)p * 3 + 2] = g[2];
+  const LocalTermTable& tab = g_local_terms;
+  const int nT = tab.n_terms;
+  const int c0 = tab.count[kColSS], c1 = c0 + tab.count[kColSZ], c2 = c1 + tab.count[kColXX];
+  const int nc = c2 + tab.count[kColZZ];
+  const int njobs = nT + 2 * nc;
+  for (int i = 0; i < ng; ++i) {
+    const int p = hh[g0 + i];
+    const PairDev pr = pairs[p];
+    const AtomDev a = atoms[pr.a], b = atoms[pr.b];
+    const ElemDev& A = elems[a.slot];
+    const ElemDev& B = elems[b.slot];
+    const MolDev m = mols[pr.mol];
+    const int N = m.nao;
+    const double* P = Pall + m.mat_off;
+    const double X = b.x - a.x, Y = b.y - a.y, Z = b.z - a.z;
+    const double R = sqrt(X * X + Y * Y + Z * Z);
+    __syncwarp();  // the previous pair's shared blocks are no longer read
+    if (lane < 16) {
+      const int r = lane >> 2, c = lane & 3;
+      s.PA[r][c] = P[(size_t)(a.ao0 + r) * N + a.ao0 + c];
+      s.PB[r][c] = P[(size_t)(b.ao0 + r) * N + b.ao0 + c];
+      s.PAB[r][c] = P[(size_t)(a.ao0 + r) * N + b.ao0 + c];
+      const size_t rc = m.mat_off + (size_t)(a.ao0 + r) * N + b.ao0 + c;
+      s.SAB[r][c] = Paall ? Paall[rc] - Pball[rc] : 0.0;
+    } else if (lane >= 30) {
+      // lane 31: the reversed frame (vector B -> A), differentiated with respect to B - A
+      const double sg = lane == 31 ? -1.0 : 1.0;
+      rotation_grad(Dual3(sg * X, sg, 0, 0), Dual3(sg * Y, 0, sg, 0), Dual3(sg * Z, 0, 0, sg),
+                    lane == 31 ? s.rb : s.ra);
+    }
+    for (int k = lane; k < 100; k += 32) s.L[k] = s.dL[k] = 0.0;
+    if (lane < 10) s.Lc[lane] = s.dLc[lane] = s.Lcb[lane] = s.dLcb[lane] = 0.0;
+    for (int j = lane; j < njobs; j += 32) {
+      double v, dv;
+      if (j < nT) {
+        term_value_grad(tab.term[j], R, A, B, false, 0.0, v, dv);
+      } else {
+        const int side = j - nT >= nc, k = j - nT - side * nc;
+        const int t = k < c0   ? tab.start[kColSS] + k
+                      : k < c1 ? tab.start[kColSZ] + (k - c0)
+                      : k < c2 ? tab.start[kColXX] + (k - c1)
+                               : tab.start[kColZZ] + (k - c2);
+        if (side) term_value_grad(tab.term[t], R, B, A, true, A.pcore, v, dv);
+        else term_value_grad(tab.term[t], R, A, B, true, B.pcore, v, dv);
+      }
+      s.v[j] = v;
+      s.dv[j] = dv;
+    }
+    OverlapSums o = {0.0, 0.0, 0.0, 0.0, 0.0}, mo = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const double R2 = X * X + Y * Y + Z * Z;
+    for (int k = lane; k < 144; k += 32) overlap_accumulate<true>(A, B, k / 36, (k % 36) / 6, k % 6, R2, o, &mo);
+    o.ss = warp_total(o.ss);
+    o.sp = warp_total(o.sp);
+    o.ps = warp_total(o.ps);
+    o.pp = warp_total(o.pp);
+    o.pp0 = warp_total(o.pp0);
+    mo.ss = warp_total(mo.ss);
+    mo.sp = warp_total(mo.sp);
+    mo.ps = warp_total(mo.ps);
+    mo.pp = warp_total(mo.pp);
+    mo.pp0 = warp_total(mo.pp0);
+    __syncwarp();
+    // entry sums: lanes 0-20 the evaluated local integrals, lanes 21-28 the
+    // core sigma entries (ss, sz, xx, zz of A against B's core, then of B
+    // against A's), stored by orbital-pair index
+    if (lane < kLocalUnique) {
+      const int t0 = tab.start[lane], t1 = t0 + tab.count[lane];
+      double acc = 0.0, dacc = 0.0;
+      for (int t = t0; t < t1; ++t) {
+        acc += s.v[t];
+        dacc += s.dv[t];
+      }
+      s.L[tab.row[lane] * 10 + tab.col[lane]] = acc;
+      s.dL[tab.row[lane] * 10 + tab.col[lane]] = dacc;
+    } else if (lane < kLocalUnique + 8) {
+      const int q = lane - kLocalUnique, e = q & 3, side = q >> 2;
+      const int lo = e == 0 ? 0 : (e == 1 ? c0 : (e == 2 ? c1 : c2));
+      const int hi = e == 0 ? c0 : (e == 1 ? c1 : (e == 2 ? c2 : nc));
+      const int idx = tab.row[e == 0 ? kColSS : (e == 1 ? kColSZ : (e == 2 ? kColXX : kColZZ))];
+      const double* vs = s.v + nT + side * nc;
+      const double* dvs = s.dv + nT + side * nc;
+      double acc = 0.0, dacc = 0.0;
+      for (int k = lo; k < hi; ++k) {
+        acc += vs[k];
+        dacc += dvs[k];
+      }
+      (side ? s.Lcb : s.Lc)[idx] = acc;
+      (side ? s.dLcb : s.dLc)[idx] = dacc;
+    }
+    __syncwarp();
+    // symmetry copies, all from evaluated entries; density factors and W
+    if (lane < 12) {
+      s.L[kLocalCopies[lane][0]] = s.L[kLocalCopies[lane][1]];
+      s.dL[kLocalCopies[lane][0]] = s.dL[kLocalCopies[lane][1]];
+    } else if (lane == 12) {
+      s.L[44] = 0.5 * (s.L[22] - s.L[25]);
+      s.dL[44] = 0.5 * (s.dL[22] - s.dL[25]);
+    } else if (lane == 13) {
+      s.Lc[5] = s.Lc[2];
+      s.dLc[5] = s.dLc[2];
+    } else if (lane == 14) {
+      s.Lcb[5] = s.Lcb[2];
+      s.dLcb[5] = s.dLcb[2];
+    }
+    for (int k = lane; k < 100; k += 32) {
+      s.W[k] = w_entry(s.ra.r, k / 10, k % 10);
+      s.F[k] = Paall ? density_factor_uhf(s.PA, s.PB, s.PAB, s.SAB, k / 10, k % 10)
+                     : density_factor(s.PA, s.PB, s.PAB, k / 10, k % 10);
+    }
+    __syncwarp();
+    // T1 = F W, T2 = F^T W (in the term slots)
+    double* T1 = s.v;
+    double* T2 = s.dv;
+    for (int k = lane; k < 100; k += 32) {
+      const int r = k / 10, c = k % 10;
+      double t1 = 0, t2 = 0;
+      for (int l = 0; l < 10; ++l) {
+        t1 += s.F[r * 10 + l] * s.W[l * 10 + c];
+        t2 += s.F[l * 10 + r] * s.W[l * 10 + c];
+      }
+      T1[k] = t1;
+      T2[k] = t2;
+    }
+    __syncwarp();
+    double adjA[4][4] = {}, adjB[4][4] = {};
+    double dR = 0, g[3] = {0, 0, 0};
+    // two-centre: dE/dW[p][q] = sum_j T1[p][j] L[q][j] + sum_a T2[p][a] L[a][q];
+    // dE/dL[x][y] = sum_g W[g][x] T1[g][y]
+    for (int k = lane; k < 100; k += 32) {
+      const int pp = k / 10, qq = k % 10;
+      double adw = 0;
+      for (int j = 0; j < 10; ++j) adw += T1[pp * 10 + j] * s.L[qq * 10 + j] + T2[pp * 10 + j] * s.L[j * 10 + qq];
+      if (adw != 0.0) w_adjoint(s.ra.r, pp, qq, adw, adjA);
+      if (s.dL[k] != 0.0) {
+        double mm = 0;
+        for (int g2 = 0; g2 < 10; ++g2) mm += s.W[g2 * 10 + pp] * T1[g2 * 10 + qq];
+        dR += s.dL[k] * mm;
+      }
+    }
+    // core attraction (both sides), 10 orbital pairs x 5 axis entries each
+    for (int k = lane; k < 100; k += 32) {
+      const int side = k / 50, g2 = (k % 50) / 5, q = axis_index(k % 5);
+      const double* Lv = side ? s.Lcb : s.Lc;
+      const double* dLv = side ? s.dLcb : s.dLc;
+      if (Lv[q] == 0.0 && dLv[q] == 0.0) continue;
+      const double f = -(side ? A.core : B.core) * atom_factor(side ? s.PB : s.PA, g2);
+      if (f == 0.0) continue;
+      const RotGrad& rg = side ? s.rb : s.ra;
+      w_adjoint(rg.r, g2, q, f * Lv[q], side ? adjB : adjA);
+      dR += f * w_entry(rg.r, g2, q) * dLv[q];
+    }
+    if (lane == 0) {
+      // overlap (resonance integrals) from the reduced sums, core repulsion
+      double f[4][4];
+      for (int r = 0; r < 4; ++r)
+        for (int c = 0; c < 4; ++c)
+          f[r][c] = ((r == 0 ? A.betaS : A.betaP) + (c == 0 ? B.betaS : B.betaP)) * s.PAB[r][c];
+      const double Rv[3] = {X, Y, Z};
+      overlap_gradient(o, mo, f, Rv, g);
+      dR += s.dErep[i];
+    }
+    g[0] += dR * X / R;
+    g[1] += dR * Y / R;
+    g[2] += dR * Z / R;
+    add_rotation_gradient(s.ra, adjA, g);
+    add_rotation_gradient(s.rb, adjB, g);
+    for (int k = 0; k < 3; ++k) g[k] = warp_total(g[k]);
+    if (lane == 0) {
+      gpair[(size_t)p * 3 + 0] = g[0];
+      gpair[(size_t)p * 3 + 1] = g[1];
+      gpair[(size_t)p * 3 + 2] = g[2];
+    }
   }
 }
 
@@ -763,7 +898,8 @@ void launch_gradient(const DeviceBatch& b, cudaStream_t s) {
                                                                    b.uhf ? b.Pb : nullptr, b.gpair);
   }
   if (b.nhh_total > 0) {
-    k_pair_gradient_heavy<<<(b.nhh_total + kGradWarps - 1) / kGradWarps, kGradWarps * 32, 0, s>>>(
+    k_pair_gradient_heavy<<<(b.nhh_total + kGradWarps * kGradGroup - 1) / (kGradWarps * kGradGroup), kGradWarps * 32,
+                            0, s>>>(
         b.hh_pairs, b.nhh_total, b.pairs, b.atoms, b.elems, b.diat, b.mols, b.method, b.P, b.uhf ? b.Pa : nullptr,
         b.uhf ? b.Pb : nullptr, b.gpair);
   }
