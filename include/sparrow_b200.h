@@ -265,6 +265,11 @@ int32_t sg_batch_event_elapsed(sg_batch* b, int32_t slot0, int32_t slot1, double
  * rotation, full diagonalisation and density phases (5 per molecule);
  * any pointer may be NULL */
 int32_t sg_batch_scf_stats(sg_batch* b, int32_t* full_diagonalisations, int32_t* jacobi_sweeps, int64_t* cycles5);
+/* per-molecule convergence measures of the last SCF iteration of the last
+ * run: |E_it - E_it-1| (Hartree) and rms(P_it - P_it-1), the quantities that
+ * the settings self_consistence_criterion and density_rmsd_criterion bound;
+ * either pointer may be NULL */
+int32_t sg_batch_convergence(sg_batch* b, double* last_delta_energy, double* last_rms_density_change);
 /* bytes copied host->device and device->host by this batch so far */
 int32_t sg_batch_transfer_bytes(const sg_batch* b, int64_t* h2d, int64_t* d2h);
 /* free device and pinned host memory cached from destroyed batches */

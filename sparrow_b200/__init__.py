@@ -527,6 +527,14 @@ class Batch:
                                               cyc.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
         return nf, sw, cyc.reshape(n, 5)
 
+    def convergence(self):
+        """Per molecule, of the last SCF iteration: |Delta E| (Hartree) and rms(Delta P)."""
+        n = self.n_molecules
+        de = np.zeros(n)
+        dp = np.zeros(n)
+        self._check(lib().sg_batch_convergence(self._h, _dptr(de), _dptr(dp)))
+        return de, dp
+
     def transfer_bytes(self):
         h, d = ctypes.c_int64(), ctypes.c_int64()
         self._check(lib().sg_batch_transfer_bytes(self._h, ctypes.byref(h), ctypes.byref(d)))

@@ -755,6 +755,18 @@ int32_t sg_batch_scf_stats(sg_batch* b, int32_t* nfull, int32_t* sweeps, int64_t
   return SG_OK;
 }
 
+int32_t sg_batch_convergence(sg_batch* b, double* last_delta_energy, double* last_rms_density_change) {
+  if (!b) return SG_ERR_INVALID_ARGUMENT;
+  std::vector<MolResult> r;
+  int rc = b->impl->fetch_raw_results(r, b->error);
+  if (rc) return rc;
+  for (size_t i = 0; i < r.size(); ++i) {
+    if (last_delta_energy) last_delta_energy[i] = r[i].last_dE;
+    if (last_rms_density_change) last_rms_density_change[i] = r[i].last_rmsd;
+  }
+  return SG_OK;
+}
+
 int32_t sg_batch_transfer_bytes(const sg_batch* b, int64_t* h2d, int64_t* d2h) {
   if (!b) return SG_ERR_INVALID_ARGUMENT;
   if (h2d) *h2d = b->impl->h2d_bytes();
