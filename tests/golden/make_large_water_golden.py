@@ -2,8 +2,12 @@
 (H2O)_512 (1536 / 3072 AOs), PM6, rms(dP) 1e-8, seed 0 of the water-cluster
 generator: the "vs the reference" column of the large-molecule path.
 
-Run from the repository root (CPU only, single-threaded oracle; about 7 and
-70 minutes):  python tests/golden/make_large_water_golden.py 256 512
+The oracle sums the energy with compensated (Neumaier) summation: a plain
+running sum over the 2.4M / 9.4M density-matrix terms lost 1.6e-8 and 6.0e-7
+Hartree at these sizes.
+
+Run from the repository root (CPU only, single-threaded oracle; about 12 and
+117 minutes):  python tests/golden/make_large_water_golden.py 256 512
 Each size is written to tests/golden/large_water_pm6_<n>.json.
 """
 import json
