@@ -109,7 +109,9 @@ def _fixtures():
 @pytest.mark.parametrize("fixture", _fixtures())
 def test_large_clusters_match_oracle_fixture(fixture):
     # the oracle's converged (H2O)_256 / (H2O)_512 PM6 energies and gradients
-    # (tests/golden/make_large_water_golden.py), FP64 and mixed-precision paths
+    # (tests/golden/make_large_water_golden.py), FP64 and mixed-precision paths.
+    # The oracle sums its energy with compensated summation, so the fixtures
+    # hold the energy to ~1e-11 Hartree and the check can be 1e-8.
     import json
     gold = json.load(open(fixture))
     Z, xa = geometry.water_cluster(gold["waters"], seed=gold["seed"])
@@ -117,5 +119,5 @@ def test_large_clusters_match_oracle_fixture(fixture):
     for path in ("large", "large_mixed"):
         _, e, g, it, conv = run_one("PM6", Z, x, path)
         assert conv
-        assert abs(e - gold["energy"]) < E_TOL, path
+        assert abs(e - gold["energy"]) < 1e-8, path
         assert np.max(np.abs(g.reshape(-1) - np.array(gold["gradient"]))) < G_TOL, path
