@@ -61,7 +61,10 @@ def parse():
     p.add_argument("--no-hessian", action="store_true", help="skip the semi-numerical Hessian leg")
     p.add_argument("--no-water32", action="store_true", help="skip the (H2O)_32 single-point leg")
     p.add_argument("--no-am1", action="store_true", help="skip the AM1 batch leg")
-    p.add_argument("--serving-loads", default="250,500,1000,2000", help="offered loads (req/s) of the serving leg")
+    p.add_argument("--serving-loads", default="500,1000,2000,4000,8000,16000,20000",
+                   help="offered loads (req/s) of the serving leg")
+    p.add_argument("--serving-seconds", type=float, default=2.0, help="arrival window per offered load")
+    p.add_argument("--serving-slots", type=int, default=8, help="concurrent batches of the request server")
     return p.parse_args()
 
 
@@ -149,19 +152,43 @@ def serving_mix(count, seed=5):
     return out
 
 
-def serving_leg(loads=(250, 500, 1000, 2000), seconds=3.0, plain_count=48, seed=5):
+def serving_offline(pool):
+    """Offline ceiling of the serving mix: the pool's requests as one batch
+    per method (energy + gradient), device time of the launch sequence after
+    a warm-up run."""
+    import sparrow_b200
+    by = {}
+    for z, x, m in pool:
+        by.setdefault(m, []).append((z, x.reshape(-1, 3)))
+    dev_ms = 0.0
+    wall_s = 0.0
+    for m, mols in by.items():
+        b = sparrow_b200.Batch(m, mols, scc=SCC, rmsd=RMSD, max_iter=MAX_ITER)
+        b.run(gradients=True)
+        t0 = time.perf_counter()
+        b.run(gradients=True)
+        b.results()
+        wall_s += time.perf_counter() - t0
+        dev_ms += float(sum(b.stage_times()))
+        del b
+    return {"requests": len(pool), "device_rps": len(pool) / (dev_ms * 1e-3), "wall_rps": len(pool) / wall_s,
+            "methods": {m: len(v) for m, v in by.items()}}
+
+
+def serving_leg(loads=(500, 1000, 2000, 4000, 8000, 16000, 20000), seconds=2.0, slots=8, plain_count=48, seed=5):
     """Open-loop Poisson arrivals into the request server at each offered load
     (req/s) for `seconds`; latency = completion - submission, timed by the
-    server.  Beside it, the plain form: the same requests one at a time
-    through one Calculator (closed loop)."""
-    import threading
+    server.  Beside it, the offline ceiling (the same mix as whole batches)
+    and the plain form: the same requests one at a time through one
+    Calculator (closed loop)."""
     import numpy as np
     import sparrow_b200
     pool = serving_mix(2048, seed)
     out = {"mix": "alkanes n~U[1,60] | (H2O)_n n~U[2,64], 70% PM6 / 30% DFTB2 (mio-1-1), "
-                  "energy+gradient, 3-384 AOs", "loads": []}
+                  "energy+gradient, 3-384 AOs", "slots": slots, "seconds_per_load": seconds, "loads": []}
+    out["offline"] = serving_offline(pool)
     rng = np.random.default_rng(seed + 1)
-    with sparrow_b200.Server(device_budget_gb=64.0, slots=8, scc=SCC, rmsd=RMSD, max_iter=MAX_ITER) as srv:
+    with sparrow_b200.Server(device_budget_gb=64.0, slots=slots, scc=SCC, rmsd=RMSD, max_iter=MAX_ITER) as srv:
         # warm-up: every code path and the arena pools
         for r in [srv.submit(m, z, x) for z, x, m in pool[:64]]:
             srv.wait(r)
@@ -821,7 +848,8 @@ def run_engine(args, rank, world):
 
     serving = None
     if rank == 0 and not args.no_serving:
-        serving = serving_leg(loads=tuple(float(v) for v in args.serving_loads.split(",")))
+        serving = serving_leg(loads=tuple(float(v) for v in args.serving_loads.split(",")),
+                              seconds=args.serving_seconds, slots=args.serving_slots)
 
     large = None
     if rank == 0 and not args.no_large:

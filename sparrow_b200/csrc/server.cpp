@@ -270,6 +270,9 @@ void Server::retire(Slot& s) {
   s.busy = false;
   inflight_bytes_ -= s.bytes;
   --inflight_;
+  // an arena grown past the slot's share (a request larger than the share)
+  // goes back to the pool instead of staying with the idle slot
+  if (s.batch && (size_t)s.batch->device_bytes() > budget_ / slots_.size()) s.batch.reset();
   cv_done_.notify_all();
 }
 
@@ -293,6 +296,10 @@ void Server::worker() {
     // method, spin treatment and size class; later matching requests follow in arrival order while
     // the device budget allows (one batch is always admitted when the device
     // is otherwise idle, so progress never depends on the budget)
+    // a batch stays within the budget's per-slot share (one request larger
+    // than that runs alone): every slot keeps its arena between batches, so
+    // the arenas held by all slots, busy or idle, stay within the budget
+    const size_t share = budget_ / slots_.size();
     for (auto& s : slots_) {
       if (s.busy || pending_.empty()) continue;
       const Method m = pending_.front().method;
@@ -306,6 +313,7 @@ void Server::worker() {
           continue;
         }
         const size_t add = it->bytes + ((int)take.size() < sms ? kScfRotationBytesPerCta : 0);
+        if (!take.empty() && bytes + add > share) break;
         if (inflight_bytes_ + bytes + add > budget_ && (!take.empty() || inflight_ > 0)) break;
         bytes += add;
         take.push_back(std::move(*it));

@@ -5,7 +5,8 @@
 // each on its own CUDA stream with its own device arena.  Whenever a slot is
 // free it admits the oldest pending requests of one method, in arrival order,
 // as long as the estimated device memory of all in-flight batches stays
-// within the budget, and launches them; finished batches are retired by
+// within the budget and the batch within the budget's per-slot share (each
+// slot keeps its arena between batches), and launches them; finished batches are retired by
 // event polling, their results handed to the waiting clients, and the slot
 // is refilled at once.  A batch holds one method and one size class (AO
 // count in steps of 64 up to 448, then larger): a batch finishes with its
