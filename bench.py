@@ -61,6 +61,7 @@ def parse():
     p.add_argument("--no-hessian", action="store_true", help="skip the semi-numerical Hessian leg")
     p.add_argument("--no-water32", action="store_true", help="skip the (H2O)_32 single-point leg")
     p.add_argument("--no-am1", action="store_true", help="skip the AM1 batch leg")
+    p.add_argument("--large-sizes", default="256,512,1024", help="water counts of the large-molecule leg")
     p.add_argument("--serving-loads", default="500,1000,2000,4000,8000,16000,20000",
                    help="offered loads (req/s) of the serving leg")
     p.add_argument("--serving-seconds", type=float, default=2.0, help="arrival window per offered load")
@@ -243,13 +244,45 @@ def serving_leg(loads=(500, 1000, 2000, 4000, 8000, 16000, 20000), seconds=2.0, 
     return out
 
 
+def cublas_bf16_product_ms(Np, reps=10):
+    """Device ms of cuBLAS (through torch) for the split-BF16 product's shape:
+    (Np x 4Np) times (4Np x Np)^T, BF16 in, FP32 accumulation (FP32 out where
+    torch offers it, else BF16 out)."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(1)
+    a = torch.randn((Np, 4 * Np), device="cuda", dtype=torch.bfloat16, generator=g)
+    b = torch.randn((Np, 4 * Np), device="cuda", dtype=torch.bfloat16, generator=g)
+    try:
+        f = lambda: torch.mm(a, b.t(), out_dtype=torch.float32)  # noqa: E731
+        f()
+        out = "fp32"
+    except (TypeError, RuntimeError):
+        f = lambda: torch.mm(a, b.t())  # noqa: E731
+        out = "bf16"
+    for _ in range(3):
+        f()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(reps):
+        f()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    del a, b
+    torch.cuda.empty_cache()
+    return ms, out
+
+
 def large_leg(sizes=(256, 512, 1024), seed=0):
     """Mixed-precision PM6 on large water clusters (the large-molecule path):
     per size the FP64 path and the split-BF16 path (energy + gradient), device
     ms of the SCF stage, wall ms of run + results, and the energy error of the
     mixed path against the FP64 GPU path and, where the oracle's fixture
     exists (tests/golden/large_water_pm6_<n>.json), of both against the
-    oracle."""
+    oracle.  The purification products are timed on the device: the mixed
+    path's tensor-core GEMM (this library's tcgen05 kernel) per product beside
+    cuBLAS on the same shape, and the FP64 squares (cuBLAS DSYRK)."""
     import numpy as np
     import sparrow_b200
     from sparrow_b200 import geometry
@@ -273,16 +306,34 @@ def large_leg(sizes=(256, 512, 1024), seed=0):
                 e, g, it, conv = b.results()
                 wall = time.perf_counter() - t0
                 st = b.stage_times()
-                nm, ns, _ = b.scf_stats()
+                nm, ns, pcyc = b.scf_stats()
+                pc = [int(v) for v in pcyc[0]]
                 del b
             r = {"energy": float(e[0]), "converged": bool(conv[0]), "iterations": int(it[0]),
                  "mixed_iterations": int(nm[0]), "sp2_steps": int(ns[0]), "scf_ms": float(st[2]),
                  "total_device_ms": float(sum(st)), "wall_ms": wall * 1e3}
+            if pc[1] > 0:
+                r["tc_gemm_products"] = int(pc[1])
+                r["tc_gemm_ms_per_product"] = pc[0] / pc[1] / 1e6
+            if pc[3] > 0:
+                r["fp64_dsyrk_products"] = int(pc[3])
+                r["fp64_dsyrk_ms_per_product"] = pc[2] / pc[3] / 1e6
             if gold is not None:
                 r["dE_vs_oracle"] = float(e[0]) - gold["energy"]
                 r["max_dgrad_vs_oracle"] = float(np.max(np.abs(g[0].reshape(-1) - np.array(gold["gradient"]))))
             row[path] = r
         warm = False
+        Np = (6 * n + 127) // 128 * 128
+        cb_ms, cb_out = cublas_bf16_product_ms(Np)
+        flops = 8.0 * Np ** 3
+        rm = row["large_mixed"]
+        row["split_bf16_product"] = {
+            "shape": "(%d x %d) x (%d x %d)^T, BF16 in, FP32 accumulation" % (Np, 4 * Np, Np, 4 * Np),
+            "flops": flops,
+            "tc_gemm_ms": rm.get("tc_gemm_ms_per_product"),
+            "tc_gemm_tflops": flops / rm["tc_gemm_ms_per_product"] / 1e9 if rm.get("tc_gemm_ms_per_product") else None,
+            "cublas_ms": cb_ms, "cublas_out": cb_out, "cublas_tflops": flops / cb_ms / 1e9,
+            "tc_over_cublas_time": rm["tc_gemm_ms_per_product"] / cb_ms if rm.get("tc_gemm_ms_per_product") else None}
         row["dE_mixed_vs_fp64"] = row["large_mixed"]["energy"] - row["large"]["energy"]
         row["speedup_mixed_over_fp64"] = row["large"]["total_device_ms"] / row["large_mixed"]["total_device_ms"]
         rows.append(row)
@@ -846,28 +897,43 @@ def run_engine(args, rank, world):
                  "batched_device_over_plain": value / world / prate, "batched_e2e_over_plain": e2e_value / world / prate}
 
 
+    def drop_caches():
+        # each side leg starts from a device free of the previous legs' idle arenas
+        import gc
+        import torch
+        gc.collect()
+        sparrow_b200.lib().sg_release_cached_memory()
+        torch.cuda.empty_cache()
+
     serving = None
     if rank == 0 and not args.no_serving:
+        drop_caches()
         serving = serving_leg(loads=tuple(float(v) for v in args.serving_loads.split(",")),
                               seconds=args.serving_seconds, slots=args.serving_slots)
 
     large = None
     if rank == 0 and not args.no_large:
-        large = large_leg()
+        drop_caches()
+        large = large_leg(sizes=tuple(int(v) for v in args.large_sizes.split(",")))
     tddftb = None
     if rank == 0 and not args.no_tddftb:
+        drop_caches()
         tddftb = tddftb_leg()
     open_shell = None
     if rank == 0 and not args.no_open_shell:
+        drop_caches()
         open_shell = open_shell_leg()
     hessian = None
     if rank == 0 and not args.no_hessian:
+        drop_caches()
         hessian = hessian_leg()
     water32 = None
     if rank == 0 and not args.no_water32:
+        drop_caches()
         water32 = water32_leg()
     am1 = None
     if rank == 0 and not args.no_am1:
+        drop_caches()
         am1 = am1_leg(mols)
 
     # roofline of the SCF kernel (average launch)

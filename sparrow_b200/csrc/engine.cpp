@@ -92,6 +92,22 @@ void release_cached_memory() {
   g_pool.clear();
 }
 
+namespace {
+
+// cudaMalloc that, when the device is full, frees the process-wide cache of
+// idle arenas and tries once more.
+cudaError_t device_alloc(void** p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    release_cached_memory();
+    e = cudaMalloc(p, bytes);
+  }
+  return e;
+}
+
+}  // namespace
+
 Batch::Batch(Method m) : method_(m) {}
 
 Batch::~Batch() {
@@ -128,13 +144,7 @@ int Batch::ensure_arena(size_t bytes, std::string& err) {
     arena_bytes_ = got;
     return kOk;
   }
-  cudaError_t e = cudaMalloc(&arena_, bytes);
-  if (e == cudaErrorMemoryAllocation) {
-    // free cached blocks and retry once
-    cudaGetLastError();
-    release_cached_memory();
-    e = cudaMalloc(&arena_, bytes);
-  }
+  cudaError_t e = device_alloc(&arena_, bytes);
   if (e != cudaSuccess) {
     cudaGetLastError();
     err = "device allocation of " + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e);
@@ -726,7 +736,7 @@ int Batch::run(const ScfParams& sp_in, bool gradient, std::string& err) {
           large_scratch_ = nullptr;
           large_scratch_bytes_ = 0;
         }
-        cudaError_t e = cudaMalloc(&large_scratch_, need);
+        cudaError_t e = device_alloc(&large_scratch_, need);
         if (e != cudaSuccess) {
           cudaGetLastError();
           large_scratch_ = nullptr;
@@ -848,7 +858,7 @@ int Batch::run_tddftb(int nroots, bool triplet, double tol, int max_iter, std::s
       td_scratch_ = nullptr;
       td_scratch_bytes_ = 0;
     }
-    cudaError_t e = cudaMalloc(&td_scratch_, need);
+    cudaError_t e = device_alloc(&td_scratch_, need);
     if (e != cudaSuccess) {
       cudaGetLastError();
       td_scratch_ = nullptr;

@@ -20,17 +20,20 @@
 // change falls below a switch threshold (1e-5 by default) the remaining
 // iterations run SP2 in FP64 (the residual correction), so the converged
 // density is the FP64 one.
-// GEMMs use cuBLAS (plain library GEMMs); the rest are the kernels below.
+// The split-BF16 product is this library's own tcgen05/TMA kernel
+// (tc_gemm.cuh); the FP64 squares and the DIIS product FP use cuBLAS.
 #include <cublas_v2.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstring>
 #include <string>
 #include <vector>
 
 #include "engine.h"
 #include "kernels.h"
+#include "tc_gemm.cuh"
 
 namespace sgb {
 
@@ -145,17 +148,17 @@ __global__ void __launch_bounds__(kLT) k_sp2_step_upper(double* X, const double*
 }
 
 // The same step when the product is X X = A + A^T (A in FP32 from the
-// split-BF16 GEMM); 32 x 32 tiles (block 32 x 8), the mirror tile of A read
-// through shared memory.
-__global__ void __launch_bounds__(kLT) k_sp2_step_sym(double* X, const float* __restrict__ A, int N, double nocc,
-                                                      const double* __restrict__ cur, double* next) {
+// split-BF16 GEMM, leading dimension lda); 32 x 32 tiles (block 32 x 8), the
+// mirror tile of A read through shared memory.
+__global__ void __launch_bounds__(kLT) k_sp2_step_sym(double* X, const float* __restrict__ A, int lda, int N,
+                                                      double nocc, const double* __restrict__ cur, double* next) {
   __shared__ float tile[32][33];
   const double tr = cur[0], tr2 = cur[1];
   const int square = fabs(tr2 - nocc) < fabs(2.0 * tr - tr2 - nocc);
   const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32, tx = threadIdx.x, ty = threadIdx.y;
   for (int r = ty; r < 32; r += 8) {
     const int i = j0 + r, j = i0 + tx;
-    tile[r][tx] = (i < N && j < N) ? A[(size_t)i * N + j] : 0.0f;
+    tile[r][tx] = (i < N && j < N) ? A[(size_t)i * lda + j] : 0.0f;
   }
   __syncthreads();
   double t = 0, t2 = 0;
@@ -163,7 +166,7 @@ __global__ void __launch_bounds__(kLT) k_sp2_step_sym(double* X, const float* __
     const int i = i0 + r, j = j0 + tx;
     if (i >= N || j >= N) continue;
     const size_t k = (size_t)i * N + j;
-    const double x2 = (double)A[k] + (double)tile[tx][r];
+    const double x2 = (double)A[(size_t)i * lda + j] + (double)tile[tx][r];
     const double x = square ? x2 : 2.0 * X[k] - x2;
     X[k] = x;
     t2 += x * x;
@@ -175,26 +178,27 @@ __global__ void __launch_bounds__(kLT) k_sp2_step_sym(double* X, const float* __
 // Three-term BF16 split X = X1 + X2 + X3 (each term the rounding of the
 // remainder).  With every term symmetric,
 //   X1 X1 + X1 X2 + X2 X1 + X1 X3 + X3 X1 + X2 X2 = A + A^T,
-//   A = X1 (X1 / 2) + X1 X2 + X1 X3 + X2 (X2 / 2) = L R^T,
-// L = [X1 X1 X1 X2], R = [X1/2 X2 X3 X2/2] (blocks of n entries): one GEMM
-// with K = 4N (halving is exact in BF16).
-__global__ void __launch_bounds__(kLT) k_split3(const double* __restrict__ X, size_t n, __nv_bfloat16* L,
-                                                __nv_bfloat16* R) {
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x) {
-    const double x = X[k];
+//   A = X1 (X1 / 2) + X1 X2 + X1 X3 + X2 (X2 / 2),
+// one tensor-core GEMM with K = 4 Np over the five stacked terms
+// T = [X1, X2, X3, X1/2, X2/2] (halving is exact in BF16), each Np x Np and
+// zero past N.
+constexpr int kTermX1 = 0, kTermX2 = 1, kTermX3 = 2, kTermX1h = 3, kTermX2h = 4, kTerms = 5;
+__global__ void __launch_bounds__(kLT) k_split_terms(const double* __restrict__ X, int N, int Np,
+                                                     __nv_bfloat16* __restrict__ T) {
+  const size_t nn = (size_t)Np * Np;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nn; k += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(k / Np), j = (int)(k % Np);
+    const double x = (i < N && j < N) ? X[(size_t)i * N + j] : 0.0;
     const __nv_bfloat16 a = __double2bfloat16(x);
     const double r1 = x - (double)__bfloat162float(a);
     const __nv_bfloat16 b = __double2bfloat16(r1);
     const double r2 = r1 - (double)__bfloat162float(b);
     const __nv_bfloat16 half = __float2bfloat16(0.5f);
-    L[k] = a;
-    L[n + k] = a;
-    L[2 * n + k] = a;
-    L[3 * n + k] = b;
-    R[k] = __hmul(a, half);
-    R[n + k] = b;
-    R[2 * n + k] = __double2bfloat16(r2);
-    R[3 * n + k] = __hmul(b, half);
+    T[kTermX1 * nn + k] = a;
+    T[kTermX2 * nn + k] = b;
+    T[kTermX3 * nn + k] = __double2bfloat16(r2);
+    T[kTermX1h * nn + k] = __hmul(a, half);
+    T[kTermX2h * nn + k] = __hmul(b, half);
   }
 }
 
@@ -280,6 +284,7 @@ constexpr int kSlotEnergy = 8;   // E_el of the last Fock build
 constexpr int kSlotDots = 16;    // kDiisMax DIIS dot products
 constexpr int kSlotCoef = 24;    // kDiisMax DIIS coefficients
 constexpr int kSlotRms = 32;     // sum (dP)^2
+constexpr int kSlotTcErr = 40;   // bounded-wait bits of the tensor-core GEMM (as unsigned)
 constexpr int kSlotTraces = 64;  // (trace X, trace X^2) per SP2 step
 constexpr int kSp2MaxSteps = 200;
 constexpr size_t kStateBytes = 8192;
@@ -346,9 +351,12 @@ bool diis_solve(const double* bm, int n, double* coef) {
 
 }  // namespace
 
+// The split-BF16 products run on Np = nao rounded up to the GEMM tile.
+int padded_order(long long nao) { return (int)((nao + tc::kBM - 1) / tc::kBM * tc::kBM); }
+
 size_t large_scf_scratch_bytes(long long nao) {
-  const size_t NN = (size_t)nao * nao;
-  return kStateBytes + align256(4 * NN * 2) + align256(4 * NN * 2) + align256(NN * 4);
+  const size_t NP = (size_t)padded_order(nao) * padded_order(nao);
+  return kStateBytes + align256(kTerms * NP * 2) + align256(NP * 4);
 }
 
 namespace {
@@ -358,9 +366,13 @@ namespace {
 struct LargeHost {
   double* hp = nullptr;
   cudaEvent_t ev[2] = {nullptr, nullptr};
+  // timing events around the purification products of one SCF iteration
+  std::vector<cudaEvent_t> pev;
   ~LargeHost() {
     if (hp) cudaFreeHost(hp);
     for (auto& e : ev)
+      if (e) cudaEventDestroy(e);
+    for (auto& e : pev)
       if (e) cudaEventDestroy(e);
   }
 };
@@ -411,9 +423,13 @@ int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, in
   const int grid = sms * 8;
   char* scr = static_cast<char*>(b.large_scratch);
   double* st = reinterpret_cast<double*>(scr);
-  __nv_bfloat16* L = reinterpret_cast<__nv_bfloat16*>(scr + kStateBytes);
-  __nv_bfloat16* R = reinterpret_cast<__nv_bfloat16*>(scr + kStateBytes + align256(4 * NN * 2));
-  float* C32 = reinterpret_cast<float*>(scr + kStateBytes + align256(4 * NN * 2) + align256(4 * NN * 2));
+  const int Np = padded_order(N);
+  const size_t NP = (size_t)Np * Np;
+  __nv_bfloat16* T = reinterpret_cast<__nv_bfloat16*>(scr + kStateBytes);
+  float* C32 = reinterpret_cast<float*>(scr + kStateBytes + align256(kTerms * NP * 2));
+  unsigned* tc_err = reinterpret_cast<unsigned*>(st + kSlotTcErr);
+  static const int a_terms[4] = {kTermX1, kTermX1, kTermX1, kTermX2};
+  static const int b_terms[4] = {kTermX1h, kTermX2, kTermX3, kTermX2h};
   double* histF = b.diis;
   double* histE = b.diis + (size_t)kDiisMax * NN;
   double* X = b.C;
@@ -423,17 +439,22 @@ int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, in
   cudaError_t ce = cudaMallocHost(&hb.hp, sizeof(double) * 2 * (kSp2MaxSteps + 2));
   if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&hb.ev[0], cudaEventDisableTiming);
   if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&hb.ev[1], cudaEventDisableTiming);
+  hb.pev.assign(2 * kSp2MaxSteps, nullptr);
+  for (auto& e : hb.pev)
+    if (ce == cudaSuccess) ce = cudaEventCreate(&e);
   if (ce != cudaSuccess) {
     err = cuda_message(ce);
     return kErrCuda;
   }
   const double one = 1.0, zero = 0.0;
-  const float onef = 1.0f, zerof = 0.0f;
   const int msize = sp.diis_size < 1 ? 1 : (sp.diis_size > kDiisMax ? kDiisMax : sp.diis_size);
   double bmat[kDiisMax * kDiisMax] = {};
   int nhist = 0, head = 0, nl = 0;
   double Eold = 0, last_dE = 0, last_rms = 0, prev_rms = 1e300;
   int it = 0, converged = 0, status = kDevOk, sp2_total = 0, mixed_iters = 0;
+  // device time and count of the purification products, split-BF16 and FP64
+  double prod_ms[2] = {0, 0};
+  long long prod_n[2] = {0, 0};
   bool mixed = precision == 1;
   const dim3 tgrid((N + 31) / 32, (N + 31) / 32), tblock(32, 8);
   auto fail_cuda = [&](cudaError_t e) {
@@ -475,24 +496,34 @@ int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, in
     const bool use_mixed = mixed;
     cudaMemsetAsync(st + kSlotKeys, 0, sizeof(double) * 2, s);
     cudaMemsetAsync(st + kSlotTraces, 0, sizeof(double) * 2 * (kSp2MaxSteps + 1), s);
+    cudaMemsetAsync(tc_err, 0, sizeof(unsigned), s);
     k_gershgorin<<<(N * 32 + kLT - 1) / kLT, kLT, 0, s>>>(b.F, N, reinterpret_cast<unsigned long long*>(st + kSlotKeys));
     k_sp2_init<<<grid, kLT, 0, s>>>(b.F, N, reinterpret_cast<const unsigned long long*>(st + kSlotKeys), X,
                                     st + kSlotTraces);
     nl += 2;
     cudaMemcpyAsync(hb.hp, st + kSlotTraces, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
     bool sp2_ok = false;
+    int nprod = 0;
     for (int k = 0; k < kSp2MaxSteps; ++k) {
+      nprod = k + 1;
       double* cur = st + kSlotTraces + 2 * k;
       if (use_mixed) {
-        k_split3<<<grid, kLT, 0, s>>>(X, NN, L, R);
-        bs = cublasGemmEx(h, CUBLAS_OP_N, CUBLAS_OP_T, N, N, 4 * N, &onef, L, CUDA_R_16BF, N, R, CUDA_R_16BF, N,
-                          &zerof, C32, CUDA_R_32F, N, CUBLAS_COMPUTE_32F, CUBLAS_GEMM_DEFAULT);
-        k_sp2_step_sym<<<tgrid, tblock, 0, s>>>(X, C32, N, nocc, cur, cur + 2);
-        nl += 2;
+        k_split_terms<<<grid, kLT, 0, s>>>(X, N, Np, T);
+        cudaEventRecord(hb.pev[2 * k], s);
+        ce = tc::gemm_terms(T, kTerms, Np, a_terms, b_terms, 4, C32, Np, tc_err, s, err);
+        cudaEventRecord(hb.pev[2 * k + 1], s);
+        if (ce != cudaSuccess) {
+          if (err.empty()) err = cuda_message(ce);
+          return kErrCuda;
+        }
+        k_sp2_step_sym<<<tgrid, tblock, 0, s>>>(X, C32, Np, N, nocc, cur, cur + 2);
+        nl += 3;
       } else {
         // X X = X X^T: half the flops of a GEMM; the column-major lower
         // triangle is the row-major upper one
+        cudaEventRecord(hb.pev[2 * k], s);
         bs = cublasDsyrk(h, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, N, N, &one, X, N, &zero, X2, N);
+        cudaEventRecord(hb.pev[2 * k + 1], s);
         k_sp2_step_upper<<<tgrid, tblock, 0, s>>>(X, X2, N, nocc, cur, cur + 2);
         ++nl;
       }
@@ -520,9 +551,24 @@ int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, in
     k_density_update<<<grid, kLT, 0, s>>>(X, NN, b.P, st + kSlotRms);
     ++nl;
     cudaMemcpyAsync(hb.hp, st + kSlotRms, sizeof(double), cudaMemcpyDeviceToHost, s);
+    cudaMemcpyAsync(hb.hp + 1, tc_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
     ce = cudaStreamSynchronize(s);
     if (ce == cudaSuccess) ce = cudaGetLastError();
     if (ce != cudaSuccess) return fail_cuda(ce);
+    for (int k = 0; k < nprod; ++k) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, hb.pev[2 * k], hb.pev[2 * k + 1]) == cudaSuccess) {
+        prod_ms[use_mixed ? 0 : 1] += ms;
+        ++prod_n[use_mixed ? 0 : 1];
+      }
+    }
+    cudaGetLastError();
+    unsigned tc_bits = 0;
+    std::memcpy(&tc_bits, hb.hp + 1, sizeof(unsigned));
+    if (tc_bits != 0) {
+      err = "tensor-core GEMM: a bounded barrier wait ran out (bits " + std::to_string(tc_bits) + ")";
+      return kErrCuda;
+    }
     const double rms = std::sqrt(hb.hp[0] / (double)NN);
     last_rms = rms;
     last_dE = it > 1 ? std::fabs(E - Eold) : 0.0;
@@ -562,7 +608,13 @@ int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, in
   r.last_rmsd = last_rms;
   r.full_diag = mixed_iters;
   r.jacobi_sweeps = sp2_total;
-  for (auto& c : r.cycles) c = 0;
+  // the cycle slots carry the purification products on this path: device ns
+  // and count of the split-BF16 tensor-core GEMMs, then of the FP64 squares
+  r.cycles[0] = (long long)(prod_ms[0] * 1e6);
+  r.cycles[1] = prod_n[0];
+  r.cycles[2] = (long long)(prod_ms[1] * 1e6);
+  r.cycles[3] = prod_n[1];
+  r.cycles[4] = 0;
   ce = cudaMemcpyAsync(b.res, &r, sizeof(MolResult), cudaMemcpyHostToDevice, s);
   // no orbitals on this path: the orbital energies read as zero
   if (ce == cudaSuccess) ce = cudaMemsetAsync(b.eps, 0, sizeof(double) * N, s);

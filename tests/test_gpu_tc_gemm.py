@@ -1,0 +1,105 @@
+"""The large-molecule path's tensor-core GEMM (tcgen05.mma, FP32 accumulator in
+tensor memory, TMA tile loads) against an FP64 product of the same BF16
+terms, through the test harness library tests/csrc/libtc_gemm_probe.so.
+
+C = sum_s T[a_s] T[b_s]^T over stacked Np x Np BF16 terms.  FP32
+accumulation of BF16 products: each entry within 1e-5 of the sum of the
+absolute products (plus 1e-30)."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(ROOT, "csrc", "libtc_gemm_probe.so")
+
+
+def _lib():
+    if not os.path.exists(LIB):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "csrc")])
+    return ctypes.CDLL(LIB)
+
+
+def run_gemm(T, a_terms, b_terms, ldc=None):
+    """T: torch bf16 (nterms, Np, Np) on cuda; returns (C as float64 numpy, err word)."""
+    import torch
+    L = _lib()
+    nterms, Np, _ = T.shape
+    ldc = Np if ldc is None else ldc
+    C = torch.full((Np, ldc), float("nan"), dtype=torch.float32, device=T.device)
+    err = torch.zeros(1, dtype=torch.int32, device=T.device)
+    a = (ctypes.c_int * len(a_terms))(*a_terms)
+    b = (ctypes.c_int * len(b_terms))(*b_terms)
+    rc = L.tc_gemm_probe(ctypes.c_void_p(T.data_ptr()), nterms, Np, a, b, len(a_terms), ctypes.c_void_p(C.data_ptr()),
+                         ldc, ctypes.c_void_p(err.data_ptr()))
+    assert rc == 0, "tc_gemm_probe returned CUDA error %d" % rc
+    return C[:, :Np].double().cpu().numpy(), int(err.item())
+
+
+def reference(T, a_terms, b_terms):
+    Td = T.double().cpu().numpy()
+    C = np.zeros(Td.shape[1:])
+    A = np.zeros(Td.shape[1:])
+    for a, b in zip(a_terms, b_terms):
+        C += Td[a] @ Td[b].T
+        A += np.abs(Td[a]) @ np.abs(Td[b]).T
+    return C, A
+
+
+SPLIT_A = [0, 0, 0, 1]
+SPLIT_B = [3, 1, 2, 4]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("Np", [128, 256, 384, 1536, 2944])
+def test_split_product_matches_fp64(Np):
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(Np)
+    T = (torch.rand((5, Np, Np), generator=g, dtype=torch.float64) * 2 - 1).to(torch.bfloat16).cuda()
+    C, err = run_gemm(T, SPLIT_A, SPLIT_B)
+    assert err == 0
+    ref, absref = reference(T, SPLIT_A, SPLIT_B)
+    assert np.all(np.isfinite(C))
+    assert np.all(np.abs(C - ref) <= 1e-5 * absref + 1e-30), np.max(np.abs(C - ref) / (absref + 1e-30))
+
+
+@pytest.mark.gpu
+def test_tile_widths_cover_both_kernels():
+    L = _lib()
+    widths = {Np: L.tc_gemm_tile_n(Np) for Np in (128, 384, 1536, 2944, 3072, 6144)}
+    assert set(widths.values()) == {128, 256}, widths
+
+
+@pytest.mark.gpu
+def test_single_segment_with_padded_leading_dimension():
+    import torch
+    Np = 256
+    g = torch.Generator(device="cpu").manual_seed(7)
+    T = torch.randn((2, Np, Np), generator=g, dtype=torch.float64).to(torch.bfloat16).cuda()
+    C, err = run_gemm(T, [0], [1], ldc=Np + 4)
+    assert err == 0
+    ref, absref = reference(T, [0], [1])
+    assert np.all(np.abs(C - ref) <= 1e-5 * absref + 1e-30)
+
+
+@pytest.mark.gpu
+def test_split_of_symmetric_matrix_reproduces_its_square():
+    """The SP2 use: X = X1 + X2 + X3 in BF16, X X ~ A + A^T to FP32 accuracy."""
+    import torch
+    Np = 384
+    rng = np.random.default_rng(3)
+    Q, _ = np.linalg.qr(rng.standard_normal((Np, Np)))
+    X = (Q * rng.uniform(0, 1, Np)) @ Q.T
+    X = 0.5 * (X + X.T)
+    t = torch.tensor(X)
+    x1 = t.to(torch.bfloat16)
+    r1 = t - x1.double()
+    x2 = r1.to(torch.bfloat16)
+    x3 = (r1 - x2.double()).to(torch.bfloat16)
+    T = torch.stack([x1, x2, x3, x1 * 0.5, x2 * 0.5]).cuda()
+    A, err = run_gemm(T, SPLIT_A, SPLIT_B)
+    assert err == 0
+    X2 = A + A.T
+    assert np.max(np.abs(X2 - X @ X)) < 1e-5
