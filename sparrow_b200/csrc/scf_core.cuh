@@ -77,19 +77,25 @@ __device__ __forceinline__ void cp_async_wait_pending() {
 }
 
 // C = alpha * op(A) * op(B) + beta * C, row-major, op(X) = X or X^T, on the
-// FP64 tensor cores (mma.sync m8n8k4 f64).  The CTA (512 threads) is split
-// into two groups of 256 that work on different 64x64 output tiles; in a
-// group each of the 8 warps owns a 16x32 block (2 x 4 MMA tiles, 16
-// accumulators per thread).  The 64x8 / 8x64 input tiles stream through a
-// kGemmStages-deep cp.async ring in shared memory, so the global-load latency
-// of the next slices overlaps the MMAs of the current one.  Their layout follows the global one so the
-// copies stay coalesced: A row-major [m][k] (stride 12) or, when op(A) = A^T,
-// [k][m] (stride 72), and likewise for B; with these strides both the copies
-// and the fragment reads touch every bank twice (two wavefronts per warp).
-__device__ __forceinline__ void dmma_8x8x4(double& c0, double& c1, double a, double b) {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-               : "+d"(c0), "+d"(c1)
-               : "d"(a), "d"(b));
+// FP64 tensor cores (mma.sync m16n8k8 f64, the sm_90+ shape: one instruction
+// for the work of four m8n8k4).  The CTA (512 threads) is split into two
+// groups of 256 that work on different 64x64 output tiles; in a group each of
+// the 8 warps owns a 16x32 block (4 MMA tiles of 16x8, 16 accumulators per
+// thread).  The 64x8 / 8x64 input tiles stream through a kGemmStages-deep
+// cp.async ring in shared memory, so the global-load latency of the next
+// slices overlaps the MMAs of the current one.  Their layout follows the
+// global one so the copies stay coalesced: A row-major [m][k] (stride 12) or,
+// when op(A) = A^T, [k][m] (stride 72), and likewise for B; with these
+// strides both the copies and the fragment reads touch every bank twice (two
+// wavefronts per warp).
+// Fragments (g = lane / 4, t = lane % 4): a[v] = A(g + 8 (v % 2), t + 4 (v / 2)),
+// b[v] = B(t + 4 v, g), c[v] = C(g + 8 (v / 2), 2 t + v % 2).
+__device__ __forceinline__ void dmma_16x8x8(double (&c)[4], const double (&a)[4], const double (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+      "{%0, %1, %2, %3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
 }
 
 // sym: the result is known to be symmetric (M == Nn): only the tiles on or
@@ -148,11 +154,15 @@ __device__ __forceinline__ void cta_gemm(int M, int Nn, int K, double alpha, con
       tn = tm + t;
     }
     const int m0 = tm * kGemmBM, n0 = tn * kGemmBN;
-    double acc[2][4][2];
+    // 8 x 8 blocks of this warp that lie inside the product: edge tiles skip
+    // the MMAs (and fragment loads) of their padding, which frees the FP64
+    // tensor pipe for the other warps of the SM (warp-uniform masks)
+    const bool rows_in = M > m0 + wm * 16;
+    const int cols_left = Nn - (n0 + wn * 32);
+    const int nbj = !rows_in ? 0 : (cols_left >= 32 ? 4 : (cols_left > 0 ? (cols_left + 7) >> 3 : 0));
+    double acc[4][4];
 #pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+    for (int j = 0; j < 4; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
 #pragma unroll
     for (int st = 0; st < kGemmStages - 1; ++st) {
       if (st < nk) load_stage(st, m0, n0, st * kGemmBK);
@@ -166,34 +176,30 @@ __device__ __forceinline__ void cta_gemm(int M, int Nn, int K, double alpha, con
       else cp_async_commit();
       const double* smA = base + (kt % kGemmStages) * kGemmStage;
       const double* smB = smA + kGemmStage / 2;
+      double a[4], b[4][2];
 #pragma unroll
-      for (int ks = 0; ks < kGemmBK; ks += 4) {
-        double a[2], b[4];
-#pragma unroll
-        for (int i = 0; i < 2; ++i) a[i] = smA[(wm * 16 + i * 8 + fr) * a_sm + (ks + fc) * a_sk];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) b[j] = smB[(wn * 32 + j * 8 + fr) * b_sn + (ks + fc) * b_sk];
-#pragma unroll
-        for (int i = 0; i < 2; ++i)
-#pragma unroll
-          for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
-      }
-    }
-    group_sync(grp);  // all reads of the last stage done before the next tile overwrites it
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
+      for (int v = 0; v < 4; ++v) a[v] = smA[(wm * 16 + fr + 8 * (v & 1)) * a_sm + (fc + 4 * (v >> 1)) * a_sk];
 #pragma unroll
       for (int j = 0; j < 4; ++j)
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const int gm = m0 + wm * 16 + i * 8 + fr, gn = n0 + wn * 32 + j * 8 + fc * 2 + h;
-          if (gm < M && gn < Nn) {
-            double* c = &C[(size_t)gm * ldc + gn];
-            const double v = beta == 0.0 ? alpha * acc[i][j][h] : alpha * acc[i][j][h] + beta * (*c);
-            *c = v;
-            if (sym && tn > tm) C[(size_t)gn * ldc + gm] = v;
-          }
+        for (int v = 0; v < 2; ++v) b[j][v] = smB[(wn * 32 + j * 8 + fr) * b_sn + (fc + 4 * v) * b_sk];
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        if (j < nbj) dmma_16x8x8(acc[j], a, b[j]);
+    }
+    group_sync(grp);  // all reads of the last stage done before the next tile overwrites it
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int gm = m0 + wm * 16 + fr + 8 * (q >> 1), gn = n0 + wn * 32 + j * 8 + fc * 2 + (q & 1);
+        if (gm < M && gn < Nn) {
+          double* c = &C[(size_t)gm * ldc + gn];
+          const double v = beta == 0.0 ? alpha * acc[j][q] : alpha * acc[j][q] + beta * (*c);
+          *c = v;
+          if (sym && tn > tm) C[(size_t)gn * ldc + gm] = v;
         }
+      }
   }
   __syncthreads();
 }
