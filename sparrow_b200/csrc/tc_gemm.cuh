@@ -165,7 +165,8 @@ struct Layout {
 template <int BN, int STAGES>
 __global__ void __launch_bounds__(kThreads, 1)
     k_tc_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, float* __restrict__ C,
-                   int ldc, int ncols, int mtiles, int ntiles, Segments seg, unsigned* __restrict__ err) {
+                   int ldc, int ncols, int mtiles, int ntiles, const __grid_constant__ Segments seg,
+                   unsigned* __restrict__ err) {
   using L = Layout<BN, STAGES>;
   constexpr int kGroupM = 16;
   extern __shared__ uint8_t smem_raw[];
