@@ -14,7 +14,12 @@ namespace {
 constexpr int kScfThreads = 512;
 constexpr int kGemmGroup = 256;       // threads per GEMM tile group
 constexpr int kJacobiMaxPairs = 512;  // supports N <= 1024
-constexpr int kGemmBM = 64, kGemmBN = 64, kGemmBK = 8;
+// K depth of one pipeline slice of the CTA GEMM (8 or 16)
+#ifndef SGB_GEMM_BK
+#define SGB_GEMM_BK 8
+#endif
+constexpr int kGemmBM = 64, kGemmBN = 64, kGemmBK = SGB_GEMM_BK;
+static_assert(kGemmBK == 8 || kGemmBK == 16, "CTA GEMM slice depth");
 constexpr size_t kRotBudgetBytes = kScfRotationBytesPerCta;
 // shared strides of the GEMM input tiles: k-contiguous rows of 8 (+4 pad) or
 // m/n-contiguous rows of 64 (+8 pad); one stage holds an A and a B tile
@@ -121,7 +126,7 @@ __device__ __forceinline__ void cta_gemm(int M, int Nn, int K, double alpha, con
     for (int r = 0; r < (kGemmBM * kGemmBK) / kGemmGroup; ++r) {
       const int e = tid + r * kGemmGroup;
       int mm, kk;
-      if (!tA) { mm = e >> 3; kk = e & 7; }
+      if (!tA) { mm = e / kGemmBK; kk = e % kGemmBK; }
       else { kk = e >> 6; mm = e & 63; }
       const int gm = m0 + mm, gk = k0 + kk;
       const bool ok = gm < M && gk < K;
@@ -133,7 +138,7 @@ __device__ __forceinline__ void cta_gemm(int M, int Nn, int K, double alpha, con
       const int e = tid + r * kGemmGroup;
       int nn, kk;
       if (!tB) { kk = e >> 6; nn = e & 63; }
-      else { nn = e >> 3; kk = e & 7; }
+      else { nn = e / kGemmBK; kk = e % kGemmBK; }
       const int gn = n0 + nn, gk = k0 + kk;
       const bool ok = gn < Nn && gk < K;
       const double* src = ok ? (tB ? B + (size_t)gn * ldb + gk : B + (size_t)gk * ldb + gn) : B;
@@ -176,16 +181,20 @@ __device__ __forceinline__ void cta_gemm(int M, int Nn, int K, double alpha, con
       else cp_async_commit();
       const double* smA = base + (kt % kGemmStages) * kGemmStage;
       const double* smB = smA + kGemmStage / 2;
-      double a[4], b[4][2];
 #pragma unroll
-      for (int v = 0; v < 4; ++v) a[v] = smA[(wm * 16 + fr + 8 * (v & 1)) * a_sm + (fc + 4 * (v >> 1)) * a_sk];
+      for (int ks = 0; ks < kGemmBK; ks += 8) {
+        double a[4], b[4][2];
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+        for (int v = 0; v < 4; ++v)
+          a[v] = smA[(wm * 16 + fr + 8 * (v & 1)) * a_sm + (ks + fc + 4 * (v >> 1)) * a_sk];
 #pragma unroll
-        for (int v = 0; v < 2; ++v) b[j][v] = smB[(wn * 32 + j * 8 + fr) * b_sn + (fc + 4 * v) * b_sk];
+        for (int j = 0; j < 4; ++j)
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
-        if (j < nbj) dmma_16x8x8(acc[j], a, b[j]);
+          for (int v = 0; v < 2; ++v) b[j][v] = smB[(wn * 32 + j * 8 + fr) * b_sn + (ks + fc + 4 * v) * b_sk];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (j < nbj) dmma_16x8x8(acc[j], a, b[j]);
+      }
     }
     group_sync(grp);  // all reads of the last stage done before the next tile overwrites it
 #pragma unroll
