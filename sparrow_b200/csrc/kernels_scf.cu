@@ -422,6 +422,21 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_scf(const MolDev* __restrict
     const int N = m.nao, no = m.nocc;
     const size_t NN = (size_t)N * N;
     const double* H = Hall + m.mat_off;
+    // The five N x N buffers of the molecule trade roles during the SCF
+    // instead of being copied into each other: role r (F, C, W1, W2, P) lives
+    // in buffer (roles >> 3r) & 7 of Fall, Call, W1all, W2all, Pall.
+    int roles = 0 | (1 << 3) | (2 << 6) | (3 << 9) | (4 << 12);
+    auto buf = [&](int r) -> double* {
+      const int b = (roles >> (3 * r)) & 7;
+      double* base = b == 0 ? Fall : b == 1 ? Call : b == 2 ? W1all : b == 3 ? W2all : Pall;
+      return base + m.mat_off;
+    };
+    auto trade = [&](int r1, int r2) {
+      const int b1 = (roles >> (3 * r1)) & 7, b2 = (roles >> (3 * r2)) & 7;
+      roles &= ~((7 << (3 * r1)) | (7 << (3 * r2)));
+      roles |= (b2 << (3 * r1)) | (b1 << (3 * r2));
+    };
+    constexpr int kRF = 0, kRC = 1, kRW1 = 2, kRW2 = 3, kRP = 4;
     double* P = Pall + m.mat_off;
     double* F = Fall + m.mat_off;
     double* Ct = Call + m.mat_off;
@@ -464,21 +479,35 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_scf(const MolDev* __restrict
 #endif
     int nfull = 0, nsweeps = 0;
     for (it = 1; it <= sp.max_iter; ++it) {
+      F = buf(kRF);
+      Ct = buf(kRC);
+      W1 = buf(kRW1);
+      W2 = buf(kRW2);
+      P = buf(kRP);
       long long t0 = clock64();
       const double E = build_fock(m, atoms, elems, pairs, ints, hh_pairs, jbuf, H, P, F, sh.red, sh.fockw, fprof);
       __syncthreads();
       long long t1 = clock64();
       cyc[0] += t1 - t0;
       const double* Fx = diis_step(N, F, P, W1, W2, histF, histE, msize, nhist, head, sh, dprof);
-      // Fx lives in F or W2; move it to F so W1/W2 are free as scratch
+      // Fx lives in F or W2: when in W2, F and W2 trade buffers
       if (Fx != F) {
-        for (size_t k = tid; k < NN; k += blockDim.x) F[k] = W2[k];
-        __syncthreads();
+        trade(kRF, kRW2);
+        F = buf(kRF);
+        W2 = buf(kRW2);
       }
       long long t2 = clock64();
       cyc[1] += t2 - t1;
       int need_full = !have_orbitals;
-      if (mode != kEigExact && have_orbitals) need_full = ov_rotation(N, no, F, Ct, W1, W2, eps, drift, sh, oprof);
+      if (mode != kEigExact && have_orbitals) {
+        int sw = 0;
+        need_full = ov_rotation(N, no, F, Ct, W1, W2, eps, drift, sh, oprof, &sw);
+        if (sw & 1) trade(kRC, kRF);
+        if (sw & 2) trade(kRC, kRW2);
+        F = buf(kRF);
+        Ct = buf(kRC);
+        W2 = buf(kRW2);
+      }
       if (mode == kEigExact || (need_full && mode == kEigHybrid)) {
         // exact: every iteration the lowest eigenvalues and the occupied
         // eigenvectors of the extrapolated F; hybrid: every eigenpair at the
@@ -514,15 +543,17 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_scf(const MolDev* __restrict
       }
       long long t4 = clock64();
       cyc[3] += t4 - t3;
-      // new density P = 2 C_occ C_occ^T = 2 Ct_o^T Ct_o into W1, rms change against P
+      // new density P = 2 C_occ C_occ^T = 2 Ct_o^T Ct_o into W1, rms change
+      // against P; then P and W1 trade buffers
       cta_gemm(N, N, no, 2.0, Ct, N, true, Ct, N, false, 0.0, W1, N, sh.gemm, true);
       double d2 = 0;
+#pragma unroll 4
       for (size_t k = tid; k < NN; k += blockDim.x) {
         const double d = W1[k] - P[k];
         d2 += d * d;
-        P[k] = W1[k];
       }
       d2 = cta_sum(d2, sh.red);
+      trade(kRP, kRW1);
       const double rms = sqrt(d2 / (double)NN);
       last_rms = rms;
       last_dE = it > 1 ? fabs(E - Eold) : 0.0;
@@ -535,6 +566,32 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_scf(const MolDev* __restrict
     }
     if (it > sp.max_iter) it = sp.max_iter;
     __syncthreads();
+    // Back to the home buffers: the density to Pall's (the gradient kernels
+    // read it), the orbitals to Call's (the canonical-orbital kernel reads
+    // them); the final Fock matrix is built in Fall's.  W1's buffer holds
+    // nothing live and takes the orbitals when they sit in the density's.
+    {
+      double* const bP = Pall + m.mat_off;
+      double* const bC = Call + m.mat_off;
+      P = buf(kRP);
+      Ct = buf(kRC);
+      if (P != bP) {
+        if (Ct == bP) {
+          W1 = buf(kRW1);
+          for (size_t k = tid; k < NN; k += blockDim.x) W1[k] = Ct[k];
+          __syncthreads();
+          Ct = W1;
+        }
+        for (size_t k = tid; k < NN; k += blockDim.x) bP[k] = P[k];
+        __syncthreads();
+      }
+      if (Ct != bC) {
+        for (size_t k = tid; k < NN; k += blockDim.x) bC[k] = Ct[k];
+        __syncthreads();
+      }
+      P = bP;
+      F = Fall + m.mat_off;
+    }
     const double Efin = build_fock(m, atoms, elems, pairs, ints, hh_pairs, jbuf, H, P, F, sh.red, sh.fockw);
     if (tid == 0) {
       MolResult& r = res[mi];

@@ -736,8 +736,13 @@ __device__ int full_diagonalise(int N, double* F, double* Ct, double* W1, double
 // prof (optional): cycles of C^T F with the diagonal, the X step and its
 // quadratic terms, the rotation product, the re-orthonormalisation added to
 // prof[0..3].
+// swaps (optional): instead of copying the rotated orbitals back into Ct, the
+// function leaves them where the product put them and reports it: bit 0 set
+// when they moved to F's buffer (Ct's buffer is then free for F's role), bit 1
+// when a re-orthonormalisation then moved them on to W2's buffer (the caller
+// exchanges the buffer roles in that order).
 __device__ int ov_rotation(int N, int no, double* F, double* Ct, double* W1, double* W2, double* eps, double& drift,
-                           ScfShared& sh, long long* prof = nullptr) {
+                           ScfShared& sh, long long* prof = nullptr, int* swaps = nullptr) {
   const int nv = N - no;
   const size_t NN = (size_t)N * N;
   const int tid = threadIdx.x;
@@ -790,8 +795,15 @@ __device__ int ov_rotation(int N, int no, double* F, double* Ct, double* W1, dou
   __syncthreads();
   prof_mark(prof, 1, tprof);
   cta_gemm(N, N, N, 1.0, W1, N, false, Ct, N, false, 0.0, F, N, sh.gemm);
-  for (size_t e = tid; e < NN; e += blockDim.x) Ct[e] = F[e];
-  __syncthreads();
+  if (swaps) {
+    double* t = Ct;
+    Ct = F;
+    F = t;
+    *swaps |= 1;
+  } else {
+    for (size_t e = tid; e < NN; e += blockDim.x) Ct[e] = F[e];
+    __syncthreads();
+  }
   prof_mark(prof, 2, tprof);
   // the second-order rotation is orthogonal up to |K|^4 / 4: re-orthonormalise when needed
   drift += 0.25 * xmax * xmax * xmax * xmax;
@@ -803,8 +815,12 @@ __device__ int ov_rotation(int N, int no, double* F, double* Ct, double* W1, dou
     __syncthreads();
     cta_gemm(N, N, N, -0.5, Ct, N, false, Ct, N, true, 1.0, W1, N, sh.gemm, true);
     cta_gemm(N, N, N, 1.0, W1, N, false, Ct, N, false, 0.0, W2, N, sh.gemm);
-    for (size_t e = tid; e < NN; e += blockDim.x) Ct[e] = W2[e];
-    __syncthreads();
+    if (swaps) {
+      *swaps |= 2;
+    } else {
+      for (size_t e = tid; e < NN; e += blockDim.x) Ct[e] = W2[e];
+      __syncthreads();
+    }
     drift = 0;
     prof_mark(prof, 3, tprof);
   }
