@@ -278,6 +278,21 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_dftb_scf(
     double* Ct = Call + m.mat_off;
     double* W1 = W1all + m.mat_off;
     double* W2 = W2all + m.mat_off;
+    // The buffers of F, C, W1, W2 and P trade roles during the SCF instead of
+    // being copied into each other: role r lives in buffer (roles >> 3r) & 7
+    // of Fall, Call, W1all, W2all, Pall.
+    int roles = 0 | (1 << 3) | (2 << 6) | (3 << 9) | (4 << 12);
+    auto buf = [&](int r) -> double* {
+      const int b = (roles >> (3 * r)) & 7;
+      double* base = b == 0 ? Fall : b == 1 ? Call : b == 2 ? W1all : b == 3 ? W2all : Pall;
+      return base + m.mat_off;
+    };
+    auto trade = [&](int r1, int r2) {
+      const int b1 = (roles >> (3 * r1)) & 7, b2 = (roles >> (3 * r2)) & 7;
+      roles &= ~((7 << (3 * r1)) | (7 << (3 * r2)));
+      roles |= (b2 << (3 * r1)) | (b1 << (3 * r2));
+    };
+    constexpr int kRF = 0, kRC = 1, kRW1 = 2, kRW2 = 3, kRP = 4;
     double* eps = epsall + m.ao_base;
     double* histF = diisall + m.diis_off;
     double* histE = histF + (size_t)kDiisMax * NN;
@@ -301,6 +316,11 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_dftb_scf(
     bool have_orbitals = false;
     double drift = 0, Eold = 0, last_dE = 0, last_rms = 0;
     for (it = 1; it <= sp.max_iter && status == kDevOk; ++it) {
+      F = buf(kRF);
+      Ct = buf(kRC);
+      W1 = buf(kRW1);
+      W2 = buf(kRW2);
+      P = buf(kRP);
       const double e23 = charges_and_shifts(m, order, atoms, el, P, S, gm, Gm, W2, q, sh4, sh.red);
       const double eb = dftb_fock(m, ao_atom, H0, S, P, sh4, F, sh.red);
       const double E = eb + e23;
@@ -309,13 +329,22 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_dftb_scf(
       cta_gemm(N, N, N, 1.0, X, N, false, W1, N, false, 0.0, F, N, sh.gemm);
       if (have_orbitals) {
         const double* Fx = diis_step(N, F, Pp, W1, W2, histF, histE, msize, nhist, head, sh);
-        if (Fx != F) {
-          for (size_t k = tid; k < NN; k += blockDim.x) F[k] = W2[k];
-          __syncthreads();
+        if (Fx != F) {  // F and W2 trade buffers
+          trade(kRF, kRW2);
+          F = buf(kRF);
+          W2 = buf(kRW2);
         }
       }
       int need_full = !have_orbitals;
-      if (have_orbitals) need_full = ov_rotation(N, no, F, Ct, W1, W2, eps, drift, sh);
+      if (have_orbitals) {
+        int sw = 0;
+        need_full = ov_rotation(N, no, F, Ct, W1, W2, eps, drift, sh, nullptr, &sw);
+        if (sw & 1) trade(kRC, kRF);
+        if (sw & 2) trade(kRC, kRW2);
+        F = buf(kRF);
+        Ct = buf(kRC);
+        W2 = buf(kRW2);
+      }
       if (need_full && scf_eig_mode(sp, N) != kEigRotation) {
         // every eigenpair of F' by the tridiagonal solver; the rotations take over
         need_full = eigh_tridiag(N, F, N, N, Ct, N, eps, sh.gemm, eig_workspace_doubles(sh, smem_raw), W2, W1, Ct, F,
@@ -343,12 +372,13 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_dftb_scf(
       cta_gemm(N, N, N, 1.0, X, N, false, Pp, N, false, 0.0, W1, N, sh.gemm);
       cta_gemm(N, N, N, 1.0, W1, N, false, X, N, false, 0.0, W2, N, sh.gemm, true);
       double d2 = 0;
+#pragma unroll 4
       for (size_t k = tid; k < NN; k += blockDim.x) {
         const double d = W2[k] - P[k];
         d2 += d * d;
-        P[k] = W2[k];
       }
       d2 = cta_sum(d2, sh.red);
+      trade(kRP, kRW2);  // the new density's buffer becomes P's
       const double rms = sqrt(d2 / (double)NN);
       last_rms = rms;
       last_dE = it > 1 ? fabs(E - Eold) : 0.0;
@@ -366,6 +396,36 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_dftb_scf(
     }
     if (it > sp.max_iter) it = sp.max_iter;
     __syncthreads();
+    // Back to the home buffers: the density to Pall's, the orbitals to
+    // Call's (the canonical-orbital and TD-DFTB kernels read them); F, W1 and
+    // W2 take theirs for the closing products (the gradient reads W1's).
+    // W2's buffer holds nothing live and takes the orbitals when they sit in
+    // the density's.
+    {
+      double* const bP = Pall + m.mat_off;
+      double* const bC = Call + m.mat_off;
+      P = buf(kRP);
+      Ct = buf(kRC);
+      if (P != bP) {
+        if (Ct == bP) {
+          W2 = buf(kRW2);
+          for (size_t k = tid; k < NN; k += blockDim.x) W2[k] = Ct[k];
+          __syncthreads();
+          Ct = W2;
+        }
+        for (size_t k = tid; k < NN; k += blockDim.x) bP[k] = P[k];
+        __syncthreads();
+      }
+      if (Ct != bC) {
+        for (size_t k = tid; k < NN; k += blockDim.x) bC[k] = Ct[k];
+        __syncthreads();
+      }
+      P = bP;
+      Ct = bC;
+      F = Fall + m.mat_off;
+      W1 = W1all + m.mat_off;
+      W2 = W2all + m.mat_off;
+    }
     // final charges, Fock matrix and energy of the converged density; W = 1/2 P F P into W1
     const double e23 = charges_and_shifts(m, order, atoms, el, P, S, gm, Gm, W2, q, sh4, sh.red);
     const double eb = dftb_fock(m, ao_atom, H0, S, P, sh4, F, sh.red);

@@ -753,6 +753,7 @@ __device__ int ov_rotation(int N, int no, double* F, double* Ct, double* W1, dou
     const int lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
     for (int k = warp; k < N; k += nwarps) {
       double s = 0;
+#pragma unroll 4
       for (int nu = lane; nu < N; nu += 32) s += W1[(size_t)k * N + nu] * Ct[(size_t)k * N + nu];
       s = warp_sum(s);
       if (lane == 0) eps[k] = s;
@@ -772,6 +773,7 @@ __device__ int ov_rotation(int N, int no, double* F, double* Ct, double* W1, dou
   double* X = W2;
   cta_gemm(nv, no, N, 1.0, Ct + (size_t)no * N, N, false, W1, N, true, 0.0, X, no, sh.gemm);
   double xmax = 0;
+#pragma unroll 4
   for (int e = tid; e < nv * no; e += blockDim.x) {
     const int a = e / no, i = e % no;
     double d = eps[i] - eps[no + a];
@@ -786,6 +788,7 @@ __device__ int ov_rotation(int N, int no, double* F, double* Ct, double* W1, dou
   //   M = [[I - X^T X / 2, X^T], [-X, I - X X^T / 2]], assembled in W1
   cta_gemm(no, no, nv, -0.5, X, no, true, X, no, false, 0.0, W1, N, sh.gemm, true);
   cta_gemm(nv, nv, no, -0.5, X, no, false, X, no, true, 0.0, W1 + (size_t)no * N + no, N, sh.gemm, true);
+#pragma unroll 4
   for (int e = tid; e < nv * no; e += blockDim.x) {
     const int a = e / no, i = e % no;
     W1[(size_t)i * N + no + a] = X[e];
