@@ -27,3 +27,41 @@ extern "C" int tc_gemm_tile_n(int Np) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   return sgb::tc::pick_bn(Np, sms);
 }
+
+namespace {
+
+// One thread waits with the GEMM's bounded barrier wait (sgb::tc::mbar_wait)
+// on a fresh barrier.  arrive = 0: nothing ever arrives, so the wait must
+// give up after its limit and report it; arrive = 1: the thread arrives
+// first, so the wait must succeed at once.  out[0] = 1 when the wait
+// succeeded, out[1] = milliseconds spent waiting.
+__global__ void k_wait_probe(int arrive, unsigned* out) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    sgb::tc::mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (arrive)
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sgb::tc::smem_u32(&bar)) : "memory");
+    const unsigned long long t0 = sgb::tc::global_ns();
+    const bool ok = sgb::tc::mbar_wait(&bar, 0);
+    const unsigned long long t1 = sgb::tc::global_ns();
+    out[0] = ok ? 1u : 0u;
+    out[1] = (unsigned)((t1 - t0) / 1000000ull);
+  }
+}
+
+}  // namespace
+
+// out: two device words.  Returns 0 or the CUDA error code.
+extern "C" int tc_wait_probe(int arrive, unsigned* out) {
+  k_wait_probe<<<1, 32>>>(arrive, out);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  return (int)e;
+}
+
+// The bounded wait's limit in milliseconds.
+extern "C" int tc_wait_limit_ms() { return (int)(sgb::tc::kWaitLimitNs / 1000000ull); }

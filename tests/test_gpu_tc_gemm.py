@@ -4,7 +4,9 @@ terms, through the test harness library tests/csrc/libtc_gemm_probe.so.
 
 C = sum_s T[a_s] T[b_s]^T over stacked Np x Np BF16 terms.  FP32
 accumulation of BF16 products: each entry within 1e-5 of the sum of the
-absolute products (plus 1e-30)."""
+absolute products (plus 1e-30).  The kernel's bounded barrier wait is
+checked on its own: a wait that nothing completes gives up after its limit
+and reports it, with the context still usable."""
 import ctypes
 import os
 import subprocess
@@ -103,3 +105,36 @@ def test_split_of_symmetric_matrix_reproduces_its_square():
     assert err == 0
     X2 = A + A.T
     assert np.max(np.abs(X2 - X @ X)) < 1e-5
+
+
+def _wait_probe(arrive):
+    import torch
+    L = _lib()
+    out = torch.zeros(2, dtype=torch.int32, device="cuda")
+    rc = L.tc_wait_probe(arrive, ctypes.c_void_p(out.data_ptr()))
+    assert rc == 0, "tc_wait_probe returned CUDA error %d" % rc
+    ok, ms = (int(v) for v in out.cpu())
+    return ok, ms
+
+
+@pytest.mark.gpu
+def test_bounded_barrier_wait_gives_up_and_reports():
+    """The GEMM's barrier waits are bounded: a wait on a barrier nothing
+    arrives at returns 'not completed' after the limit instead of spinning
+    for ever, and the context stays usable (a product right after it is
+    exact).  A wait whose arrival came first returns at once."""
+    import torch
+    L = _lib()
+    limit = L.tc_wait_limit_ms()
+    ok, ms = _wait_probe(0)
+    assert ok == 0
+    assert limit <= ms <= limit + 2000, (ms, limit)
+    ok, ms = _wait_probe(1)
+    assert ok == 1 and ms < 100
+    Np = 128
+    g = torch.Generator(device="cpu").manual_seed(11)
+    T = torch.randn((2, Np, Np), generator=g, dtype=torch.float64).to(torch.bfloat16).cuda()
+    C, err = run_gemm(T, [0], [1])
+    assert err == 0
+    ref, absref = reference(T, [0], [1])
+    assert np.all(np.abs(C - ref) <= 1e-5 * absref + 1e-30)
