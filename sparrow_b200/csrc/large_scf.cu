@@ -29,6 +29,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "engine.h"
@@ -366,16 +367,35 @@ namespace {
 struct LargeHost {
   double* hp = nullptr;
   cudaEvent_t ev[2] = {nullptr, nullptr};
-  // timing events around the purification products of one SCF iteration
-  std::vector<cudaEvent_t> pev;
   ~LargeHost() {
     if (hp) cudaFreeHost(hp);
     for (auto& e : ev)
       if (e) cudaEventDestroy(e);
-    for (auto& e : pev)
-      if (e) cudaEventDestroy(e);
   }
 };
+
+// Timing events around the purification products of one SCF iteration
+// (two per product), created once per host thread and device and reused by
+// every later call.
+const std::vector<cudaEvent_t>* product_events(cudaError_t& ce) {
+  thread_local std::unordered_map<int, std::vector<cudaEvent_t>> per_device;
+  int dev = 0;
+  ce = cudaGetDevice(&dev);
+  if (ce != cudaSuccess) return nullptr;
+  std::vector<cudaEvent_t>& ev = per_device[dev];
+  if (!ev.empty()) return &ev;
+  for (int k = 0; k < 2 * kSp2MaxSteps; ++k) {
+    cudaEvent_t e = nullptr;
+    ce = cudaEventCreate(&e);
+    if (ce != cudaSuccess) {
+      for (auto& x : ev) cudaEventDestroy(x);
+      ev.clear();
+      return nullptr;
+    }
+    ev.push_back(e);
+  }
+  return &ev;
+}
 
 const char* blas_message(cublasStatus_t st) {
   switch (st) {
@@ -439,13 +459,12 @@ int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, in
   cudaError_t ce = cudaMallocHost(&hb.hp, sizeof(double) * 2 * (kSp2MaxSteps + 2));
   if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&hb.ev[0], cudaEventDisableTiming);
   if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&hb.ev[1], cudaEventDisableTiming);
-  hb.pev.assign(2 * kSp2MaxSteps, nullptr);
-  for (auto& e : hb.pev)
-    if (ce == cudaSuccess) ce = cudaEventCreate(&e);
-  if (ce != cudaSuccess) {
+  const std::vector<cudaEvent_t>* pevp = ce == cudaSuccess ? product_events(ce) : nullptr;
+  if (ce != cudaSuccess || !pevp) {
     err = cuda_message(ce);
     return kErrCuda;
   }
+  const std::vector<cudaEvent_t>& pev = *pevp;
   const double one = 1.0, zero = 0.0;
   const int msize = sp.diis_size < 1 ? 1 : (sp.diis_size > kDiisMax ? kDiisMax : sp.diis_size);
   double bmat[kDiisMax * kDiisMax] = {};
@@ -509,9 +528,9 @@ int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, in
       double* cur = st + kSlotTraces + 2 * k;
       if (use_mixed) {
         k_split_terms<<<grid, kLT, 0, s>>>(X, N, Np, T);
-        cudaEventRecord(hb.pev[2 * k], s);
+        cudaEventRecord(pev[2 * k], s);
         ce = tc::gemm_terms(T, kTerms, Np, a_terms, b_terms, 4, C32, Np, tc_err, s, err);
-        cudaEventRecord(hb.pev[2 * k + 1], s);
+        cudaEventRecord(pev[2 * k + 1], s);
         if (ce != cudaSuccess) {
           if (err.empty()) err = cuda_message(ce);
           return kErrCuda;
@@ -521,9 +540,9 @@ int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, in
       } else {
         // X X = X X^T: half the flops of a GEMM; the column-major lower
         // triangle is the row-major upper one
-        cudaEventRecord(hb.pev[2 * k], s);
+        cudaEventRecord(pev[2 * k], s);
         bs = cublasDsyrk(h, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, N, N, &one, X, N, &zero, X2, N);
-        cudaEventRecord(hb.pev[2 * k + 1], s);
+        cudaEventRecord(pev[2 * k + 1], s);
         k_sp2_step_upper<<<tgrid, tblock, 0, s>>>(X, X2, N, nocc, cur, cur + 2);
         ++nl;
       }
@@ -557,7 +576,7 @@ int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, in
     if (ce != cudaSuccess) return fail_cuda(ce);
     for (int k = 0; k < nprod; ++k) {
       float ms = 0;
-      if (cudaEventElapsedTime(&ms, hb.pev[2 * k], hb.pev[2 * k + 1]) == cudaSuccess) {
+      if (cudaEventElapsedTime(&ms, pev[2 * k], pev[2 * k + 1]) == cudaSuccess) {
         prod_ms[use_mixed ? 0 : 1] += ms;
         ++prod_n[use_mixed ? 0 : 1];
       }

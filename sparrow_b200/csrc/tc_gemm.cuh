@@ -1,6 +1,6 @@
 // BF16 tensor-core GEMM for sm_100a: tcgen05.mma with the FP32 accumulator in
 // tensor memory, operand tiles brought into shared memory by TMA
-// (cp.async.bulk.tensor, 128-byte swizzle), one CTA per output tile.
+// (cp.async.bulk.tensor, 128-byte swizzle); persistent, one CTA per SM.
 //
 //   C[i][j] = sum_s sum_c T[a_term[s]][i][c] * T[b_term[s]][j][c]
 //
@@ -14,9 +14,9 @@
 // Warp roles (192 threads): warp 0 issues the TMA loads into a ring of
 // STAGES shared-memory stages, warp 1 owns the tensor-memory allocation and
 // issues the MMAs (one elected thread; each stage is released back to the
-// producer by tcgen05.commit on its "empty" barrier), warps 2-5 read the
-// accumulator back with tcgen05.ld (each warp the 32 lanes of its quarter)
-// and store it.  Every barrier wait is bounded (kWaitLimitNs): a wait that
+// producer by tcgen05.commit on its "empty" barrier) into one of two
+// accumulators, warps 2-5 read the other accumulator back with tcgen05.ld
+// (each warp the 32 lanes of its quarter) and store it.  Every barrier wait is bounded (kWaitLimitNs): a wait that
 // runs out sets a bit in the caller's error word, the thread stops issuing,
 // the producer first waits (bounded) for its own loads in flight, and the
 // CTA still frees its tensor memory before it returns.
@@ -154,50 +154,66 @@ struct Layout {
   static constexpr int kBBytes = BN * kBK * 2;
   static constexpr int kStage = kABytes + kBBytes;
   static constexpr int kBarOff = STAGES * kStage;
-  // ring, then full[STAGES], empty[STAGES], acc, tensor-memory address
-  static constexpr int kBytes = kBarOff + (2 * STAGES + 1) * 8 + 16;
+  // ring, then full[STAGES], empty[STAGES], acc_full[2], acc_empty[2],
+  // tensor-memory address
+  static constexpr int kBytes = kBarOff + (2 * STAGES + 4) * 8 + 16;
   static constexpr int kDynamic = kBytes + 1024;  // slack for the 1024-byte alignment of the ring
+  static constexpr int kTmemCols = 2 * BN;        // two accumulators
+  static_assert(kTmemCols <= 512, "tensor memory columns");
 };
 
-// One output tile per CTA.  Tiles are rastered in groups of kGroupM tile rows
-// (column by column inside a group) so the CTAs of one wave share A and B
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Output tile t of the grouped raster: groups of kGroupM tile rows, column by
+// column inside a group, so the CTAs working at the same time share A and B
 // panels in L2.
+__device__ __forceinline__ void tile_coords(int t, int mtiles, int ntiles, int& mt, int& nt) {
+  constexpr int kGroupM = 16;
+  const int per_group = kGroupM * ntiles;
+  const int g = t / per_group, first_m = g * kGroupM;
+  const int gm = min(mtiles - first_m, kGroupM);
+  mt = first_m + (t % per_group) % gm;
+  nt = (t % per_group) / gm;
+}
+
+// Persistent: CTA b takes tiles b, b + gridDim.x, ...  The load ring runs on
+// across tiles; the accumulator alternates between two tensor-memory buffers,
+// so the epilogue of one tile overlaps the main loop of the next (acc_full[b]:
+// the MMAs of a tile into buffer b are complete; acc_empty[b]: the four
+// epilogue warps have read buffer b out).
 template <int BN, int STAGES>
 __global__ void __launch_bounds__(kThreads, 1)
     k_tc_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, float* __restrict__ C,
                    int ldc, int ncols, int mtiles, int ntiles, const __grid_constant__ Segments seg,
                    unsigned* __restrict__ err) {
   using L = Layout<BN, STAGES>;
-  constexpr int kGroupM = 16;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + L::kBarOff);
   uint64_t* empty = full + STAGES;
-  uint64_t* accf = empty + STAGES;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(accf + 1);
+  uint64_t* accf = empty + STAGES;  // [2]
+  uint64_t* acce = accf + 2;        // [2]
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(acce + 2);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-
-  // grouped raster of the linear block index
-  const int bid = blockIdx.x;
-  const int per_group = kGroupM * ntiles;
-  const int g = bid / per_group, first_m = g * kGroupM;
-  const int gm = min(mtiles - first_m, kGroupM);
-  const int mt = first_m + (bid % per_group) % gm;
-  const int nt = (bid % per_group) / gm;
-  const int m0 = mt * kBM, n0 = nt * BN;
+  const int total = mtiles * ntiles;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
-    mbar_init(accf, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&accf[b], 1);
+      mbar_init(&acce[b], 4);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
-                 "r"(BN)
+                 "r"(L::kTmemCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -209,76 +225,107 @@ __global__ void __launch_bounds__(kThreads, 1)
 
   if (warp == 0) {
     if (lane == 0) {
-      int issued = 0;
+      long long issued = 0;
       bool ok = true;
-      for (int kb = 0; kb < nk; ++kb) {
-        const int s = kb % STAGES;
-        const unsigned ph = (kb / STAGES) & 1;
-        if (!mbar_wait(&empty[s], ph ^ 1u)) {
-          atomicOr(err, kErrEmpty);
-          ok = false;
-          break;
+      for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
+        int mt, nt;
+        tile_coords(t, mtiles, ntiles, mt, nt);
+        const int m0 = mt * kBM, n0 = nt * BN;
+        for (int kb = 0; kb < nk; ++kb) {
+          const int s = (int)(issued % STAGES);
+          const unsigned ph = (unsigned)((issued / STAGES) & 1);
+          if (!mbar_wait(&empty[s], ph ^ 1u)) {
+            atomicOr(err, kErrEmpty);
+            ok = false;
+            break;
+          }
+          uint8_t* sa = smem + s * L::kStage;
+          uint8_t* sb = sa + L::kABytes;
+          const int sg = kb / seg.kb_per_seg, kx = (kb % seg.kb_per_seg) * kBK;
+          mbar_expect_tx(&full[s], L::kStage);
+          tma_load_2d(sa, &ta, &full[s], kx, seg.a_row[sg] + m0);
+          tma_load_2d(sb, &tb, &full[s], kx, seg.b_row[sg] + n0);
+          ++issued;
         }
-        uint8_t* sa = smem + s * L::kStage;
-        uint8_t* sb = sa + L::kABytes;
-        const int sg = kb / seg.kb_per_seg, kx = (kb % seg.kb_per_seg) * kBK;
-        mbar_expect_tx(&full[s], L::kStage);
-        tma_load_2d(sa, &ta, &full[s], kx, seg.a_row[sg] + m0);
-        tma_load_2d(sb, &tb, &full[s], kx, seg.b_row[sg] + n0);
-        issued = kb + 1;
       }
       if (!ok) {
         // wait (bounded) for this thread's loads still in flight
-        for (int kb = issued - STAGES < 0 ? 0 : issued - STAGES; kb < issued; ++kb)
-          if (!mbar_wait(&full[kb % STAGES], (kb / STAGES) & 1)) atomicOr(err, kErrInflight);
+        for (long long q = issued - STAGES < 0 ? 0 : issued - STAGES; q < issued; ++q)
+          if (!mbar_wait(&full[q % STAGES], (unsigned)((q / STAGES) & 1))) atomicOr(err, kErrInflight);
       }
     }
   } else if (warp == 1) {
     if (lane == 0) {
       constexpr uint32_t idesc = instr_desc_bf16(BN);
-      for (int kb = 0; kb < nk; ++kb) {
-        const int s = kb % STAGES;
-        if (!mbar_wait(&full[s], (kb / STAGES) & 1)) {
-          atomicOr(err, kErrFull);
+      long long consumed = 0;
+      int i = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < total && ok; t += gridDim.x, ++i) {
+        const int b = i & 1;
+        // the epilogue has read buffer b out of its previous tile (none on first use)
+        if (!mbar_wait(&acce[b], (unsigned)(((i >> 1) & 1) ^ 1))) {
+          atomicOr(err, kErrAcc);
           break;
         }
         tc_fence_after();
-        const uint32_t a0 = smem_u32(smem + s * L::kStage);
-        const uint32_t b0 = a0 + L::kABytes;
+        const uint32_t acc = tmem + (uint32_t)(b * BN);
+        for (int kb = 0; kb < nk; ++kb) {
+          const int s = (int)(consumed % STAGES);
+          if (!mbar_wait(&full[s], (unsigned)((consumed / STAGES) & 1))) {
+            atomicOr(err, kErrFull);
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(smem + s * L::kStage);
+          const uint32_t b0 = a0 + L::kABytes;
 #pragma unroll
-        for (int k = 0; k < kBK / kUmmaK; ++k)
-          umma_bf16(tmem, smem_desc_sw128(a0 + k * kUmmaK * 2), smem_desc_sw128(b0 + k * kUmmaK * 2), idesc,
-                    (kb | k) != 0);
-        umma_commit(&empty[s]);
+          for (int k = 0; k < kBK / kUmmaK; ++k)
+            umma_bf16(acc, smem_desc_sw128(a0 + k * kUmmaK * 2), smem_desc_sw128(b0 + k * kUmmaK * 2), idesc,
+                      (kb | k) != 0);
+          umma_commit(&empty[s]);
+          ++consumed;
+        }
+        // buffer b complete (also on an early exit, so the epilogue is released)
+        umma_commit(&accf[b]);
       }
-      // always signal the epilogue once every issued MMA has completed
-      umma_commit(accf);
     }
   } else {
     const int q = warp & 3;  // tensor-memory lane quarter of this warp
-    const bool ready = __all_sync(0xffffffffu, mbar_wait(accf, 0));
-    if (!ready && lane == 0) atomicOr(err, kErrAcc);
-    tc_fence_after();
-    if (ready) {
-      const int row = m0 + q * 32 + lane;
+    int i = 0;
+    for (int t = blockIdx.x; t < total; t += gridDim.x, ++i) {
+      const int b = i & 1;
+      const bool ready = __all_sync(0xffffffffu, mbar_wait(&accf[b], (unsigned)((i >> 1) & 1)));
+      if (!ready) {
+        if (lane == 0) atomicOr(err, kErrAcc);
+        break;
+      }
+      tc_fence_after();
+      int mt, nt;
+      tile_coords(t, mtiles, ntiles, mt, nt);
+      const int row = mt * kBM + q * 32 + lane, n0 = nt * BN;
       float* crow = C + (size_t)row * ldc + n0;
 #pragma unroll 1
       for (int c0 = 0; c0 < BN; c0 += 32) {
         float v[32];
-        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, v);
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * BN + c0), v);
         if (n0 + c0 < ncols) {
           float4* dst = reinterpret_cast<float4*>(crow + c0);
 #pragma unroll
           for (int u = 0; u < 8; ++u) dst[u] = make_float4(v[4 * u], v[4 * u + 1], v[4 * u + 2], v[4 * u + 3]);
         }
       }
+      // this warp's reads of buffer b are done: hand it back to the MMA thread
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce[b]);
     }
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   if (warp == 1)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(BN) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(L::kTmemCols) : "memory");
 }
 
 inline PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
@@ -348,7 +395,7 @@ inline cudaError_t gemm_terms(const __nv_bfloat16* T, int nterms, int Np, const 
     return cudaErrorInvalidValue;
   }
   const int mtiles = Np / kBM, ntiles = (Np + bn - 1) / bn;
-  const int blocks = mtiles * ntiles;
+  const int blocks = mtiles * ntiles < sms ? mtiles * ntiles : sms;  // persistent: at most one CTA per SM
   cudaError_t e;
   if (bn == 256) {
     using Lt = Layout<256, 4>;
