@@ -178,11 +178,11 @@ class _Settings:
 
     _INT = ("molecular_charge", "spin_multiplicity", "max_scf_iterations")
     _REAL = ("self_consistence_criterion", "density_rmsd_criterion")
-    _STR = ("spin_mode", "scf_mixer", "method_parameters")
+    _STR = ("spin_mode", "scf_mixer", "method_parameters", "scf_path")
 
     def __init__(self, calc):
         self._calc = calc
-        self._str = {"spin_mode": "any", "scf_mixer": "diis", "method_parameters": ""}
+        self._str = {"spin_mode": "any", "scf_mixer": "diis", "method_parameters": "", "scf_path": "auto"}
 
     def __setitem__(self, key, value):
         L, h = lib(), self._calc._h

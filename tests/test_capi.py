@@ -50,6 +50,13 @@ def test_settings_round_trip_and_validation():
         c.settings["scf_mixer"] = "ediis"
     with pytest.raises(KeyError):
         c.settings["no_such_key"] = 1
+    assert c.settings["scf_path"] == "auto"
+    for path in ("batched", "large", "large_mixed", "auto"):
+        c.settings["scf_path"] = path
+        assert c.settings["scf_path"] == path
+    with pytest.raises(sparrow_b200.SparrowError):
+        c.settings["scf_path"] = "fast"
+    assert c.settings["scf_path"] == "auto"
 
 
 def test_empty_structure_and_bad_input_fail_on_host():
