@@ -545,13 +545,9 @@ __global__ void __launch_bounds__(kScfThreads, 1) k_scf(const MolDev* __restrict
       cyc[3] += t4 - t3;
       // new density P = 2 C_occ C_occ^T = 2 Ct_o^T Ct_o into W1, rms change
       // against P; then P and W1 trade buffers
-      cta_gemm(N, N, no, 2.0, Ct, N, true, Ct, N, false, 0.0, W1, N, sh.gemm, true);
+      // (the squared change against P is summed in the product's epilogue)
       double d2 = 0;
-#pragma unroll 4
-      for (size_t k = tid; k < NN; k += blockDim.x) {
-        const double d = W1[k] - P[k];
-        d2 += d * d;
-      }
+      cta_gemm<true>(N, N, no, 2.0, Ct, N, true, Ct, N, false, 0.0, W1, N, sh.gemm, true, P, &d2);
       d2 = cta_sum(d2, sh.red);
       trade(kRP, kRW1);
       const double rms = sqrt(d2 / (double)NN);

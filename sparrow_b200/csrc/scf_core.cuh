@@ -105,9 +105,15 @@ __device__ __forceinline__ void dmma_16x8x8(double (&c)[4], const double (&a)[4]
 
 // sym: the result is known to be symmetric (M == Nn): only the tiles on or
 // above the diagonal are computed, off-diagonal tiles are mirrored.
+// kDiff: the epilogue also adds to *diff2 this thread's share of the squared
+// difference sum_ij (C_ij - ref_ij)^2 over the whole result (a mirrored entry
+// counts twice, so ref must be symmetric when sym is set), sparing a pass
+// over C and ref.
+template <bool kDiff = false>
 __device__ __forceinline__ void cta_gemm(int M, int Nn, int K, double alpha, const double* __restrict__ A, int lda, bool tA,
                          const double* __restrict__ B, int ldb, bool tB, double beta, double* C, int ldc,
-                         double* smem, bool sym = false) {
+                         double* smem, bool sym = false, const double* __restrict__ ref = nullptr,
+                         double* diff2 = nullptr) {
   const int grp = threadIdx.x / kGemmGroup, tid = threadIdx.x % kGemmGroup;
   const int lane = tid & 31, warp = tid >> 5;
   const int wm = warp >> 1, wn = warp & 1;
@@ -207,6 +213,10 @@ __device__ __forceinline__ void cta_gemm(int M, int Nn, int K, double alpha, con
           const double v = beta == 0.0 ? alpha * acc[j][q] : alpha * acc[j][q] + beta * (*c);
           *c = v;
           if (sym && tn > tm) C[(size_t)gn * ldc + gm] = v;
+          if (kDiff) {
+            const double d = v - ref[(size_t)gm * ldc + gn];
+            *diff2 += (sym && tn > tm ? 2.0 : 1.0) * d * d;
+          }
         }
       }
   }
