@@ -149,17 +149,19 @@ __global__ void __launch_bounds__(kLT) k_sp2_step_upper(double* X, const double*
 }
 
 // The same step when the product is X X = A + A^T (A in FP32 from the
-// split-BF16 GEMM, leading dimension lda); 32 x 32 tiles (block 32 x 8), the
-// mirror tile of A read through shared memory.
-__global__ void __launch_bounds__(kLT) k_sp2_step_sym(double* X, const float* __restrict__ A, int lda, int N,
-                                                      double nocc, const double* __restrict__ cur, double* next) {
+// split-BF16 GEMM, leading dimension lda; A = A1 + A2 when the GEMM split its
+// K range, A2 null otherwise); 32 x 32 tiles (block 32 x 8), the mirror tile
+// of A read through shared memory.
+__global__ void __launch_bounds__(kLT) k_sp2_step_sym(double* X, const float* __restrict__ A,
+                                                      const float* __restrict__ A2, int lda, int N, double nocc,
+                                                      const double* __restrict__ cur, double* next) {
   __shared__ float tile[32][33];
   const double tr = cur[0], tr2 = cur[1];
   const int square = fabs(tr2 - nocc) < fabs(2.0 * tr - tr2 - nocc);
   const int i0 = blockIdx.y * 32, j0 = blockIdx.x * 32, tx = threadIdx.x, ty = threadIdx.y;
   for (int r = ty; r < 32; r += 8) {
     const int i = j0 + r, j = i0 + tx;
-    tile[r][tx] = (i < N && j < N) ? A[(size_t)i * lda + j] : 0.0f;
+    tile[r][tx] = (i < N && j < N) ? A[(size_t)i * lda + j] + (A2 ? A2[(size_t)i * lda + j] : 0.0f) : 0.0f;
   }
   __syncthreads();
   double t = 0, t2 = 0;
@@ -167,7 +169,8 @@ __global__ void __launch_bounds__(kLT) k_sp2_step_sym(double* X, const float* __
     const int i = i0 + r, j = j0 + tx;
     if (i >= N || j >= N) continue;
     const size_t k = (size_t)i * N + j;
-    const double x2 = (double)A[(size_t)i * lda + j] + (double)tile[tx][r];
+    const size_t ka = (size_t)i * lda + j;
+    const double x2 = (double)A[ka] + (A2 ? (double)A2[ka] : 0.0) + (double)tile[tx][r];
     const double x = square ? x2 : 2.0 * X[k] - x2;
     X[k] = x;
     t2 += x * x;
@@ -357,7 +360,7 @@ int padded_order(long long nao) { return (int)((nao + tc::kBM - 1) / tc::kBM * t
 
 size_t large_scf_scratch_bytes(long long nao) {
   const size_t NP = (size_t)padded_order(nao) * padded_order(nao);
-  return kStateBytes + align256(kTerms * NP * 2) + align256(NP * 4);
+  return kStateBytes + align256(kTerms * NP * 2) + 2 * align256(NP * 4);
 }
 
 namespace {
@@ -447,6 +450,7 @@ int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, in
   const size_t NP = (size_t)Np * Np;
   __nv_bfloat16* T = reinterpret_cast<__nv_bfloat16*>(scr + kStateBytes);
   float* C32 = reinterpret_cast<float*>(scr + kStateBytes + align256(kTerms * NP * 2));
+  float* C32b = reinterpret_cast<float*>(scr + kStateBytes + align256(kTerms * NP * 2) + align256(NP * 4));
   unsigned* tc_err = reinterpret_cast<unsigned*>(st + kSlotTcErr);
   static const int a_terms[4] = {kTermX1, kTermX1, kTermX1, kTermX2};
   static const int b_terms[4] = {kTermX1h, kTermX2, kTermX3, kTermX2h};
@@ -529,13 +533,14 @@ int run_large_scf(const DeviceBatch& b, const MolDev& m, const ScfParams& sp, in
       if (use_mixed) {
         k_split_terms<<<grid, kLT, 0, s>>>(X, N, Np, T);
         cudaEventRecord(pev[2 * k], s);
-        ce = tc::gemm_terms(T, kTerms, Np, a_terms, b_terms, 4, C32, Np, tc_err, s, err);
+        int ksplit = 1;
+        ce = tc::gemm_terms(T, kTerms, Np, a_terms, b_terms, 4, C32, C32b, Np, tc_err, s, err, &ksplit);
         cudaEventRecord(pev[2 * k + 1], s);
         if (ce != cudaSuccess) {
           if (err.empty()) err = cuda_message(ce);
           return kErrCuda;
         }
-        k_sp2_step_sym<<<tgrid, tblock, 0, s>>>(X, C32, Np, N, nocc, cur, cur + 2);
+        k_sp2_step_sym<<<tgrid, tblock, 0, s>>>(X, C32, ksplit == 2 ? C32b : nullptr, Np, N, nocc, cur, cur + 2);
         nl += 3;
       } else {
         // X X = X X^T: half the flops of a GEMM; the column-major lower

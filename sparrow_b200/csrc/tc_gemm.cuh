@@ -178,16 +178,18 @@ __device__ __forceinline__ void tile_coords(int t, int mtiles, int ntiles, int& 
   nt = (t % per_group) / gm;
 }
 
-// Persistent: CTA b takes tiles b, b + gridDim.x, ...  The load ring runs on
-// across tiles; the accumulator alternates between two tensor-memory buffers,
-// so the epilogue of one tile overlaps the main loop of the next (acc_full[b]:
-// the MMAs of a tile into buffer b are complete; acc_empty[b]: the four
-// epilogue warps have read buffer b out).
+// Persistent: CTA b takes work units b, b + gridDim.x, ...  A unit is a
+// tile, or with ksplit = 2 half of a tile's K blocks (the first half's sum
+// goes to C, the second's to C2; the caller adds them).  The load ring runs
+// on across units; the accumulator alternates between two tensor-memory
+// buffers, so the epilogue of one unit overlaps the main loop of the next
+// (acc_full[b]: the MMAs of a unit into buffer b are complete; acc_empty[b]:
+// the four epilogue warps have read buffer b out).
 template <int BN, int STAGES>
 __global__ void __launch_bounds__(kThreads, 1)
     k_tc_gemm_bf16(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, float* __restrict__ C,
-                   int ldc, int ncols, int mtiles, int ntiles, const __grid_constant__ Segments seg,
-                   unsigned* __restrict__ err) {
+                   float* __restrict__ C2, int ksplit, int ldc, int ncols, int mtiles, int ntiles,
+                   const __grid_constant__ Segments seg, unsigned* __restrict__ err) {
   using L = Layout<BN, STAGES>;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -197,7 +199,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   uint64_t* acce = accf + 2;        // [2]
   uint32_t* tslot = reinterpret_cast<uint32_t*>(acce + 2);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int total = mtiles * ntiles;
+  const int total = mtiles * ntiles * ksplit;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
@@ -221,7 +223,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  const int nk = seg.nseg * seg.kb_per_seg;
+  const int nk = seg.nseg * seg.kb_per_seg / ksplit;  // K blocks per unit
 
   if (warp == 0) {
     if (lane == 0) {
@@ -229,9 +231,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       bool ok = true;
       for (int t = blockIdx.x; t < total && ok; t += gridDim.x) {
         int mt, nt;
-        tile_coords(t, mtiles, ntiles, mt, nt);
-        const int m0 = mt * kBM, n0 = nt * BN;
-        for (int kb = 0; kb < nk; ++kb) {
+        tile_coords(t / ksplit, mtiles, ntiles, mt, nt);
+        const int m0 = mt * kBM, n0 = nt * BN, kb0 = (t % ksplit) * nk;
+        for (int kb = kb0; kb < kb0 + nk; ++kb) {
           const int s = (int)(issued % STAGES);
           const unsigned ph = (unsigned)((issued / STAGES) & 1);
           if (!mbar_wait(&empty[s], ph ^ 1u)) {
@@ -302,9 +304,9 @@ __global__ void __launch_bounds__(kThreads, 1)
       }
       tc_fence_after();
       int mt, nt;
-      tile_coords(t, mtiles, ntiles, mt, nt);
+      tile_coords(t / ksplit, mtiles, ntiles, mt, nt);
       const int row = mt * kBM + q * 32 + lane, n0 = nt * BN;
-      float* crow = C + (size_t)row * ldc + n0;
+      float* crow = (t % ksplit ? C2 : C) + (size_t)row * ldc + n0;
 #pragma unroll 1
       for (int c0 = 0; c0 < BN; c0 += 32) {
         float v[32];
@@ -363,21 +365,36 @@ inline int pick_bn(int Np, int sms) {
   return eff(256) + 0.02 >= eff(128) ? 256 : 128;
 }
 
+// K split of the launch: 2 (with 256-wide tiles) when C2 is given and the
+// 256-wide tiles of Np number at most half the SMs, else 1.  Sizes that fill
+// the SMs only with 128-wide tiles run 256-wide tiles on half the K range each
+// instead: twice the arithmetic per byte loaded, the same number of CTAs.
+inline int pick_ksplit(int Np, int sms, int nseg, bool have_c2) {
+  const long long t256 = (long long)(Np / kBM) * ((Np + 255) / 256);
+  return have_c2 && (nseg * (Np / kBK)) % 2 == 0 && 2 * t256 <= sms ? 2 : 1;
+}
+
 // C (Np x Np, ldc) = the segment sum above over the stacked terms T
-// (nterms x Np x Np BF16).  Returns cudaSuccess or the launch error; err_msg
-// names a host-side failure.  *d_err (device word) collects the kernel's
-// bounded-wait bits; the caller clears and reads it.
+// (nterms x Np x Np BF16); with C2 (same shape, may be null) the launch may
+// split K in two, and then C + C2 is the product (*ksplit_out tells which:
+// 1 means C alone holds it).  Returns cudaSuccess or the launch error;
+// err_msg names a host-side failure.  *d_err (device word) collects the
+// kernel's bounded-wait bits; the caller clears and reads it.
 inline cudaError_t gemm_terms(const __nv_bfloat16* T, int nterms, int Np, const int* a_term, const int* b_term,
-                              int nseg, float* C, int ldc, unsigned* d_err, cudaStream_t s, std::string& err_msg) {
+                              int nseg, float* C, float* C2, int ldc, unsigned* d_err, cudaStream_t s,
+                              std::string& err_msg, int* ksplit_out = nullptr) {
   if (Np <= 0 || Np % kBM != 0 || nseg < 1 || nseg > kMaxSeg || ldc < Np || (ldc % 4) != 0 ||
-      (reinterpret_cast<uintptr_t>(T) & 15) != 0 || (reinterpret_cast<uintptr_t>(C) & 15) != 0) {
+      (reinterpret_cast<uintptr_t>(T) & 15) != 0 || (reinterpret_cast<uintptr_t>(C) & 15) != 0 ||
+      (reinterpret_cast<uintptr_t>(C2) & 15) != 0) {
     err_msg = "tensor-core GEMM: invalid shape or alignment";
     return cudaErrorInvalidValue;
   }
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int bn = pick_bn(Np, sms);
+  const int ksplit = pick_ksplit(Np, sms, nseg, C2 != nullptr);
+  const int bn = ksplit == 2 ? 256 : pick_bn(Np, sms);
+  if (ksplit_out) *ksplit_out = ksplit;
   Segments sg{};
   sg.nseg = nseg;
   sg.kb_per_seg = Np / kBK;
@@ -395,18 +412,21 @@ inline cudaError_t gemm_terms(const __nv_bfloat16* T, int nterms, int Np, const 
     return cudaErrorInvalidValue;
   }
   const int mtiles = Np / kBM, ntiles = (Np + bn - 1) / bn;
-  const int blocks = mtiles * ntiles < sms ? mtiles * ntiles : sms;  // persistent: at most one CTA per SM
+  const int units = mtiles * ntiles * ksplit;
+  const int blocks = units < sms ? units : sms;  // persistent: at most one CTA per SM
   cudaError_t e;
   if (bn == 256) {
     using Lt = Layout<256, 4>;
     e = cudaFuncSetAttribute(k_tc_gemm_bf16<256, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, Lt::kDynamic);
     if (e != cudaSuccess) return e;
-    k_tc_gemm_bf16<256, 4><<<blocks, kThreads, Lt::kDynamic, s>>>(ma, mb, C, ldc, Np, mtiles, ntiles, sg, d_err);
+    k_tc_gemm_bf16<256, 4><<<blocks, kThreads, Lt::kDynamic, s>>>(ma, mb, C, C2, ksplit, ldc, Np, mtiles, ntiles, sg,
+                                                                   d_err);
   } else {
     using Lt = Layout<128, 6>;
     e = cudaFuncSetAttribute(k_tc_gemm_bf16<128, 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, Lt::kDynamic);
     if (e != cudaSuccess) return e;
-    k_tc_gemm_bf16<128, 6><<<blocks, kThreads, Lt::kDynamic, s>>>(ma, mb, C, ldc, Np, mtiles, ntiles, sg, d_err);
+    k_tc_gemm_bf16<128, 6><<<blocks, kThreads, Lt::kDynamic, s>>>(ma, mb, C, C2, ksplit, ldc, Np, mtiles, ntiles, sg,
+                                                                   d_err);
   }
   return cudaGetLastError();
 }

@@ -11,11 +11,13 @@
 // T: nterms stacked Np x Np BF16 matrices; C: Np x ldc FP32; err: one
 // device word.  Returns 0 on success, else the CUDA error code (a host-side
 // argument error is cudaErrorInvalidValue).
+// C2 (may be null): second output of a launch that splits K (the product is
+// then C + C2); *ksplit_out reports the split the launcher chose.
 extern "C" int tc_gemm_probe(const void* T, int nterms, int Np, const int* a_term, const int* b_term, int nseg,
-                             float* C, int ldc, unsigned* err) {
+                             float* C, float* C2, int ldc, unsigned* err, int* ksplit_out) {
   std::string msg;
-  cudaError_t e = sgb::tc::gemm_terms(static_cast<const __nv_bfloat16*>(T), nterms, Np, a_term, b_term, nseg, C, ldc,
-                                      err, 0, msg);
+  cudaError_t e = sgb::tc::gemm_terms(static_cast<const __nv_bfloat16*>(T), nterms, Np, a_term, b_term, nseg, C, C2,
+                                      ldc, err, 0, msg, ksplit_out);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   return (int)e;
 }

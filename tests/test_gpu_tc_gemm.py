@@ -24,20 +24,32 @@ def _lib():
     return ctypes.CDLL(LIB)
 
 
-def run_gemm(T, a_terms, b_terms, ldc=None):
-    """T: torch bf16 (nterms, Np, Np) on cuda; returns (C as float64 numpy, err word)."""
+def run_gemm(T, a_terms, b_terms, ldc=None, allow_split=False, want_split=None):
+    """T: torch bf16 (nterms, Np, Np) on cuda; returns (C as float64 numpy, err word).
+    allow_split: pass the second output, so the launcher may split K (the
+    product is then the sum of both); want_split: the split it must choose."""
     import torch
     L = _lib()
     nterms, Np, _ = T.shape
     ldc = Np if ldc is None else ldc
     C = torch.full((Np, ldc), float("nan"), dtype=torch.float32, device=T.device)
+    C2 = torch.full((Np, ldc), float("nan"), dtype=torch.float32, device=T.device) if allow_split else None
     err = torch.zeros(1, dtype=torch.int32, device=T.device)
+    ks = ctypes.c_int(0)
     a = (ctypes.c_int * len(a_terms))(*a_terms)
     b = (ctypes.c_int * len(b_terms))(*b_terms)
     rc = L.tc_gemm_probe(ctypes.c_void_p(T.data_ptr()), nterms, Np, a, b, len(a_terms), ctypes.c_void_p(C.data_ptr()),
-                         ldc, ctypes.c_void_p(err.data_ptr()))
+                         ctypes.c_void_p(C2.data_ptr()) if C2 is not None else None, ldc,
+                         ctypes.c_void_p(err.data_ptr()), ctypes.byref(ks))
     assert rc == 0, "tc_gemm_probe returned CUDA error %d" % rc
-    return C[:, :Np].double().cpu().numpy(), int(err.item())
+    if want_split is not None:
+        assert ks.value == want_split, ks.value
+    out = C[:, :Np].double()
+    if ks.value == 2:
+        out = out + C2[:, :Np].double()
+    else:
+        assert ks.value == 1
+    return out.cpu().numpy(), int(err.item())
 
 
 def reference(T, a_terms, b_terms):
@@ -65,6 +77,32 @@ def test_split_product_matches_fp64(Np):
     ref, absref = reference(T, SPLIT_A, SPLIT_B)
     assert np.all(np.isfinite(C))
     assert np.all(np.abs(C - ref) <= 1e-5 * absref + 1e-30), np.max(np.abs(C - ref) / (absref + 1e-30))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("Np", [384, 1536])
+def test_split_k_launch_matches_fp64(Np):
+    """Small sizes run 256-wide tiles over half the K range each into two
+    outputs; their sum is the product."""
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(100 + Np)
+    T = (torch.rand((5, Np, Np), generator=g, dtype=torch.float64) * 2 - 1).to(torch.bfloat16).cuda()
+    C, err = run_gemm(T, SPLIT_A, SPLIT_B, allow_split=True, want_split=2)
+    assert err == 0
+    ref, absref = reference(T, SPLIT_A, SPLIT_B)
+    assert np.all(np.abs(C - ref) <= 1e-5 * absref + 1e-30), np.max(np.abs(C - ref) / (absref + 1e-30))
+
+
+@pytest.mark.gpu
+def test_large_sizes_do_not_split():
+    import torch
+    Np = 3072
+    g = torch.Generator(device="cpu").manual_seed(5)
+    T = (torch.rand((2, Np, Np), generator=g, dtype=torch.float64) * 2 - 1).to(torch.bfloat16).cuda()
+    C, err = run_gemm(T, [0], [1], allow_split=True, want_split=1)
+    assert err == 0
+    ref, absref = reference(T, [0], [1])
+    assert np.all(np.abs(C - ref) <= 1e-5 * absref + 1e-30)
 
 
 @pytest.mark.gpu
