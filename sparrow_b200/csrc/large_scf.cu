@@ -380,8 +380,17 @@ struct LargeHost {
 // Timing events around the purification products of one SCF iteration
 // (two per product), created once per host thread and device and reused by
 // every later call.
+struct EventSets {
+  std::unordered_map<int, std::vector<cudaEvent_t>> per_device;
+  ~EventSets() {
+    for (auto& kv : per_device)
+      for (auto e : kv.second) cudaEventDestroy(e);
+  }
+};
+
 const std::vector<cudaEvent_t>* product_events(cudaError_t& ce) {
-  thread_local std::unordered_map<int, std::vector<cudaEvent_t>> per_device;
+  thread_local EventSets sets;
+  auto& per_device = sets.per_device;
   int dev = 0;
   ce = cudaGetDevice(&dev);
   if (ce != cudaSuccess) return nullptr;
