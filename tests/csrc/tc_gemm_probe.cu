@@ -67,3 +67,10 @@ extern "C" int tc_wait_probe(int arrive, unsigned* out) {
 
 // The bounded wait's limit in milliseconds.
 extern "C" int tc_wait_limit_ms() { return (int)(sgb::tc::kWaitLimitNs / 1000000ull); }
+
+// The launcher's plan for Np on a device with `sms` SMs (host logic only, no
+// device call): tile width and K split, with and without a second output.
+extern "C" void tc_gemm_plan(int Np, int sms, int nseg, int have_c2, int* bn, int* ksplit) {
+  *ksplit = sgb::tc::pick_ksplit(Np, sms, nseg, have_c2 != 0);
+  *bn = *ksplit == 2 ? 256 : sgb::tc::pick_bn(Np, sms);
+}

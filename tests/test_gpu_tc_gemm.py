@@ -176,3 +176,22 @@ def test_bounded_barrier_wait_gives_up_and_reports():
     assert err == 0
     ref, absref = reference(T, [0], [1])
     assert np.all(np.abs(C - ref) <= 1e-5 * absref + 1e-30)
+
+
+def test_launch_plan_on_the_host():
+    """The launcher's tile width and K split (host logic, no GPU): 148 SMs,
+    the four-segment split-BF16 product."""
+    L = _lib()
+
+    def plan(Np, have_c2):
+        bn, ks = ctypes.c_int(0), ctypes.c_int(0)
+        L.tc_gemm_plan(Np, 148, 4, 1 if have_c2 else 0, ctypes.byref(bn), ctypes.byref(ks))
+        return bn.value, ks.value
+
+    # (H2O)_256: 128 x 256 tiles would fill half the SMs, so K is split
+    assert plan(1536, True) == (256, 2)
+    assert plan(1536, False) == (128, 1)
+    # (H2O)_512 and (H2O)_1024: 288 and 1152 tiles of 128 x 256, no split
+    assert plan(3072, True) == (256, 1)
+    assert plan(6144, True) == (256, 1)
+
